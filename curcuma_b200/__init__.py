@@ -1,0 +1,9 @@
+"""curcuma_b200: GFN-FF energy + analytic gradient on NVIDIA B200 (sm_100a).
+
+A drop-in for curcuma's ``-method gfnff -gpu cuda`` path: host setup (topology and
+parameters) once per molecule, then energy + gradient per geometry on the GPU through the
+C ABI declared in ``include/gfnff_b200.h``.
+"""
+from .gfnff import FP64, MIXED, GFNFF  # noqa: F401
+
+__all__ = ["GFNFF", "FP64", "MIXED"]

@@ -1,0 +1,256 @@
+// C ABI of gfnff_b200 (include/gfnff_b200.h): host setup + device engine per handle.
+#include "../../include/gfnff_b200.h"
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <exception>
+#include <memory>
+#include <stdexcept>
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "device/engine.h"
+#include "setup/model.h"
+
+using namespace gfnff;
+
+struct gfnff_handle {
+    gfnff_options opt{};
+    std::unique_ptr<Engine> eng;
+    Model model;
+    bool ready = false;
+    std::string err;
+    std::vector<double> hb_ref;    // bohr, geometry of the last HB/XB detection
+    double* pin_xyz = nullptr;      // pinned staging for host coordinates
+    double* pin_grad = nullptr;
+    double* pin_out = nullptr;      // terms + status + msd
+    int* pin_status = nullptr;
+    ~gfnff_handle()
+    {
+        if (pin_xyz) cudaFreeHost(pin_xyz);
+        if (pin_grad) cudaFreeHost(pin_grad);
+        if (pin_out) cudaFreeHost(pin_out);
+        if (pin_status) cudaFreeHost(pin_status);
+    }
+};
+
+static thread_local std::string g_static_err;
+
+static gfnff_status fail(gfnff_handle* h, gfnff_status s, const std::string& msg)
+{
+    if (h) h->err = msg;
+    else g_static_err = msg;
+    return s;
+}
+
+extern "C" {
+
+void gfnff_default_options(gfnff_options* o)
+{
+    if (!o) return;
+    o->precision = GFNFF_FP64;
+    o->device = 0;
+    o->hbond = 1;
+    o->hb_rmsd_bohr = 0.3;
+}
+
+gfnff_status gfnff_create(const gfnff_options* opts, gfnff_handle** out)
+{
+    if (!out) return fail(nullptr, GFNFF_INVALID_ARG, "out is NULL");
+    *out = nullptr;
+    auto h = std::make_unique<gfnff_handle>();
+    if (opts) h->opt = *opts;
+    else gfnff_default_options(&h->opt);
+    if (h->opt.precision != GFNFF_FP64 && h->opt.precision != GFNFF_MIXED)
+        return fail(nullptr, GFNFF_INVALID_ARG, "unknown precision");
+    try {
+        EngineOptions eo;
+        eo.precision = h->opt.precision;
+        eo.device = h->opt.device;
+        h->eng = std::make_unique<Engine>(eo);
+    } catch (const std::exception& e) {
+        return fail(nullptr, GFNFF_CUDA_ERROR, e.what());
+    }
+    *out = h.release();
+    return GFNFF_OK;
+}
+
+gfnff_status gfnff_setup(gfnff_handle* h, int n, const int* Z, const double* xyz, int charge)
+{
+    if (!h) return fail(nullptr, GFNFF_INVALID_ARG, "handle is NULL");
+    if (n <= 0 || !Z || !xyz) return fail(h, GFNFF_INVALID_ARG, "invalid molecule");
+    h->ready = false;
+    try {
+        SetupOptions so;
+        so.hbond = h->opt.hbond != 0;
+        h->model = build_model(n, Z, xyz, charge, so);
+    } catch (const std::exception& e) {
+        return fail(h, GFNFF_SETUP_FAILED, e.what());
+    }
+    try {
+        h->eng->upload(h->model);
+        if (h->pin_xyz) cudaFreeHost(h->pin_xyz);
+        if (h->pin_grad) cudaFreeHost(h->pin_grad);
+        if (!h->pin_out && cudaMallocHost(&h->pin_out, 32 * sizeof(double)) != cudaSuccess)
+            throw std::runtime_error("cudaMallocHost failed");
+        if (!h->pin_status && cudaMallocHost(&h->pin_status, sizeof(int)) != cudaSuccess)
+            throw std::runtime_error("cudaMallocHost failed");
+        if (cudaMallocHost(&h->pin_xyz, 3 * (size_t)n * sizeof(double)) != cudaSuccess ||
+            cudaMallocHost(&h->pin_grad, 3 * (size_t)n * sizeof(double)) != cudaSuccess)
+            throw std::runtime_error("cudaMallocHost failed");
+    } catch (const std::exception& e) {
+        return fail(h, GFNFF_CUDA_ERROR, e.what());
+    }
+    h->hb_ref = h->model.xyz_setup;
+    h->ready = true;
+    return GFNFF_OK;
+}
+
+gfnff_status gfnff_energy_and_gradient(gfnff_handle* h, const double* xyz, double* energy, double* grad,
+                                       double* terms)
+{
+    if (!h) return fail(nullptr, GFNFF_INVALID_ARG, "handle is NULL");
+    if (!h->ready) return fail(h, GFNFF_NOT_READY, "gfnff_setup has not been called");
+    if (!xyz || !energy) return fail(h, GFNFF_INVALID_ARG, "NULL coordinates or energy");
+    const int n = h->model.n;
+    for (int k = 0; k < 3 * n; ++k)
+        if (!std::isfinite(xyz[k])) return fail(h, GFNFF_NONFINITE, "non-finite coordinate");
+    try {
+        // HB/XB refresh when the RMSD-like measure sqrt(sum d^2)/N exceeds the threshold
+        // (gfnff_method.cpp:2228-2259): re-detect on the host before this evaluation
+        if (h->opt.hbond) {
+            double s = 0.0;
+            for (int k = 0; k < 3 * n; ++k) {
+                const double d = xyz[k] * kAngToBohr - h->hb_ref[k];
+                s += d * d;
+            }
+            if (std::sqrt(s) / (double)n > h->opt.hb_rmsd_bohr) {
+                std::vector<double> xb(3 * (size_t)n);
+                for (int k = 0; k < 3 * n; ++k) xb[k] = xyz[k] * kAngToBohr;
+                redetect_hbxb(h->model, xb.data());
+                h->eng->upload_hbxb(h->model);
+                h->hb_ref = xb;
+            }
+        }
+        std::memcpy(h->pin_xyz, xyz, 3 * (size_t)n * sizeof(double));
+        cudaStream_t s = (cudaStream_t)h->eng->stream();
+        if (cudaMemcpyAsync(h->eng->d_xyz_scratch(), h->pin_xyz, 3 * (size_t)n * sizeof(double),
+                            cudaMemcpyHostToDevice, s) != cudaSuccess)
+            throw std::runtime_error("H2D copy failed");
+        h->eng->enqueue(h->eng->d_xyz_scratch(), false);
+        h->eng->fetch(h->pin_out, h->pin_grad, h->pin_status, nullptr);
+        if (*h->pin_status == GFNFF_NOT_SPD && h->eng->switch_to_lu()) {
+            h->eng->enqueue(h->eng->d_xyz_scratch(), false);
+            h->eng->fetch(h->pin_out, h->pin_grad, h->pin_status, nullptr);
+        }
+    } catch (const std::exception& e) {
+        return fail(h, GFNFF_CUDA_ERROR, e.what());
+    }
+    const int st = *h->pin_status;
+    *energy = h->pin_out[GFNFF_E_TOTAL];
+    if (terms) std::memcpy(terms, h->pin_out, GFNFF_NTERMS * sizeof(double));
+    if (grad) std::memcpy(grad, h->pin_grad, 3 * (size_t)n * sizeof(double));
+    if (st != GFNFF_OK) {
+        *energy = 0.0;   // curcuma's convention: an energy of 0.0 signals an error
+        return fail(h, (gfnff_status)st, st == GFNFF_NOT_SPD ? "EEQ matrix not positive definite"
+                                                            : "non-finite energy or gradient");
+    }
+    return GFNFF_OK;
+}
+
+gfnff_status gfnff_energy_and_gradient_device(gfnff_handle* h, const double* d_xyz, double* d_energy,
+                                              double* d_grad, int* d_status)
+{
+    if (!h) return fail(nullptr, GFNFF_INVALID_ARG, "handle is NULL");
+    if (!h->ready) return fail(h, GFNFF_NOT_READY, "gfnff_setup has not been called");
+    if (!d_xyz) return fail(h, GFNFF_INVALID_ARG, "NULL coordinates");
+    try {
+        h->eng->enqueue(d_xyz, true);
+        cudaStream_t s = (cudaStream_t)h->eng->stream();
+        const int n = h->model.n;
+        if (d_energy &&
+            cudaMemcpyAsync(d_energy, h->eng->d_terms() + GFNFF_E_TOTAL, sizeof(double), cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+            throw std::runtime_error("D2D copy failed");
+        if (d_grad &&
+            cudaMemcpyAsync(d_grad, h->eng->d_grad(), 3 * (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+            throw std::runtime_error("D2D copy failed");
+        if (d_status &&
+            cudaMemcpyAsync(d_status, h->eng->d_status(), sizeof(int), cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+            throw std::runtime_error("D2D copy failed");
+    } catch (const std::exception& e) {
+        return fail(h, GFNFF_CUDA_ERROR, e.what());
+    }
+    return GFNFF_OK;
+}
+
+void* gfnff_stream(gfnff_handle* h) { return h && h->eng ? h->eng->stream() : nullptr; }
+
+static gfnff_status copy_atoms(gfnff_handle* h, const double* dsrc, double* out)
+{
+    if (!h) return fail(nullptr, GFNFF_INVALID_ARG, "handle is NULL");
+    if (!h->ready) return fail(h, GFNFF_NOT_READY, "gfnff_setup has not been called");
+    if (!out) return fail(h, GFNFF_INVALID_ARG, "NULL output");
+    cudaStream_t s = (cudaStream_t)h->eng->stream();
+    if (cudaMemcpyAsync(out, dsrc, (size_t)h->model.n * sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return fail(h, GFNFF_CUDA_ERROR, "D2H copy failed");
+    return GFNFF_OK;
+}
+
+gfnff_status gfnff_charges(gfnff_handle* h, double* q) { return copy_atoms(h, h ? h->eng->d_charges() : nullptr, q); }
+gfnff_status gfnff_coordination_numbers(gfnff_handle* h, double* cn) { return copy_atoms(h, h ? h->eng->d_cn() : nullptr, cn); }
+
+gfnff_status gfnff_get_topology(gfnff_handle* h, int kind, int* out, long cap, long* count)
+{
+    if (!h) return fail(nullptr, GFNFF_INVALID_ARG, "handle is NULL");
+    if (!h->ready) return fail(h, GFNFF_NOT_READY, "gfnff_setup has not been called");
+    const Model& m = h->model;
+    std::vector<int> v;
+    long cnt = 0;
+    try {
+        switch (kind) {
+            case 0: for (auto& b : m.bonds) { v.push_back(b.i); v.push_back(b.j); } cnt = (long)m.bonds.size(); break;
+            case 1: for (auto& a : m.angles) v.insert(v.end(), {a.i, a.j, a.k}); cnt = (long)m.angles.size(); break;
+            case 2: for (auto& t : m.torsions) v.insert(v.end(), {t.i, t.j, t.k, t.l}); cnt = (long)m.torsions.size(); break;
+            case 3: for (auto& t : m.inversions) v.insert(v.end(), {t.i, t.j, t.k, t.l}); cnt = (long)m.inversions.size(); break;
+            case 4: v = h->eng->device_dispersion_pairs(); cnt = (long)v.size() / 2; break;
+            case 5: for (auto& r : m.rep_nonbonded) { v.push_back(r.i); v.push_back(r.j); } cnt = (long)m.rep_nonbonded.size(); break;
+            case 6: for (auto& t : m.hbonds) v.insert(v.end(), {t.a, t.h, t.b, t.case_type}); cnt = (long)m.hbonds.size(); break;
+            case 7: for (auto& t : m.xbonds) v.insert(v.end(), {t.a, t.x, t.b}); cnt = (long)m.xbonds.size(); break;
+            case 8: v = m.hyb; cnt = m.n; break;
+            case 9: v = m.frag; cnt = m.n; break;
+            case 10: v = m.pi_frag; cnt = m.n; break;
+            case 11: for (auto& r : m.rep_bonded) { v.push_back(r.i); v.push_back(r.j); } cnt = (long)m.rep_bonded.size(); break;
+            case 12: for (auto& t : m.atm) v.insert(v.end(), {t.i, t.j, t.k}); cnt = (long)m.atm.size(); break;
+            case 13: for (auto& t : m.batm) v.insert(v.end(), {t.i, t.j, t.k}); cnt = (long)m.batm.size(); break;
+            default: return fail(h, GFNFF_INVALID_ARG, "unknown topology kind");
+        }
+    } catch (const std::exception& e) {
+        return fail(h, GFNFF_CUDA_ERROR, e.what());
+    }
+    if (count) *count = cnt;
+    if (out) std::memcpy(out, v.data(), std::min<long>((long)v.size(), cap) * sizeof(int));
+    return GFNFF_OK;
+}
+
+gfnff_status gfnff_sizes(gfnff_handle* h, int* natoms, int* nfrag)
+{
+    if (!h) return fail(nullptr, GFNFF_INVALID_ARG, "handle is NULL");
+    if (!h->ready) return fail(h, GFNFF_NOT_READY, "gfnff_setup has not been called");
+    if (natoms) *natoms = h->model.n;
+    if (nfrag) *nfrag = h->model.nfrag;
+    return GFNFF_OK;
+}
+
+const char* gfnff_last_error(gfnff_handle* h) { return h ? h->err.c_str() : g_static_err.c_str(); }
+
+gfnff_status gfnff_destroy(gfnff_handle* h)
+{
+    delete h;
+    return GFNFF_OK;
+}
+
+}  // extern "C"

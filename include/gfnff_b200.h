@@ -1,0 +1,105 @@
+/*
+ * gfnff_b200 - GFN-FF energy + analytic gradient on NVIDIA B200 (sm_100a).
+ *
+ * C ABI of the drop-in for curcuma's `-method gfnff -gpu cuda` path.  One handle owns
+ * one molecule (or one batch of molecules), its topology and parameters cached on the
+ * device, and one CUDA stream.  Handles are not thread-safe.
+ *
+ * Units: coordinates in Angstrom at the boundary (as curcuma's Mol geometry),
+ * energies in Hartree, gradients in Hartree/bohr (row-major N x 3), like
+ * ComputationalMethod::getGradient().
+ */
+#ifndef GFNFF_B200_H
+#define GFNFF_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    GFNFF_OK = 0,
+    GFNFF_INVALID_ARG = 1,        /* bad pointer, size or element */
+    GFNFF_SETUP_FAILED = 2,       /* topology / parameter generation failed */
+    GFNFF_NOT_SPD = 3,            /* EEQ matrix not positive definite */
+    GFNFF_NONFINITE = 4,          /* non-finite energy or gradient */
+    GFNFF_REFINE_NOT_CONVERGED = 5,/* mixed-precision refinement did not reach 1e-10 */
+    GFNFF_CUDA_ERROR = 6,         /* CUDA / cuSOLVER failure */
+    GFNFF_NOT_READY = 7           /* gfnff_setup has not been called */
+} gfnff_status;
+
+/* precision of the per-geometry evaluation */
+enum { GFNFF_FP64 = 0, GFNFF_MIXED = 1 };
+
+/* per-term energies reported through gfnff_terms (Hartree) */
+enum {
+    GFNFF_E_BOND = 0, GFNFF_E_ANGLE, GFNFF_E_TORSION, GFNFF_E_INVERSION, GFNFF_E_STORSION,
+    GFNFF_E_DISPERSION, GFNFF_E_BONDED_REP, GFNFF_E_NONBONDED_REP, GFNFF_E_COULOMB,
+    GFNFF_E_HBOND, GFNFF_E_XBOND, GFNFF_E_ATM, GFNFF_E_BATM, GFNFF_E_TOTAL, GFNFF_NTERMS
+};
+
+typedef struct {
+    int precision;          /* GFNFF_FP64 (default) or GFNFF_MIXED */
+    int device;             /* CUDA device ordinal */
+    int hbond;              /* 1: hydrogen/halogen bonds on (default) */
+    double hb_rmsd_bohr;    /* HB/XB list refresh threshold, default 0.3 */
+} gfnff_options;
+
+typedef struct gfnff_handle gfnff_handle;
+
+/* Fills opts with the defaults (FP64, device 0, HB on, 0.3 bohr). */
+void gfnff_default_options(gfnff_options* opts);
+
+/* Replaces GFNFFGPUComputationalMethod construction
+ * (src/core/energy_calculators/qm_methods/gfnff_gpu_method.h:52-194). */
+gfnff_status gfnff_create(const gfnff_options* opts, gfnff_handle** out);
+
+/* Replaces ComputationalMethod::setMolecule -> GFNFF::InitialiseMolecule
+ * (computational_method.h:43-360, ff_methods/gfnff_method.cpp:709-848): topology and
+ * parameters are generated on the host and cached on the device. */
+gfnff_status gfnff_setup(gfnff_handle* h, int natoms, const int* Z, const double* xyz_angstrom,
+                         int total_charge);
+
+/* Replaces updateGeometry + calculateEnergy(true) + copyGradientTo
+ * (gfnff_method.cpp:1692-2226, computational_method.h:121-123).  energy and grad are
+ * host pointers; grad may be NULL for energy only (the gradient is still computed);
+ * terms may be NULL, else GFNFF_NTERMS doubles. */
+gfnff_status gfnff_energy_and_gradient(gfnff_handle* h, const double* xyz_angstrom, double* energy,
+                                       double* grad, double* terms);
+
+/* Device-resident variant for MD/optimisation loops and CUDA-graph capture:
+ * d_xyz_bohr (N*3 doubles, bohr) and the outputs are device pointers; the call only
+ * enqueues work on the handle's stream (no host synchronisation).  d_status receives
+ * a gfnff_status code. */
+gfnff_status gfnff_energy_and_gradient_device(gfnff_handle* h, const double* d_xyz_bohr,
+                                              double* d_energy, double* d_grad, int* d_status);
+
+/* The handle's CUDA stream (a cudaStream_t). */
+void* gfnff_stream(gfnff_handle* h);
+
+/* Phase-2 EEQ charges of the last evaluation (ComputationalMethod::getCharges). */
+gfnff_status gfnff_charges(gfnff_handle* h, double* q);
+
+/* Coordination numbers of the last evaluation. */
+gfnff_status gfnff_coordination_numbers(gfnff_handle* h, double* cn);
+
+/* Topology lists for bit-exact comparison (same kinds as the oracle's list export):
+ * 0 bonds(i,j) 1 angles(i,j,k) 2 torsions(i,j,k,l) 3 inversions 4 dispersion pairs
+ * (device-enumerated) 5 non-bonded repulsion pairs 6 hbonds(a,h,b,case) 7 xbonds
+ * 8 hybridisation 9 fragment 10 pi fragment 11 bonded repulsion 12 ATM 13 BATM.
+ * Writes the record count to *count and up to cap ints into out (may be NULL). */
+gfnff_status gfnff_get_topology(gfnff_handle* h, int kind, int* out, long cap, long* count);
+
+/* Atom count and fragment count of the set-up system. */
+gfnff_status gfnff_sizes(gfnff_handle* h, int* natoms, int* nfrag);
+
+/* Last error message of the handle (static storage when h is NULL). */
+const char* gfnff_last_error(gfnff_handle* h);
+
+/* Frees all host and device resources. */
+gfnff_status gfnff_destroy(gfnff_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GFNFF_B200_H */

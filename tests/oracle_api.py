@@ -1,0 +1,97 @@
+"""ctypes access to the CPU oracle (oracle/_build/liboracle.so) for the tests.
+
+The oracle is test infrastructure: a CPU restatement of curcuma's per-geometry GFN-FF
+energy + gradient that the GPU path is checked against.  It is built from oracle/ by
+``make -C oracle`` (``__graft_entry__.build()`` does that too).
+"""
+import ctypes
+import json
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent.parent
+LIB = ROOT / "oracle" / "_build" / "liboracle.so"
+GOLDEN = ROOT / "tests" / "golden"
+TERMS = ["bond", "angle", "torsion", "inversion", "storsion", "dispersion", "bonded_rep",
+         "nonbonded_rep", "coulomb", "hbond", "xbond", "atm", "batm", "total"]
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIB.exists():
+            subprocess.run(["make", "-C", str(ROOT / "oracle")], check=True, capture_output=True)
+        L = ctypes.CDLL(str(LIB))
+        c_v, c_i = ctypes.c_void_p, ctypes.c_int
+        L.oracle_create.restype = c_v
+        L.oracle_create.argtypes = [c_i, c_v, c_v, c_i]
+        L.oracle_destroy.argtypes = [c_v]
+        L.oracle_last_error.restype = ctypes.c_char_p
+        L.oracle_engrad.argtypes = [c_v, c_v, c_v, c_v, c_v, c_v, c_i]
+        L.oracle_engrad.restype = c_i
+        L.oracle_redetect_hbxb.argtypes = [c_v, c_v]
+        L.oracle_list.argtypes = [c_v, c_i, c_v, ctypes.c_long]
+        L.oracle_list.restype = ctypes.c_long
+        L.oracle_atom_data.argtypes = [c_v, c_i, c_v]
+        L.oracle_nfrag.argtypes = [c_v]
+        _lib = L
+    return _lib
+
+
+class Oracle:
+    def __init__(self, Z, xyz, charge=0):
+        self.Z = np.ascontiguousarray(Z, dtype=np.int32)
+        X = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+        self.n = len(self.Z)
+        self.h = lib().oracle_create(self.n, self.Z.ctypes.data, X.ctypes.data, int(charge))
+        if not self.h:
+            raise RuntimeError(lib().oracle_last_error().decode())
+
+    def engrad(self, xyz, nthreads=0):
+        X = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+        T = np.zeros(len(TERMS))
+        G = np.zeros((self.n, 3))
+        q = np.zeros(self.n)
+        cn = np.zeros(self.n)
+        rc = lib().oracle_engrad(self.h, X.ctypes.data, T.ctypes.data, G.ctypes.data, q.ctypes.data,
+                                 cn.ctypes.data, nthreads)
+        if rc != 0:
+            raise RuntimeError(lib().oracle_last_error().decode())
+        return dict(zip(TERMS, T)), G, q, cn
+
+    def redetect_hbxb(self, xyz):
+        X = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+        lib().oracle_redetect_hbxb(self.h, X.ctypes.data)
+
+    def topology(self, kind, width):
+        cnt = lib().oracle_list(self.h, kind, None, 0)
+        out = np.zeros(max(1, cnt * width), dtype=np.int32)
+        lib().oracle_list(self.h, kind, out.ctypes.data, out.size)
+        return out[:cnt * width].reshape(cnt, width) if width > 1 else out[:cnt]
+
+    def atom_data(self, which):
+        out = np.zeros(self.n)
+        lib().oracle_atom_data(self.h, which, out.ctypes.data)
+        return out
+
+    @property
+    def nfrag(self):
+        return lib().oracle_nfrag(self.h)
+
+    def __del__(self):
+        try:
+            if self.h:
+                lib().oracle_destroy(self.h)
+        except Exception:
+            pass
+
+
+def golden(name):
+    return json.loads((GOLDEN / f"{name}.json").read_text())
+
+
+def golden_names():
+    return sorted(p.stem for p in GOLDEN.glob("*.json") if not p.stem.startswith("cli_"))

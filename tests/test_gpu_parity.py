@@ -1,0 +1,133 @@
+"""GPU (FP64 form) against the CPU oracle on the same inputs, through the C ABI.
+
+Bar (north-star plain form): energy within 1e-8 Eh, gradient within 1e-7 Eh/bohr
+(max-abs), topology lists bit-exact."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from curcuma_b200 import GFNFF, workloads
+from tests.oracle_api import Oracle, golden, golden_names
+
+E_TOL = 1e-8
+G_TOL = 1e-7
+
+pytestmark = pytest.mark.gpu
+
+
+def _compare(Z, X, charge=0, e_tol=E_TOL, g_tol=G_TOL):
+    gpu = GFNFF()
+    assert gpu.setMolecule(Z, X, charge), gpu.getErrorMessage()
+    e = gpu.calculateEnergy(True)
+    assert not gpu.hasError(), gpu.getErrorMessage()
+    o = Oracle(Z, X, charge)
+    T, G, q, cn = o.engrad(X)
+    terms = gpu.getEnergyDecomposition()
+    for k, v in T.items():
+        assert abs(terms[k] - v) < e_tol, f"{k}: gpu {terms[k]!r} oracle {v!r}"
+    assert abs(e - T["total"]) < e_tol
+    g = gpu.getGradient()
+    assert np.abs(g - G).max() < g_tol, np.abs(g - G).max()
+    assert np.abs(gpu.getCharges() - q).max() < 1e-9
+    assert np.abs(gpu.getCoordinationNumbers() - cn).max() < 1e-12
+    return gpu, o
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_golden_molecules(name):
+    g = golden(name)
+    _compare(np.array(g["Z"]), np.array(g["xyz_angstrom"]))
+
+
+@pytest.mark.parametrize("name", ["cli_complex", "cli_caffeine"])
+def test_cli_molecules(name):
+    g = golden(name)
+    gpu, _ = _compare(np.array(g["Z"]), np.array(g["xyz_angstrom"]))
+    assert abs(gpu.getEnergyDecomposition()["total"] - g["total_energy"]) < g["tolerance"]
+
+
+def test_alkane_c64():
+    Z, X = workloads.alkane(64, 1001)
+    _compare(Z, X)
+
+
+def test_water_cluster_small():
+    Z, X = workloads.water_cluster(60, 77)
+    gpu, o = _compare(Z, X)
+    assert gpu.sizes() == (180, 60)
+
+
+def test_conformers():
+    for Z, X in workloads.conformer_batch(6, 1004):
+        _compare(Z, X)
+
+
+def test_peptide_small():
+    Z, X = workloads.solvated_peptide(6, 40, 55)
+    _compare(Z, X)
+
+
+def test_topology_bit_exact():
+    Z, X = workloads.water_cluster(40, 5)
+    gpu = GFNFF()
+    assert gpu.setMolecule(Z, X)
+    o = Oracle(Z, X)
+    # dispersion pairs are enumerated on the device from the setup geometry
+    assert np.array_equal(gpu.topology(4, 2), o.topology(4, 2))
+    for kind, width in [(0, 2), (1, 3), (2, 4), (3, 4), (5, 2), (6, 4), (8, 1), (9, 1), (11, 2), (12, 3), (13, 3)]:
+        assert np.array_equal(gpu.topology(kind, width), o.topology(kind, width)), kind
+
+
+def test_hb_refresh_matches_oracle():
+    Z, X = workloads.water_cluster(30, 9)
+    gpu = GFNFF()
+    assert gpu.setMolecule(Z, X)
+    X2 = X.copy()
+    # translate 20 of the 30 waters by 3 bohr per axis: sqrt(sum d^2)/N = 0.45 > 0.3 bohr
+    X2[: 3 * 20] += 3.0 * 0.529177210903
+    gpu.updateGeometry(X2)
+    e = gpu.calculateEnergy(True)
+    o = Oracle(Z, X)
+    o.redetect_hbxb(X2)
+    T, G, q, cn = o.engrad(X2)
+    assert abs(e - T["total"]) < E_TOL
+    assert np.abs(gpu.getGradient() - G).max() < G_TOL
+
+
+def test_device_entry_point_matches_host():
+    import torch
+    Z, X = workloads.alkane(12, 3)
+    gpu = GFNFF()
+    assert gpu.setMolecule(Z, X)
+    e_host = gpu.calculateEnergy(True)
+    g_host = gpu.getGradient()
+    lib = gpu._lib
+    xb = torch.tensor(X / 0.529177210903, dtype=torch.float64, device="cuda")
+    e = torch.zeros(1, dtype=torch.float64, device="cuda")
+    g = torch.zeros(len(Z) * 3, dtype=torch.float64, device="cuda")
+    st = torch.zeros(1, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    rc = lib.gfnff_energy_and_gradient_device(gpu.handle, ctypes.c_void_p(xb.data_ptr()), ctypes.c_void_p(e.data_ptr()),
+                                             ctypes.c_void_p(g.data_ptr()), ctypes.c_void_p(st.data_ptr()))
+    assert rc == 0
+    torch.cuda.synchronize()
+    assert int(st.item()) == 0
+    assert abs(e.item() - e_host) < 1e-12
+    assert np.abs(g.cpu().numpy().reshape(-1, 3) - g_host).max() < 1e-12
+
+
+def test_error_paths():
+    gpu = GFNFF()
+    Z = np.array([8, 1, 1])
+    X = np.array([[0.0, 0.0, 0.0], [0.0, 0.0, 0.0], [0.0, 0.9, 0.0]])
+    assert not gpu.setMolecule(Z, X)           # coincident atoms -> setup failure
+    assert gpu.hasError()
+    X = np.array([[0.0, 0.0, 0.0], [0.96, 0.0, 0.0], [-0.24, 0.93, 0.0]])
+    assert gpu.setMolecule(Z, X)
+    Xn = X.copy()
+    Xn[1, 0] = np.nan
+    gpu.updateGeometry(Xn)
+    assert gpu.calculateEnergy(True) == 0.0 and gpu.hasError()
+    gpu.updateGeometry(X)
+    assert gpu.calculateEnergy(True) != 0.0 and not gpu.hasError()
