@@ -1,0 +1,347 @@
+#!/usr/bin/env python3
+"""GFN-FF energy + gradient throughput on B200.
+
+Default workload: BASELINE config 2, a seeded 1000-water cluster (3000 atoms, 1000
+fragments, 1.0 g/cm^3), FP64 form.  One step = one energy + analytic gradient
+evaluation of a fresh geometry (MD-like perturbation of the cluster).
+
+* ``value``: evaluations/s with coordinates resident in HBM, through the device entry
+  point ``gfnff_energy_and_gradient_device``; each step timed with CUDA events on the
+  handle's stream, L2 flushed (256 MiB write) before every timed step.
+* ``e2e``: evaluations/s through the host C-ABI call ``gfnff_energy_and_gradient``
+  (host coordinates in, energy + gradient + terms out, copies inside the timed region).
+* ``roofline``: the dominant phase of the step against its arithmetic (FP64 FMA, measured
+  by the library's microbenchmark) or HBM (MEASURED_PEAKS.json) bound.
+* ``cpu_baseline``: the CPU oracle (a restatement of curcuma's CPU gfnff path, all host
+  threads) on the same structure; rank 0 at N=1 only.
+
+``--impl reference`` times that CPU restatement alone as the reference arm (the
+reference's own CPU code cannot be built here: Eigen and friends are fetched at configure
+time).  Multi-GPU: ``--gpus N`` under torchrun runs independent replicas (weak scaling, no
+collective on the data path); timings are reduced with MAX over ranks.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "GFN-FF E+grad evals/s"
+UNIT = "evals/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", type=int, default=2)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload(cfg):
+    from curcuma_b200 import workloads as W
+    if cfg == 1:
+        return "n-C64H130 all-trans, 0.05 A noise (seed 1001)", *W.alkane(64, 1001)
+    if cfg == 2:
+        return "1000 H2O cluster, 1.0 g/cm3 (seed 1002)", *W.water_cluster(1000, 1002)
+    if cfg == 3:
+        return "Gly50 + 1500 H2O (seed 1003)", *W.solvated_peptide(50, 1500, 1003)
+    if cfg == 5:
+        return "6000 H2O + 40 C20H42 (seed 1005)", *W.large_cluster(6000, 40, 20, 1005)
+    raise SystemExit(f"config {cfg} is not a single-structure workload")
+
+
+def perturbed(X, k, sigma=0.01, seed=7):
+    rng = np.random.default_rng(seed + k)
+    return X + rng.normal(scale=sigma, size=X.shape)
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, device):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={device}", f"--query-gpu={q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        self.p.wait()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().split("\n") if r.strip()]
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = max(mx, float(r[2]))
+                for k, nm in enumerate(names):
+                    if r[5 + k].strip().lower().startswith("active"):
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                pass
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def pair_counts(Z, X):
+    """Unique pairs evaluated per step: Coulomb r <= 100 bohr, D4 r <= 50 bohr within the
+    60 bohr setup list (same geometry)."""
+    Xb = X / 0.529177210903
+    n = len(Z)
+    nc = nd = 0
+    for i0 in range(0, n, 512):
+        d = np.linalg.norm(Xb[i0:i0 + 512, None, :] - Xb[None, :, :], axis=-1)
+        idx = np.arange(i0, min(n, i0 + 512))[:, None] < np.arange(n)[None, :]
+        nc += int(((d <= 100.0) & idx).sum())
+        nd += int(((d <= 50.0) & idx).sum())
+    return nc, nd
+
+
+def roofline(phase_avg, info, fp64_peak, hbm_peak, hbm_src):
+    """Algorithmic work per launch of the dominant phase.  FLOP conventions (erf/exp/
+    sqrt/div = 1 op): Coulomb E+G 40/pair, D4 E+G 45/pair, repulsion 30/pair, CN+dCN
+    35/pair, EEQ element 20; Cholesky n^3/3 + 2 n^2 (solve)."""
+    name = max(phase_avg, key=phase_avg.get)
+    ms = phase_avg[name]
+    n, nred = info["n"], info["nred"]
+    if name == "pairs":
+        flops = 40.0 * info["coulomb_pairs"] + 45.0 * info["disp_pairs"]
+        bound, unit, peak = "fp64", "TFLOP/s", fp64_peak
+        achieved = flops / (ms * 1e-3) / 1e12
+    elif name == "eeq_factor_solve":
+        flops = nred ** 3 / 3.0 + 2.0 * nred ** 2
+        bound, unit, peak = "fp64", "TFLOP/s", fp64_peak
+        achieved = flops / (ms * 1e-3) / 1e12
+    elif name in ("eeq_matrix", "eeq_reduce"):
+        # HBM: the dense matrix is written once and read once per phase
+        m = n if name == "eeq_matrix" else nred
+        bytes_ = 2.0 * 8.0 * m * m
+        bound, unit, peak = "hbm", "GB/s", hbm_peak
+        achieved = bytes_ / (ms * 1e-3) / 1e9
+    else:
+        # list-driven phases: term records + 24 B coordinates + 24 B gradient per atom ref
+        bytes_ = info.get(f"bytes_{name}", 0.0)
+        bound, unit, peak = "hbm", "GB/s", hbm_peak
+        achieved = bytes_ / (ms * 1e-3) / 1e9 if bytes_ else 0.0
+    traffic = None
+    tf = ROOT / "profiles" / "traffic.json"
+    if tf.exists():
+        traffic = json.loads(tf.read_text()).get(f"config{info['config']}", {}).get(name)
+    return {"kernel": name, "bound": bound, "achieved": achieved, "peak": peak, "unit": unit,
+            "frac": achieved / peak if peak else None, "traffic": traffic, "ms": ms,
+            "peak_source": "measured (fma microbenchmark)" if bound == "fp64" else hbm_src}
+
+
+def cpu_oracle_rate(Z, X, steps, warmup):
+    from tests.oracle_api import Oracle
+    o = Oracle(Z, X)
+    for k in range(warmup):
+        o.engrad(perturbed(X, 1000 + k))
+    t = time.perf_counter()
+    for k in range(steps):
+        o.engrad(perturbed(X, 2000 + k))
+    dt = time.perf_counter() - t
+    return steps / dt, dt
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    desc, Z, X = workload(args.config)
+    threads = os.cpu_count()
+    rate, dt = cpu_oracle_rate(Z, X, args.steps, args.warmup)
+    line = {"metric": METRIC, "value": rate, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": f"config {args.config}: {desc}", "natoms": int(len(Z))},
+            "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"{args.steps} full E+grad evaluations of the workload"},
+            "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "CPU restatement of curcuma's gfnff path (oracle/), all host threads; the "
+                    "reference's own build needs network-fetched Eigen and is unavailable here"}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    from curcuma_b200 import GFNFF, _lib
+
+    desc, Z, X = workload(args.config)
+    n = len(Z)
+    prec = 0 if args.precision == "fp64" else 1
+    gpu = GFNFF(precision=prec, device=local)
+    t0 = time.perf_counter()
+    if not gpu.setMolecule(Z, X):
+        raise SystemExit(gpu.getErrorMessage())
+    setup_s = time.perf_counter() - t0
+    natoms, nfrag = gpu.sizes()
+    lib = gpu._lib
+    h = gpu.handle
+    stream = torch.cuda.ExternalStream(lib.gfnff_stream(h), device=torch.device("cuda", local))
+    steps, warm = args.steps, args.warmup
+    geoms = torch.tensor(np.stack([perturbed(X, k) / 0.529177210903 for k in range(steps + warm)]),
+                         dtype=torch.float64, device="cuda")
+    d_e = torch.zeros(1, dtype=torch.float64, device="cuda")
+    d_g = torch.zeros(3 * n, dtype=torch.float64, device="cuda")
+    d_st = torch.zeros(1, dtype=torch.int32, device="cuda")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    P = ctypes.c_void_p
+
+    def step(k):
+        rc = lib.gfnff_energy_and_gradient_device(h, P(geoms[k].data_ptr()), P(d_e.data_ptr()),
+                                                 P(d_g.data_ptr()), P(d_st.data_ptr()))
+        if rc != 0:
+            raise SystemExit(lib.gfnff_last_error(h).decode())
+
+    lib.gfnff_set_phase_timing(h, 1)
+    for k in range(warm):
+        step(k)
+    torch.cuda.synchronize()
+    events = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    phases = np.zeros(len(_lib.PHASES))
+    buf = (ctypes.c_double * len(_lib.PHASES))()
+    clocks = Clocks(local)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        for k in range(steps):
+            flush.zero_()
+            events[k][0].record(stream)
+            step(warm + k)
+            events[k][1].record(stream)
+            events[k][1].synchronize()
+            lib.gfnff_phase_times(h, buf, len(buf))
+            phases += np.array(buf[:])
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    step_ms = [a.elapsed_time(b) for a, b in events]
+    total_ms = float(sum(step_ms))
+    status = int(d_st.item())
+    if world > 1:
+        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * steps / (total_ms * 1e-3)
+    phase_avg = {k: v / steps for k, v in zip(_lib.PHASES, phases)}
+    lib.gfnff_set_phase_timing(h, 0)
+
+    # end-to-end through the host C ABI
+    hostX = [perturbed(X, 5000 + k) for k in range(steps)]
+    for k in range(min(3, warm)):
+        gpu.updateGeometry(hostX[k])
+        gpu.calculateEnergy(True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    for k in range(steps):
+        gpu.updateGeometry(hostX[k])
+        e = gpu.calculateEnergy(True)
+        if gpu.hasError():
+            raise SystemExit(gpu.getErrorMessage())
+    e2e_s = time.perf_counter() - t
+    if world > 1:
+        tt = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_s = float(tt.item())
+    e2e = {"value": world * steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 3 * n * 8,
+           "d2h_bytes_per_step": (3 * n + 14) * 8 + 4}
+
+    counts = {k: len(gpu.topology(kind, w)) for k, kind, w in
+              [("bonds", 0, 2), ("angles", 1, 3), ("torsions", 2, 4), ("inversions", 3, 4), ("hbonds", 6, 4),
+               ("xbonds", 7, 3), ("atm", 12, 3), ("batm", 13, 3)]}
+    fixed = 12   # positions, cn, d4w, eeq A, residual, reduce, expand, repulsion, pairs, post, chain, finish
+    launches = fixed + sum(1 for k in ("bonds", "angles", "torsions", "inversions", "hbonds", "xbonds", "atm", "batm")
+                           if counts[k] > 0)
+    if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
+        return
+    nc, nd = pair_counts(Z, X)
+    # HB record: 3 atoms + neighbours; bytes = 19 scalars * 8 + atom refs * 48
+    hbs = gpu.topology(6, 4)
+    info = {"n": n, "nred": n - nfrag, "config": args.config, "coulomb_pairs": nc, "disp_pairs": nd,
+            "bytes_hbonds": len(hbs) * (19 * 8 + 3 * 48 + 2 * 48)}
+    hbm_peak, hbm_src = measured_peaks()
+    fp64_peak = lib.gfnff_fma_peak_tflops(local, 1)
+    roof = roofline(phase_avg, info, fp64_peak, hbm_peak, hbm_src)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps, "warmup": warm,
+            "ms_per_step": total_ms / steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if prec == 0 else "mixed(f32/f64)", "data": "synthetic",
+            "config": {"workload": f"config {args.config}: {desc}", "natoms": natoms, "nfrag": nfrag,
+                       "precision": args.precision, "l2": "flushed before every timed step (256 MiB write)",
+                       "parallelism": f"replicas x{world}", "setup_s": round(setup_s, 3)},
+            "e2e": e2e, "gpu_launches": launches * steps, "roofline": roof,
+            "phase_ms": {k: round(v, 4) for k, v in phase_avg.items()},
+            "step_ms_median": statistics.median(step_ms), "status": status,
+            "pairs": {"coulomb": nc, "dispersion": nd},
+            "terms": counts, "clocks": clk}
+    if world == 1 and not args.no_cpu_baseline:
+        rate, dt = cpu_oracle_rate(Z, X, 2 if n >= 2000 else 5, 1)
+        line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                                "sample": f"{2 if n >= 2000 else 5} full E+grad evaluations of the same workload "
+                                          f"({dt:.1f} s)"}
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -19,7 +19,9 @@ NTERMS = len(TERM_NAMES)
 EXPORTED = ["gfnff_default_options", "gfnff_create", "gfnff_setup", "gfnff_energy_and_gradient",
             "gfnff_energy_and_gradient_device", "gfnff_stream", "gfnff_charges",
             "gfnff_coordination_numbers", "gfnff_get_topology", "gfnff_sizes", "gfnff_last_error",
-            "gfnff_destroy"]
+            "gfnff_destroy", "gfnff_set_phase_timing", "gfnff_phase_times", "gfnff_fma_peak_tflops"]
+PHASES = ["positions", "cn", "d4_weights", "eeq_matrix", "eeq_reduce", "eeq_factor_solve", "bonded",
+          "hbonds", "repulsion", "pairs", "post_chain", "finish"]
 
 
 class Options(ctypes.Structure):
@@ -55,8 +57,12 @@ def load():
     lib.gfnff_last_error.argtypes = [c_v]
     lib.gfnff_last_error.restype = ctypes.c_char_p
     lib.gfnff_destroy.argtypes = [c_v]
+    lib.gfnff_set_phase_timing.argtypes = [c_v, c_i]
+    lib.gfnff_phase_times.argtypes = [c_v, P(c_d), c_i]
+    lib.gfnff_fma_peak_tflops.argtypes = [c_i, c_i]
+    lib.gfnff_fma_peak_tflops.restype = c_d
     for name in EXPORTED:
-        if name not in ("gfnff_default_options", "gfnff_stream", "gfnff_last_error"):
+        if name not in ("gfnff_default_options", "gfnff_stream", "gfnff_last_error", "gfnff_fma_peak_tflops"):
             getattr(lib, name).restype = c_i
     _lib = lib
     return lib

@@ -245,6 +245,31 @@ gfnff_status gfnff_sizes(gfnff_handle* h, int* natoms, int* nfrag)
     return GFNFF_OK;
 }
 
+gfnff_status gfnff_set_phase_timing(gfnff_handle* h, int on)
+{
+    if (!h) return fail(nullptr, GFNFF_INVALID_ARG, "handle is NULL");
+    try {
+        h->eng->set_timing(on != 0);
+    } catch (const std::exception& e) {
+        return fail(h, GFNFF_CUDA_ERROR, e.what());
+    }
+    return GFNFF_OK;
+}
+
+int gfnff_phase_times(gfnff_handle* h, double* ms, int cap)
+{
+    if (!h || !ms) return -1;
+    try {
+        auto v = h->eng->phase_ms();
+        const int n = std::min<int>(cap, (int)v.size());
+        for (int k = 0; k < n; ++k) ms[k] = v[k];
+        return (int)v.size();
+    } catch (const std::exception& e) {
+        fail(h, GFNFF_CUDA_ERROR, e.what());
+        return -1;
+    }
+}
+
 const char* gfnff_last_error(gfnff_handle* h) { return h ? h->err.c_str() : g_static_err.c_str(); }
 
 gfnff_status gfnff_destroy(gfnff_handle* h)

@@ -267,34 +267,26 @@ __global__ void k_positions(int n, const double* __restrict__ xyz, double scale,
 // ------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(kBlock) k_cn(View V)
 {
-    __shared__ double4 sp[kBlock];
-    __shared__ double sr[kBlock];
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool act = i < V.n;
-    const double4 pi = act ? V.pos[i] : make_double4(0, 0, 0, 0);
-    const double ri = act ? V.rcov_cn[i] : 0.0;
+    // one warp per atom i, lanes stride over the partners j
+    const int i = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (i >= V.n) return;
+    const double4 pi = V.pos[i];
+    const double ri = V.rcov_cn[i];
     const double kn = -7.5;
     double s = 0.0;
-    for (int t0 = 0; t0 < V.n; t0 += kBlock) {
-        const int j = t0 + threadIdx.x;
-        __syncthreads();
-        if (j < V.n) { sp[threadIdx.x] = V.pos[j]; sr[threadIdx.x] = V.rcov_cn[j]; }
-        __syncthreads();
-        const int m = min(kBlock, V.n - t0);
-        if (act)
-            for (int k = 0; k < m; ++k) {
-                const int jj = t0 + k;
-                if (jj == i) continue;
-                const double4 pj = sp[k];
-                const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-                const double d2 = dx * dx + dy * dy + dz * dz;
-                if (!(d2 < 36.0)) continue;
-                const double r = sqrt(d2);
-                const double rc = ri + sr[k];
-                s += 0.5 * (1.0 + erf(kn * ((r - rc) / rc)));
-            }
+    for (int j = lane; j < V.n; j += 32) {
+        if (j == i) continue;
+        const double4 pj = V.pos[j];
+        const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+        const double d2 = dx * dx + dy * dy + dz * dz;
+        if (!(d2 < 36.0)) continue;
+        const double r = sqrt(d2);
+        const double rc = ri + V.rcov_cn[j];
+        s += 0.5 * (1.0 + erf(kn * ((r - rc) / rc)));
     }
-    if (act) {
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0) {
         const double cnmax = 4.4;
         V.cnraw[i] = s;
         V.cn[i] = log(1.0 + exp(cnmax)) - log(1.0 + exp(cnmax - s));
@@ -1027,15 +1019,15 @@ __global__ void k_xbonds(View V, XBSoA S)
 // repulsion over per-atom CSR lists holding both pair directions
 // (ff_workspace_gfnff.cpp:774-848); kind 0 = bonded, 1 = non-bonded
 // ------------------------------------------------------------------------------------
-__global__ void k_repulsion(View V, const int* off, const int* nbj, const double* alpha,
-                            const double* repab, const unsigned char* kind)
+__global__ void __launch_bounds__(kBlock) k_repulsion(View V, const int* off, const int* nbj, const double* alpha,
+                                                     const double* repab, const unsigned char* kind)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    double eb = 0.0, enb = 0.0;
+    const int i = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    double eb = 0.0, enb = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
     if (i < V.n) {
         const double4 pi = V.pos[i];
-        double gx = 0.0, gy = 0.0, gz = 0.0;
-        for (int p = off[i]; p < off[i + 1]; ++p) {
+        for (int p = off[i] + lane; p < off[i + 1]; p += 32) {
             const double4 pj = V.pos[nbj[p]];
             const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
             const double r = sqrt(dx * dx + dy * dy + dz * dz);
@@ -1047,9 +1039,16 @@ __global__ void k_repulsion(View V, const int* off, const int* nbj, const double
             const double f = dEdr / r;
             gx += f * dx; gy += f * dy; gz += f * dz;
         }
-        V.grad[3 * i] += gx;
-        V.grad[3 * i + 1] += gy;
-        V.grad[3 * i + 2] += gz;
+        for (int o = 16; o > 0; o >>= 1) {
+            gx += __shfl_down_sync(0xffffffffu, gx, o);
+            gy += __shfl_down_sync(0xffffffffu, gy, o);
+            gz += __shfl_down_sync(0xffffffffu, gz, o);
+        }
+        if (lane == 0) {
+            V.grad[3 * i] += gx;
+            V.grad[3 * i + 1] += gy;
+            V.grad[3 * i + 2] += gz;
+        }
     }
     block_add(eb, V.E + T_BREP);
     block_add(enb, V.E + T_NBREP);
@@ -1061,76 +1060,47 @@ __global__ void k_repulsion(View V, const int* off, const int* nbj, const double
 // :715-772, d4param_generator.cpp:1959-2092) with the frozen setup C6 and the
 // per-step dC6/dCN chain term.  One thread owns one row i; energies are halved.
 // ------------------------------------------------------------------------------------
-struct PairTile {
-    double4 p, p0;
-    double alp, q, zeta, szr;
-    int slot, nref;
-    double w0[7], w[7];
-};
-
 __global__ void __launch_bounds__(kBlock) k_pairs(View V)
 {
-    __shared__ PairTile st[kBlock];
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool act = i < V.n;
-    double4 pi = make_double4(0, 0, 0, 0), p0i = pi;
-    double ai = 1.0, qi = 0.0, zi = 0.0, szi = 0.0;
-    if (act) {
-        pi = V.pos[i];
-        p0i = V.pos0[i];
-        ai = V.alpeeq[i];
-        qi = V.q[i];
-        zi = V.zeta[i];
-        szi = V.szr[i];
-    }
-    const double* g0i = V.g0 + (size_t)(act ? i : 0) * V.K * 7;
-    const double* dgi = V.hdg + (size_t)(act ? i : 0) * V.K * 7;
+    // one warp per row i, lanes stride over the partners j (coalesced SoA loads)
+    const int i = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
     double ec = 0.0, ed = 0.0, gx = 0.0, gy = 0.0, gz = 0.0, dcn = 0.0;
-    const double a1 = 0.58, a2 = 4.80, tsp = 2.0 / 1.772453850905516;
-    for (int t0 = 0; t0 < V.n; t0 += kBlock) {
-        const int j = t0 + threadIdx.x;
-        __syncthreads();
-        if (j < V.n) {
-            PairTile& s = st[threadIdx.x];
-            s.p = V.pos[j];
-            s.p0 = V.pos0[j];
-            s.alp = V.alpeeq[j];
-            s.q = V.q[j];
-            s.zeta = V.zeta[j];
-            s.szr = V.szr[j];
-            s.slot = V.slot[j];
-            s.nref = V.nref[j];
-            for (int b = 0; b < 7; ++b) { s.w0[b] = V.w0[j * 7 + b]; s.w[b] = V.w[j * 7 + b]; }
-        }
-        __syncthreads();
-        if (!act) continue;
-        const int m = min(kBlock, V.n - t0);
-        for (int k = 0; k < m; ++k) {
-            if (t0 + k == i) continue;
-            const PairTile& s = st[k];
-            const double dx = pi.x - s.p.x, dy = pi.y - s.p.y, dz = pi.z - s.p.z;
+    if (i < V.n) {
+        const double4 pi = V.pos[i], p0i = V.pos0[i];
+        const double ai = V.alpeeq[i], qi = V.q[i], zi = V.zeta[i], szi = V.szr[i];
+        const double* g0i = V.g0 + (size_t)i * V.K * 7;
+        const double* dgi = V.hdg + (size_t)i * V.K * 7;
+        const double a1 = 0.58, a2 = 4.80, tsp = 2.0 / 1.772453850905516;
+        for (int j = lane; j < V.n; j += 32) {
+            if (j == i) continue;
+            const double4 pj = V.pos[j];
+            const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
             const double r = sqrt(dx * dx + dy * dy + dz * dz);
             double dEdr = 0.0;
             if (r <= 100.0 && r >= 1e-10) {
-                const double g = 1.0 / sqrt(ai + s.alp);
+                const double g = 1.0 / sqrt(ai + V.alpeeq[j]);
                 const double gr = g * r;
                 const double ef = erf(gr);
-                const double qq = qi * s.q;
+                const double qq = qi * V.q[j];
                 ec += qq * ef / r;
                 dEdr += qq * ((g * exp(-gr * gr) * tsp) / r - ef / (r * r));
             }
-            if (r <= 50.0 && r >= 1e-10 && d2_exact(p0i, s.p0) <= 3600.0) {
-                const double* g0 = g0i + s.slot * 7;
-                const double* dg = dgi + s.slot * 7;
+            if (r <= 50.0 && r >= 1e-10 && d2_exact(p0i, V.pos0[j]) <= 3600.0) {
+                const int sj = V.slot[j], nr = V.nref[j];
+                const double* g0 = g0i + sj * 7;
+                const double* dg = dgi + sj * 7;
+                const double* w0 = V.w0 + (size_t)j * 7;
+                const double* w = V.w + (size_t)j * 7;
                 double c6 = 0.0, dc6 = 0.0;
-                for (int b = 0; b < s.nref; ++b) {
-                    c6 += g0[b] * s.w0[b];
-                    dc6 += dg[b] * s.w[b];
+                for (int b = 0; b < nr; ++b) {
+                    c6 += g0[b] * w0[b];
+                    dc6 += dg[b] * w[b];
                 }
-                const double r4r2 = 3.0 * szi * s.szr;
+                const double r4r2 = 3.0 * szi * V.szr[j];
                 const double t = a1 * sqrt(r4r2) + a2;
                 const double r0sq = t * t;
-                const double zz = zi * s.zeta;
+                const double zz = zi * V.zeta[j];
                 const double r2 = r * r, r6 = r2 * r2 * r2, r06 = r0sq * r0sq * r0sq;
                 const double t6 = 1.0 / (r6 + r06);
                 const double t8 = 1.0 / (r6 * r2 + r06 * r0sq);
@@ -1145,12 +1115,18 @@ __global__ void __launch_bounds__(kBlock) k_pairs(View V)
                 gx += f * dx; gy += f * dy; gz += f * dz;
             }
         }
-    }
-    if (act) {
-        V.grad[3 * i] += gx;
-        V.grad[3 * i + 1] += gy;
-        V.grad[3 * i + 2] += gz;
-        V.dEdcn[i] += dcn;
+        for (int o = 16; o > 0; o >>= 1) {
+            gx += __shfl_down_sync(0xffffffffu, gx, o);
+            gy += __shfl_down_sync(0xffffffffu, gy, o);
+            gz += __shfl_down_sync(0xffffffffu, gz, o);
+            dcn += __shfl_down_sync(0xffffffffu, dcn, o);
+        }
+        if (lane == 0) {
+            V.grad[3 * i] += gx;
+            V.grad[3 * i + 1] += gy;
+            V.grad[3 * i + 2] += gz;
+            V.dEdcn[i] += dcn;
+        }
     }
     block_add(0.5 * ec, V.E + T_COUL);
     block_add(0.5 * ed, V.E + T_DISP);
@@ -1179,37 +1155,33 @@ __global__ void k_post(View V)
 // over the 6 bohr neighbours (gfnff_method.cpp:5837-6260, forcefieldthread.h:80-109)
 __global__ void __launch_bounds__(kBlock) k_cn_chain(View V)
 {
-    __shared__ double4 sp[kBlock];
-    __shared__ double sr[kBlock], su[kBlock];
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool act = i < V.n;
-    const double4 pi = act ? V.pos[i] : make_double4(0, 0, 0, 0);
-    const double ri = act ? V.rcov_cn[i] : 0.0;
-    const double ui = act ? V.dlog[i] * V.v[i] : 0.0;
+    const int i = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (i >= V.n) return;
+    const double4 pi = V.pos[i];
+    const double ri = V.rcov_cn[i];
+    const double ui = V.dlog[i] * V.v[i];
     const double kn = -7.5, sqrtpi = 1.77245385091;
     double gx = 0.0, gy = 0.0, gz = 0.0;
-    for (int t0 = 0; t0 < V.n; t0 += kBlock) {
-        const int j = t0 + threadIdx.x;
-        __syncthreads();
-        if (j < V.n) { sp[threadIdx.x] = V.pos[j]; sr[threadIdx.x] = V.rcov_cn[j]; su[threadIdx.x] = V.dlog[j] * V.v[j]; }
-        __syncthreads();
-        if (!act) continue;
-        const int m = min(kBlock, V.n - t0);
-        for (int k = 0; k < m; ++k) {
-            if (t0 + k == i) continue;
-            const double4 pj = sp[k];
-            const double dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
-            const double d2 = dx * dx + dy * dy + dz * dz;
-            if (!(d2 < 36.0)) continue;
-            const double r = sqrt(d2);
-            const double rs = ri + sr[k];
-            const double dr = (r - rs) / rs;
-            const double de = (kn / sqrtpi) * exp(-kn * kn * dr * dr) / rs;
-            const double f = -(de / r) * (ui + su[k]);
-            gx += f * dx; gy += f * dy; gz += f * dz;
-        }
+    for (int j = lane; j < V.n; j += 32) {
+        if (j == i) continue;
+        const double4 pj = V.pos[j];
+        const double dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
+        const double d2 = dx * dx + dy * dy + dz * dz;
+        if (!(d2 < 36.0)) continue;
+        const double r = sqrt(d2);
+        const double rs = ri + V.rcov_cn[j];
+        const double dr = (r - rs) / rs;
+        const double de = (kn / sqrtpi) * exp(-kn * kn * dr * dr) / rs;
+        const double f = -(de / r) * (ui + V.dlog[j] * V.v[j]);
+        gx += f * dx; gy += f * dy; gz += f * dz;
     }
-    if (act) {
+    for (int o = 16; o > 0; o >>= 1) {
+        gx += __shfl_down_sync(0xffffffffu, gx, o);
+        gy += __shfl_down_sync(0xffffffffu, gy, o);
+        gz += __shfl_down_sync(0xffffffffu, gz, o);
+    }
+    if (lane == 0) {
         V.grad[3 * i] += gx;
         V.grad[3 * i + 1] += gy;
         V.grad[3 * i + 2] += gz;
@@ -1300,6 +1272,12 @@ struct Engine::Impl {
     DBuf<int> info, info2, status, ipiv;
     int lwork = 0;
     bool use_lu = false;   // reduced EEQ matrix not positive definite: pivoted LU instead
+    bool timing = false;
+    cudaEvent_t ev[Engine::kNumPhases + 1] = {};
+    void mark(int k)
+    {
+        if (timing) CK(cudaEventRecord(ev[k], stream));
+    }
     int nb = 0, na = 0, nt = 0, ns = 0, ninv = 0, natm = 0, nbatm = 0, nhb = 0, nxb = 0;
 
     View view() const
@@ -1325,8 +1303,34 @@ Engine::Engine(const EngineOptions& opt) : p_(new Impl)
     CS(cusolverDnSetStream(p_->sol, p_->stream));
 }
 
+const char* const Engine::kPhaseNames[] = {"positions", "cn", "d4_weights", "eeq_matrix", "eeq_reduce",
+                                           "eeq_factor_solve", "bonded", "hbonds", "repulsion", "pairs",
+                                           "post_chain", "finish"};
+
+void Engine::set_timing(bool on)
+{
+    if (on && !p_->ev[0])
+        for (int k = 0; k <= kNumPhases; ++k) CK(cudaEventCreate(&p_->ev[k]));
+    p_->timing = on;
+}
+
+std::vector<double> Engine::phase_ms()
+{
+    std::vector<double> out(kNumPhases, 0.0);
+    if (!p_->timing) return out;
+    CK(cudaEventSynchronize(p_->ev[kNumPhases]));
+    for (int k = 0; k < kNumPhases; ++k) {
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, p_->ev[k], p_->ev[k + 1]));
+        out[k] = ms;
+    }
+    return out;
+}
+
 Engine::~Engine()
 {
+    for (auto& e : p_->ev)
+        if (e) cudaEventDestroy(e);
     if (p_->sol) cusolverDnDestroy(p_->sol);
     if (p_->stream) cudaStreamDestroy(p_->stream);
 }
@@ -1573,21 +1577,29 @@ void Engine::enqueue(const double* d_xyz, bool bohr)
     cudaStream_t s = P.stream;
     const int n = P.n;
     View V = P.view();
+    P.mark(0);
     CK(cudaMemsetAsync(P.grad.p, 0, 3 * (size_t)n * sizeof(double), s));
     CK(cudaMemsetAsync(P.dEdcn.p, 0, (size_t)n * sizeof(double), s));
     CK(cudaMemsetAsync(P.msd.p, 0, sizeof(double), s));
     const double scale = bohr ? 1.0 : kAngToBohr;
     k_positions<<<nblk(n), kBlock, 0, s>>>(n, d_xyz, scale, P.pos.p, P.hbref.p, P.msd.p, P.E.p, P.status.p);
-    k_cn<<<nblk(n), kBlock, 0, s>>>(V);
+    P.mark(1);
+    k_cn<<<nblk((long)n * 32), kBlock, 0, s>>>(V);
+    P.mark(2);
     k_d4_weights<<<nblk(n), kBlock, 0, s>>>(V);
     // EEQ
     {
+        P.mark(3);
         dim3 g(nblk(n), n);
         k_eeq_matrix<<<g, kBlock, 0, s>>>(V, P.A.p);
         k_eeq_residual<<<nblk((long)n * 32), kBlock, 0, s>>>(V, P.A.p, P.q0.p, P.rvec.p);
+        P.mark(4);
         if (P.nred > 0) {
             dim3 g2(nblk(P.nred), P.nred);
             k_eeq_reduce<<<g2, kBlock, 0, s>>>(V, P.A.p, P.red2atom.p, P.anchor.p, P.rvec.p, P.M.p, P.bvec.p);
+        }
+        P.mark(5);
+        if (P.nred > 0) {
             if (!P.use_lu) {
                 CS(cusolverDnDpotrf(P.sol, CUBLAS_FILL_MODE_LOWER, P.nred, P.M.p, P.nred, P.work.p, P.lwork, P.info.p));
                 CS(cusolverDnDpotrs(P.sol, CUBLAS_FILL_MODE_LOWER, P.nred, 1, P.M.p, P.nred, P.bvec.p, P.nred, P.info2.p));
@@ -1598,6 +1610,7 @@ void Engine::enqueue(const double* d_xyz, bool bohr)
         }
         k_eeq_expand<<<nblk(n), kBlock, 0, s>>>(V, P.q0.p, P.atom2red.p, P.frag_off.p, P.frag_atoms.p, P.anchor.p, P.bvec.p);
     }
+    P.mark(6);
     if (P.nb) {
         BondSoA B{P.nb, P.b_i.p, P.b_j.p, P.b_h.p, P.b_off.p, P.b_hb.p, P.b_fc.p, P.b_al.p,
                   P.b_r0i.p, P.b_r0j.p, P.b_cki.p, P.b_ckj.p, P.b_sh.p, P.b_ff.p};
@@ -1609,17 +1622,23 @@ void Engine::enqueue(const double* d_xyz, bool bohr)
     if (P.ninv) k_inversions<<<nblk(P.ninv), kBlock, 0, s>>>(V, InvSoA{P.ninv, P.v_i.p, P.v_j.p, P.v_k.p, P.v_l.p, P.v_t.p, P.v_fc.p, P.v_om.p});
     if (P.natm) k_atm<<<nblk(P.natm), kBlock, 0, s>>>(V, TripSoA{P.natm, P.at_i.p, P.at_j.p, P.at_k.p, P.at_c9.p, P.at_r0ij.p, P.at_r0ik.p, P.at_r0jk.p, P.at_sc.p});
     if (P.nbatm) k_batm<<<nblk(P.nbatm), kBlock, 0, s>>>(V, TripSoA{P.nbatm, P.ba_i.p, P.ba_j.p, P.ba_k.p, P.ba_c9.p, nullptr, nullptr, nullptr, nullptr});
+    P.mark(7);
     if (P.nhb) {
         HBSoA H{P.nhb, P.h_a.p, P.h_h.p, P.h_b.p, P.h_c.p, P.h_pc.p, P.h_nbo.p, P.h_nb.p, P.h_nco.p, P.h_nc.p,
                 P.h_ba.p, P.h_bb.p, P.h_aa.p, P.h_ab.p, P.h_QH.p, P.h_QA.p, P.h_QB.p, P.h_rv.p, P.h_zlp.p, P.h_nfl.p};
         k_hbonds<<<nblk(P.nhb), kBlock, 0, s>>>(V, H);
     }
     if (P.nxb) k_xbonds<<<nblk(P.nxb), kBlock, 0, s>>>(V, XBSoA{P.nxb, P.x_a.p, P.x_x.p, P.x_b.p, P.x_pre.p, P.x_rv.p});
-    k_repulsion<<<nblk(n), kBlock, 0, s>>>(V, P.r_off.p, P.r_j.p, P.r_al.p, P.r_ab.p, P.r_kind.p);
-    k_pairs<<<nblk(n), kBlock, 0, s>>>(V);
+    P.mark(8);
+    k_repulsion<<<nblk((long)n * 32), kBlock, 0, s>>>(V, P.r_off.p, P.r_j.p, P.r_al.p, P.r_ab.p, P.r_kind.p);
+    P.mark(9);
+    k_pairs<<<nblk((long)n * 32), kBlock, 0, s>>>(V);
+    P.mark(10);
     k_post<<<nblk(n), kBlock, 0, s>>>(V);
-    k_cn_chain<<<nblk(n), kBlock, 0, s>>>(V);
+    k_cn_chain<<<nblk((long)n * 32), kBlock, 0, s>>>(V);
+    P.mark(11);
     k_finish<<<1, 256, 0, s>>>(V, P.nred > 0 ? P.info.p : nullptr, P.e0, nullptr, nullptr);
+    P.mark(12);
     CK(cudaGetLastError());
 }
 

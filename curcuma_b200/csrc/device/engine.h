@@ -51,6 +51,12 @@ public:
     void set_hb_reference(const double* xyz_bohr);
     // switches the EEQ solve to pivoted LU (after a NOT_SPD status); false if already
     bool switch_to_lu();
+    // per-phase CUDA-event timing of enqueue(); phase_ms returns the milliseconds of the
+    // last evaluation per phase (order of kPhaseNames) after the stream has finished
+    void set_timing(bool on);
+    std::vector<double> phase_ms();
+    static const char* const kPhaseNames[];
+    static constexpr int kNumPhases = 12;
 
     static constexpr int kNumTerms = 14;
 

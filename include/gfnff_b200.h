@@ -92,6 +92,20 @@ gfnff_status gfnff_get_topology(gfnff_handle* h, int kind, int* out, long cap, l
 /* Atom count and fragment count of the set-up system. */
 gfnff_status gfnff_sizes(gfnff_handle* h, int* natoms, int* nfrag);
 
+/* Per-phase CUDA-event timing of every evaluation (off by default; costs two event
+ * records per phase).  gfnff_phase_times copies the milliseconds of the last
+ * evaluation, in the order positions, cn, d4_weights, eeq_matrix, eeq_reduce,
+ * eeq_factor_solve, bonded, hbonds, repulsion, pairs, post_chain, finish, and returns
+ * the number of phases (or -1).  Diagnostics without a counterpart in the reference
+ * (curcuma prints phase timings at verbosity >= 2 instead, gfnff.h:742). */
+gfnff_status gfnff_set_phase_timing(gfnff_handle* h, int on);
+int gfnff_phase_times(gfnff_handle* h, double* ms, int cap);
+
+/* FMA throughput of the device in TFLOP/s (fp64 != 0: FP64, else FP32), measured by a
+ * short microbenchmark; the roofline denominator of the SIMT pair kernels.  No
+ * counterpart in the reference. */
+double gfnff_fma_peak_tflops(int device, int fp64);
+
 /* Last error message of the handle (static storage when h is NULL). */
 const char* gfnff_last_error(gfnff_handle* h);
 
