@@ -19,7 +19,8 @@ NTERMS = len(TERM_NAMES)
 EXPORTED = ["gfnff_default_options", "gfnff_create", "gfnff_setup", "gfnff_energy_and_gradient",
             "gfnff_energy_and_gradient_device", "gfnff_stream", "gfnff_charges",
             "gfnff_coordination_numbers", "gfnff_get_topology", "gfnff_sizes", "gfnff_last_error",
-            "gfnff_destroy", "gfnff_set_phase_timing", "gfnff_phase_times", "gfnff_fma_peak_tflops"]
+            "gfnff_destroy", "gfnff_set_phase_timing", "gfnff_phase_times", "gfnff_fma_peak_tflops",
+            "gfnff_eeq_charges_noalloc"]
 PHASES = ["positions", "cn", "d4_weights", "eeq_matrix", "eeq_reduce", "eeq_factor_solve", "bonded",
           "hbonds", "repulsion", "pairs", "post_chain", "finish"]
 
@@ -61,6 +62,7 @@ def load():
     lib.gfnff_phase_times.argtypes = [c_v, P(c_d), c_i]
     lib.gfnff_fma_peak_tflops.argtypes = [c_i, c_i]
     lib.gfnff_fma_peak_tflops.restype = c_d
+    lib.gfnff_eeq_charges_noalloc.argtypes = [c_i, c_i] + [c_v] * 11
     for name in EXPORTED:
         if name not in ("gfnff_default_options", "gfnff_stream", "gfnff_last_error", "gfnff_fma_peak_tflops"):
             getattr(lib, name).restype = c_i

@@ -106,6 +106,25 @@ int gfnff_phase_times(gfnff_handle* h, double* ms, int cap);
  * counterpart in the reference. */
 double gfnff_fma_peak_tflops(int device, int fp64);
 
+/* Allocation-free EEQ charges, for callers that cannot allocate device memory (code
+ * running inside another framework's memory pool, loops that forbid allocations after
+ * start-up).  No counterpart in the reference.  Every buffer is a device pointer owned
+ * by the caller: d_xyz_bohr (N*3), per-atom d_alpha (alpha^2 as in the EEQ matrix),
+ * d_gam (hardness incl. corrections), d_chi (-chi + corrections), d_cnf, d_cn, d_frag
+ * (0-based fragment ids), d_qfrag (nfrag target charges); outputs d_q (N) and d_status
+ * (1 int, gfnff_status of the device solve: GFNFF_NOT_SPD when the reduced EEQ matrix
+ * has no Cholesky factor).  Work is enqueued on `stream` (a cudaStream_t, NULL = legacy
+ * default) without host synchronisation.  All intermediate storage is one file-scope
+ * device array sized for GFNFF_NOALLOC_MAX_ATOMS atoms (about 17 MB, held by every GPU
+ * that loads the library until exit); larger systems return GFNFF_INVALID_ARG.  The first
+ * call on a device looks the array up (cudaGetSymbolAddress) and should come before any
+ * stream capture.  All calls share the array: calls that overlap on the GPU race. */
+#define GFNFF_NOALLOC_MAX_ATOMS 1024
+gfnff_status gfnff_eeq_charges_noalloc(int natoms, int nfrag, const double* d_xyz_bohr, const double* d_alpha,
+                                       const double* d_gam, const double* d_chi, const double* d_cnf,
+                                       const double* d_cn, const int* d_frag, const double* d_qfrag,
+                                       double* d_q, int* d_status, void* stream);
+
 /* Last error message of the handle (static storage when h is NULL). */
 const char* gfnff_last_error(gfnff_handle* h);
 

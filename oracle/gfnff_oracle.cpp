@@ -938,6 +938,7 @@ int oracle_atom_data(oracle_handle* h, int which, double* out)
         case 2: src = &m.alpeeq; break;
         case 3: src = &m.gam; break;
         case 4: src = &m.chi_base; break;
+        case 5: src = &m.cnf; break;
         default: return 1;
     }
     std::copy(src->begin(), src->end(), out);
