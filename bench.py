@@ -134,7 +134,8 @@ def pair_counts(Z, X):
 def roofline(phase_avg, info, fp64_peak, hbm_peak, hbm_src):
     """Algorithmic work per launch of the dominant phase.  FLOP conventions (erf/exp/
     sqrt/div = 1 op): Coulomb E+G 40/pair, D4 E+G 45/pair, repulsion 30/pair, CN+dCN
-    35/pair, EEQ element 20; Cholesky n^3/3 + 2 n^2 (solve)."""
+    35/pair, EEQ element 20; Cholesky n^3/3 + 2 n^2 (solve).  Pair counts are unique pairs
+    (i < j): the algorithmic work, whatever the kernel evaluates."""
     name = max(phase_avg, key=phase_avg.get)
     ms = phase_avg[name]
     n, nred = info["n"], info["nred"]
@@ -142,16 +143,15 @@ def roofline(phase_avg, info, fp64_peak, hbm_peak, hbm_src):
         flops = 40.0 * info["coulomb_pairs"] + 45.0 * info["disp_pairs"]
         bound, unit, peak = "fp64", "TFLOP/s", fp64_peak
         achieved = flops / (ms * 1e-3) / 1e12
-    elif name == "eeq_factor_solve":
+    elif name == "eeq_solve":
         flops = nred ** 3 / 3.0 + 2.0 * nred ** 2
         bound, unit, peak = "fp64", "TFLOP/s", fp64_peak
         achieved = flops / (ms * 1e-3) / 1e12
-    elif name in ("eeq_matrix", "eeq_reduce"):
-        # HBM: the dense matrix is written once and read once per phase
-        m = n if name == "eeq_matrix" else nred
-        bytes_ = 2.0 * 8.0 * m * m
-        bound, unit, peak = "hbm", "GB/s", hbm_peak
-        achieved = bytes_ / (ms * 1e-3) / 1e9
+    elif name == "eeq_matrix":
+        # lower triangle of the reduced matrix, four EEQ elements (20 FLOP each) per entry
+        flops = 80.0 * nred * (nred + 1) / 2.0
+        bound, unit, peak = "fp64", "TFLOP/s", fp64_peak
+        achieved = flops / (ms * 1e-3) / 1e12
     else:
         # list-driven phases: term records + 24 B coordinates + 24 B gradient per atom ref
         bytes_ = info.get(f"bytes_{name}", 0.0)

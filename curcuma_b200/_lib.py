@@ -21,7 +21,7 @@ EXPORTED = ["gfnff_default_options", "gfnff_create", "gfnff_setup", "gfnff_energ
             "gfnff_coordination_numbers", "gfnff_get_topology", "gfnff_sizes", "gfnff_last_error",
             "gfnff_destroy", "gfnff_set_phase_timing", "gfnff_phase_times", "gfnff_fma_peak_tflops",
             "gfnff_eeq_charges_noalloc"]
-PHASES = ["positions", "cn", "d4_weights", "eeq_matrix", "eeq_reduce", "eeq_factor_solve", "bonded",
+PHASES = ["positions", "cn", "d4_weights", "eeq_matrix", "eeq_rhs", "eeq_solve", "bonded",
           "hbonds", "repulsion", "pairs", "post_chain", "finish"]
 
 

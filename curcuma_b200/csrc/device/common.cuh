@@ -1,0 +1,243 @@
+// Shared device-side definitions of the GFN-FF engine: error macros, device buffers,
+// small vector helpers, the model view passed to every kernel and the per-molecule
+// energy reduction.  Included inside namespace gfnff by engine.cu (one translation unit).
+#pragma once
+
+#define CK(x)                                                                                \
+    do {                                                                                     \
+        cudaError_t e_ = (x);                                                                \
+        if (e_ != cudaSuccess)                                                               \
+            throw std::runtime_error(std::string("CUDA: ") + cudaGetErrorString(e_) + " at " + \
+                                     __FILE__ + ":" + std::to_string(__LINE__));             \
+    } while (0)
+
+#define CS(x)                                                                                \
+    do {                                                                                     \
+        cusolverStatus_t s_ = (x);                                                           \
+        if (s_ != CUSOLVER_STATUS_SUCCESS)                                                   \
+            throw std::runtime_error("cuSOLVER error " + std::to_string((int)s_) + " at " +   \
+                                     std::to_string(__LINE__));                              \
+    } while (0)
+
+namespace {
+
+
+enum {
+    T_BOND = 0, T_ANGLE, T_TORSION, T_INVERSION, T_STORSION, T_DISP, T_BREP, T_NBREP, T_COUL,
+    T_HB, T_XB, T_ATM, T_BATM, T_TOTAL
+};
+
+constexpr int kBlock = 128;
+constexpr double kPi = 3.14159265358979323846;
+
+template <class T>
+struct DBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    void alloc(size_t cnt)
+    {
+        free();
+        n = cnt;
+        if (cnt) CK(cudaMalloc(&p, cnt * sizeof(T)));
+    }
+    void upload(const std::vector<T>& v)
+    {
+        alloc(v.size());
+        if (!v.empty()) CK(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    }
+    void free()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    ~DBuf() { free(); }
+};
+
+// ------------------------------------------------------------------------------------
+// small device helpers
+// ------------------------------------------------------------------------------------
+struct D3 {
+    double x, y, z;
+};
+__device__ __forceinline__ D3 mk(double x, double y, double z) { return {x, y, z}; }
+__device__ __forceinline__ D3 operator-(D3 a, D3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ D3 operator+(D3 a, D3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ D3 operator*(double s, D3 a) { return {s * a.x, s * a.y, s * a.z}; }
+__device__ __forceinline__ double dot(D3 a, D3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ D3 cross(D3 a, D3 b)
+{
+    return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+__device__ __forceinline__ double nrm(D3 a) { return sqrt(dot(a, a)); }
+__device__ __forceinline__ D3 ld(const double4* p, int i)
+{
+    double4 v = p[i];
+    return {v.x, v.y, v.z};
+}
+__device__ __forceinline__ void agrad(double* g, int i, D3 v)
+{
+    atomicAdd(g + 3 * i, v.x);
+    atomicAdd(g + 3 * i + 1, v.y);
+    atomicAdd(g + 3 * i + 2, v.z);
+}
+
+// block-wide sum of one value, one atomicAdd per block into *dst
+__device__ __forceinline__ void block_add(double v, double* dst)
+{
+    __shared__ double red[32];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) red[w] = v;
+    __syncthreads();
+    if (w == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+        v = lane < nw ? red[lane] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0 && v != 0.0) atomicAdd(dst, v);
+    }
+}
+
+// bond-angle cosine and d(theta)/dx (forcefieldfunctions.h:47-83)
+__device__ double angle_cos(D3 i, D3 j, D3 k, D3 d[3])
+{
+    D3 rij = i - j, rkj = k - j;
+    const double a = nrm(rij), b = nrm(rkj);
+    d[0] = d[1] = d[2] = mk(0, 0, 0);
+    if (a < 1e-10 || b < 1e-10) return 1.0;
+    D3 nij = (1.0 / a) * rij, nkj = (1.0 / b) * rkj;
+    double c = dot(rij, rkj) / (a * b);
+    c = fmax(-1.0, fmin(1.0, c));
+    const double s = sqrt(fmax(0.0, 1.0 - c * c));
+    if (s < 1e-14) return c;
+    const double f = 1.0 / s;
+    d[0] = (-f / a) * (nkj - c * nij);
+    d[2] = (-f / b) * (nij - c * nkj);
+    d[1] = -1.0 * (d[0] + d[2]);
+    return c;
+}
+
+// dihedral angle and d(phi)/dx (gfnff_geometry.h:66-160)
+__device__ double dihedral(D3 ri, D3 rj, D3 rk, D3 rl, D3 g[4])
+{
+    for (int a = 0; a < 4; ++a) g[a] = mk(0, 0, 0);
+    D3 v1 = rj - ri, v2 = rk - rj, v3 = rl - rk;
+    D3 n1 = cross(v1, v2), n2 = cross(v2, v3);
+    const double n1n = nrm(n1), n2n = nrm(n2), v2n = nrm(v2);
+    if (n1n < 1e-10 || n2n < 1e-10 || v2n < 1e-10) return 0.0;
+    D3 h1 = (1.0 / n1n) * n1, h2 = (1.0 / n2n) * n2;
+    const double cphi = dot(h1, h2);
+    double sphi = (v2n * dot(h1, v3)) / n2n;
+    sphi = fmax(-1.0, fmin(1.0, sphi));
+    const double phi = atan2(sphi, cphi);
+    const double nen = n1n * n2n * sin(phi);
+    if (fabs(nen) < 1e-14) return phi;
+    const double o = 1.0 / nen;
+    D3 rab = cross(n1, v2), rbb = cross(n2, v2), rac = cross(n1, v3), rbc = cross(n2, v3);
+    D3 rba = cross(n2, v1), raa = cross(n1, v1);
+    D3 rapb = v1 + v2, rbpc = v2 + v3;
+    D3 rapba = cross(rapb, n1), rapbb = cross(rapb, n2), rbpca = cross(rbpc, n1), rbpcb = cross(rbpc, n2);
+    g[0] = o * ((cphi * n2n / n1n) * rab - rbb);
+    g[1] = o * (cphi * ((n2n / n1n) * rapba + (n1n / n2n) * rbc) - (rac + rapbb));
+    g[2] = o * (cphi * ((n2n / n1n) * raa + (n1n / n2n) * rbpcb) - (rba + rbpca));
+    g[3] = o * ((cphi * n1n / n2n) * rbb - rab);
+    return phi;
+}
+
+// out-of-plane angle and its derivative (gfnff_geometry.h:207-265)
+__device__ double oop(D3 ri, D3 rj, D3 rk, D3 rl, D3 g[4])
+{
+    for (int a = 0; a < 4; ++a) g[a] = mk(0, 0, 0);
+    D3 re = ri - rj, rd = rk - rj, rv = rl - ri;
+    D3 rn = cross(re, rd);
+    const double rnn = nrm(rn), rvn = nrm(rv);
+    if (rnn < 1e-10 || rvn < 1e-10) return 0.0;
+    double so = dot((1.0 / rnn) * rn, (1.0 / rvn) * rv);
+    so = fmax(-1.0, fmin(1.0, so));
+    const double om = asin(so);
+    const double nen = rnn * rvn * cos(om);
+    if (fabs(nen) < 1e-14) return om;
+    const double o = 1.0 / nen, s = sin(om);
+    D3 rdme = rd - re, rve = cross(rv, re), rne = cross(rn, re), rdv = cross(rd, rv), rdn = cross(rd, rn);
+    D3 rvdme = cross(rv, rdme), rndme = cross(rn, rdme);
+    g[0] = o * (rdv - rn - s * ((rvn / rnn) * rdn - (rnn / rvn) * rv));
+    g[1] = o * (rvdme - (s * rvn / rnn) * rndme);
+    g[2] = o * (rve - (s * rvn / rnn) * rne);
+    g[3] = o * (rn - (s * rnn / rvn) * rv);
+    return om;
+}
+
+// squared distance evaluated without FMA contraction, bit-identical to the host list
+// builders ((dx*dx + dy*dy) + dz*dz)
+__device__ __forceinline__ double d2_exact(double4 a, double4 b)
+{
+    const double dx = __dsub_rn(a.x, b.x), dy = __dsub_rn(a.y, b.y), dz = __dsub_rn(a.z, b.z);
+    return __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+}
+
+// ------------------------------------------------------------------------------------
+// device view of the model.  Atoms are stored in the engine's internal order (molecules
+// contiguous, atoms of a molecule sorted along a Morton curve of the setup geometry);
+// perm maps an internal index to the caller's index.
+// ------------------------------------------------------------------------------------
+struct View {
+    int n, nfrag, K, nred, nmol;
+    const int* mol;           // molecule of each atom
+    const int2* jr;           // [first, last+1) atom range of the atom's molecule
+    const int* perm;          // internal -> caller index
+    const double4* pos;       // current geometry (bohr)
+    const double4* pos0;      // setup geometry (bohr)
+    const double* rcov_cn;
+    const double* rcov43;     // 4/3 * covalent_rad_d3 (angle/torsion damping)
+    const double* rcov_d3;
+    const double* chi_base;
+    const double* cnf;
+    const double* gam;
+    const double* alpeeq;
+    const double* adiag;      // EEQ diagonal gam + sqrt(2/pi)/sqrt(alpha)
+    const double* qa;
+    const int* slot;
+    const int* nref;
+    const double* refcn;      // n*7
+    const double* w0;         // n*7 setup weights
+    const double* g0;         // n*K*7 setup half contraction
+    const double* c6ref;      // K*K*49
+    const double* zeta;
+    const double* szr;        // sqrt(0.5 r4/r2 sqrt Z)
+    // per step
+    double* cnraw;
+    double* cn;
+    double* dlog;
+    double* w;                // n*7
+    double* dw;
+    double* hg;               // n*K*7
+    double* hdg;
+    double* q;
+    double* dEdcn;
+    double* v;
+    double* grad;
+    double* E;                // nmol*16 term energies
+    int* status;              // nmol
+};
+
+// Adds v to term `term` of molecule `mol` (mol < 0: nothing to add).  Every thread of
+// the block calls it.  Single-molecule models reduce over the block; batches reduce
+// over the warp when its lanes share a molecule and add per thread otherwise.
+__device__ __forceinline__ void eadd(const View& V, double v, int mol, int term)
+{
+    if (V.nmol == 1) {
+        block_add(v, V.E + term);
+        return;
+    }
+    const unsigned full = 0xffffffffu;
+    const int m0 = __shfl_sync(full, mol, 0);
+    if (__all_sync(full, mol == m0 || mol < 0)) {
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(full, v, o);
+        if ((threadIdx.x & 31) == 0 && m0 >= 0 && v != 0.0) atomicAdd(V.E + 16 * m0 + term, v);
+    } else if (mol >= 0 && v != 0.0) {
+        atomicAdd(V.E + 16 * mol + term, v);
+    }
+}
+
+}  // namespace

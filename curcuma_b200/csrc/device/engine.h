@@ -1,5 +1,6 @@
-// Device engine: the GFN-FF model cached in HBM and the per-geometry energy + gradient
-// pipeline (host-side interface; kernels live in engine.cu).
+// Device engine: the GFN-FF model of one molecule or of a batch of independent molecules
+// cached in HBM, and the per-geometry energy + gradient pipeline (host-side interface;
+// kernels live in engine.cu and the k_*.cuh files it includes).
 #pragma once
 
 #include <memory>
@@ -22,32 +23,39 @@ public:
     Engine(const Engine&) = delete;
     Engine& operator=(const Engine&) = delete;
 
-    // uploads the model; throws std::runtime_error on CUDA failure
+    // Uploads one model (upload) or a batch of independent molecules (upload_batch; the
+    // molecules do not interact, their atoms are concatenated in the given order).
+    // Throws std::runtime_error on CUDA failure.
     void upload(const Model& m);
-    // re-uploads the HB/XB lists and the bond<->HB cross reference of m
+    void upload_batch(const std::vector<const Model*>& mols);
+    // re-uploads the HB/XB lists and the bond<->HB cross reference (single model)
     void upload_hbxb(const Model& m);
 
-    // Enqueues one energy+gradient evaluation.  xyz is N*3 doubles, device pointer,
-    // in bohr when bohr=true else Angstrom.  Results stay on the device (see below).
+    // Enqueues one energy+gradient evaluation.  xyz is N*3 doubles (all atoms of the
+    // batch in upload order), device pointer, in bohr when bohr=true else Angstrom.
+    // Results stay on the device (below), in the caller's atom order.
     void enqueue(const double* d_xyz, bool bohr);
 
     // device result buffers of the last enqueue
-    const double* d_terms() const;     // kNumTerms doubles
+    const double* d_terms() const;     // 16 doubles per molecule (kNumTerms used)
     const double* d_grad() const;      // N*3
     const double* d_charges() const;   // N
     const double* d_cn() const;        // N
-    const int* d_status() const;       // 1 int (gfnff_status)
+    const int* d_status() const;       // 1 int (gfnff_status) per molecule
     const double* d_hb_msd() const;    // sum of squared displacements vs HB reference
     double* d_xyz_scratch();           // N*3 staging buffer for host coordinates
 
     void* stream() const;
     int natoms() const;
+    int nmol() const;
     void sync();
-    // copies the last results to the host
+    // copies the last results to the host (molecule 0's terms and status)
     void fetch(double* terms, double* grad, int* status, double* hb_msd);
-    // device-enumerated dispersion pair list (i<j) at the setup geometry
+    // every molecule's 16 term slots, status per molecule, the whole gradient
+    void fetch_batch(double* terms16, double* grad, int* status);
+    // device-enumerated dispersion pair list (i<j, caller indices) at the setup geometry
     std::vector<int> device_dispersion_pairs();
-    // sets the HB reference geometry (bohr, host) for the refresh test
+    // sets the HB reference geometry (bohr, host, caller order) for the refresh test
     void set_hb_reference(const double* xyz_bohr);
     // switches the EEQ solve to pivoted LU (after a NOT_SPD status); false if already
     bool switch_to_lu();

@@ -1,0 +1,404 @@
+// Non-bonded GFN-FF kernels: geometry in, coordination numbers, D4 weights, repulsion,
+// all-pairs Coulomb + D4 dispersion, self energy, CN chain rule and the outputs.
+// Included inside namespace gfnff by engine.cu (one translation unit).
+//
+// The all-pairs kernels share one layout: a block owns kTile consecutive atoms i (one per
+// thread) and walks the partners j of its molecule range in tiles of kTile staged through
+// shared memory, so every partner record is read from L2 once per block and broadcast to
+// all threads.  grid.y splits the partner range of an i-block (nsplit slices) so that small
+// systems still fill the 148 SMs; per-atom partial sums then meet in FP64 atomics.  Atoms
+// are Morton-sorted at upload, so the lanes of a warp are spatial neighbours and the
+// short-range branches (erf, exp) stay coherent.
+#pragma once
+
+namespace {
+
+constexpr int kTile = 128;
+
+// partner range [jb, je) of this block's slice
+__device__ __forceinline__ void tile_range(const View& V, int i0, int nsplit, int& jb, int& je)
+{
+    const int last = min(V.n, i0 + kTile) - 1;
+    const int lo = V.jr[i0].x, hi = V.jr[last].y;
+    const int ntiles = (hi - lo + kTile - 1) / kTile;
+    const int per = (ntiles + nsplit - 1) / nsplit;
+    jb = lo + (int)blockIdx.y * per * kTile;
+    je = min(hi, jb + per * kTile);
+}
+
+// ------------------------------------------------------------------------------------
+// geometry in (caller order -> internal order) and the HB refresh metric
+// (gfnff_method.cpp:2228-2259)
+// ------------------------------------------------------------------------------------
+__global__ void k_positions(int n, const int* __restrict__ perm, const double* __restrict__ xyz, double scale,
+                            double4* pos, const double4* __restrict__ ref, double* msd)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double s = 0.0;
+    if (i < n) {
+        const int o = perm[i];
+        const double x = xyz[3 * o] * scale, y = xyz[3 * o + 1] * scale, z = xyz[3 * o + 2] * scale;
+        pos[i] = make_double4(x, y, z, 0.0);
+        const double4 r = ref[i];
+        s = (x - r.x) * (x - r.x) + (y - r.y) * (y - r.y) + (z - r.z) * (z - r.z);
+    }
+    block_add(s, msd);
+}
+
+// ------------------------------------------------------------------------------------
+// coordination numbers: erf counting over partners closer than 6 bohr
+// (cn_calculator.cpp:367-428); the log-squash is applied in k_d4_weights
+// ------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(kTile) k_cn(View V, int nsplit)
+{
+    __shared__ double sx[kTile], sy[kTile], sz[kTile], sr[kTile];
+    const int i0 = blockIdx.x * kTile, i = i0 + threadIdx.x;
+    int jb, je;
+    tile_range(V, i0, nsplit, jb, je);
+    const bool act = i < V.n;
+    const double4 pi = act ? V.pos[i] : make_double4(0.0, 0.0, 0.0, 0.0);
+    const double ri = act ? V.rcov_cn[i] : 0.0;
+    const int2 rg = act ? V.jr[i] : make_int2(0, 0);
+    const double kn = -7.5;
+    double s = 0.0;
+    for (int t0 = jb; t0 < je; t0 += kTile) {
+        __syncthreads();
+        const int jl = t0 + threadIdx.x;
+        if (jl < je) {
+            const double4 p = V.pos[jl];
+            sx[threadIdx.x] = p.x; sy[threadIdx.x] = p.y; sz[threadIdx.x] = p.z;
+            sr[threadIdx.x] = V.rcov_cn[jl];
+        }
+        __syncthreads();
+        const int cnt = min(kTile, je - t0);
+        if (act) {
+            for (int jj = 0; jj < cnt; ++jj) {
+                const double dx = pi.x - sx[jj], dy = pi.y - sy[jj], dz = pi.z - sz[jj];
+                const double d2 = dx * dx + dy * dy + dz * dz;
+                const int j = t0 + jj;
+                if (!(d2 < 36.0) || j == i || j < rg.x || j >= rg.y) continue;
+                const double r = sqrt(d2);
+                const double rc = ri + sr[jj];
+                s += 0.5 * (1.0 + erf(kn * ((r - rc) / rc)));
+            }
+        }
+    }
+    if (act && s != 0.0) atomicAdd(V.cnraw + i, s);
+}
+
+// ------------------------------------------------------------------------------------
+// CN log-squash (cnmax = 4.4) and its derivative, D4 Gaussian weights (wf = 4) and the
+// half contraction with the reference C6 (d4param_generator.cpp:1079-1290, :1692-1740)
+// ------------------------------------------------------------------------------------
+__global__ void k_d4_weights(View V)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= V.n) return;
+    {
+        const double cnmax = 4.4, s = V.cnraw[i];
+        V.cn[i] = log(1.0 + exp(cnmax)) - log(1.0 + exp(cnmax - s));
+        V.dlog[i] = exp(cnmax) / (exp(cnmax) + exp(s));
+    }
+    const int nr = V.nref[i];
+    const double cn = V.cn[i];
+    double ex[7], dex[7], w[7], dw[7];
+    double norm = 0.0, dnorm = 0.0;
+    for (int r = 0; r < 7; ++r) {
+        ex[r] = dex[r] = w[r] = dw[r] = 0.0;
+        if (r < nr) {
+            const double d = cn - V.refcn[i * 7 + r];
+            ex[r] = exp(-4.0 * d * d);
+            dex[r] = (-2.0 * 4.0) * d * ex[r];
+            norm += ex[r];
+            dnorm += dex[r];
+        }
+    }
+    if (nr > 0) {
+        if (norm > 1e-10) {
+            const double inv = 1.0 / norm, inv2 = 1.0 / (norm * norm);
+            for (int r = 0; r < nr; ++r) {
+                w[r] = ex[r] * inv;
+                dw[r] = (dex[r] * norm - ex[r] * dnorm) * inv2;
+            }
+        } else {
+            w[0] = 1.0;
+        }
+    }
+    for (int r = 0; r < 7; ++r) { V.w[i * 7 + r] = w[r]; V.dw[i * 7 + r] = dw[r]; }
+    const int si = V.slot[i];
+    for (int s = 0; s < V.K; ++s) {
+        const double* C = V.c6ref + ((size_t)(si * V.K + s)) * 49;
+        for (int b = 0; b < 7; ++b) {
+            double g = 0.0, dg = 0.0;
+            for (int a = 0; a < nr; ++a) {
+                g += w[a] * C[a * 7 + b];
+                dg += dw[a] * C[a * 7 + b];
+            }
+            V.hg[((size_t)i * V.K + s) * 7 + b] = g;
+            V.hdg[((size_t)i * V.K + s) * 7 + b] = dg;
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// repulsion over per-atom CSR lists holding both pair directions
+// (ff_workspace_gfnff.cpp:774-848); kind 0 = bonded, 1 = non-bonded.  One warp per atom.
+// ------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(kBlock) k_repulsion(View V, const int* off, const int* nbj, const double* alpha,
+                                                     const double* repab, const unsigned char* kind)
+{
+    const int i = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    double eb = 0.0, enb = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
+    if (i < V.n) {
+        const double4 pi = V.pos[i];
+        for (int p = off[i] + lane; p < off[i + 1]; p += 32) {
+            const double4 pj = V.pos[nbj[p]];
+            const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+            const double r = sqrt(dx * dx + dy * dy + dz * dz);
+            if (r > 20.0 || r < 1e-8) continue;
+            const double sr = sqrt(r);
+            const double e = repab[p] * exp(-alpha[p] * (r * sr)) / r;
+            if (kind[p]) enb += 0.5 * e; else eb += 0.5 * e;
+            const double dEdr = -e / r - 1.5 * alpha[p] * sr * e;
+            const double f = dEdr / r;
+            gx += f * dx; gy += f * dy; gz += f * dz;
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            gx += __shfl_down_sync(0xffffffffu, gx, o);
+            gy += __shfl_down_sync(0xffffffffu, gy, o);
+            gz += __shfl_down_sync(0xffffffffu, gz, o);
+        }
+        if (lane == 0) {
+            V.grad[3 * i] += gx;
+            V.grad[3 * i + 1] += gy;
+            V.grad[3 * i + 2] += gz;
+        }
+    }
+    const int m = i < V.n ? V.mol[i] : -1;
+    eadd(V, eb, m, T_BREP);
+    eadd(V, enb, m, T_NBREP);
+}
+
+// ------------------------------------------------------------------------------------
+// all-pairs Coulomb (r <= 100 bohr; ff_workspace_gfnff.cpp:850-900) and D4 dispersion
+// over the setup pair list (setup distance <= 60 bohr, evaluated for r <= 50;
+// :715-772, d4param_generator.cpp:1959-2092) with the frozen setup C6 and the per-step
+// dC6/dCN chain term.  Both directions of a pair are evaluated (row i collects its own
+// gradient and dE/dCN_i); energies are halved.
+//
+// Coulomb fast path: erf(x) rounds to exactly 1 in double for x >= 6 (erfc(6) = 2.2e-17
+// is below half an ulp of 1), i.e. for r^2 >= 36 (a_i + a_j); the pair is then q q / r and
+// its exp(-x^2) gradient term is below 2e-15 relative, so both are dropped there.
+// ------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(kTile) k_pairs(View V, int nsplit)
+{
+    __shared__ double sx[kTile], sy[kTile], sz[kTile], s0x[kTile], s0y[kTile], s0z[kTile];
+    __shared__ double sq[kTile], sa[kTile], sze[kTile], ssz[kTile];
+    __shared__ double sw0[7][kTile], sw[7][kTile];
+    __shared__ int ssl[kTile], snr[kTile];
+    const int i0 = blockIdx.x * kTile, i = i0 + threadIdx.x;
+    int jb, je;
+    tile_range(V, i0, nsplit, jb, je);
+    const bool act = i < V.n;
+    const int ic = act ? i : i0;
+    const double4 pi = V.pos[ic], p0i = V.pos0[ic];
+    const double ai = V.alpeeq[ic], qi = V.q[ic], zi = V.zeta[ic], szi = V.szr[ic];
+    const int2 rg = act ? V.jr[i] : make_int2(0, 0);
+    const double* g0i = V.g0 + (size_t)ic * V.K * 7;
+    const double* dgi = V.hdg + (size_t)ic * V.K * 7;
+    const double a1 = 0.58, a2 = 4.80, tsp = 2.0 / 1.772453850905516;
+    double ec = 0.0, ed = 0.0, gx = 0.0, gy = 0.0, gz = 0.0, dcn = 0.0;
+    for (int t0 = jb; t0 < je; t0 += kTile) {
+        __syncthreads();
+        const int jl = t0 + threadIdx.x;
+        if (jl < je) {
+            const int u = threadIdx.x;
+            const double4 p = V.pos[jl], p0 = V.pos0[jl];
+            sx[u] = p.x; sy[u] = p.y; sz[u] = p.z;
+            s0x[u] = p0.x; s0y[u] = p0.y; s0z[u] = p0.z;
+            sq[u] = V.q[jl]; sa[u] = V.alpeeq[jl]; sze[u] = V.zeta[jl]; ssz[u] = V.szr[jl];
+            ssl[u] = V.slot[jl]; snr[u] = V.nref[jl];
+#pragma unroll
+            for (int b = 0; b < 7; ++b) {
+                sw0[b][u] = V.w0[(size_t)jl * 7 + b];
+                sw[b][u] = V.w[(size_t)jl * 7 + b];
+            }
+        }
+        __syncthreads();
+        const int cnt = min(kTile, je - t0);
+        if (!act) continue;
+        for (int jj = 0; jj < cnt; ++jj) {
+            const int j = t0 + jj;
+            if (j == i || j < rg.x || j >= rg.y) continue;
+            const double dx = pi.x - sx[jj], dy = pi.y - sy[jj], dz = pi.z - sz[jj];
+            const double d2 = dx * dx + dy * dy + dz * dz;
+            if (d2 < 1e-20) continue;
+            double f = 0.0;   // dE/dr / r
+            if (d2 <= 10000.0) {
+                const double s = ai + sa[jj];
+                const double qq = qi * sq[jj];
+                if (d2 >= 36.0 * s) {
+                    const double ir = rsqrt(d2);
+                    const double e = qq * ir;
+                    ec += e;
+                    f -= e * ir * ir;
+                } else {
+                    const double r = sqrt(d2);
+                    const double g = 1.0 / sqrt(s);
+                    const double gr = g * r;
+                    const double ef = erf(gr);
+                    ec += qq * ef / r;
+                    f += qq * ((g * exp(-gr * gr) * tsp) / r - ef / d2) / r;
+                }
+            }
+            if (d2 <= 2500.0 &&
+                d2_exact(p0i, make_double4(s0x[jj], s0y[jj], s0z[jj], 0.0)) <= 3600.0) {
+                const int sj = ssl[jj], nr = snr[jj];
+                const double* g0 = g0i + sj * 7;
+                const double* dg = dgi + sj * 7;
+                double c6 = 0.0, dc6 = 0.0;
+                for (int b = 0; b < nr; ++b) {
+                    c6 += __ldg(g0 + b) * sw0[b][jj];
+                    dc6 += dg[b] * sw[b][jj];
+                }
+                const double r4r2 = 3.0 * szi * ssz[jj];
+                const double t = a1 * sqrt(r4r2) + a2;
+                const double r0sq = t * t;
+                const double zz = zi * sze[jj];
+                const double r6 = d2 * d2 * d2, r06 = r0sq * r0sq * r0sq;
+                const double t6 = 1.0 / (r6 + r06);
+                const double t8 = 1.0 / (r6 * d2 + r06 * r0sq);
+                const double sum = t6 + 2.0 * r4r2 * t8;
+                ed -= c6 * sum * zz;
+                const double d6 = -6.0 * d2 * d2 * t6 * t6, d8 = -8.0 * r6 * t8 * t8;
+                f -= c6 * zz * (d6 + 2.0 * r4r2 * d8);
+                dcn -= dc6 * sum * zz;
+            }
+            gx += f * dx; gy += f * dy; gz += f * dz;
+        }
+    }
+    if (act) {
+        if (gx != 0.0) atomicAdd(V.grad + 3 * i, gx);
+        if (gy != 0.0) atomicAdd(V.grad + 3 * i + 1, gy);
+        if (gz != 0.0) atomicAdd(V.grad + 3 * i + 2, gz);
+        if (dcn != 0.0) atomicAdd(V.dEdcn + i, dcn);
+    }
+    const int m = act ? V.mol[i] : -1;
+    eadd(V, 0.5 * ec, m, T_COUL);
+    eadd(V, 0.5 * ed, m, T_DISP);
+}
+
+// ------------------------------------------------------------------------------------
+// Coulomb self terms and the CN-chain weight u = dlogCN (dE/dCN - q cnf/(2 sqrt CN))
+// (ff_workspace.cpp:415-536)
+// ------------------------------------------------------------------------------------
+__global__ void k_post(View V)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double e = 0.0;
+    if (i < V.n) {
+        const double q = V.q[i], cn = fmax(V.cn[i], 0.0);
+        const int2 rg = V.jr[i];
+        if (rg.y - rg.x >= 2 && V.alpeeq[i] > 0.0) {
+            const double chi = V.chi_base[i] + V.cnf[i] * sqrt(cn);
+            e = -q * chi + 0.5 * q * q * V.adiag[i];
+        }
+        V.v[i] = V.dlog[i] * (V.dEdcn[i] - q * V.cnf[i] / (2.0 * sqrt(cn) + 1e-16));
+    }
+    eadd(V, e, i < V.n ? V.mol[i] : -1, T_COUL);
+}
+
+// CN chain rule: grad_i += sum_j dS_ij/dr (u_i + u_j) (x_i - x_j)/r over the 6 bohr
+// neighbours (gfnff_method.cpp:5837-6260, forcefieldthread.h:80-109)
+__global__ void __launch_bounds__(kTile) k_cn_chain(View V, int nsplit)
+{
+    __shared__ double sx[kTile], sy[kTile], sz[kTile], sr[kTile], su[kTile];
+    const int i0 = blockIdx.x * kTile, i = i0 + threadIdx.x;
+    int jb, je;
+    tile_range(V, i0, nsplit, jb, je);
+    const bool act = i < V.n;
+    const double4 pi = act ? V.pos[i] : make_double4(0.0, 0.0, 0.0, 0.0);
+    const double ri = act ? V.rcov_cn[i] : 0.0;
+    const double ui = act ? V.v[i] : 0.0;
+    const int2 rg = act ? V.jr[i] : make_int2(0, 0);
+    const double kn = -7.5, sqrtpi = 1.77245385091;
+    double gx = 0.0, gy = 0.0, gz = 0.0;
+    for (int t0 = jb; t0 < je; t0 += kTile) {
+        __syncthreads();
+        const int jl = t0 + threadIdx.x;
+        if (jl < je) {
+            const double4 p = V.pos[jl];
+            sx[threadIdx.x] = p.x; sy[threadIdx.x] = p.y; sz[threadIdx.x] = p.z;
+            sr[threadIdx.x] = V.rcov_cn[jl];
+            su[threadIdx.x] = V.v[jl];
+        }
+        __syncthreads();
+        const int cnt = min(kTile, je - t0);
+        if (!act) continue;
+        for (int jj = 0; jj < cnt; ++jj) {
+            const double dx = sx[jj] - pi.x, dy = sy[jj] - pi.y, dz = sz[jj] - pi.z;
+            const double d2 = dx * dx + dy * dy + dz * dz;
+            const int j = t0 + jj;
+            if (!(d2 < 36.0) || j == i || j < rg.x || j >= rg.y) continue;
+            const double r = sqrt(d2);
+            const double rs = ri + sr[jj];
+            const double dr = (r - rs) / rs;
+            const double de = (kn / sqrtpi) * exp(-kn * kn * dr * dr) / rs;
+            const double f = -(de / r) * (ui + su[jj]);
+            gx += f * dx; gy += f * dy; gz += f * dz;
+        }
+    }
+    if (act) {
+        if (gx != 0.0) atomicAdd(V.grad + 3 * i, gx);
+        if (gy != 0.0) atomicAdd(V.grad + 3 * i + 1, gy);
+        if (gz != 0.0) atomicAdd(V.grad + 3 * i + 2, gz);
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// outputs in the caller's atom order, finiteness flags per molecule
+// ------------------------------------------------------------------------------------
+__global__ void k_outputs(View V, double* gout, double* qout, double* cnout, int* bad)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= V.n) return;
+    const int o = V.perm[i];
+    const double gx = V.grad[3 * i], gy = V.grad[3 * i + 1], gz = V.grad[3 * i + 2];
+    gout[3 * o] = gx;
+    gout[3 * o + 1] = gy;
+    gout[3 * o + 2] = gz;
+    qout[o] = V.q[i];
+    cnout[o] = V.cn[i];
+    if (!isfinite(gx) || !isfinite(gy) || !isfinite(gz)) atomicOr(bad + V.mol[i], 1);
+}
+
+// per molecule: total energy, status (NOT_SPD from the EEQ factorisation, NONFINITE)
+__global__ void k_finish(View V, const int* eeq_info, const int* bad, const double* e0, double* out_e)
+{
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= V.nmol) return;
+    double tot = e0[m];
+    for (int t = 0; t < T_TOTAL; ++t) tot += V.E[16 * m + t];
+    V.E[16 * m + T_TOTAL] = tot;
+    if (out_e) out_e[m] = tot;
+    int st = 0;
+    if (eeq_info && eeq_info[m] != 0) st = GFNFF_NOT_SPD;
+    else if (!isfinite(tot) || bad[m]) st = GFNFF_NONFINITE;
+    V.status[m] = st;
+}
+
+// device enumeration of the D4 pair list at the setup geometry (topology check)
+__global__ void k_disp_count(int n, const double4* pos0, const int2* jr, unsigned long long* cnt, int2* out,
+                             unsigned long long cap)
+{
+    const int i = blockIdx.y;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j <= i || j >= n || j >= jr[i].y) return;
+    if (d2_exact(pos0[i], pos0[j]) <= 3600.0) {
+        const unsigned long long s = atomicAdd(cnt, 1ull);
+        if (out && s < cap) out[s] = make_int2(i, j);
+    }
+}
+
+}  // namespace
