@@ -80,7 +80,7 @@ class Clocks:
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.p = subprocess.Popen(["nvidia-smi", f"--id={device}", f"--query-gpu={q}",
-                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                       "--format=csv,noheader,nounits", "-lms", "50"],
                                       stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.p = None
@@ -239,6 +239,7 @@ def run_ours(args):
         if rc != 0:
             raise SystemExit(lib.gfnff_last_error(h).decode())
 
+    clocks = Clocks(local)
     lib.gfnff_set_phase_timing(h, 1)
     for k in range(warm):
         step(k)
@@ -246,7 +247,6 @@ def run_ours(args):
     events = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
     phases = np.zeros(len(_lib.PHASES))
     buf = (ctypes.c_double * len(_lib.PHASES))()
-    clocks = Clocks(local)
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
@@ -262,7 +262,6 @@ def run_ours(args):
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    clk = clocks.stop()
     step_ms = [a.elapsed_time(b) for a, b in events]
     total_ms = float(sum(step_ms))
     status = int(d_st.item())
@@ -289,6 +288,7 @@ def run_ours(args):
         if gpu.hasError():
             raise SystemExit(gpu.getErrorMessage())
     e2e_s = time.perf_counter() - t
+    clk = clocks.stop()
     if world > 1:
         tt = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)

@@ -20,7 +20,7 @@ EXPORTED = ["gfnff_default_options", "gfnff_create", "gfnff_setup", "gfnff_energ
             "gfnff_energy_and_gradient_device", "gfnff_stream", "gfnff_charges",
             "gfnff_coordination_numbers", "gfnff_get_topology", "gfnff_sizes", "gfnff_last_error",
             "gfnff_destroy", "gfnff_set_phase_timing", "gfnff_phase_times", "gfnff_fma_peak_tflops",
-            "gfnff_eeq_charges_noalloc"]
+            "gfnff_eeq_charges_noalloc", "gfnff_eeq_solver", "gfnff_eeq_iterations"]
 PHASES = ["positions", "cn", "d4_weights", "eeq_matrix", "eeq_rhs", "eeq_solve", "bonded",
           "hbonds", "repulsion", "pairs", "post_chain", "finish"]
 
@@ -63,8 +63,12 @@ def load():
     lib.gfnff_fma_peak_tflops.argtypes = [c_i, c_i]
     lib.gfnff_fma_peak_tflops.restype = c_d
     lib.gfnff_eeq_charges_noalloc.argtypes = [c_i, c_i] + [c_v] * 11
+    lib.gfnff_eeq_solver.argtypes = [c_v]
+    lib.gfnff_eeq_solver.restype = ctypes.c_char_p
+    lib.gfnff_eeq_iterations.argtypes = [c_v]
     for name in EXPORTED:
-        if name not in ("gfnff_default_options", "gfnff_stream", "gfnff_last_error", "gfnff_fma_peak_tflops"):
+        if name not in ("gfnff_default_options", "gfnff_stream", "gfnff_last_error", "gfnff_fma_peak_tflops",
+                        "gfnff_eeq_solver"):
             getattr(lib, name).restype = c_i
     _lib = lib
     return lib

@@ -142,7 +142,11 @@ gfnff_status gfnff_energy_and_gradient(gfnff_handle* h, const double* xyz, doubl
             throw std::runtime_error("H2D copy failed");
         h->eng->enqueue(h->eng->d_xyz_scratch(), false);
         h->eng->fetch(h->pin_out, h->pin_grad, h->pin_status, nullptr);
-        if (*h->pin_status == GFNFF_NOT_SPD && h->eng->switch_to_lu()) {
+        // an indefinite reduced matrix moves to LU, a stalled iterative solve to the
+        // direct one; either way this geometry is evaluated again
+        const bool retry = (*h->pin_status == GFNFF_NOT_SPD && h->eng->switch_to_lu()) ||
+                           (*h->pin_status == GFNFF_REFINE_NOT_CONVERGED && h->eng->switch_to_direct());
+        if (retry) {
             h->eng->enqueue(h->eng->d_xyz_scratch(), false);
             h->eng->fetch(h->pin_out, h->pin_grad, h->pin_status, nullptr);
         }
@@ -155,8 +159,11 @@ gfnff_status gfnff_energy_and_gradient(gfnff_handle* h, const double* xyz, doubl
     if (grad) std::memcpy(grad, h->pin_grad, 3 * (size_t)n * sizeof(double));
     if (st != GFNFF_OK) {
         *energy = 0.0;   // curcuma's convention: an energy of 0.0 signals an error
-        return fail(h, (gfnff_status)st, st == GFNFF_NOT_SPD ? "EEQ matrix not positive definite"
-                                                            : "non-finite energy or gradient");
+        const char* why = st == GFNFF_NOT_SPD                ? "EEQ matrix not positive definite"
+                          : st == GFNFF_REFINE_NOT_CONVERGED ? "EEQ iterative solve did not converge"
+                          : st == GFNFF_CUDA_ERROR           ? "device wait gave up in the EEQ solve"
+                                                             : "non-finite energy or gradient";
+        return fail(h, (gfnff_status)st, why);
     }
     return GFNFF_OK;
 }
@@ -264,6 +271,23 @@ int gfnff_phase_times(gfnff_handle* h, double* ms, int cap)
         const int n = std::min<int>(cap, (int)v.size());
         for (int k = 0; k < n; ++k) ms[k] = v[k];
         return (int)v.size();
+    } catch (const std::exception& e) {
+        fail(h, GFNFF_CUDA_ERROR, e.what());
+        return -1;
+    }
+}
+
+const char* gfnff_eeq_solver(gfnff_handle* h)
+{
+    if (!h || !h->ready) return "";
+    return h->eng->solver_name();
+}
+
+int gfnff_eeq_iterations(gfnff_handle* h)
+{
+    if (!h || !h->ready) return -1;
+    try {
+        return h->eng->eeq_iterations();
     } catch (const std::exception& e) {
         fail(h, GFNFF_CUDA_ERROR, e.what());
         return -1;

@@ -25,6 +25,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
+#include <cstring>
 #include <map>
 #include <numeric>
 #include <stdexcept>
@@ -41,6 +43,8 @@ namespace gfnff {
 #include "k_bonded.cuh"
 #include "k_nonbonded.cuh"
 #include "k_eeq.cuh"
+#include "k_chol.cuh"
+#include "k_pcg.cuh"
 
 namespace {
 
@@ -80,6 +84,34 @@ std::vector<int> morton_order(const double* xyz, int n)
         code[i] = c;
     }
     std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return code[a] < code[b]; });
+    return ord;
+}
+
+// Atom order inside one molecule: fragments (bonded components) contiguous, ordered
+// along a Morton curve of their centroids, atoms of a fragment along a Morton curve of
+// their positions.  Spatial neighbours share warps in the pair kernels, and the EEQ
+// unknowns of a fragment form one contiguous range.
+std::vector<int> fragment_order(const Model& m)
+{
+    const int n = m.n, nf = std::max(1, m.nfrag);
+    std::vector<std::vector<int>> members(nf);
+    for (int i = 0; i < n; ++i) members[m.frag[i]].push_back(i);
+    std::vector<double> cen(3 * (size_t)nf, 0.0);
+    for (int f = 0; f < nf; ++f) {
+        for (int i : members[f])
+            for (int d = 0; d < 3; ++d) cen[3 * f + d] += m.xyz_setup[3 * i + d];
+        for (int d = 0; d < 3; ++d) cen[3 * f + d] /= std::max<size_t>(1, members[f].size());
+    }
+    const std::vector<int> ford = morton_order(cen.data(), nf);
+    std::vector<int> ord;
+    ord.reserve(n);
+    for (int f : ford) {
+        const auto& mem = members[f];
+        std::vector<double> x(3 * mem.size());
+        for (size_t k = 0; k < mem.size(); ++k)
+            for (int d = 0; d < 3; ++d) x[3 * k + d] = m.xyz_setup[3 * mem[k] + d];
+        for (int k : morton_order(x.data(), (int)mem.size())) ord.push_back(mem[k]);
+    }
     return ord;
 }
 
@@ -145,7 +177,49 @@ struct Engine::Impl {
     DBuf<double> work;
     DBuf<int> info, info2, status, ipiv, bad;
     int lwork = 0;
+    int lda = 1;           // leading dimension of M (nred + 1: row nred holds b for k_chol)
     bool use_lu = false;   // reduced EEQ matrix not positive definite: pivoted LU instead
+    // EEQ solver of a single-molecule engine (chosen at upload, see upload_batch)
+    enum { SOLVE_LIBRARY = 0, SOLVE_TILED = 1, SOLVE_PCG = 2 };
+    int solver = SOLVE_LIBRARY;
+    // persistent tiled Cholesky (k_chol)
+    DBuf<int4> ctasks;
+    DBuf<int> cflags;      // next, err, cnt[nt*nt], fin[nt*nt], ydone[nt]
+    DBuf<double> rdiag, ysol;
+    int chol_nt = 0, chol_ntasks = 0, chol_grid = 0;
+    size_t chol_smem = 0;
+    void chol_launch()
+    {
+        CK(cudaMemsetAsync(cflags.p, 0, cflags.n * sizeof(int), stream));
+        CholArgs A;
+        A.M = M.p; A.lda = lda; A.n = nred; A.nt = chol_nt; A.tasks = ctasks.p; A.ntasks = chol_ntasks;
+        A.next = cflags.p; A.err = cflags.p + 1; A.cnt = cflags.p + 2; A.fin = A.cnt + chol_nt * chol_nt;
+        A.ydone = A.fin + chol_nt * chol_nt; A.rdiag = rdiag.p; A.y = ysol.p;
+        void* args[] = {&A};
+        CK(cudaLaunchCooperativeKernel((const void*)k_chol, dim3(chol_grid), dim3(kCholThreads), args, chol_smem, stream));
+        k_chol_info<<<1, 1, 0, stream>>>(cflags.p + 1, info.p);
+    }
+    // block-Jacobi PCG (k_pcg)
+    DBuf<int2> pblocks;
+    DBuf<long long> pboff;
+    DBuf<int4> ppart;
+    DBuf<int> prblk;
+    DBuf<double> pbinv, px, pr, pz, ppartial;
+    DBuf<unsigned int> pbar;
+    DBuf<int> piters;
+    int pcg_grid = 0, pcg_max_iter = 200;
+    size_t pcg_smem = 0;
+    bool pcg_ready = false;
+    void pcg_launch()
+    {
+        CK(cudaMemsetAsync(pbar.p, 0, sizeof(unsigned int), stream));
+        PCGArgs A;
+        A.M = M.p; A.lda = lda; A.n = nred; A.b = bvec.p; A.x = px.p; A.r = pr.p; A.z = pz.p;
+        A.blocks = pblocks.p; A.boff = pboff.p; A.binv = pbinv.p; A.part = ppart.p; A.rblk = prblk.p; A.partial = ppartial.p;
+        A.bar = pbar.p; A.info = info.p; A.iters = piters.p; A.max_iter = pcg_max_iter; A.tol = 1e-12;
+        void* args[] = {&A};
+        CK(cudaLaunchCooperativeKernel((const void*)k_pcg, dim3(pcg_grid), dim3(kPcgThreads), args, pcg_smem, stream));
+    }
     bool timing = false;
     cudaEvent_t ev[Engine::kNumPhases + 1] = {};
     void mark(int k)
@@ -296,7 +370,7 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
     std::vector<int2> hjr(n);
     for (int m = 0; m < nm; ++m) {
         const int a0 = P.h_aoff[m], na = mols[m]->n;
-        auto ord = morton_order(mols[m]->xyz_setup.data(), na);
+        auto ord = fragment_order(*mols[m]);
         for (int s = 0; s < na; ++s) {
             P.h_perm[a0 + s] = a0 + ord[s];
             P.h_iperm[a0 + ord[s]] = a0 + s;
@@ -574,18 +648,90 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
     P.hg.alloc((size_t)n * K * 7); P.hdg.alloc((size_t)n * K * 7);
     P.q.alloc(n); P.dEdcn.alloc(n); P.v.alloc(n); P.grad.alloc(3 * (size_t)n); P.E.alloc(16 * (size_t)nm);
     P.gout.alloc(3 * (size_t)n); P.qout.alloc(n); P.cnout.alloc(n);
-    P.M.alloc((size_t)std::max<long long>(1, nm == 1 ? (long long)P.nred * P.nred : P.msize));
+    P.lda = P.nred + 1;
+    P.M.alloc((size_t)std::max<long long>(1, nm == 1 ? (long long)P.lda * P.nred : P.msize));
     P.bvec.alloc(std::max(1, P.nred)); P.xyz_stage.alloc(3 * (size_t)n); P.msd.alloc(1);
     P.info.alloc(nm); P.info2.alloc(1); P.status.alloc(nm); P.bad.alloc(nm);
     CK(cudaMemset(P.info.p, 0, nm * sizeof(int)));
     P.use_lu = false;
     if (nm == 1 && P.nred > 0) {
         int l1 = 0, l2 = 0;
-        CS(cusolverDnDpotrf_bufferSize(P.sol, CUBLAS_FILL_MODE_LOWER, P.nred, P.M.p, P.nred, &l1));
-        CS(cusolverDnDgetrf_bufferSize(P.sol, P.nred, P.nred, P.M.p, P.nred, &l2));
+        CS(cusolverDnDpotrf_bufferSize(P.sol, CUBLAS_FILL_MODE_LOWER, P.nred, P.M.p, P.lda, &l1));
+        CS(cusolverDnDgetrf_bufferSize(P.sol, P.nred, P.nred, P.M.p, P.lda, &l2));
         P.lwork = std::max(l1, l2);
         P.work.alloc(std::max(1, P.lwork));
         P.ipiv.alloc(P.nred);
+        int nsm = 0;
+        CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, P.opt.device));
+        // persistent tiled Cholesky: task list, flags, co-resident grid
+        {
+            auto tasks = chol_tasks(P.nred);
+            P.chol_nt = (P.nred + 1 + CB - 1) / CB;
+            P.chol_ntasks = (int)tasks.size();
+            P.ctasks.upload(tasks);
+            P.cflags.alloc(2 + 2 * (size_t)P.chol_nt * P.chol_nt + P.chol_nt);
+            P.rdiag.alloc(P.nred);
+            P.ysol.alloc(P.nred);
+            P.chol_smem = (2 * CB * CLD + CB) * sizeof(double);
+            CK(cudaFuncSetAttribute((const void*)k_chol, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P.chol_smem));
+            int per_sm = 0;
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)k_chol, kCholThreads, P.chol_smem));
+            P.chol_grid = std::max(1, std::min(per_sm * nsm, P.chol_ntasks));
+        }
+        // block-Jacobi PCG: each fragment's contiguous reduced range in blocks of <= 64
+        P.pcg_ready = false;
+        std::vector<int2> blocks;
+        {
+            std::vector<int> fr(n);
+            const Model& M0 = *mols[0];
+            for (int a = 0; a < n; ++a) fr[P.ix(0, a)] = M0.frag[a];
+            int r = 0, i = 0;
+            while (i < n) {
+                int j = i;
+                while (j < n && fr[j] == fr[i]) ++j;
+                const int nr = j - i - 1;   // the fragment's anchor is its first atom
+                for (int c = 0; c < nr; c += kPcgMaxBlock)
+                    blocks.push_back(make_int2(r + c, std::min(kPcgMaxBlock, nr - c)));
+                r += nr;
+                i = j;
+            }
+            if (r != P.nred) blocks.clear();   // fragments not contiguous: no PCG
+        }
+        if (!blocks.empty()) {
+            // rows per grid block: whole preconditioner blocks, about nred / nsm rows each
+            std::vector<int4> part;
+            std::vector<long long> boff;
+            long long bo = 0;
+            for (auto& b : blocks) { boff.push_back(bo); bo += (long long)b.y * b.y; }
+            const int G = std::max(1, std::min(nsm, (int)blocks.size()));
+            size_t bk = 0;
+            int maxrows = 1;
+            for (int g = 0; g < G; ++g) {
+                const int target = (int)(((long long)P.nred * (g + 1)) / G);
+                const int b0 = (int)bk, r0 = bk < blocks.size() ? blocks[bk].x : P.nred;
+                while (bk < blocks.size() && (blocks[bk].x + blocks[bk].y <= target || g == G - 1)) ++bk;
+                const int r1 = bk < blocks.size() ? blocks[bk].x : P.nred;
+                part.push_back(make_int4(r0, r1, b0, (int)bk));
+                maxrows = std::max(maxrows, r1 - r0);
+            }
+            const size_t smem = ((size_t)P.nred + kPcgMaxBlock * (kPcgMaxBlock + 1) + maxrows) * sizeof(double);
+            if (smem <= 220 * 1024) {
+                std::vector<int> rblk(P.nred);
+                for (size_t q = 0; q < blocks.size(); ++q)
+                    for (int r = 0; r < blocks[q].y; ++r) rblk[blocks[q].x + r] = (int)q;
+                P.pblocks.upload(blocks); P.pboff.upload(boff); P.ppart.upload(part); P.prblk.upload(rblk);
+                P.pbinv.alloc((size_t)bo); P.px.alloc(P.nred); P.pr.alloc(P.nred); P.pz.alloc(P.nred);
+                P.ppartial.alloc(4 * (size_t)G); P.pbar.alloc(2); P.piters.alloc(1);
+                CK(cudaMemset(P.pbar.p, 0, 2 * sizeof(unsigned int)));
+                CK(cudaMemset(P.piters.p, 0, sizeof(int)));
+                P.pcg_grid = G;
+                P.pcg_smem = smem;
+                CK(cudaFuncSetAttribute((const void*)k_pcg, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                int per_sm = 0;
+                CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)k_pcg, kPcgThreads, smem));
+                P.pcg_ready = per_sm >= 1;
+            }
+        }
     }
     CK(cudaDeviceSynchronize());
     // The reduced EEQ matrix is indefinite for some systems (hydrogen has a negative
@@ -597,10 +743,56 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
         DBuf<double> x;
         std::vector<double> h(mols[0]->xyz_setup);
         x.upload(h);
+        P.solver = Impl::SOLVE_LIBRARY;
         enqueue(x.p, true);
         int st = 0;
         fetch(nullptr, nullptr, &st, nullptr);
         if (st == GFNFF_NOT_SPD) P.use_lu = true;
+        // Solver: GFNFF_EEQ_SOLVER=library|tiled|pcg forces one; otherwise the fastest of
+        // the available ones over three evaluations at the setup geometry
+        if (!P.use_lu) {
+            const char* env = std::getenv("GFNFF_EEQ_SOLVER");
+            std::vector<int> cand;
+            if (env && !std::strcmp(env, "library")) cand = {Impl::SOLVE_LIBRARY};
+            else if (env && !std::strcmp(env, "tiled")) cand = {Impl::SOLVE_TILED};
+            else if (env && !std::strcmp(env, "pcg") && P.pcg_ready) cand = {Impl::SOLVE_PCG};
+            else {
+                cand = {Impl::SOLVE_LIBRARY, Impl::SOLVE_TILED};
+                if (P.pcg_ready) cand.push_back(Impl::SOLVE_PCG);
+            }
+            if (cand.size() == 1) {
+                P.solver = cand[0];
+            } else {
+                cudaEvent_t e0, e1;
+                CK(cudaEventCreate(&e0));
+                CK(cudaEventCreate(&e1));
+                float best = 1e30f;
+                int pick = Impl::SOLVE_LIBRARY;
+                for (int c : cand) {
+                    P.solver = c;
+                    if (c == Impl::SOLVE_PCG) P.pcg_max_iter = 200;
+                    enqueue(x.p, true);
+                    fetch(nullptr, nullptr, &st, nullptr);
+                    if (st != GFNFF_OK) continue;
+                    if (c == Impl::SOLVE_PCG) {
+                        int it = 0;
+                        CK(cudaMemcpy(&it, P.piters.p, sizeof(int), cudaMemcpyDeviceToHost));
+                        P.pcg_max_iter = std::min(500, 4 * it + 20);
+                    }
+                    CK(cudaEventRecord(e0, P.stream));
+                    for (int rep = 0; rep < 3; ++rep) enqueue(x.p, true);
+                    CK(cudaEventRecord(e1, P.stream));
+                    CK(cudaEventSynchronize(e1));
+                    float ms = 0.f;
+                    CK(cudaEventElapsedTime(&ms, e0, e1));
+                    fetch(nullptr, nullptr, &st, nullptr);
+                    if (st == GFNFF_OK && ms < best) { best = ms; pick = c; }
+                }
+                cudaEventDestroy(e0);
+                cudaEventDestroy(e1);
+                P.solver = pick;
+            }
+        }
     }
 }
 
@@ -609,6 +801,29 @@ bool Engine::switch_to_lu()
     if (p_->use_lu || p_->nred == 0 || p_->nmol != 1) return false;
     p_->use_lu = true;
     return true;
+}
+
+bool Engine::switch_to_direct()
+{
+    if (p_->nmol != 1 || p_->solver != Impl::SOLVE_PCG) return false;
+    p_->solver = Impl::SOLVE_LIBRARY;
+    return true;
+}
+
+const char* Engine::solver_name() const
+{
+    if (p_->nmol != 1) return "batched";
+    if (p_->use_lu) return "lu";
+    return p_->solver == Impl::SOLVE_PCG ? "pcg" : (p_->solver == Impl::SOLVE_TILED ? "tiled" : "library");
+}
+
+int Engine::eeq_iterations()
+{
+    if (p_->nmol != 1 || p_->use_lu || p_->solver != Impl::SOLVE_PCG) return 0;
+    int it = 0;
+    CK(cudaStreamSynchronize(p_->stream));
+    CK(cudaMemcpy(&it, p_->piters.p, sizeof(int), cudaMemcpyDeviceToHost));
+    return it;
 }
 
 void Engine::enqueue(const double* d_xyz, bool bohr)
@@ -634,20 +849,29 @@ void Engine::enqueue(const double* d_xyz, bool bohr)
     // EEQ
     P.mark(3);
     if (P.nmol == 1) {
+        const int sv = P.use_lu ? -1 : P.solver;
+        const bool full = sv == -1 || sv == Impl::SOLVE_PCG;
+        const bool aug = sv == Impl::SOLVE_TILED;
         if (P.nred > 0) {
-            dim3 g(nblk(P.nred), std::min(P.nred, 65535));
-            k_eeq_M<<<g, kBlock, 0, s>>>(V, P.red2atom.p, P.anchor.p, P.M.p, P.use_lu ? 1 : 0);
+            dim3 g(nblk(P.nred), std::min(P.nred, 128));
+            k_eeq_M<<<g, kBlock, 0, s>>>(V, P.red2atom.p, P.anchor.p, P.M.p, P.lda, full ? 1 : 0);
         }
         P.mark(4);
-        if (P.nred > 0) k_eeq_rhs<<<nblk(P.nred), kBlock, 0, s>>>(V, P.red2atom.p, P.anchor.p, P.qlist.p, P.nq, P.q0.p, P.bvec.p);
+        if (P.nred > 0)
+            k_eeq_rhs<<<nblk(P.nred), kBlock, 0, s>>>(V, P.red2atom.p, P.anchor.p, P.qlist.p, P.nq, P.q0.p, P.bvec.p,
+                                                      aug ? P.M.p + P.nred : nullptr, P.lda);
         P.mark(5);
         if (P.nred > 0) {
-            if (!P.use_lu) {
-                CS(cusolverDnDpotrf(P.sol, CUBLAS_FILL_MODE_LOWER, P.nred, P.M.p, P.nred, P.work.p, P.lwork, P.info.p));
-                CS(cusolverDnDpotrs(P.sol, CUBLAS_FILL_MODE_LOWER, P.nred, 1, P.M.p, P.nred, P.bvec.p, P.nred, P.info2.p));
+            if (sv == Impl::SOLVE_TILED) {
+                P.chol_launch();
+            } else if (sv == Impl::SOLVE_PCG) {
+                P.pcg_launch();
+            } else if (sv == Impl::SOLVE_LIBRARY) {
+                CS(cusolverDnDpotrf(P.sol, CUBLAS_FILL_MODE_LOWER, P.nred, P.M.p, P.lda, P.work.p, P.lwork, P.info.p));
+                CS(cusolverDnDpotrs(P.sol, CUBLAS_FILL_MODE_LOWER, P.nred, 1, P.M.p, P.lda, P.bvec.p, P.nred, P.info2.p));
             } else {
-                CS(cusolverDnDgetrf(P.sol, P.nred, P.nred, P.M.p, P.nred, P.work.p, P.ipiv.p, P.info.p));
-                CS(cusolverDnDgetrs(P.sol, CUBLAS_OP_N, P.nred, 1, P.M.p, P.nred, P.ipiv.p, P.bvec.p, P.nred, P.info2.p));
+                CS(cusolverDnDgetrf(P.sol, P.nred, P.nred, P.M.p, P.lda, P.work.p, P.ipiv.p, P.info.p));
+                CS(cusolverDnDgetrs(P.sol, CUBLAS_OP_N, P.nred, 1, P.M.p, P.lda, P.ipiv.p, P.bvec.p, P.nred, P.info2.p));
             }
         }
     } else {
@@ -656,12 +880,15 @@ void Engine::enqueue(const double* d_xyz, bool bohr)
         EEQBatch B{P.roff.p, P.moff.p, P.red2atom.p, P.anchor.p, P.qlist.p, P.nq, P.q0.p, P.M.p, P.bvec.p, P.info.p};
         k_eeq_batch<<<P.nmol, 256, 0, s>>>(V, B);
     }
-    k_eeq_expand<<<nblk(n), kBlock, 0, s>>>(V, P.q0.p, P.atom2red.p, P.frag_off.p, P.frag_atoms.p, P.bvec.p);
+    const double* ysol = P.bvec.p;
+    if (P.nmol == 1 && !P.use_lu && P.solver == Impl::SOLVE_TILED) ysol = P.ysol.p;
+    if (P.nmol == 1 && !P.use_lu && P.solver == Impl::SOLVE_PCG) ysol = P.px.p;
+    k_eeq_expand<<<nblk(n), kBlock, 0, s>>>(V, P.q0.p, P.atom2red.p, P.frag_off.p, P.frag_atoms.p, ysol);
     P.mark(6);
     if (P.nb) {
         BondSoA B{P.nb, P.b_i.p, P.b_j.p, P.b_h.p, P.b_off.p, P.b_hb.p, P.b_fc.p, P.b_al.p,
                   P.b_r0i.p, P.b_r0j.p, P.b_cki.p, P.b_ckj.p, P.b_sh.p, P.b_ff.p};
-        k_bonds<<<nblk(P.nb), kBlock, 0, s>>>(V, B);
+        k_bonds<<<nblk((long)P.nb * 32), kBlock, 0, s>>>(V, B);
     }
     if (P.na) k_angles<<<nblk(P.na), kBlock, 0, s>>>(V, AngleSoA{P.na, P.a_i.p, P.a_j.p, P.a_k.p, P.a_fc.p, P.a_th.p});
     if (P.nt) k_torsions<<<nblk(P.nt), kBlock, 0, s>>>(V, TorsSoA{P.nt, P.t_i.p, P.t_j.p, P.t_k.p, P.t_l.p, P.t_V.p, P.t_n.p, P.t_p.p}, 0);

@@ -59,6 +59,12 @@ public:
     void set_hb_reference(const double* xyz_bohr);
     // switches the EEQ solve to pivoted LU (after a NOT_SPD status); false if already
     bool switch_to_lu();
+    // switches an iterative EEQ solve to the direct one (after REFINE_NOT_CONVERGED)
+    bool switch_to_direct();
+    // EEQ solver in use: "library", "tiled", "pcg", "lu" or "batched"
+    const char* solver_name() const;
+    // iterations of the last iterative EEQ solve (0 for direct solvers)
+    int eeq_iterations();
     // per-phase CUDA-event timing of enqueue(); phase_ms returns the milliseconds of the
     // last evaluation per phase (order of kPhaseNames) after the stream has finished
     void set_timing(bool on);

@@ -1,8 +1,16 @@
-// Bonded GFN-FF terms: one thread per term, gradient scattered with FP64 atomics, term
-// energies summed per molecule.  Included by engine.cu (one translation unit).
+// Bonded GFN-FF terms: one thread per term (one warp per bond), gradient scattered with
+// FP64 atomics, term energies summed per molecule.  Included by engine.cu (one translation unit).
 #pragma once
 
 namespace {
+
+// x^6 (the HB/XB damping exponent is the integer 6)
+__device__ __forceinline__ double pow6(double x)
+{
+    const double x3 = x * x * x;
+    return x3 * x3;
+}
+
 // ------------------------------------------------------------------------------------
 // bonded terms
 // ------------------------------------------------------------------------------------
@@ -13,10 +21,13 @@ struct BondSoA {
 };
 
 // bonds with the HB-modulated exponent and the r0(CN) chain rule
-// (ff_workspace_gfnff.cpp:46-182)
-__global__ void k_bonds(View V, BondSoA B)
+// (ff_workspace_gfnff.cpp:46-182).  One warp per bond: the lanes share the loops over the
+// HB acceptors that modulate an X-H bond.
+__global__ void __launch_bounds__(kBlock) k_bonds(View V, BondSoA B)
 {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    const unsigned full = 0xffffffffu;
     double e = 0.0;
     if (t < B.n) {
         const int i = B.i[t], j = B.j[t];
@@ -29,10 +40,11 @@ __global__ void k_bonds(View V, BondSoA B)
         double alpha = B.alpha[t];
         const int H = B.hbh[t];
         const double kn = 27.5, isp = 0.5641895835477563;
+        D3 ph = mk(0.0, 0.0, 0.0);
         if (H >= 0) {
             double hcn = 0.0;
-            D3 ph = ld(V.pos, H);
-            for (int p = B.hb_off[t]; p < B.hb_off[t + 1]; ++p) {
+            ph = ld(V.pos, H);
+            for (int p = B.hb_off[t] + lane; p < B.hb_off[t + 1]; p += 32) {
                 const int b = B.hb_b[p];
                 D3 d = ld(V.pos, b) - ph;
                 const double r2 = d.x * d.x + d.y * d.y + d.z * d.z;
@@ -42,16 +54,23 @@ __global__ void k_bonds(View V, BondSoA B)
                 const double arg = -kn * (rr - rc) / rc;
                 hcn += 0.5 * (1.0 + erf(arg));
             }
+            for (int o = 16; o > 0; o >>= 1) hcn += __shfl_xor_sync(full, hcn, o);
             alpha = (-(1.0 - 0.9) * hcn + 1.0) * B.alpha[t];
         }
-        e = B.fc[t] * exp(-alpha * dr * dr);
-        const double dEdr = -2.0 * alpha * dr * e;
-        agrad(V.grad, i, dEdr * d0);
-        agrad(V.grad, j, (-dEdr) * d0);
+        const double eb = B.fc[t] * exp(-alpha * dr * dr);
+        const double dEdr = -2.0 * alpha * dr * eb;
+        if (lane == 0) {
+            e = eb;
+            agrad(V.grad, i, dEdr * d0);
+            agrad(V.grad, j, (-dEdr) * d0);
+            const double yy = -dEdr;
+            atomicAdd(V.dEdcn + i, yy * B.ff[t] * B.cki[t]);
+            atomicAdd(V.dEdcn + j, yy * B.ff[t] * B.ckj[t]);
+        }
         if (H >= 0) {
-            const double zz = 0.1 * B.alpha[t] * dr * dr * e;
-            D3 ph = ld(V.pos, H);
-            for (int p = B.hb_off[t]; p < B.hb_off[t + 1]; ++p) {
+            const double zz = 0.1 * B.alpha[t] * dr * dr * eb;
+            D3 gh = mk(0.0, 0.0, 0.0);
+            for (int p = B.hb_off[t] + lane; p < B.hb_off[t + 1]; p += 32) {
                 const int b = B.hb_b[p];
                 D3 d = ld(V.pos, b) - ph;
                 const double r2 = d.x * d.x + d.y * d.y + d.z * d.z;
@@ -60,13 +79,16 @@ __global__ void k_bonds(View V, BondSoA B)
                 const double rc = 1.78 * (4.0 / 3.0) * (V.rcov_d3[H] + V.rcov_d3[b]);
                 const double arg = -kn * (rr - rc) / rc;
                 const double dcn = isp * (-kn / rc) * exp(-arg * arg) / rr;
-                agrad(V.grad, H, (zz * -dcn) * d);
+                gh = gh + (zz * -dcn) * d;
                 agrad(V.grad, b, (zz * dcn) * d);
             }
+            for (int o = 16; o > 0; o >>= 1) {
+                gh.x += __shfl_xor_sync(full, gh.x, o);
+                gh.y += __shfl_xor_sync(full, gh.y, o);
+                gh.z += __shfl_xor_sync(full, gh.z, o);
+            }
+            if (lane == 0) agrad(V.grad, H, gh);
         }
-        const double yy = -dEdr;
-        atomicAdd(V.dEdcn + i, yy * B.ff[t] * B.cki[t]);
-        atomicAdd(V.dEdcn + j, yy * B.ff[t] * B.ckj[t]);
     }
     eadd(V, e, t < B.n ? V.mol[B.i[t]] : -1, T_BOND);
 }
@@ -327,8 +349,11 @@ __global__ void __launch_bounds__(kBlock) k_hbonds(View V, HBSoA S)
             const double bas = (QA * S.bas_a[t] * rAH4 + QB * S.bas_b[t] * rHB4) * den;
             const double aci = (S.aci_b[t] * rAH4 + S.aci_a[t] * rHB4) * den;
             const double rv = S.rv[t];
-            const double dsh = 1.0 / (1.0 + pow(HB_SCUT * rv / (rAB * rAB), HB_ALP));
-            const double dlg = 1.0 / (1.0 + pow(rAB * rAB / HB_LONGCUT, HB_ALP));
+            // HB_ALP = 6: integer powers
+            const double ratio1 = pow6(rAB * rAB / HB_LONGCUT);
+            const double ratio3 = pow6(HB_SCUT * rv / (rAB * rAB));
+            const double dsh = 1.0 / (1.0 + ratio3);
+            const double dlg = 1.0 / (1.0 + ratio1);
             const double denv = dsh * dlg;
             double doutl;
             {
@@ -409,8 +434,6 @@ __global__ void __launch_bounds__(kBlock) k_hbonds(View V, HBSoA S)
             D3 drab = pA - pB, drah = pA - pH, drbh = pB - pH;
             const double rab2 = rAB * rAB, rbh2 = rHB * rHB, rah2 = rAH * rAH;
             const double rahprbh = rAH + rHB + 1e-12;
-            const double ratio1 = pow(rab2 / HB_LONGCUT, HB_ALP);
-            const double ratio3 = pow(HB_SCUT * rv / rab2, HB_ALP);
             const double ddamp = (-2.0 * HB_ALP * ratio1 / (1.0 + ratio1)) + (2.0 * HB_ALP * ratio3 / (1.0 + ratio3));
             const double expo = (HB_BACUT / rv) * (rahprbh / rAB - 1.0);
             if (expo <= 15.0) {
@@ -479,7 +502,7 @@ __global__ void __launch_bounds__(kBlock) k_hbonds(View V, HBSoA S)
                         if (vn > 1e-10) {
                             const double lv[3] = {lpv.x, lpv.y, lpv.z}, gl3[3] = {glp.x, glp.y, glp.z};
                             double out[3] = {0, 0, 0};
-                            const double vn3 = pow(vn, 3.0);
+                            const double vn3 = vn * vn * vn;
                             for (int col = 0; col < 3; ++col)
                                 for (int row = 0; row < 3; ++row) {
                                     const double unit = (row == col) ? -1.0 : 0.0;
@@ -576,16 +599,16 @@ __global__ void k_xbonds(View V, XBSoA S)
         const double ex = XB_BACUT * ((rAX + rXB) / rAB - 1.0);
         if (rXB <= 20.0 && ex <= 15.0) {
             const double rv = S.rv[t];
-            const double dsh = 1.0 / (1.0 + pow(XB_SCUT * rv / (rXB * rXB), ALP));
-            const double dlg = 1.0 / (1.0 + pow(rXB * rXB / LC, ALP));
+            const double dsh = 1.0 / (1.0 + pow6(XB_SCUT * rv / (rXB * rXB)));
+            const double dlg = 1.0 / (1.0 + pow6(rXB * rXB / LC));
             const double dol = 2.0 / (1.0 + exp(ex));
             const double r3 = rXB * rXB * rXB;
             const double R = dsh * dlg * dol / r3;
             const double pre = S.pre[t];
             etot = R * pre;
-            const double st = pow(XB_SCUT * rv / (rXB * rXB), ALP);
+            const double st = pow6(XB_SCUT * rv / (rXB * rXB));
             const double dds = -2.0 * ALP * dsh * st / (rXB * (1.0 + st));
-            const double lt = pow((rXB * rXB) / LC, ALP);
+            const double lt = pow6((rXB * rXB) / LC);
             const double ddl = -2.0 * ALP * rXB * dlg * lt / (LC * (1.0 + lt));
             const double et = exp(ex), de = 1.0 + et;
             const double do_ax = -2.0 * et * XB_BACUT / (rAB * de * de);

@@ -25,9 +25,11 @@ __device__ __forceinline__ double eeq_a(const View& V, int a, int b)
     return erf(r / sqrt(s)) / r;
 }
 
-// reduced matrix, column-major: M[c*nred + r]; lower triangle only unless full
+// reduced matrix, column-major with leading dimension lda: M[c*lda + r]; lower triangle
+// only unless full.  Each thread keeps its row's atoms in registers and walks the
+// columns blockIdx.y, blockIdx.y + gridDim.y, ...
 __global__ void k_eeq_M(View V, const int* __restrict__ red2atom, const int* __restrict__ anchor, double* M,
-                        int full)
+                        int lda, int full)
 {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= V.nred) return;
@@ -35,7 +37,7 @@ __global__ void k_eeq_M(View V, const int* __restrict__ red2atom, const int* __r
     for (int c = blockIdx.y; c < V.nred; c += gridDim.y) {
         if (!full && r < c) continue;
         const int l = red2atom[c], al = anchor[l];
-        M[(size_t)c * V.nred + r] = eeq_a(V, k, l) - eeq_a(V, k, al) - eeq_a(V, ak, l) + eeq_a(V, ak, al);
+        M[(size_t)c * lda + r] = eeq_a(V, k, l) - eeq_a(V, k, al) - eeq_a(V, ak, l) + eeq_a(V, ak, al);
     }
 }
 
@@ -51,14 +53,25 @@ __device__ __forceinline__ double eeq_rhs_atom(const View& V, int i, const int* 
     return x;
 }
 
-// reduced right-hand side b = B^T (x - A q0)
+// reduced right-hand side b = B^T (x - A q0); also written with stride lda to aug (the
+// augmented row of the matrix) when aug is non-null
 __global__ void k_eeq_rhs(View V, const int* __restrict__ red2atom, const int* __restrict__ anchor,
-                          const int* __restrict__ qlist, int nq, const double* __restrict__ q0, double* b)
+                          const int* __restrict__ qlist, int nq, const double* __restrict__ q0, double* b,
+                          double* aug, int lda)
 {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= V.nred) return;
     const int k = red2atom[r];
-    b[r] = eeq_rhs_atom(V, k, qlist, nq, q0) - eeq_rhs_atom(V, anchor[k], qlist, nq, q0);
+    const double v = eeq_rhs_atom(V, k, qlist, nq, q0) - eeq_rhs_atom(V, anchor[k], qlist, nq, q0);
+    b[r] = v;
+    if (aug) aug[(size_t)r * lda] = v;
+}
+
+// status of the persistent Cholesky: info = 1 not positive definite, 2 a wait gave up
+__global__ void k_chol_info(const int* err, int* info)
+{
+    const int e = *err;
+    *info = (e & 2) ? 2 : ((e & 1) ? 1 : 0);
 }
 
 // q = q0 + B y

@@ -383,7 +383,9 @@ __global__ void k_finish(View V, const int* eeq_info, const int* bad, const doub
     V.E[16 * m + T_TOTAL] = tot;
     if (out_e) out_e[m] = tot;
     int st = 0;
-    if (eeq_info && eeq_info[m] != 0) st = GFNFF_NOT_SPD;
+    if (eeq_info && eeq_info[m] == 2) st = GFNFF_CUDA_ERROR;
+    else if (eeq_info && eeq_info[m] == 3) st = GFNFF_REFINE_NOT_CONVERGED;
+    else if (eeq_info && eeq_info[m] != 0) st = GFNFF_NOT_SPD;
     else if (!isfinite(tot) || bad[m]) st = GFNFF_NONFINITE;
     V.status[m] = st;
 }

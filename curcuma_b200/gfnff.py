@@ -107,6 +107,14 @@ class GFNFF:
                                                  out.size, ctypes.byref(cnt)))
         return out[:cnt.value * width].reshape(cnt.value, width) if width > 1 else out[:cnt.value]
 
+    def eeqSolver(self) -> str:
+        """EEQ solver chosen at setup ("library", "tiled", "pcg", "lu", "batched")."""
+        return self._lib.gfnff_eeq_solver(self._h).decode()
+
+    def eeqIterations(self) -> int:
+        """Iterations of the last iterative EEQ solve (0 for direct solvers)."""
+        return int(self._lib.gfnff_eeq_iterations(self._h))
+
     def sizes(self):
         n, f = ctypes.c_int(), ctypes.c_int()
         self._check(self._lib.gfnff_sizes(self._h, ctypes.byref(n), ctypes.byref(f)))

@@ -94,8 +94,8 @@ gfnff_status gfnff_sizes(gfnff_handle* h, int* natoms, int* nfrag);
 
 /* Per-phase CUDA-event timing of every evaluation (off by default; costs two event
  * records per phase).  gfnff_phase_times copies the milliseconds of the last
- * evaluation, in the order positions, cn, d4_weights, eeq_matrix, eeq_reduce,
- * eeq_factor_solve, bonded, hbonds, repulsion, pairs, post_chain, finish, and returns
+ * evaluation, in the order positions, cn, d4_weights, eeq_matrix, eeq_rhs,
+ * eeq_solve, bonded, hbonds, repulsion, pairs, post_chain, finish, and returns
  * the number of phases (or -1).  Diagnostics without a counterpart in the reference
  * (curcuma prints phase timings at verbosity >= 2 instead, gfnff.h:742). */
 gfnff_status gfnff_set_phase_timing(gfnff_handle* h, int on);
@@ -124,6 +124,18 @@ gfnff_status gfnff_eeq_charges_noalloc(int natoms, int nfrag, const double* d_xy
                                        const double* d_gam, const double* d_chi, const double* d_cnf,
                                        const double* d_cn, const int* d_frag, const double* d_qfrag,
                                        double* d_q, int* d_status, void* stream);
+
+/* Name of the EEQ solver chosen for the handle's molecule at setup: "library" (cuSOLVER
+ * Cholesky), "tiled" (persistent tiled Cholesky), "pcg" (block-Jacobi conjugate
+ * gradients, true residual <= 1e-12 max|b|), "lu" (indefinite matrix) or "batched"; ""
+ * before setup.  curcuma's EEQSolver also picks among several solvers
+ * (eeq_solver.cpp:1448-2086); this query has no counterpart there. */
+const char* gfnff_eeq_solver(gfnff_handle* h);
+
+/* Iterations of the last iterative EEQ solve (0 for the direct solvers, -1 before
+ * setup); synchronises the handle's stream.  Diagnostic without a counterpart in the
+ * reference. */
+int gfnff_eeq_iterations(gfnff_handle* h);
 
 /* Last error message of the handle (static storage when h is NULL). */
 const char* gfnff_last_error(gfnff_handle* h);

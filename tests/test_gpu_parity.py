@@ -131,3 +131,18 @@ def test_error_paths():
     assert gpu.calculateEnergy(True) == 0.0 and gpu.hasError()
     gpu.updateGeometry(X)
     assert gpu.calculateEnergy(True) != 0.0 and not gpu.hasError()
+
+
+@pytest.mark.parametrize("solver", ["tiled", "library", "pcg"])
+@pytest.mark.parametrize("system", ["water64", "water200", "alkane", "peptide"])
+def test_eeq_solvers(solver, system, monkeypatch):
+    """Every EEQ solver of the reduced system against the oracle; the 64-water cluster
+    has 128 reduced unknowns, so the tiled Cholesky's right-hand-side row forms a tile of
+    its own, and the alkane (one fragment) exercises the PCG with 64-row blocks."""
+    monkeypatch.setenv("GFNFF_EEQ_SOLVER", solver)
+    Z, X = {"water64": lambda: workloads.water_cluster(64, 9),
+            "water200": lambda: workloads.water_cluster(200, 10),
+            "alkane": lambda: workloads.alkane(64, 1001),
+            "peptide": lambda: workloads.solvated_peptide(8, 60, 12)}[system]()
+    gpu, _ = _compare(Z, X)
+    assert gpu.eeqSolver() == solver
