@@ -25,9 +25,7 @@ import ctypes
 import json
 import os
 import statistics
-import subprocess
 import sys
-import tempfile
 import time
 from pathlib import Path
 
@@ -36,7 +34,7 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-METRIC = "GFN-FF E+grad evals/s"
+METRIC = "GFN-FF E+grad evals/s: mixed vs FP64 GPU at \u0394E\u22641e-6 Eh, \u0394F\u22641e-5 Eh/bohr"
 UNIT = "evals/s"
 
 
@@ -47,7 +45,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", type=int, default=2)
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -71,42 +69,55 @@ def perturbed(X, k, sigma=0.01, seed=7):
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region."""
+    """SM clock and clock-event reasons sampled through NVML (read-only queries) every
+    5 ms by a background thread while the measurement runs; nvidia-smi's own polling
+    loop is too coarse for timed regions of a few tens of milliseconds."""
+
+    NAMES = {"hw_slowdown": "nvmlClocksEventReasonHwSlowdown",
+             "hw_thermal_slowdown": "nvmlClocksEventReasonHwThermalSlowdown",
+             "sw_thermal_slowdown": "nvmlClocksEventReasonSwThermalSlowdown",
+             "sw_power_cap": "nvmlClocksEventReasonSwPowerCap"}
 
     def __init__(self, device):
-        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
-        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        import threading
+        self.samples, self.reasons, self.max_mhz = [], set(), 0.0
+        self._stop = threading.Event()
         try:
-            self.p = subprocess.Popen(["nvidia-smi", f"--id={device}", f"--query-gpu={q}",
-                                       "--format=csv,noheader,nounits", "-lms", "50"],
-                                      stdout=self.f, stderr=subprocess.DEVNULL)
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+            idx = int(vis.split(",")[device]) if vis else device
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(idx)
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM))
         except Exception:
-            self.p = None
+            self.nv = None
+            return
+        self.t = threading.Thread(target=self._run, daemon=True)
+        self.t.start()
+
+    def _run(self):
+        nv = self.nv
+        while not self._stop.is_set():
+            try:
+                self.samples.append(float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)))
+                mask = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                for k, attr in self.NAMES.items():
+                    if mask & getattr(nv, attr):
+                        self.reasons.add(k)
+            except Exception:
+                pass
+            time.sleep(0.005)
 
     def stop(self):
-        if self.p is None:
+        if self.nv is None:
             return None
-        self.p.terminate()
-        self.p.wait()
-        self.f.seek(0)
-        rows = [r.split(",") for r in self.f.read().strip().split("\n") if r.strip()]
-        sm, mx, reasons = [], 0.0, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for r in rows:
-            try:
-                sm.append(float(r[1]))
-                mx = max(mx, float(r[2]))
-                for k, nm in enumerate(names):
-                    if r[5 + k].strip().lower().startswith("active"):
-                        reasons.add(nm)
-            except (ValueError, IndexError):
-                pass
-        if not sm:
+        self._stop.set()
+        self.t.join()
+        if not self.samples:
             return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(self.samples), "source": "nvml"}
 
 
 def measured_peaks():
@@ -198,31 +209,17 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def run_ours(args):
-    import torch
-    import torch.distributed as dist
-
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
+def measure(args, precision, Z, X, torch, dist, world, local):
+    """Device-timed and end-to-end throughput of one precision form on the workload."""
     from curcuma_b200 import GFNFF, _lib
 
-    desc, Z, X = workload(args.config)
     n = len(Z)
-    prec = 0 if args.precision == "fp64" else 1
-    gpu = GFNFF(precision=prec, device=local)
+    gpu = GFNFF(precision=0 if precision == "fp64" else 1, device=local)
     t0 = time.perf_counter()
     if not gpu.setMolecule(Z, X):
         raise SystemExit(gpu.getErrorMessage())
     setup_s = time.perf_counter() - t0
-    natoms, nfrag = gpu.sizes()
-    lib = gpu._lib
-    h = gpu.handle
+    lib, h = gpu._lib, gpu.handle
     stream = torch.cuda.ExternalStream(lib.gfnff_stream(h), device=torch.device("cuda", local))
     steps, warm = args.steps, args.warmup
     geoms = torch.tensor(np.stack([perturbed(X, k) / 0.529177210903 for k in range(steps + warm)]),
@@ -250,6 +247,7 @@ def run_ours(args):
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
+    worst = 0
     with torch.cuda.stream(stream):
         for k in range(steps):
             flush.zero_()
@@ -259,24 +257,21 @@ def run_ours(args):
             events[k][1].synchronize()
             lib.gfnff_phase_times(h, buf, len(buf))
             phases += np.array(buf[:])
+            worst = max(worst, int(d_st.item()))
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
     step_ms = [a.elapsed_time(b) for a, b in events]
     total_ms = float(sum(step_ms))
-    status = int(d_st.item())
     if world > 1:
         t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
-    value = world * steps / (total_ms * 1e-3)
-    phase_avg = {k: v / steps for k, v in zip(_lib.PHASES, phases)}
     lib.gfnff_set_phase_timing(h, 0)
-
-    # end-to-end through the host C ABI
+    # end to end through the host C ABI: host coordinates in, energy + gradient out
     hostX = [perturbed(X, 5000 + k) for k in range(steps)]
     for k in range(min(3, warm)):
-        gpu.updateGeometry(hostX[k])
+        gpu.updateGeometry(perturbed(X, 4000 + k))
         gpu.calculateEnergy(True)
     if world > 1:
         dist.barrier()
@@ -284,7 +279,7 @@ def run_ours(args):
     t = time.perf_counter()
     for k in range(steps):
         gpu.updateGeometry(hostX[k])
-        e = gpu.calculateEnergy(True)
+        gpu.calculateEnergy(True)
         if gpu.hasError():
             raise SystemExit(gpu.getErrorMessage())
     e2e_s = time.perf_counter() - t
@@ -293,13 +288,48 @@ def run_ours(args):
         tt = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         e2e_s = float(tt.item())
-    e2e = {"value": world * steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 3 * n * 8,
-           "d2h_bytes_per_step": (3 * n + 14) * 8 + 4}
+    return {"gpu": gpu, "value": world * steps / (total_ms * 1e-3), "total_ms": total_ms, "step_ms": step_ms,
+            "phase_avg": {k: v / steps for k, v in zip(_lib.PHASES, phases)}, "status": worst,
+            "e2e": {"value": world * steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 3 * n * 8,
+                    "d2h_bytes_per_step": (3 * n + 14) * 8 + 4},
+            "clocks": clk, "setup_s": setup_s, "solver": gpu.eeqSolver()}
 
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    desc, Z, X = workload(args.config)
+    n = len(Z)
+    # headline: the requested form; the other form is measured beside it
+    forms = [args.precision] + [p for p in ("mixed", "fp64") if p != args.precision]
+    res = {p: measure(args, p, Z, X, torch, dist, world, local) for p in forms}
+    main = res[args.precision]
+    gpu = main["gpu"]
+    natoms, nfrag = gpu.sizes()
+    # accuracy of the mixed form against the FP64 form on one geometry
+    Xc = perturbed(X, 9999)
+    em, ef = [], []
+    for p in ("mixed", "fp64"):
+        g = res[p]["gpu"]
+        g.updateGeometry(Xc)
+        em.append(g.calculateEnergy(True))
+        ef.append(g.getGradient())
+    err = {"dE_eh": abs(em[0] - em[1]), "max_dF_eh_per_bohr": float(np.abs(ef[0] - ef[1]).max())}
     counts = {k: len(gpu.topology(kind, w)) for k, kind, w in
               [("bonds", 0, 2), ("angles", 1, 3), ("torsions", 2, 4), ("inversions", 3, 4), ("hbonds", 6, 4),
                ("xbonds", 7, 3), ("atm", 12, 3), ("batm", 13, 3)]}
-    fixed = 12   # positions, cn, d4w, eeq A, residual, reduce, expand, repulsion, pairs, post, chain, finish
+    # kernels of this library per step: positions, cn, d4w, eeq matrix, rhs, solve (+info),
+    # expand, repulsion, pairs, post, chain, outputs, finish, and one per non-empty term list
+    fixed = 13 + (1 if main["solver"] in ("pcg", "tiled") else 0)
     launches = fixed + sum(1 for k in ("bonds", "angles", "torsions", "inversions", "hbonds", "xbonds", "atm", "batm")
                            if counts[k] > 0)
     if rank != 0:
@@ -307,24 +337,31 @@ def run_ours(args):
             dist.destroy_process_group()
         return
     nc, nd = pair_counts(Z, X)
-    # HB record: 3 atoms + neighbours; bytes = 19 scalars * 8 + atom refs * 48
     hbs = gpu.topology(6, 4)
     info = {"n": n, "nred": n - nfrag, "config": args.config, "coulomb_pairs": nc, "disp_pairs": nd,
             "bytes_hbonds": len(hbs) * (19 * 8 + 3 * 48 + 2 * 48)}
     hbm_peak, hbm_src = measured_peaks()
-    fp64_peak = lib.gfnff_fma_peak_tflops(local, 1)
-    roof = roofline(phase_avg, info, fp64_peak, hbm_peak, hbm_src)
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps, "warmup": warm,
-            "ms_per_step": total_ms / steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64" if prec == 0 else "mixed(f32/f64)", "data": "synthetic",
+    fp64_peak = gpu._lib.gfnff_fma_peak_tflops(local, 1)
+    roof = roofline(main["phase_avg"], info, fp64_peak, hbm_peak, hbm_src)
+    steps = args.steps
+    line = {"metric": METRIC, "value": main["value"], "unit": UNIT, "n_gpus": world, "steps": steps,
+            "warmup": args.warmup, "ms_per_step": main["total_ms"] / steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "mixed(f32 short-range, f64 long-range/EEQ/sums)",
+            "data": "synthetic",
             "config": {"workload": f"config {args.config}: {desc}", "natoms": natoms, "nfrag": nfrag,
-                       "precision": args.precision, "l2": "flushed before every timed step (256 MiB write)",
-                       "parallelism": f"replicas x{world}", "setup_s": round(setup_s, 3)},
-            "e2e": e2e, "gpu_launches": launches * steps, "roofline": roof,
-            "phase_ms": {k: round(v, 4) for k, v in phase_avg.items()},
-            "step_ms_median": statistics.median(step_ms), "status": status,
-            "pairs": {"coulomb": nc, "dispersion": nd},
-            "terms": counts, "clocks": clk}
+                       "precision": args.precision, "eeq_solver": main["solver"],
+                       "l2": "flushed before every timed step (256 MiB write)",
+                       "parallelism": f"replicas x{world}", "setup_s": round(main["setup_s"], 3)},
+            "e2e": main["e2e"], "gpu_launches": launches * steps, "roofline": roof,
+            "phase_ms": {k: round(v, 4) for k, v in main["phase_avg"].items()},
+            "step_ms_median": statistics.median(main["step_ms"]), "status": main["status"],
+            "forms": {p: {"value": r["value"], "e2e": r["e2e"]["value"], "eeq_solver": r["solver"],
+                          "phase_ms": {k: round(v, 4) for k, v in r["phase_avg"].items()}}
+                      for p, r in res.items()},
+            "mixed_vs_fp64": res["mixed"]["value"] / res["fp64"]["value"],
+            "mixed_error_vs_fp64": err,
+            "pairs": {"coulomb": nc, "dispersion": nd}, "terms": counts, "clocks": main["clocks"]}
     if world == 1 and not args.no_cpu_baseline:
         rate, dt = cpu_oracle_rate(Z, X, 2 if n >= 2000 else 5, 1)
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",

@@ -57,29 +57,48 @@ struct DBuf {
 // ------------------------------------------------------------------------------------
 // small device helpers
 // ------------------------------------------------------------------------------------
-struct D3 {
-    double x, y, z;
+// 3-vector in the arithmetic type R of a kernel (double in the FP64 form, float for the
+// FP32 arithmetic of the mixed form); D3 is the double version
+template <class R>
+struct V3 {
+    R x, y, z;
 };
+using D3 = V3<double>;
 __device__ __forceinline__ D3 mk(double x, double y, double z) { return {x, y, z}; }
-__device__ __forceinline__ D3 operator-(D3 a, D3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
-__device__ __forceinline__ D3 operator+(D3 a, D3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
-__device__ __forceinline__ D3 operator*(double s, D3 a) { return {s * a.x, s * a.y, s * a.z}; }
-__device__ __forceinline__ double dot(D3 a, D3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
-__device__ __forceinline__ D3 cross(D3 a, D3 b)
+template <class R>
+__device__ __forceinline__ V3<R> operator-(V3<R> a, V3<R> b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+template <class R>
+__device__ __forceinline__ V3<R> operator+(V3<R> a, V3<R> b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+template <class R>
+__device__ __forceinline__ V3<R> operator*(R s, V3<R> a) { return {s * a.x, s * a.y, s * a.z}; }
+template <class R>
+__device__ __forceinline__ R dot(V3<R> a, V3<R> b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+template <class R>
+__device__ __forceinline__ V3<R> cross(V3<R> a, V3<R> b)
 {
     return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
 }
-__device__ __forceinline__ double nrm(D3 a) { return sqrt(dot(a, a)); }
+template <class R>
+__device__ __forceinline__ R nrm(V3<R> a) { return sqrt(dot(a, a)); }
 __device__ __forceinline__ D3 ld(const double4* p, int i)
 {
     double4 v = p[i];
     return {v.x, v.y, v.z};
 }
-__device__ __forceinline__ void agrad(double* g, int i, D3 v)
+// position of atom i relative to the origin o, in the arithmetic type R (the FP64
+// difference is taken first, so FP32 keeps the relative precision of short vectors)
+template <class R>
+__device__ __forceinline__ V3<R> ldr(const double4* p, int i, double4 o)
 {
-    atomicAdd(g + 3 * i, v.x);
-    atomicAdd(g + 3 * i + 1, v.y);
-    atomicAdd(g + 3 * i + 2, v.z);
+    const double4 v = p[i];
+    return {(R)(v.x - o.x), (R)(v.y - o.y), (R)(v.z - o.z)};
+}
+template <class R>
+__device__ __forceinline__ void agrad(double* g, int i, V3<R> v)
+{
+    atomicAdd(g + 3 * i, (double)v.x);
+    atomicAdd(g + 3 * i + 1, (double)v.y);
+    atomicAdd(g + 3 * i + 2, (double)v.z);
 }
 
 // block-wide sum of one value, one atomicAdd per block into *dst
@@ -119,25 +138,27 @@ __device__ double angle_cos(D3 i, D3 j, D3 k, D3 d[3])
 }
 
 // dihedral angle and d(phi)/dx (gfnff_geometry.h:66-160)
-__device__ double dihedral(D3 ri, D3 rj, D3 rk, D3 rl, D3 g[4])
+template <class R>
+__device__ R dihedral(V3<R> ri, V3<R> rj, V3<R> rk, V3<R> rl, V3<R> g[4])
 {
-    for (int a = 0; a < 4; ++a) g[a] = mk(0, 0, 0);
-    D3 v1 = rj - ri, v2 = rk - rj, v3 = rl - rk;
-    D3 n1 = cross(v1, v2), n2 = cross(v2, v3);
-    const double n1n = nrm(n1), n2n = nrm(n2), v2n = nrm(v2);
-    if (n1n < 1e-10 || n2n < 1e-10 || v2n < 1e-10) return 0.0;
-    D3 h1 = (1.0 / n1n) * n1, h2 = (1.0 / n2n) * n2;
-    const double cphi = dot(h1, h2);
-    double sphi = (v2n * dot(h1, v3)) / n2n;
-    sphi = fmax(-1.0, fmin(1.0, sphi));
-    const double phi = atan2(sphi, cphi);
-    const double nen = n1n * n2n * sin(phi);
-    if (fabs(nen) < 1e-14) return phi;
-    const double o = 1.0 / nen;
-    D3 rab = cross(n1, v2), rbb = cross(n2, v2), rac = cross(n1, v3), rbc = cross(n2, v3);
-    D3 rba = cross(n2, v1), raa = cross(n1, v1);
-    D3 rapb = v1 + v2, rbpc = v2 + v3;
-    D3 rapba = cross(rapb, n1), rapbb = cross(rapb, n2), rbpca = cross(rbpc, n1), rbpcb = cross(rbpc, n2);
+    using P3 = V3<R>;
+    for (int a = 0; a < 4; ++a) g[a] = P3{R(0), R(0), R(0)};
+    P3 v1 = rj - ri, v2 = rk - rj, v3 = rl - rk;
+    P3 n1 = cross(v1, v2), n2 = cross(v2, v3);
+    const R n1n = nrm(n1), n2n = nrm(n2), v2n = nrm(v2);
+    if (n1n < R(1e-10) || n2n < R(1e-10) || v2n < R(1e-10)) return R(0);
+    P3 h1 = (R(1) / n1n) * n1, h2 = (R(1) / n2n) * n2;
+    const R cphi = dot(h1, h2);
+    R sphi = (v2n * dot(h1, v3)) / n2n;
+    sphi = fmax(R(-1), fmin(R(1), sphi));
+    const R phi = atan2(sphi, cphi);
+    const R nen = n1n * n2n * sin(phi);
+    if (fabs(nen) < R(1e-14)) return phi;
+    const R o = R(1) / nen;
+    P3 rab = cross(n1, v2), rbb = cross(n2, v2), rac = cross(n1, v3), rbc = cross(n2, v3);
+    P3 rba = cross(n2, v1), raa = cross(n1, v1);
+    P3 rapb = v1 + v2, rbpc = v2 + v3;
+    P3 rapba = cross(rapb, n1), rapbb = cross(rapb, n2), rbpca = cross(rbpc, n1), rbpcb = cross(rbpc, n2);
     g[0] = o * ((cphi * n2n / n1n) * rab - rbb);
     g[1] = o * (cphi * ((n2n / n1n) * rapba + (n1n / n2n) * rbc) - (rac + rapbb));
     g[2] = o * (cphi * ((n2n / n1n) * raa + (n1n / n2n) * rbpcb) - (rba + rbpca));

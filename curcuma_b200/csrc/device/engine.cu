@@ -115,6 +115,40 @@ std::vector<int> fragment_order(const Model& m)
     return ord;
 }
 
+// HB terms by increasing setup distance r_AB, so that neighbouring threads of the HB
+// kernel take the same branch (strong terms near the front of the list)
+std::vector<int> hb_order(const Model& m)
+{
+    std::vector<double> d(m.hbonds.size());
+    for (size_t k = 0; k < d.size(); ++k) {
+        const auto& t = m.hbonds[k];
+        double s = 0.0;
+        for (int c = 0; c < 3; ++c) {
+            const double x = m.xyz_setup[3 * t.a + c] - m.xyz_setup[3 * t.b + c];
+            s += x * x;
+        }
+        d[k] = s;
+    }
+    std::vector<int> o(d.size());
+    std::iota(o.begin(), o.end(), 0);
+    std::stable_sort(o.begin(), o.end(), [&](int x, int y) { return d[x] < d[y]; });
+    return o;
+}
+
+int hb_near_count(const Model& m)
+{
+    int c = 0;
+    for (const auto& t : m.hbonds) {
+        double s = 0.0;
+        for (int k = 0; k < 3; ++k) {
+            const double x = m.xyz_setup[3 * t.a + k] - m.xyz_setup[3 * t.b + k];
+            s += x * x;
+        }
+        c += s < 100.0;
+    }
+    return c;
+}
+
 // blocks of a tiled pair kernel: enough partner slices to give every SM a few blocks
 int pair_splits(int n, int max_range)
 {
@@ -177,7 +211,7 @@ struct Engine::Impl {
     DBuf<double> work;
     DBuf<int> info, info2, status, ipiv, bad;
     int lwork = 0;
-    int lda = 1;           // leading dimension of M (nred + 1: row nred holds b for k_chol)
+    int lda = 2;           // leading dimension of M (>= nred + 1, even; row nred holds b for k_chol)
     bool use_lu = false;   // reduced EEQ matrix not positive definite: pivoted LU instead
     // EEQ solver of a single-molecule engine (chosen at upload, see upload_batch)
     enum { SOLVE_LIBRARY = 0, SOLVE_TILED = 1, SOLVE_PCG = 2 };
@@ -204,18 +238,18 @@ struct Engine::Impl {
     DBuf<long long> pboff;
     DBuf<int4> ppart;
     DBuf<int> prblk;
-    DBuf<double> pbinv, px, pr, pz, ppartial;
+    DBuf<double> px, pz, ppartial;
     DBuf<unsigned int> pbar;
     DBuf<int> piters;
-    int pcg_grid = 0, pcg_max_iter = 200;
+    int pcg_grid = 0, pcg_max_iter = 200, pcg_maxrows = 1, pcg_maxinv = 1;
     size_t pcg_smem = 0;
     bool pcg_ready = false;
     void pcg_launch()
     {
         CK(cudaMemsetAsync(pbar.p, 0, sizeof(unsigned int), stream));
         PCGArgs A;
-        A.M = M.p; A.lda = lda; A.n = nred; A.b = bvec.p; A.x = px.p; A.r = pr.p; A.z = pz.p;
-        A.blocks = pblocks.p; A.boff = pboff.p; A.binv = pbinv.p; A.part = ppart.p; A.rblk = prblk.p; A.partial = ppartial.p;
+        A.M = M.p; A.lda = lda; A.n = nred; A.b = bvec.p; A.x = px.p; A.z = pz.p;
+        A.blocks = pblocks.p; A.boff = pboff.p; A.maxrows = pcg_maxrows; A.maxinv = pcg_maxinv; A.part = ppart.p; A.rblk = prblk.p; A.partial = ppartial.p;
         A.bar = pbar.p; A.info = info.p; A.iters = piters.p; A.max_iter = pcg_max_iter; A.tol = 1e-12;
         void* args[] = {&A};
         CK(cudaLaunchCooperativeKernel((const void*)k_pcg, dim3(pcg_grid), dim3(kPcgThreads), args, pcg_smem, stream));
@@ -227,6 +261,7 @@ struct Engine::Impl {
         if (timing) CK(cudaEventRecord(ev[k], stream));
     }
     int nb = 0, na = 0, nt = 0, ns = 0, ninv = 0, natm = 0, nbatm = 0, nhb = 0, nxb = 0;
+    int nhb_near = 0;   // HB terms (sorted by setup r_AB) with setup r_AB < 10 bohr
 
     View view() const
     {
@@ -315,7 +350,8 @@ void Engine::upload_hbxb(const Model& m)
         std::vector<int> a, h, b, c, pc, nbo{0}, nb, nco{0}, nc, nfl;
         std::vector<double> ba, bb, aa, ab, QH, QA, QB, rv, zlp;
         auto qs = [](double q, double st, double sf) { const double e = std::exp(st * q); return e / (e + sf); };
-        for (auto& t : m.hbonds) {
+        for (int ti : hb_order(m)) {
+            const HBTerm& t = m.hbonds[ti];
             a.push_back(X(t.a)); h.push_back(X(t.h)); b.push_back(X(t.b)); c.push_back(t.case_type);
             pc.push_back(t.parent_c >= 0 ? X(t.parent_c) : -1);
             for (int x : t.nb_b) nb.push_back(X(x));
@@ -330,6 +366,7 @@ void Engine::upload_hbxb(const Model& m)
             nfl.push_back((zb == 7 && t.nb_b.size() == 1) ? 1 : 0);
         }
         P.nhb = (int)m.hbonds.size();
+        P.nhb_near = hb_near_count(m);
         P.h_a.upload(a); P.h_h.upload(h); P.h_b.upload(b); P.h_c.upload(c); P.h_pc.upload(pc);
         P.h_nbo.upload(nbo); P.h_nb.upload(nb); P.h_nco.upload(nco); P.h_nc.upload(nc);
         P.h_ba.upload(ba); P.h_bb.upload(bb); P.h_aa.upload(aa); P.h_ab.upload(ab);
@@ -610,7 +647,8 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
                 if (H >= 0) for (int x : byH[H]) hb.push_back(X(x));
                 off.push_back((int)hb.size());
             }
-            for (auto& t : M.hbonds) {
+            for (int ti : hb_order(M)) {
+                const HBTerm& t = M.hbonds[ti];
                 a.push_back(X(t.a)); h.push_back(X(t.h)); b.push_back(X(t.b)); c.push_back(t.case_type);
                 pc.push_back(t.parent_c >= 0 ? X(t.parent_c) : -1);
                 for (int x : t.nb_b) nbv.push_back(X(x));
@@ -635,6 +673,7 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
         P.b_fc.upload(fc); P.b_al.upload(al); P.b_r0i.upload(r0i); P.b_r0j.upload(r0j);
         P.b_cki.upload(cki); P.b_ckj.upload(ckj); P.b_sh.upload(sh); P.b_ff.upload(ff);
         P.nhb = (int)a.size();
+        P.nhb_near = P.nhb;   // batches: every HB term in FP64
         P.h_a.upload(a); P.h_h.upload(h); P.h_b.upload(b); P.h_c.upload(c); P.h_pc.upload(pc);
         P.h_nbo.upload(nbo); P.h_nb.upload(nbv); P.h_nco.upload(nco); P.h_nc.upload(ncv);
         P.h_ba.upload(ba); P.h_bb.upload(bb); P.h_aa.upload(aa); P.h_ab.upload(abv);
@@ -648,7 +687,7 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
     P.hg.alloc((size_t)n * K * 7); P.hdg.alloc((size_t)n * K * 7);
     P.q.alloc(n); P.dEdcn.alloc(n); P.v.alloc(n); P.grad.alloc(3 * (size_t)n); P.E.alloc(16 * (size_t)nm);
     P.gout.alloc(3 * (size_t)n); P.qout.alloc(n); P.cnout.alloc(n);
-    P.lda = P.nred + 1;
+    P.lda = (P.nred + 2) & ~1;   // >= nred + 1 and even: 16-byte aligned columns
     P.M.alloc((size_t)std::max<long long>(1, nm == 1 ? (long long)P.lda * P.nred : P.msize));
     P.bvec.alloc(std::max(1, P.nred)); P.xyz_stage.alloc(3 * (size_t)n); P.msd.alloc(1);
     P.info.alloc(nm); P.info2.alloc(1); P.status.alloc(nm); P.bad.alloc(nm);
@@ -706,6 +745,7 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
             const int G = std::max(1, std::min(nsm, (int)blocks.size()));
             size_t bk = 0;
             int maxrows = 1;
+            long long maxinv = 1;
             for (int g = 0; g < G; ++g) {
                 const int target = (int)(((long long)P.nred * (g + 1)) / G);
                 const int b0 = (int)bk, r0 = bk < blocks.size() ? blocks[bk].x : P.nred;
@@ -713,16 +753,24 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
                 const int r1 = bk < blocks.size() ? blocks[bk].x : P.nred;
                 part.push_back(make_int4(r0, r1, b0, (int)bk));
                 maxrows = std::max(maxrows, r1 - r0);
+                maxinv = std::max(maxinv, (bk < blocks.size() ? boff[bk] : bo) - (b0 < (int)blocks.size() ? boff[b0] : bo));
             }
-            const size_t smem = ((size_t)P.nred + kPcgMaxBlock * (kPcgMaxBlock + 1) + maxrows) * sizeof(double);
+            // p (n), Gauss-Jordan scratch, x/r/z/Mp of the owned rows, owned block inverses
+            maxinv = (maxinv + 1) & ~1ll;   // keeps the int4 row records behind it 16-byte aligned
+            const size_t smem =
+                ((size_t)((P.nred + 1) & ~1) + kPcgMaxBlock * (kPcgMaxBlock + 1) + 4 * (size_t)maxrows + maxinv) *
+                    sizeof(double) +
+                (size_t)maxrows * sizeof(int4);
             if (smem <= 220 * 1024) {
                 std::vector<int> rblk(P.nred);
                 for (size_t q = 0; q < blocks.size(); ++q)
                     for (int r = 0; r < blocks[q].y; ++r) rblk[blocks[q].x + r] = (int)q;
                 P.pblocks.upload(blocks); P.pboff.upload(boff); P.ppart.upload(part); P.prblk.upload(rblk);
-                P.pbinv.alloc((size_t)bo); P.px.alloc(P.nred); P.pr.alloc(P.nred); P.pz.alloc(P.nred);
-                P.ppartial.alloc(4 * (size_t)G); P.pbar.alloc(2); P.piters.alloc(1);
-                CK(cudaMemset(P.pbar.p, 0, 2 * sizeof(unsigned int)));
+                P.px.alloc(P.nred); P.pz.alloc(P.nred);
+                P.pcg_maxrows = maxrows;
+                P.pcg_maxinv = (int)maxinv;
+                P.ppartial.alloc(4 * (size_t)G); P.pbar.alloc(2 * kBarGen); P.piters.alloc(1);
+                CK(cudaMemset(P.pbar.p, 0, 2 * kBarGen * sizeof(unsigned int)));
                 CK(cudaMemset(P.piters.p, 0, sizeof(int)));
                 P.pcg_grid = G;
                 P.pcg_smem = smem;
@@ -833,6 +881,10 @@ void Engine::enqueue(const double* d_xyz, bool bohr)
     const int n = P.n;
     View V = P.view();
     const dim3 tgrid(nblk(n, kTile), P.nsplit);
+    // mixed form: FP32 arithmetic in the CN erf counting and the weak hydrogen bonds; FP64
+    // everywhere else (per-pair float<->double conversions cost more than FP32 saves in
+    // the pair and CN-chain kernels) and in every accumulation
+    const bool mixed = P.opt.precision == 1;
     P.mark(0);
     CK(cudaMemsetAsync(P.grad.p, 0, 3 * (size_t)n * sizeof(double), s));
     CK(cudaMemsetAsync(P.dEdcn.p, 0, (size_t)n * sizeof(double), s));
@@ -843,7 +895,7 @@ void Engine::enqueue(const double* d_xyz, bool bohr)
     const double scale = bohr ? 1.0 : kAngToBohr;
     k_positions<<<nblk(n), kBlock, 0, s>>>(n, P.perm.p, d_xyz, scale, P.pos.p, P.hbref.p, P.msd.p);
     P.mark(1);
-    k_cn<<<tgrid, kTile, 0, s>>>(V, P.nsplit);
+    (mixed ? k_cn<float> : k_cn<double>)<<<tgrid, kTile, 0, s>>>(V, P.nsplit);
     P.mark(2);
     k_d4_weights<<<nblk(n), kBlock, 0, s>>>(V);
     // EEQ
@@ -900,16 +952,18 @@ void Engine::enqueue(const double* d_xyz, bool bohr)
     if (P.nhb) {
         HBSoA H{P.nhb, P.h_a.p, P.h_h.p, P.h_b.p, P.h_c.p, P.h_pc.p, P.h_nbo.p, P.h_nb.p, P.h_nco.p, P.h_nc.p,
                 P.h_ba.p, P.h_bb.p, P.h_aa.p, P.h_ab.p, P.h_QH.p, P.h_QA.p, P.h_QB.p, P.h_rv.p, P.h_zlp.p, P.h_nfl.p};
-        k_hbonds<<<nblk(P.nhb), kBlock, 0, s>>>(V, H);
+        const int split = mixed ? P.nhb_near : P.nhb;
+        if (split > 0) k_hbonds<double><<<nblk(split), kBlock, 0, s>>>(V, H, 0, split);
+        if (P.nhb > split) k_hbonds<float><<<nblk(P.nhb - split), kBlock, 0, s>>>(V, H, split, P.nhb);
     }
     if (P.nxb) k_xbonds<<<nblk(P.nxb), kBlock, 0, s>>>(V, XBSoA{P.nxb, P.x_a.p, P.x_x.p, P.x_b.p, P.x_pre.p, P.x_rv.p});
     P.mark(8);
-    k_repulsion<<<nblk((long)n * 32), kBlock, 0, s>>>(V, P.r_off.p, P.r_j.p, P.r_al.p, P.r_ab.p, P.r_kind.p);
+    k_repulsion<double><<<nblk((long)n * 32), kBlock, 0, s>>>(V, P.r_off.p, P.r_j.p, P.r_al.p, P.r_ab.p, P.r_kind.p);
     P.mark(9);
-    k_pairs<<<tgrid, kTile, 0, s>>>(V, P.nsplit);
+    k_pairs<double><<<tgrid, kTile, 0, s>>>(V, P.nsplit);
     P.mark(10);
     k_post<<<nblk(n), kBlock, 0, s>>>(V);
-    k_cn_chain<<<tgrid, kTile, 0, s>>>(V, P.nsplit);
+    k_cn_chain<double><<<tgrid, kTile, 0, s>>>(V, P.nsplit);
     P.mark(11);
     k_outputs<<<nblk(n), kBlock, 0, s>>>(V, P.gout.p, P.qout.p, P.cnout.p, P.bad.p);
     k_finish<<<nblk(P.nmol), kBlock, 0, s>>>(V, (P.nred > 0 || P.nmol > 1) ? P.info.p : nullptr, P.bad.p, P.e0.p, nullptr);

@@ -2,12 +2,19 @@
 // FP64 atomics, term energies summed per molecule.  Included by engine.cu (one translation unit).
 #pragma once
 
+// resident blocks per SM requested for the HB kernel: 4 caps it at 128 registers (a few
+// spills), which measured 1.5x faster than the uncapped 190 registers at 2 blocks per SM
+#ifndef GFNFF_HB_MINBLOCKS
+#define GFNFF_HB_MINBLOCKS 4
+#endif
+
 namespace {
 
 // x^6 (the HB/XB damping exponent is the integer 6)
-__device__ __forceinline__ double pow6(double x)
+template <class R = double>
+__device__ __forceinline__ R pow6(R x)
 {
-    const double x3 = x * x * x;
+    const R x3 = x * x * x;
     return x3 * x3;
 }
 
@@ -331,207 +338,219 @@ struct HBSoA {
     const int* nflag;   // acceptor is N with a single neighbour: neighbour cutoff 2.0
 };
 
-// hydrogen bonds, cases 1-4 (ff_workspace_gfnff.cpp:938-1409)
-__global__ void __launch_bounds__(kBlock) k_hbonds(View V, HBSoA S)
+// hydrogen bonds, cases 1-4 (ff_workspace_gfnff.cpp:938-1409).  R = double is the FP64
+// form; R = float evaluates the term in FP32 relative to the H atom (the FP64 position
+// differences are taken first), energies and gradients accumulate in FP64.  The damping
+// derivatives use d(ex)/d(sum) = (cut / rv) / rAB in closed form instead of the
+// reference's ex / (sum - rAB), which is the same value but 0/0 for collinear atoms.
+// One thread per HB term of the range [t0, t1).  The list is sorted by the setup
+// distance r_AB and split at 10 bohr: the mixed form evaluates the real hydrogen bonds
+// before the split (up to ~0.01 Eh each) with R = double and only the weak remainder with
+// R = float, because the FP32 rounding of per-element-pair constants is the same for
+// every strong bond and would add up over thousands of them.
+template <class R>
+__global__ void __launch_bounds__(kBlock, GFNFF_HB_MINBLOCKS) k_hbonds(View V, HBSoA S, int t0, int t1)
 {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    double etot = 0.0;
-    if (t < S.n) {
-        const double HB_BACUT = 49.0, HB_SCUT = 22.0, HB_ALP = 6.0, HB_LONGCUT = 85.0, HB_NBCUT = 11.20;
-        const double TORS_HB = 0.94, BEND_HB = 0.20, HBLPCUT = 56.0;
+    const int t = t0 + blockIdx.x * blockDim.x + threadIdx.x;
+    R etot = R(0.0);
+    if (t < t1) {
+        using P3 = V3<R>;
+        const double4 org = V.pos[S.h[t]];   // H as the local origin
+        const R HB_BACUT = R(49.0), HB_SCUT = R(22.0), HB_ALP = R(6.0), HB_LONGCUT = R(85.0), HB_NBCUT = R(11.20);
+        const R TORS_HB = R(0.94), BEND_HB = R(0.20), HBLPCUT = R(56.0);
         const int A = S.a[t], H = S.h[t], Bq = S.b[t], cs = S.cas[t];
-        D3 pA = ld(V.pos, A), pH = ld(V.pos, H), pB = ld(V.pos, Bq);
-        const double rAH = nrm(pH - pA), rHB = nrm(pB - pH), rAB = nrm(pB - pA);
-        if (rAB <= 50.0) {
-            const double rAH4 = rAH * rAH * rAH * rAH, rHB4 = rHB * rHB * rHB * rHB;
-            const double den = 1.0 / (rAH4 + rHB4);
-            const double QH = S.QH[t], QA = S.QA[t], QB = S.QB[t];
-            const double bas = (QA * S.bas_a[t] * rAH4 + QB * S.bas_b[t] * rHB4) * den;
-            const double aci = (S.aci_b[t] * rAH4 + S.aci_a[t] * rHB4) * den;
-            const double rv = S.rv[t];
+        P3 pA = ldr<R>(V.pos, A, org), pH = ldr<R>(V.pos, H, org), pB = ldr<R>(V.pos, Bq, org);
+        const R rAH = nrm(pH - pA), rHB = nrm(pB - pH), rAB = nrm(pB - pA);
+        if (rAB <= R(50.0)) {
+            const R rAH4 = rAH * rAH * rAH * rAH, rHB4 = rHB * rHB * rHB * rHB;
+            const R den = R(1.0) / (rAH4 + rHB4);
+            const R QH = S.QH[t], QA = S.QA[t], QB = S.QB[t];
+            const R bas = (QA * S.bas_a[t] * rAH4 + QB * S.bas_b[t] * rHB4) * den;
+            const R aci = (S.aci_b[t] * rAH4 + S.aci_a[t] * rHB4) * den;
+            const R rv = S.rv[t];
             // HB_ALP = 6: integer powers
-            const double ratio1 = pow6(rAB * rAB / HB_LONGCUT);
-            const double ratio3 = pow6(HB_SCUT * rv / (rAB * rAB));
-            const double dsh = 1.0 / (1.0 + ratio3);
-            const double dlg = 1.0 / (1.0 + ratio1);
-            const double denv = dsh * dlg;
-            double doutl;
+            const R ratio1 = pow6<R>(rAB * rAB / HB_LONGCUT);
+            const R ratio3 = pow6<R>(HB_SCUT * rv / (rAB * rAB));
+            const R dsh = R(1.0) / (R(1.0) + ratio3);
+            const R dlg = R(1.0) / (R(1.0) + ratio1);
+            const R denv = dsh * dlg;
+            R doutl;
             {
-                const double ex = (HB_BACUT / rv) * ((rAH + rHB) / rAB - 1.0);
-                doutl = ex > 15.0 ? 0.0 : 2.0 / (1.0 + exp(ex));
+                const R ex = (HB_BACUT / rv) * ((rAH + rHB) / rAB - R(1.0));
+                doutl = ex > R(15.0) ? R(0.0) : R(2.0) / (R(1.0) + exp(ex));
             }
             const int nb0 = S.nbb_off[t], nb1 = S.nbb_off[t + 1];
-            const double nbcut = S.nflag[t] ? 2.0 : HB_NBCUT;
-            double onb = 1.0;
+            const R nbcut = S.nflag[t] ? R(2.0) : HB_NBCUT;
+            R onb = R(1.0);
             if (cs >= 2)
                 for (int p = nb0; p < nb1; ++p) {
-                    D3 pn = ld(V.pos, S.nbb[p]);
-                    const double ra = nrm(pn - pA), rb = nrm(pn - pB);
-                    const double ex = (nbcut / rv) * ((ra + rb) / rAB - 1.0);
-                    onb *= (2.0 / (1.0 + exp(-ex)) - 1.0);
+                    P3 pn = ldr<R>(V.pos, S.nbb[p], org);
+                    const R ra = nrm(pn - pA), rb = nrm(pn - pB);
+                    const R ex = (nbcut / rv) * ((ra + rb) / rAB - R(1.0));
+                    onb *= (R(2.0) / (R(1.0) + exp(-ex)) - R(1.0));
                 }
-            const double rdamp = cs >= 2 ? denv * (1.8 / (rHB * rHB * rHB) - 0.8 / (rAB * rAB * rAB))
+            const R rdamp = cs >= 2 ? denv * (R(1.8) / (rHB * rHB * rHB) - R(0.8) / (rAB * rAB * rAB))
                                          : denv / (rAB * rAB * rAB);
-            double olp = 1.0, lpd = 0.0;
+            R olp = R(1.0), lpd = R(0.0);
             int nlp = 0;
-            D3 lpv = mk(0, 0, 0), lpp = pB;
+            P3 lpv = P3{0, 0, 0}, lpp = pB;
             if (cs == 4) {
-                lpd = 0.50 - 0.018 * S.zlp[t];
+                lpd = R(0.50) - R(0.018) * S.zlp[t];
                 nlp = nb1 - nb0;
-                for (int p = nb0; p < nb1; ++p) lpv = lpv + (ld(V.pos, S.nbb[p]) - pB);
-                const double vn = nrm(lpv);
-                if (vn > 1e-10 && nlp > 0) {
-                    lpp = pB + (-lpd) * ((1.0 / vn) * lpv);
-                    const double ral = nrm(pA - lpp);
-                    const double ex = (HBLPCUT / rv) * ((ral + lpd + 1e-12) / rAB - 1.0);
-                    olp = 2.0 / (1.0 + exp(ex));
+                for (int p = nb0; p < nb1; ++p) lpv = lpv + (ldr<R>(V.pos, S.nbb[p], org) - pB);
+                const R vn = nrm(lpv);
+                if (vn > R(1e-10) && nlp > 0) {
+                    lpp = pB + (-lpd) * ((R(1.0) / vn) * lpv);
+                    const R ral = nrm(pA - lpp);
+                    const R ex = (HBLPCUT / rv) * ((ral + lpd + R(1e-12)) / rAB - R(1.0));
+                    olp = R(2.0) / (R(1.0) + exp(ex));
                 } else {
                     nlp = 0;
-                    olp = 1.0;
+                    olp = R(1.0);
                 }
             }
-            const double qhoutl = QH * doutl * onb * olp;
-            double eangl = 1.0, etors = 1.0;
-            D3 ga3[3] = {mk(0, 0, 0), mk(0, 0, 0), mk(0, 0, 0)};
+            const R qhoutl = QH * doutl * onb * olp;
+            R eangl = R(1.0), etors = R(1.0);
+            P3 ga3[3] = {P3{0, 0, 0}, P3{0, 0, 0}, P3{0, 0, 0}};
             const int Ci = S.pc[t];
             const bool c3 = (cs == 3 && Ci != -1);
             if (c3) {
-                const double c0 = 120.0 * kPi / 180.0;
-                const double kijk = (1.0 - BEND_HB) / ((cos(0.0) - cos(c0)) * (cos(0.0) - cos(c0)));
-                D3 va = ld(V.pos, Ci), vb = pB, vc = pH;
-                D3 vab = va - vb, vcb = vc - vb;
-                const double rab2 = dot(vab, vab), rcb2 = dot(vcb, vcb);
-                D3 vp = cross(vcb, vab);
-                const double rp = nrm(vp) + 1e-14;
-                double ca = dot(vab, vcb) / (sqrt(rab2) * sqrt(rcb2) + 1e-14);
-                ca = fmax(-1.0, fmin(1.0, ca));
-                const double th = acos(ca);
-                const double ea = kijk * (ca - cos(c0)) * (ca - cos(c0));
-                const double deddt = 2.0 * kijk * sin(th) * (cos(c0) - ca);
-                eangl = 1.0 - ea;
-                D3 deda = (-deddt / (rab2 * rp)) * cross(vab, vp);
-                D3 dedc = (deddt / (rcb2 * rp)) * cross(vcb, vp);
+                const R c0 = R(120.0) * R(kPi) / R(180.0);
+                const R kijk = (R(1.0) - BEND_HB) / ((cos(R(0.0)) - cos(c0)) * (cos(R(0.0)) - cos(c0)));
+                P3 va = ldr<R>(V.pos, Ci, org), vb = pB, vc = pH;
+                P3 vab = va - vb, vcb = vc - vb;
+                const R rab2 = dot(vab, vab), rcb2 = dot(vcb, vcb);
+                P3 vp = cross(vcb, vab);
+                const R rp = nrm(vp) + R(1e-14);
+                R ca = dot(vab, vcb) / (sqrt(rab2) * sqrt(rcb2) + R(1e-14));
+                ca = fmax(-R(1.0), fmin(R(1.0), ca));
+                const R th = acos(ca);
+                const R ea = kijk * (ca - cos(c0)) * (ca - cos(c0));
+                const R deddt = R(2.0) * kijk * sin(th) * (cos(c0) - ca);
+                eangl = R(1.0) - ea;
+                P3 deda = (-deddt / (rab2 * rp)) * cross(vab, vp);
+                P3 dedc = (deddt / (rcb2 * rp)) * cross(vcb, vp);
                 ga3[0] = deda + dedc;
-                ga3[1] = -1.0 * deda;
-                ga3[2] = -1.0 * dedc;
+                ga3[1] = -R(1.0) * deda;
+                ga3[2] = -R(1.0) * dedc;
                 for (int p = S.nbc_off[t]; p < S.nbc_off[t + 1]; ++p) {
                     const int D = S.nbc[p];
                     if (D == Bq) continue;
-                    D3 g[4];
-                    const double phi = dihedral(ld(V.pos, D), pB, va, pH, g);
-                    const double fct = (1.0 - TORS_HB) / 2.0;
-                    const double c1 = 2 * (phi - kPi / 2.0) + kPi;
-                    etors *= (1.0 + cos(c1)) * fct + TORS_HB;
+                    P3 g[4];
+                    const R phi = dihedral(ldr<R>(V.pos, D, org), pB, va, pH, g);
+                    const R fct = (R(1.0) - TORS_HB) / R(2.0);
+                    const R c1 = 2 * (phi - R(kPi) / R(2.0)) + R(kPi);
+                    etors *= (R(1.0) + cos(c1)) * fct + TORS_HB;
                 }
             }
-            double gs = 1.0;
-            if (cs == 2 || cs == 4) gs = 0.268;
-            else if (cs == 3) gs = 0.350;
-            const double cst = S.aci_a[t] * S.bas_b[t] * QA * QB * gs;
-            const double E = cs >= 2 ? -rdamp * qhoutl * cst * eangl * etors : -bas * aci * rdamp * qhoutl;
+            R gs = R(1.0);
+            if (cs == 2 || cs == 4) gs = R(0.268);
+            else if (cs == 3) gs = R(0.350);
+            const R cst = S.aci_a[t] * S.bas_b[t] * QA * QB * gs;
+            const R E = cs >= 2 ? -rdamp * qhoutl * cst * eangl * etors : -bas * aci * rdamp * qhoutl;
             etot = E;
 
-            D3 drab = pA - pB, drah = pA - pH, drbh = pB - pH;
-            const double rab2 = rAB * rAB, rbh2 = rHB * rHB, rah2 = rAH * rAH;
-            const double rahprbh = rAH + rHB + 1e-12;
-            const double ddamp = (-2.0 * HB_ALP * ratio1 / (1.0 + ratio1)) + (2.0 * HB_ALP * ratio3 / (1.0 + ratio3));
-            const double expo = (HB_BACUT / rv) * (rahprbh / rAB - 1.0);
-            if (expo <= 15.0) {
-                const double ratio2 = exp(expo);
-                D3 ga = mk(0, 0, 0), gb = mk(0, 0, 0), gh = mk(0, 0, 0);
+            P3 drab = pA - pB, drah = pA - pH, drbh = pB - pH;
+            const R rab2 = rAB * rAB, rbh2 = rHB * rHB, rah2 = rAH * rAH;
+            const R rahprbh = rAH + rHB + R(1e-12);
+            const R ddamp = (-R(2.0) * HB_ALP * ratio1 / (R(1.0) + ratio1)) + (R(2.0) * HB_ALP * ratio3 / (R(1.0) + ratio3));
+            const R expo = (HB_BACUT / rv) * (rahprbh / rAB - R(1.0));
+            if (expo <= R(15.0)) {
+                const R ratio2 = exp(expo);
+                P3 ga = P3{0, 0, 0}, gb = P3{0, 0, 0}, gh = P3{0, 0, 0};
                 if (cs >= 2) {
-                    const double rbhdamp = denv * 1.8 / (rbh2 * rHB);
-                    const double rabdamp = denv * (-0.8) / (rab2 * rAB);
-                    const double dterm = -qhoutl * eangl * etors * cst;
-                    const double aterm = -rdamp * QH * onb * olp * eangl * etors * cst;
-                    const double nbterm = -rdamp * QH * doutl * olp * eangl * etors * cst;
-                    double gi = ((rabdamp + rbhdamp) * ddamp - 3.0 * rabdamp) / rab2;
+                    const R rbhdamp = denv * R(1.8) / (rbh2 * rHB);
+                    const R rabdamp = denv * (-R(0.8)) / (rab2 * rAB);
+                    const R dterm = -qhoutl * eangl * etors * cst;
+                    const R aterm = -rdamp * QH * onb * olp * eangl * etors * cst;
+                    const R nbterm = -rdamp * QH * doutl * olp * eangl * etors * cst;
+                    R gi = ((rabdamp + rbhdamp) * ddamp - R(3.0) * rabdamp) / rab2;
                     gi *= dterm;
-                    D3 dg = gi * drab;
+                    P3 dg = gi * drab;
                     ga = dg;
-                    gb = -1.0 * dg;
-                    gi = -3.0 * rbhdamp / rbh2;
+                    gb = -R(1.0) * dg;
+                    gi = -R(3.0) * rbhdamp / rbh2;
                     gi *= dterm;
                     dg = gi * drbh;
                     gb = gb + dg;
-                    gh = -1.0 * dg;
-                    const double tmp1 = -2.0 * aterm * ratio2 * expo / ((1.0 + ratio2) * (1.0 + ratio2)) / (rahprbh - rAB);
+                    gh = -R(1.0) * dg;
+                    const R tmp1 = -R(2.0) * aterm * ratio2 * (HB_BACUT / rv) / rAB / ((R(1.0) + ratio2) * (R(1.0) + ratio2));
                     gi = -tmp1 * rahprbh / rab2;
                     dg = gi * drab;
                     ga = ga + dg;
                     gb = gb - dg;
-                    D3 dgao = (tmp1 / rAH) * drah, dgbo = (tmp1 / rHB) * drbh;
+                    P3 dgao = (tmp1 / rAH) * drah, dgbo = (tmp1 / rHB) * drbh;
                     ga = ga + dgao;
                     gb = gb + dgbo;
                     gh = gh - dgao - dgbo;
                     for (int p = nb0; p < nb1; ++p) {
                         const int nb = S.nbb[p];
-                        D3 pn = ld(V.pos, nb);
-                        D3 dranb = pA - pn, drbnb = pB - pn;
-                        const double ranb = nrm(dranb), rbnb = nrm(drbnb);
-                        const double sum = ranb + rbnb + 1e-12;
-                        const double ex = (nbcut / rv) * (sum / rAB - 1.0);
-                        const double r2n = exp(-ex);
-                        const double oi = 2.0 / (1.0 + r2n) - 1.0;
-                        const double others = fabs(oi) > 1e-12 ? onb / oi : 1.0;
-                        const double tmp2 = 2.0 * nbterm * others * r2n * ex / ((1.0 + r2n) * (1.0 + r2n)) / (sum - rAB);
+                        P3 pn = ldr<R>(V.pos, nb, org);
+                        P3 dranb = pA - pn, drbnb = pB - pn;
+                        const R ranb = nrm(dranb), rbnb = nrm(drbnb);
+                        const R sum = ranb + rbnb + R(1e-12);
+                        const R ex = (nbcut / rv) * (sum / rAB - R(1.0));
+                        const R r2n = exp(-ex);
+                        const R oi = R(2.0) / (R(1.0) + r2n) - R(1.0);
+                        const R others = fabs(oi) > R(1e-12) ? onb / oi : R(1.0);
+                        const R tmp2 = R(2.0) * nbterm * others * r2n * (nbcut / rv) / rAB / ((R(1.0) + r2n) * (R(1.0) + r2n));
                         dg = (-tmp2 * sum / rab2) * drab;
                         ga = ga + dg;
                         gb = gb - dg;
-                        D3 dgan = (tmp2 / ranb) * dranb, dgbn = (tmp2 / rbnb) * drbnb;
+                        P3 dgan = (tmp2 / ranb) * dranb, dgbn = (tmp2 / rbnb) * drbnb;
                         ga = ga + dgan;
                         gb = gb + dgbn;
-                        agrad(V.grad, nb, -1.0 * dgan - dgbn);
+                        agrad(V.grad, nb, -R(1.0) * dgan - dgbn);
                     }
                     if (cs == 4 && nlp > 0) {
-                        const double lpterm = -rdamp * QH * doutl * onb * cst;
-                        const double ral = nrm(pA - lpp);
-                        const double sum = ral + lpd + 1e-12;
-                        const double ex = (HBLPCUT / rv) * (sum / rAB - 1.0);
-                        const double r2l = exp(ex);
-                        const double tmp3 = -2.0 * lpterm * r2l * ex / ((1.0 + r2l) * (1.0 + r2l)) / (sum - rAB);
-                        D3 dgl = (-tmp3 * sum / rab2) * drab;
+                        const R lpterm = -rdamp * QH * doutl * onb * cst;
+                        const R ral = nrm(pA - lpp);
+                        const R sum = ral + lpd + R(1e-12);
+                        const R ex = (HBLPCUT / rv) * (sum / rAB - R(1.0));
+                        const R r2l = exp(fmin(ex, R(80.0)));   // e^-80: the term vanishes, no overflow
+                        const R tmp3 = -R(2.0) * lpterm * r2l * (HBLPCUT / rv) / rAB / ((R(1.0) + r2l) * (R(1.0) + r2l));
+                        P3 dgl = (-tmp3 * sum / rab2) * drab;
                         ga = ga + dgl;
                         gb = gb - dgl;
-                        D3 dral = pA - lpp;
-                        D3 dgal = (tmp3 / (ral + 1e-12)) * dral;
+                        P3 dral = pA - lpp;
+                        P3 dgal = (tmp3 / (ral + R(1e-12))) * dral;
                         ga = ga + dgal;
                         gb = gb - dgal;
-                        D3 glp = -1.0 * dgal;
-                        const double vn = nrm(lpv);
-                        if (vn > 1e-10) {
-                            const double lv[3] = {lpv.x, lpv.y, lpv.z}, gl3[3] = {glp.x, glp.y, glp.z};
-                            double out[3] = {0, 0, 0};
-                            const double vn3 = vn * vn * vn;
+                        P3 glp = -R(1.0) * dgal;
+                        const R vn = nrm(lpv);
+                        if (vn > R(1e-10)) {
+                            const R lv[3] = {lpv.x, lpv.y, lpv.z}, gl3[3] = {glp.x, glp.y, glp.z};
+                            R out[3] = {0, 0, 0};
+                            const R vn3 = vn * vn * vn;
                             for (int col = 0; col < 3; ++col)
                                 for (int row = 0; row < 3; ++row) {
-                                    const double unit = (row == col) ? -1.0 : 0.0;
-                                    out[row] += -lpd * (double)nlp * (unit / vn + lv[row] * lv[col] / vn3) * gl3[col];
+                                    const R unit = (row == col) ? -R(1.0) : R(0.0);
+                                    out[row] += -lpd * (R)nlp * (unit / vn + lv[row] * lv[col] / vn3) * gl3[col];
                                 }
-                            D3 gnb = mk(out[0], out[1], out[2]);
+                            P3 gnb = P3{out[0], out[1], out[2]};
                             gb = gb + gnb;
-                            D3 share = (1.0 / (double)nlp) * gnb;
-                            for (int p = nb0; p < nb1; ++p) agrad(V.grad, S.nbb[p], -1.0 * share);
+                            P3 share = (R(1.0) / (R)nlp) * gnb;
+                            for (int p = nb0; p < nb1; ++p) agrad(V.grad, S.nbb[p], -R(1.0) * share);
                         }
                     }
                     if (c3) {
-                        const double bterm = -rdamp * qhoutl * etors * cst;
-                        const double tterm = -rdamp * qhoutl * eangl * cst;
+                        const R bterm = -rdamp * qhoutl * etors * cst;
+                        const R tterm = -rdamp * qhoutl * eangl * cst;
                         agrad(V.grad, Bq, bterm * ga3[0]);
                         agrad(V.grad, Ci, bterm * ga3[1]);
                         agrad(V.grad, H, bterm * ga3[2]);
-                        D3 va = ld(V.pos, Ci);
+                        P3 va = ldr<R>(V.pos, Ci, org);
                         for (int p = S.nbc_off[t]; p < S.nbc_off[t + 1]; ++p) {
                             const int D = S.nbc[p];
                             if (D == Bq) continue;
-                            D3 g[4];
-                            const double phi = dihedral(ld(V.pos, D), pB, va, pH, g);
-                            const double fct = (1.0 - TORS_HB) / 2.0;
-                            const double c1 = 2 * (phi - kPi / 2.0) + kPi;
-                            const double ek = (1.0 + cos(c1)) * fct + TORS_HB;
-                            const double dij = -2 * sin(c1) * fct;
-                            const double fk = fabs(ek) > 1e-12 ? etors / ek : 0.0;
-                            const double tk = fk * tterm;
+                            P3 g[4];
+                            const R phi = dihedral(ldr<R>(V.pos, D, org), pB, va, pH, g);
+                            const R fct = (R(1.0) - TORS_HB) / R(2.0);
+                            const R c1 = 2 * (phi - R(kPi) / R(2.0)) + R(kPi);
+                            const R ek = (R(1.0) + cos(c1)) * fct + TORS_HB;
+                            const R dij = -2 * sin(c1) * fct;
+                            const R fk = fabs(ek) > R(1e-12) ? etors / ek : R(0.0);
+                            const R tk = fk * tterm;
                             agrad(V.grad, D, (tk * dij) * g[0]);
                             agrad(V.grad, Bq, (tk * dij) * g[1]);
                             agrad(V.grad, Ci, (tk * dij) * g[2]);
@@ -539,34 +558,34 @@ __global__ void __launch_bounds__(kBlock) k_hbonds(View V, HBSoA S)
                         }
                     }
                 } else {
-                    const double caa = QA * S.bas_a[t], cbb = QB * S.bas_b[t];
-                    const double rterm = -aci * rdamp * qhoutl, dterm = -aci * bas * qhoutl;
-                    const double sterm = -rdamp * bas * qhoutl, aterm = -aci * bas * rdamp * QH;
-                    const double dv = 1.0 / (rAH4 + rHB4);
-                    const double tmp = dv * dv * 4.0;
-                    const double dd24a = rah2 * rHB4 * tmp, dd24b = rbh2 * rAH4 * tmp;
-                    double gi = (caa - cbb) * dd24a * rterm;
+                    const R caa = QA * S.bas_a[t], cbb = QB * S.bas_b[t];
+                    const R rterm = -aci * rdamp * qhoutl, dterm = -aci * bas * qhoutl;
+                    const R sterm = -rdamp * bas * qhoutl, aterm = -aci * bas * rdamp * QH;
+                    const R dv = R(1.0) / (rAH4 + rHB4);
+                    const R tmp = dv * dv * R(4.0);
+                    const R dd24a = rah2 * rHB4 * tmp, dd24b = rbh2 * rAH4 * tmp;
+                    R gi = (caa - cbb) * dd24a * rterm;
                     ga = gi * drah;
                     gi = (cbb - caa) * dd24b * rterm;
                     gb = gi * drbh;
-                    gh = -1.0 * ga - gb;
+                    gh = -R(1.0) * ga - gb;
                     gi = (S.aci_b[t] - S.aci_a[t]) * dd24a;
-                    D3 dga = (gi * sterm) * drah;
+                    P3 dga = (gi * sterm) * drah;
                     ga = ga + dga;
                     gi = (S.aci_a[t] - S.aci_b[t]) * dd24b;
-                    D3 dgb = (gi * sterm) * drbh;
+                    P3 dgb = (gi * sterm) * drbh;
                     gb = gb + dgb;
                     gh = gh - dga - dgb;
-                    gi = rdamp * (ddamp - 3.0) / rab2;
-                    D3 dg = (gi * dterm) * drab;
+                    gi = rdamp * (ddamp - R(3.0)) / rab2;
+                    P3 dg = (gi * dterm) * drab;
                     ga = ga + dg;
                     gb = gb - dg;
-                    gi = aterm * 2.0 * ratio2 * expo * rahprbh / ((1.0 + ratio2) * (1.0 + ratio2)) / (rahprbh - rAB) / rab2;
+                    gi = aterm * R(2.0) * ratio2 * (HB_BACUT / rv) / rAB * rahprbh / ((R(1.0) + ratio2) * (R(1.0) + ratio2)) / rab2;
                     dg = gi * drab;
                     ga = ga + dg;
                     gb = gb - dg;
-                    const double to = -2.0 * aterm * ratio2 * expo / ((1.0 + ratio2) * (1.0 + ratio2)) / (rahprbh - rAB);
-                    D3 dgao = (to / rAH) * drah, dgbo = (to / rHB) * drbh;
+                    const R to = -R(2.0) * aterm * ratio2 * (HB_BACUT / rv) / rAB / ((R(1.0) + ratio2) * (R(1.0) + ratio2));
+                    P3 dgao = (to / rAH) * drah, dgbo = (to / rHB) * drbh;
                     ga = ga + dgao;
                     gb = gb + dgbo;
                     gh = gh - dgao - dgbo;
@@ -577,8 +596,9 @@ __global__ void __launch_bounds__(kBlock) k_hbonds(View V, HBSoA S)
             }
         }
     }
-    eadd(V, etot, t < S.n ? V.mol[S.a[t]] : -1, T_HB);
+    eadd(V, (double)etot, t < t1 ? V.mol[S.a[t]] : -1, T_HB);
 }
+
 
 struct XBSoA {
     int n;

@@ -49,6 +49,7 @@ __global__ void k_positions(int n, const int* __restrict__ perm, const double* _
 // coordination numbers: erf counting over partners closer than 6 bohr
 // (cn_calculator.cpp:367-428); the log-squash is applied in k_d4_weights
 // ------------------------------------------------------------------------------------
+template <class R>
 __global__ void __launch_bounds__(kTile) k_cn(View V, int nsplit)
 {
     __shared__ double sx[kTile], sy[kTile], sz[kTile], sr[kTile];
@@ -77,9 +78,9 @@ __global__ void __launch_bounds__(kTile) k_cn(View V, int nsplit)
                 const double d2 = dx * dx + dy * dy + dz * dz;
                 const int j = t0 + jj;
                 if (!(d2 < 36.0) || j == i || j < rg.x || j >= rg.y) continue;
-                const double r = sqrt(d2);
-                const double rc = ri + sr[jj];
-                s += 0.5 * (1.0 + erf(kn * ((r - rc) / rc)));
+                const R r = sqrt((R)d2);
+                const R rc = (R)(ri + sr[jj]);
+                s += (double)(R(0.5) * (R(1) + erf(R(kn) * ((r - rc) / rc))));
             }
         }
     }
@@ -144,6 +145,7 @@ __global__ void k_d4_weights(View V)
 // repulsion over per-atom CSR lists holding both pair directions
 // (ff_workspace_gfnff.cpp:774-848); kind 0 = bonded, 1 = non-bonded.  One warp per atom.
 // ------------------------------------------------------------------------------------
+template <class R>
 __global__ void __launch_bounds__(kBlock) k_repulsion(View V, const int* off, const int* nbj, const double* alpha,
                                                      const double* repab, const unsigned char* kind)
 {
@@ -155,13 +157,14 @@ __global__ void __launch_bounds__(kBlock) k_repulsion(View V, const int* off, co
         for (int p = off[i] + lane; p < off[i + 1]; p += 32) {
             const double4 pj = V.pos[nbj[p]];
             const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-            const double r = sqrt(dx * dx + dy * dy + dz * dz);
-            if (r > 20.0 || r < 1e-8) continue;
-            const double sr = sqrt(r);
-            const double e = repab[p] * exp(-alpha[p] * (r * sr)) / r;
-            if (kind[p]) enb += 0.5 * e; else eb += 0.5 * e;
-            const double dEdr = -e / r - 1.5 * alpha[p] * sr * e;
-            const double f = dEdr / r;
+            const double d2 = dx * dx + dy * dy + dz * dz;
+            const R r = sqrt((R)d2);
+            if (r > R(20) || r < R(1e-8)) continue;
+            const R sr = sqrt(r), al = (R)alpha[p];
+            const R e = (R)repab[p] * exp(-al * (r * sr)) / r;
+            if (kind[p]) enb += 0.5 * (double)e; else eb += 0.5 * (double)e;
+            const R dEdr = -e / r - R(1.5) * al * sr * e;
+            const double f = (double)(dEdr / r);
             gx += f * dx; gy += f * dy; gz += f * dz;
         }
         for (int o = 16; o > 0; o >>= 1) {
@@ -190,7 +193,38 @@ __global__ void __launch_bounds__(kBlock) k_repulsion(View V, const int* off, co
 // Coulomb fast path: erf(x) rounds to exactly 1 in double for x >= 6 (erfc(6) = 2.2e-17
 // is below half an ulp of 1), i.e. for r^2 >= 36 (a_i + a_j); the pair is then q q / r and
 // its exp(-x^2) gradient term is below 2e-15 relative, so both are dropped there.
+// R is the arithmetic type of the D4 part beyond 15 bohr: double in the FP64 form,
+// float in the mixed form (nearer D4 pairs are FP64 in both).  Coulomb (both branches), the distances and every sum stay FP64 in both forms:
+// single Coulomb pairs reach 0.1 Eh and there are ~N^2/2 of them, so FP32 rounding in
+// them would add up to more than 1e-6 Eh.
 // ------------------------------------------------------------------------------------
+// one D4 pair in arithmetic type R: energy e, dE/dr / r in dedr, dE/dCN_i in dc
+template <class R>
+__device__ __forceinline__ void d4_pair(double d2, const double* g0, const double* dg, const double (*sw0)[kTile],
+                                        const double (*sw)[kTile], int jj, int nr, double szi, double szj,
+                                        double zz_d, double& e, double& dedr, double& dc)
+{
+    R c6 = R(0), dc6 = R(0);
+    for (int b = 0; b < nr; ++b) {
+        c6 += (R)__ldg(g0 + b) * (R)sw0[b][jj];
+        dc6 += (R)dg[b] * (R)sw[b][jj];
+    }
+    const R q2 = (R)d2;
+    const R r4r2 = R(3) * (R)szi * (R)szj;
+    const R t = R(0.58) * sqrt(r4r2) + R(4.80);
+    const R r0sq = t * t;
+    const R zz = (R)zz_d;
+    const R r6 = q2 * q2 * q2, r06 = r0sq * r0sq * r0sq;
+    const R t6 = R(1) / (r6 + r06);
+    const R t8 = R(1) / (r6 * q2 + r06 * r0sq);
+    const R sum = t6 + R(2) * r4r2 * t8;
+    e = -(double)(c6 * sum * zz);
+    const R d6 = R(-6) * q2 * q2 * t6 * t6, d8 = R(-8) * r6 * t8 * t8;
+    dedr = -(double)(c6 * zz * (d6 + R(2) * r4r2 * d8));
+    dc = -(double)(dc6 * sum * zz);
+}
+
+template <class R>
 __global__ void __launch_bounds__(kTile) k_pairs(View V, int nsplit)
 {
     __shared__ double sx[kTile], sy[kTile], sz[kTile], s0x[kTile], s0y[kTile], s0z[kTile];
@@ -207,7 +241,7 @@ __global__ void __launch_bounds__(kTile) k_pairs(View V, int nsplit)
     const int2 rg = act ? V.jr[i] : make_int2(0, 0);
     const double* g0i = V.g0 + (size_t)ic * V.K * 7;
     const double* dgi = V.hdg + (size_t)ic * V.K * 7;
-    const double a1 = 0.58, a2 = 4.80, tsp = 2.0 / 1.772453850905516;
+    const double tsp = 2.0 / 1.772453850905516;
     double ec = 0.0, ed = 0.0, gx = 0.0, gy = 0.0, gz = 0.0, dcn = 0.0;
     for (int t0 = jb; t0 < je; t0 += kTile) {
         __syncthreads();
@@ -257,23 +291,15 @@ __global__ void __launch_bounds__(kTile) k_pairs(View V, int nsplit)
                 const int sj = ssl[jj], nr = snr[jj];
                 const double* g0 = g0i + sj * 7;
                 const double* dg = dgi + sj * 7;
-                double c6 = 0.0, dc6 = 0.0;
-                for (int b = 0; b < nr; ++b) {
-                    c6 += __ldg(g0 + b) * sw0[b][jj];
-                    dc6 += dg[b] * sw[b][jj];
-                }
-                const double r4r2 = 3.0 * szi * ssz[jj];
-                const double t = a1 * sqrt(r4r2) + a2;
-                const double r0sq = t * t;
-                const double zz = zi * sze[jj];
-                const double r6 = d2 * d2 * d2, r06 = r0sq * r0sq * r0sq;
-                const double t6 = 1.0 / (r6 + r06);
-                const double t8 = 1.0 / (r6 * d2 + r06 * r0sq);
-                const double sum = t6 + 2.0 * r4r2 * t8;
-                ed -= c6 * sum * zz;
-                const double d6 = -6.0 * d2 * d2 * t6 * t6, d8 = -8.0 * r6 * t8 * t8;
-                f -= c6 * zz * (d6 + 2.0 * r4r2 * d8);
-                dcn -= dc6 * sum * zz;
+                double e, dedr, dc;
+                // mixed form: pairs closer than 15 bohr (the strong ones) stay FP64
+                if (sizeof(R) == sizeof(double) || d2 < 225.0)
+                    d4_pair<double>(d2, g0, dg, sw0, sw, jj, nr, szi, ssz[jj], zi * sze[jj], e, dedr, dc);
+                else
+                    d4_pair<R>(d2, g0, dg, sw0, sw, jj, nr, szi, ssz[jj], zi * sze[jj], e, dedr, dc);
+                ed += e;
+                f += dedr;
+                dcn += dc;
             }
             gx += f * dx; gy += f * dy; gz += f * dz;
         }
@@ -311,6 +337,7 @@ __global__ void k_post(View V)
 
 // CN chain rule: grad_i += sum_j dS_ij/dr (u_i + u_j) (x_i - x_j)/r over the 6 bohr
 // neighbours (gfnff_method.cpp:5837-6260, forcefieldthread.h:80-109)
+template <class R>
 __global__ void __launch_bounds__(kTile) k_cn_chain(View V, int nsplit)
 {
     __shared__ double sx[kTile], sy[kTile], sz[kTile], sr[kTile], su[kTile];
@@ -341,11 +368,11 @@ __global__ void __launch_bounds__(kTile) k_cn_chain(View V, int nsplit)
             const double d2 = dx * dx + dy * dy + dz * dz;
             const int j = t0 + jj;
             if (!(d2 < 36.0) || j == i || j < rg.x || j >= rg.y) continue;
-            const double r = sqrt(d2);
-            const double rs = ri + sr[jj];
-            const double dr = (r - rs) / rs;
-            const double de = (kn / sqrtpi) * exp(-kn * kn * dr * dr) / rs;
-            const double f = -(de / r) * (ui + su[jj]);
+            const R r = sqrt((R)d2);
+            const R rs = (R)(ri + sr[jj]);
+            const R dr = (r - rs) / rs;
+            const R de = R(kn / sqrtpi) * exp(R(-kn * kn) * dr * dr) / rs;
+            const double f = -(double)(de / r) * (ui + su[jj]);
             gx += f * dx; gy += f * dy; gz += f * dz;
         }
     }

@@ -28,45 +28,60 @@ struct PCGArgs {
     int lda, n;
     const double* b;
     double* x;            // solution
-    double* r;            // residual
-    double* z;            // preconditioned residual
+    double* z;            // preconditioned residual (shared between grid blocks)
     const int2* blocks;   // preconditioner blocks {first row, size}
     const long long* boff;
-    double* binv;         // inverse of every block (row-major, size^2)
+    int maxrows;          // most rows owned by one grid block
+    int maxinv;           // most inverse entries held by one grid block
     const int4* part;     // per grid block: rows [x, y), preconditioner blocks [z, w)
     const int* rblk;      // preconditioner block of every row
     double* partial;      // gridDim.x * 4
-    unsigned int* bar;    // {arrival count, generation}
+    unsigned int* bar;    // arrival count at [0], generation at [kBarGen]
     int* info;
     int* iters;
     int max_iter;
     double tol;           // converged when max|b - M x| <= tol * max|b|
 };
 
-// grid-wide barrier (all blocks co-resident); false when the wait gave up
+// grid-wide barrier (all blocks co-resident); false when the wait gave up.  The block's
+// threads meet at __syncthreads, then thread 0 alone arrives with a release atomic
+// (covering the block's writes ordered before it by the block barrier) and polls with
+// acquire loads.  The arrival
+// counter bar[0] and the generation bar[kBarGen] sit on different 128-byte lines, so the
+// polling reads do not queue behind the arrival atomics; the generation counter makes
+// the barrier reusable without a reset in between.
+constexpr int kBarGen = 32;
+__device__ __forceinline__ unsigned int atom_add_release(unsigned int* p, unsigned int v)
+{
+    unsigned int old;
+    asm volatile("atom.add.release.gpu.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+__device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p)
+{
+    unsigned int v;
+    asm volatile("ld.acquire.gpu.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
 __device__ bool grid_sync(unsigned int* bar, unsigned int& gen)
 {
     __shared__ int ok_s;
-    __threadfence();
     __syncthreads();
     if (threadIdx.x == 0) {
         ok_s = 1;
         const unsigned int want = gen + 1;
-        if (atomicAdd(bar, 1u) + 1u == gridDim.x) {
+        if (atom_add_release(bar, 1u) + 1u == gridDim.x) {
             atomicExch(bar, 0u);
-            __threadfence();
-            atomicAdd(bar + 1, 1u);
+            atom_add_release(bar + kBarGen, 1u);
         } else {
             long long polls = 0;
-            while ((int)(*(volatile unsigned int*)(bar + 1) - want) < 0) {
-                if (++polls > (1ll << 22)) {
+            while ((int)(ld_acquire(bar + kBarGen) - want) < 0) {
+                if (++polls > (1ll << 24)) {
                     ok_s = 0;
                     break;
                 }
-                __nanosleep(32);
             }
         }
-        __threadfence();
         gen = want;
     }
     __syncthreads();
@@ -93,72 +108,108 @@ __device__ void block_sum_max(double s, double m, double* out)
     }
 }
 
-// the same totals in every block: warp 0 reads the partials (lane l takes blocks l,
-// l + 32, ...) and combines them in a fixed order, so every block gets identical sums
+// the same totals in every block: thread k loads block k's partials (one round trip for
+// all of them), then a fixed reduction tree combines them, so every block gets
+// identical sums
 __device__ void grid_totals(const double* partial, int slot, double& sum, double& mx)
 {
-    __shared__ double t0, t1;
+    __shared__ double ws[32], wm[32];
     __syncthreads();
-    if (threadIdx.x < 32) {
-        double a = 0.0, b = 0.0;
-        for (int k = threadIdx.x; k < (int)gridDim.x; k += 32) {
-            a += __ldcg(partial + 4 * k + slot);
-            b = fmax(b, __ldcg(partial + 4 * k + slot + 1));
-        }
-        for (int o = 16; o > 0; o >>= 1) {
-            a += __shfl_xor_sync(0xffffffffu, a, o);
-            b = fmax(b, __shfl_xor_sync(0xffffffffu, b, o));
-        }
-        if (threadIdx.x == 0) {
-            t0 = a;
-            t1 = b;
-        }
+    double a = 0.0, b = 0.0;
+    for (int k = threadIdx.x; k < (int)gridDim.x; k += blockDim.x) {
+        a += __ldcg(partial + 4 * k + slot);
+        b = fmax(b, __ldcg(partial + 4 * k + slot + 1));
     }
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_xor_sync(0xffffffffu, a, o);
+        b = fmax(b, __shfl_xor_sync(0xffffffffu, b, o));
+    }
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) { ws[w] = a; wm[w] = b; }
     __syncthreads();
-    sum = t0;
-    mx = t1;
+    a = 0.0;
+    b = 0.0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) { a += ws[k]; b = fmax(b, wm[k]); }
+    sum = a;
+    mx = b;
 }
 
-// z = P^-1 r on the owned rows (one thread per row, rblk[r] = its preconditioner block);
-// returns the thread's part of r.z
-__device__ double apply_precond(const PCGArgs& A, int row0, int row1)
+// p = z + beta p over all n entries (z from global memory, several loads in flight);
+// beta == 0 overwrites p without reading it
+__device__ void update_p(double* p, const double* z, int n, double beta)
+{
+    constexpr int U = 8;
+    for (int c0 = threadIdx.x; c0 < n; c0 += U * blockDim.x) {
+        double zv[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int c = c0 + u * blockDim.x;
+            zv[u] = c < n ? __ldcg(z + c) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int c = c0 + u * blockDim.x;
+            if (c < n) p[c] = beta == 0.0 ? zv[u] : zv[u] + beta * p[c];
+        }
+    }
+}
+
+// z = P^-1 r on the owned rows (one thread per row, rblk[r] = its preconditioner block),
+// everything in shared memory: r, z and the block inverses of this grid block; returns
+// the thread's part of r.z
+// meta[k] = {first local row of row k's block, block size, offset of row k's inverse row}
+__device__ double apply_precond(int nrow, const int4* meta, const double* binv, const double* r, double* z)
 {
     double rz = 0.0;
-    for (int rr = row0 + threadIdx.x; rr < row1; rr += blockDim.x) {
-        const int bk = A.rblk[rr];
-        const int2 bl = A.blocks[bk];
-        const double* Bi = A.binv + A.boff[bk] + (size_t)(rr - bl.x) * bl.y;
+    for (int k = threadIdx.x; k < nrow; k += blockDim.x) {
+        const int4 m = meta[k];
+        const double* Bi = binv + m.z;
+        const double* rb = r + m.x;
         double s = 0.0;
-        for (int j = 0; j < bl.y; ++j) s += __ldcg(Bi + j) * __ldcg(A.r + bl.x + j);
-        __stcg(A.z + rr, s);
-        rz += s * __ldcg(A.r + rr);
+        for (int j = 0; j < m.y; ++j) s += Bi[j] * rb[j];
+        z[k] = s;
+        rz += s * r[k];
     }
     return rz;
 }
 
-// out[r - row0] = (M v)_r for the owned rows; the rows are shared out to the warps, each
-// lane keeps four independent partial sums so that several loads are in flight.
+// out[r - row0] = (M v)_r for the owned rows (warp per row).  Rows are read as 16-byte
+// pairs (lda is even) with eight independent pairs in flight per lane, so that one
+// row of L2-resident M costs a few L2 round trips rather than one per 32 elements.
 // Returns the thread's part of sum_r v_r (M v)_r.
 __device__ double matvec_rows(const PCGArgs& A, const double* v, int row0, int row1, double* out)
 {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const int n2 = A.n >> 1;
+    const double2* v2 = reinterpret_cast<const double2*>(v);
     double vmv = 0.0;
     for (int rr = row0 + warp; rr < row1; rr += nw) {
         const double* col = A.M + (size_t)rr * A.lda;
-        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+        const double2* c2 = reinterpret_cast<const double2*>(col);
+        double s[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) s[u] = 0.0;
         int c = lane;
-        for (; c + 96 < A.n; c += 128) {
-            s0 += col[c] * v[c];
-            s1 += col[c + 32] * v[c + 32];
-            s2 += col[c + 64] * v[c + 64];
-            s3 += col[c + 96] * v[c + 96];
+        for (; c + 7 * 32 < n2; c += 8 * 32) {
+            double2 m[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) m[u] = c2[c + 32 * u];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const double2 w = v2[c + 32 * u];
+                s[u] += m[u].x * w.x + m[u].y * w.y;
+            }
         }
-        for (; c < A.n; c += 32) s0 += col[c] * v[c];
-        double s = (s0 + s1) + (s2 + s3);
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        for (; c < n2; c += 32) {
+            const double2 m = c2[c], w = v2[c];
+            s[0] += m.x * w.x + m.y * w.y;
+        }
+        if ((A.n & 1) && lane == 0) s[0] += col[A.n - 1] * v[A.n - 1];
+        double t = ((s[0] + s[1]) + (s[2] + s[3])) + ((s[4] + s[5]) + (s[6] + s[7]));
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
         if (lane == 0) {
-            out[rr - row0] = s;
-            vmv += s * v[rr];
+            out[rr - row0] = t;
+            vmv += t * v[rr];
         }
     }
     return vmv;
@@ -167,7 +218,7 @@ __device__ double matvec_rows(const PCGArgs& A, const double* v, int row0, int r
 // inverse of a preconditioner block of at most kPcgSmall rows by one thread
 // (Gauss-Jordan in registers-sized local storage)
 constexpr int kPcgSmall = 4;
-__device__ void invert_small(const PCGArgs& A, int bk)
+__device__ void invert_small(const PCGArgs& A, int bk, double* I)
 {
     const int2 bl = A.blocks[bk];
     const int s = bl.y;
@@ -186,37 +237,43 @@ __device__ void invert_small(const PCGArgs& A, int bk)
             for (int j = 0; j < s; ++j) { g[i][j] -= f * g[c][j]; inv[i][j] -= f * inv[c][j]; }
         }
     }
-    double* I = A.binv + A.boff[bk];
     for (int i = 0; i < s; ++i)
-        for (int j = 0; j < s; ++j) __stcg(I + i * s + j, inv[i][j]);
+        for (int j = 0; j < s; ++j) I[i * s + j] = inv[i][j];
 }
 
 __global__ void __launch_bounds__(kPcgThreads) k_pcg(PCGArgs A)
 {
     extern __shared__ double sm[];
     constexpr int GL = kPcgMaxBlock + 1;
-    double* p = sm;                              // n
-    double* G = sm + A.n;                        // kPcgMaxBlock x GL
-    double* Ap = G + kPcgMaxBlock * GL;          // rows of this block
+    const int4 pt = A.part[blockIdx.x];
+    const int row0 = pt.x, row1 = pt.y, nrow = row1 - row0;
+    const long long boff0 = pt.z < pt.w ? A.boff[pt.z] : 0;
+    double* p = sm;                              // n: search direction, replicated
+    double* G = p + ((A.n + 1) & ~1);            // kPcgMaxBlock x GL scratch (even offsets
+                                                 // keep the int4 records 16-byte aligned)
+    double* xs = G + kPcgMaxBlock * GL;          // owned rows: x, r, z, M p
+    double* rs = xs + A.maxrows;
+    double* zs = rs + A.maxrows;
+    double* Ap = zs + A.maxrows;
+    double* Bs = Ap + A.maxrows;                 // inverses of the owned blocks
+    int4* meta = reinterpret_cast<int4*>(Bs + A.maxinv);   // per owned row, see apply_precond
     __shared__ unsigned int gen;
     __shared__ double piv;
-    const int4 pt = A.part[blockIdx.x];
-    const int row0 = pt.x, row1 = pt.y;
-    if (threadIdx.x == 0) gen = *(volatile unsigned int*)(A.bar + 1);
+    if (threadIdx.x == 0) gen = *(volatile unsigned int*)(A.bar + kBarGen);
     // ---- inverse of every owned preconditioner block (Gauss-Jordan on [M_bb | I]; SPD,
-    // no pivoting): M_bb in shared memory, the inverse built in place in binv
+    // no pivoting); small blocks one per thread, larger ones by the whole grid block
     for (int bk = pt.z + threadIdx.x; bk < pt.w; bk += blockDim.x)
-        if (A.blocks[bk].y <= kPcgSmall) invert_small(A, bk);
+        if (A.blocks[bk].y <= kPcgSmall) invert_small(A, bk, Bs + (A.boff[bk] - boff0));
     for (int bk = pt.z; bk < pt.w; ++bk) {
         const int2 bl = A.blocks[bk];
         const int s = bl.y;
         if (s <= kPcgSmall) continue;
-        double* I = A.binv + A.boff[bk];
+        double* I = Bs + (A.boff[bk] - boff0);
         __syncthreads();
         for (int e = threadIdx.x; e < s * s; e += blockDim.x) {
             const int i = e / s, j = e % s;
             G[i * GL + j] = A.M[(size_t)(bl.x + j) * A.lda + bl.x + i];
-            __stcg(I + e, i == j ? 1.0 : 0.0);
+            I[e] = i == j ? 1.0 : 0.0;
         }
         __syncthreads();
         for (int c = 0; c < s; ++c) {
@@ -225,19 +282,17 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(PCGArgs A)
             const double pv = piv;
             for (int j = threadIdx.x; j < s; j += blockDim.x) {
                 G[c * GL + j] *= pv;
-                __stcg(I + c * s + j, __ldcg(I + c * s + j) * pv);
+                I[c * s + j] *= pv;
             }
             __syncthreads();
             for (int e = threadIdx.x; e < s * s; e += blockDim.x) {
                 const int i = e / s, j = e % s;
-                if (i == c) continue;
-                __stcg(I + i * s + j, __ldcg(I + i * s + j) - G[i * GL + c] * __ldcg(I + c * s + j));
+                if (i != c) I[i * s + j] -= G[i * GL + c] * I[c * s + j];
             }
             __syncthreads();
             for (int e = threadIdx.x; e < s * s; e += blockDim.x) {
                 const int i = e / s, j = e % s;
-                if (i == c || j == c) continue;
-                G[i * GL + j] -= G[i * GL + c] * G[c * GL + j];
+                if (i != c && j != c) G[i * GL + j] -= G[i * GL + c] * G[c * GL + j];
             }
             __syncthreads();
             for (int i = threadIdx.x; i < s; i += blockDim.x)
@@ -245,22 +300,27 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(PCGArgs A)
             __syncthreads();
         }
     }
-    __syncthreads();
+    for (int k = threadIdx.x; k < nrow; k += blockDim.x) {
+        const int rr = row0 + k, bk = A.rblk[rr];
+        const int2 bl = A.blocks[bk];
+        meta[k] = make_int4(bl.x - row0, bl.y, (int)(A.boff[bk] - boff0) + (rr - bl.x) * bl.y, 0);
+    }
     // ---- x = 0, r = b, z = P^-1 r
     double bmax_t = 0.0;
-    for (int rr = row0 + threadIdx.x; rr < row1; rr += blockDim.x) {
-        const double bv = A.b[rr];
-        __stcg(A.x + rr, 0.0);
-        __stcg(A.r + rr, bv);
+    for (int k = threadIdx.x; k < nrow; k += blockDim.x) {
+        const double bv = A.b[row0 + k];
+        xs[k] = 0.0;
+        rs[k] = bv;
         bmax_t = fmax(bmax_t, fabs(bv));
     }
     __syncthreads();
-    double rz_t = apply_precond(A, row0, row1);
+    double rz_t = apply_precond(nrow, meta, Bs, rs, zs);
+    for (int k = threadIdx.x; k < nrow; k += blockDim.x) __stcg(A.z + row0 + k, zs[k]);
     block_sum_max(rz_t, bmax_t, A.partial + 4 * blockIdx.x);
     bool ok = grid_sync(A.bar, gen);
     double rz = 0.0, bmax = 0.0;
     if (ok) grid_totals(A.partial, 0, rz, bmax);
-    for (int c = threadIdx.x; c < A.n; c += blockDim.x) p[c] = __ldcg(A.z + c);
+    update_p(p, A.z, A.n, 0.0);
     int it = 0;
     bool conv = ok && bmax == 0.0;
     while (ok && !conv && it < A.max_iter) {
@@ -274,14 +334,14 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(PCGArgs A)
         grid_totals(A.partial, 0, pap, unused);
         const double alpha = rz / pap;
         double rmax_t = 0.0;
-        for (int rr = row0 + threadIdx.x; rr < row1; rr += blockDim.x) {
-            __stcg(A.x + rr, __ldcg(A.x + rr) + alpha * p[rr]);
-            const double nr = __ldcg(A.r + rr) - alpha * Ap[rr - row0];
-            __stcg(A.r + rr, nr);
-            rmax_t = fmax(rmax_t, fabs(nr));
+        for (int k = threadIdx.x; k < nrow; k += blockDim.x) {
+            xs[k] += alpha * p[row0 + k];
+            rs[k] -= alpha * Ap[k];
+            rmax_t = fmax(rmax_t, fabs(rs[k]));
         }
         __syncthreads();
-        rz_t = apply_precond(A, row0, row1);
+        rz_t = apply_precond(nrow, meta, Bs, rs, zs);
+        for (int k = threadIdx.x; k < nrow; k += blockDim.x) __stcg(A.z + row0 + k, zs[k]);
         block_sum_max(rz_t, rmax_t, A.partial + 4 * blockIdx.x + 2);
         ok = grid_sync(A.bar, gen);
         if (!ok) break;
@@ -289,18 +349,21 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(PCGArgs A)
         grid_totals(A.partial, 2, rzn, rmax);
         if (rmax <= A.tol * bmax) {
             // accept only on the true residual r = b - M x; otherwise restart from it
-            for (int c = threadIdx.x; c < A.n; c += blockDim.x) p[c] = __ldcg(A.x + c);
+            for (int k = threadIdx.x; k < nrow; k += blockDim.x) __stcg(A.x + row0 + k, xs[k]);
+            ok = grid_sync(A.bar, gen);
+            if (!ok) break;
+            update_p(p, A.x, A.n, 0.0);
             __syncthreads();
             matvec_rows(A, p, row0, row1, Ap);
             __syncthreads();
             rmax_t = 0.0;
-            for (int rr = row0 + threadIdx.x; rr < row1; rr += blockDim.x) {
-                const double tr = A.b[rr] - Ap[rr - row0];
-                __stcg(A.r + rr, tr);
-                rmax_t = fmax(rmax_t, fabs(tr));
+            for (int k = threadIdx.x; k < nrow; k += blockDim.x) {
+                rs[k] = A.b[row0 + k] - Ap[k];
+                rmax_t = fmax(rmax_t, fabs(rs[k]));
             }
             __syncthreads();
-            rz_t = apply_precond(A, row0, row1);
+            rz_t = apply_precond(nrow, meta, Bs, rs, zs);
+            for (int k = threadIdx.x; k < nrow; k += blockDim.x) __stcg(A.z + row0 + k, zs[k]);
             block_sum_max(rz_t, rmax_t, A.partial + 4 * blockIdx.x + 2);
             ok = grid_sync(A.bar, gen);
             if (!ok) break;
@@ -310,13 +373,15 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(PCGArgs A)
                 break;
             }
             rz = rzn;
-            for (int c = threadIdx.x; c < A.n; c += blockDim.x) p[c] = __ldcg(A.z + c);
+            update_p(p, A.z, A.n, 0.0);
             continue;
         }
         const double beta = rzn / rz;
         rz = rzn;
-        for (int c = threadIdx.x; c < A.n; c += blockDim.x) p[c] = __ldcg(A.z + c) + beta * p[c];
+        update_p(p, A.z, A.n, beta);
     }
+    __syncthreads();
+    for (int k = threadIdx.x; k < nrow; k += blockDim.x) A.x[row0 + k] = xs[k];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         *A.info = !ok ? 2 : (conv ? 0 : 3);
         *A.iters = it;
