@@ -60,7 +60,12 @@ def workload(cfg):
         return "Gly50 + 1500 H2O (seed 1003)", *W.solvated_peptide(50, 1500, 1003)
     if cfg == 5:
         return "6000 H2O + 40 C20H42 (seed 1005)", *W.large_cluster(6000, 40, 20, 1005)
-    raise SystemExit(f"config {cfg} is not a single-structure workload")
+    if cfg == 4:
+        mols = W.conformer_batch(512, 1004)
+        Z = np.concatenate([z for z, _ in mols])
+        X = np.concatenate([x for _, x in mols])
+        return "512 saturated C/N/O chains, 20-300 atoms log-uniform (seed 1004)", Z, X, mols
+    raise SystemExit(f"unknown config {cfg}")
 
 
 def perturbed(X, k, sigma=0.01, seed=7):
@@ -155,7 +160,7 @@ def roofline(phase_avg, info, fp64_peak, hbm_peak, hbm_src):
         bound, unit, peak = "fp64", "TFLOP/s", fp64_peak
         achieved = flops / (ms * 1e-3) / 1e12
     elif name == "eeq_solve":
-        flops = nred ** 3 / 3.0 + 2.0 * nred ** 2
+        flops = info.get("eeq_flops", nred ** 3 / 3.0 + 2.0 * nred ** 2)
         bound, unit, peak = "fp64", "TFLOP/s", fp64_peak
         achieved = flops / (ms * 1e-3) / 1e12
     elif name == "eeq_matrix":
@@ -209,14 +214,17 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def measure(args, precision, Z, X, torch, dist, world, local):
-    """Device-timed and end-to-end throughput of one precision form on the workload."""
+def measure(args, precision, Z, X, torch, dist, world, local, mols=None):
+    """Device-timed and end-to-end throughput of one precision form on the workload
+    (molecule evaluations per second; a batch handle evaluates all molecules per step)."""
     from curcuma_b200 import GFNFF, _lib
 
     n = len(Z)
+    nmol = len(mols) if mols else 1
     gpu = GFNFF(precision=0 if precision == "fp64" else 1, device=local)
     t0 = time.perf_counter()
-    if not gpu.setMolecule(Z, X):
+    ok = gpu.setMoleculeBatch(mols) if mols else gpu.setMolecule(Z, X)
+    if not ok:
         raise SystemExit(gpu.getErrorMessage())
     setup_s = time.perf_counter() - t0
     lib, h = gpu._lib, gpu.handle
@@ -224,9 +232,9 @@ def measure(args, precision, Z, X, torch, dist, world, local):
     steps, warm = args.steps, args.warmup
     geoms = torch.tensor(np.stack([perturbed(X, k) / 0.529177210903 for k in range(steps + warm)]),
                          dtype=torch.float64, device="cuda")
-    d_e = torch.zeros(1, dtype=torch.float64, device="cuda")
+    d_e = torch.zeros(nmol, dtype=torch.float64, device="cuda")
     d_g = torch.zeros(3 * n, dtype=torch.float64, device="cuda")
-    d_st = torch.zeros(1, dtype=torch.int32, device="cuda")
+    d_st = torch.zeros(nmol, dtype=torch.int32, device="cuda")
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     P = ctypes.c_void_p
 
@@ -257,7 +265,7 @@ def measure(args, precision, Z, X, torch, dist, world, local):
             events[k][1].synchronize()
             lib.gfnff_phase_times(h, buf, len(buf))
             phases += np.array(buf[:])
-            worst = max(worst, int(d_st.item()))
+            worst = max(worst, int(d_st.max().item()))
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
@@ -270,16 +278,17 @@ def measure(args, precision, Z, X, torch, dist, world, local):
     lib.gfnff_set_phase_timing(h, 0)
     # end to end through the host C ABI: host coordinates in, energy + gradient out
     hostX = [perturbed(X, 5000 + k) for k in range(steps)]
+    evaluate = gpu.calculateEnergyBatch if mols else (lambda: gpu.calculateEnergy(True))
     for k in range(min(3, warm)):
         gpu.updateGeometry(perturbed(X, 4000 + k))
-        gpu.calculateEnergy(True)
+        evaluate()
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
     t = time.perf_counter()
     for k in range(steps):
         gpu.updateGeometry(hostX[k])
-        gpu.calculateEnergy(True)
+        evaluate()
         if gpu.hasError():
             raise SystemExit(gpu.getErrorMessage())
     e2e_s = time.perf_counter() - t
@@ -288,11 +297,36 @@ def measure(args, precision, Z, X, torch, dist, world, local):
         tt = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         e2e_s = float(tt.item())
-    return {"gpu": gpu, "value": world * steps / (total_ms * 1e-3), "total_ms": total_ms, "step_ms": step_ms,
+    return {"gpu": gpu, "value": world * nmol * steps / (total_ms * 1e-3), "total_ms": total_ms, "step_ms": step_ms,
             "phase_avg": {k: v / steps for k, v in zip(_lib.PHASES, phases)}, "status": worst,
-            "e2e": {"value": world * steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 3 * n * 8,
-                    "d2h_bytes_per_step": (3 * n + 14) * 8 + 4},
+            "e2e": {"value": world * nmol * steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 3 * n * 8,
+                    "d2h_bytes_per_step": (3 * n + 16 * nmol) * 8 + 4 * nmol},
             "clocks": clk, "setup_s": setup_s, "solver": gpu.eeqSolver()}
+
+
+def per_molecule_loop(mols, local):
+    """The plain FP64 form called one molecule at a time through the host C ABI (one
+    handle per molecule, set up beforehand): the way a per-molecule loop over a conformer
+    set runs without batching."""
+    from curcuma_b200 import GFNFF
+
+    handles = []
+    for z, x in mols:
+        g = GFNFF(device=local)
+        if not g.setMolecule(z, x):
+            raise SystemExit(g.getErrorMessage())
+        handles.append((g, x))
+    for g, x in handles:
+        g.calculateEnergy(True)
+    t = time.perf_counter()
+    for k, (g, x) in enumerate(handles):
+        g.updateGeometry(perturbed(x, 7000 + k))
+        g.calculateEnergy(True)
+    dt = time.perf_counter() - t
+    for g, _ in handles:
+        g.close()
+    return {"value": len(mols) / dt, "unit": UNIT, "seconds": dt,
+            "what": "one host-API E+grad call per molecule, FP64, every molecule once"}
 
 
 def run_ours(args):
@@ -307,11 +341,13 @@ def run_ours(args):
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
-    desc, Z, X = workload(args.config)
+    wl = workload(args.config)
+    desc, Z, X = wl[:3]
+    mols = wl[3] if len(wl) > 3 else None
     n = len(Z)
     # headline: the requested form; the other form is measured beside it
     forms = [args.precision] + [p for p in ("mixed", "fp64") if p != args.precision]
-    res = {p: measure(args, p, Z, X, torch, dist, world, local) for p in forms}
+    res = {p: measure(args, p, Z, X, torch, dist, world, local, mols) for p in forms}
     main = res[args.precision]
     gpu = main["gpu"]
     natoms, nfrag = gpu.sizes()
@@ -321,25 +357,40 @@ def run_ours(args):
     for p in ("mixed", "fp64"):
         g = res[p]["gpu"]
         g.updateGeometry(Xc)
-        em.append(g.calculateEnergy(True))
+        em.append(np.atleast_1d(g.calculateEnergyBatch()[0] if mols else g.calculateEnergy(True)))
         ef.append(g.getGradient())
-    err = {"dE_eh": abs(em[0] - em[1]), "max_dF_eh_per_bohr": float(np.abs(ef[0] - ef[1]).max())}
-    counts = {k: len(gpu.topology(kind, w)) for k, kind, w in
-              [("bonds", 0, 2), ("angles", 1, 3), ("torsions", 2, 4), ("inversions", 3, 4), ("hbonds", 6, 4),
-               ("xbonds", 7, 3), ("atm", 12, 3), ("batm", 13, 3)]}
+    err = {"dE_eh": float(np.abs(em[0] - em[1]).max()), "max_dF_eh_per_bohr": float(np.abs(ef[0] - ef[1]).max())}
+    if mols:
+        counts = {"molecules": len(mols)}
+        loop = per_molecule_loop(mols, local)
+    else:
+        counts = {k: len(gpu.topology(kind, w)) for k, kind, w in
+                  [("bonds", 0, 2), ("angles", 1, 3), ("torsions", 2, 4), ("inversions", 3, 4), ("hbonds", 6, 4),
+                   ("xbonds", 7, 3), ("atm", 12, 3), ("batm", 13, 3)]}
     # kernels of this library per step: positions, cn, d4w, eeq matrix, rhs, solve (+info),
     # expand, repulsion, pairs, post, chain, outputs, finish, and one per non-empty term list
     fixed = 13 + (1 if main["solver"] in ("pcg", "tiled") else 0)
-    launches = fixed + sum(1 for k in ("bonds", "angles", "torsions", "inversions", "hbonds", "xbonds", "atm", "batm")
-                           if counts[k] > 0)
+    launches = fixed + (8 if mols else
+                        sum(1 for k in ("bonds", "angles", "torsions", "inversions", "hbonds", "xbonds", "atm", "batm")
+                            if counts[k] > 0))
     if rank != 0:
         if world > 1:
             dist.destroy_process_group()
         return
-    nc, nd = pair_counts(Z, X)
-    hbs = gpu.topology(6, 4)
+    if mols:
+        nc = nd = 0
+        for z, x in mols:
+            a_, b_ = pair_counts(z, x)
+            nc += a_
+            nd += b_
+        hbs = []
+    else:
+        nc, nd = pair_counts(Z, X)
+        hbs = gpu.topology(6, 4)
     info = {"n": n, "nred": n - nfrag, "config": args.config, "coulomb_pairs": nc, "disp_pairs": nd,
             "bytes_hbonds": len(hbs) * (19 * 8 + 3 * 48 + 2 * 48)}
+    if mols:   # block-diagonal EEQ: one reduced system per molecule (one fragment each)
+        info["eeq_flops"] = sum((len(z) - 1) ** 3 / 3.0 + 2.0 * (len(z) - 1) ** 2 for z, _ in mols)
     hbm_peak, hbm_src = measured_peaks()
     fp64_peak = gpu._lib.gfnff_fma_peak_tflops(local, 1)
     roof = roofline(main["phase_avg"], info, fp64_peak, hbm_peak, hbm_src)
@@ -362,6 +413,9 @@ def run_ours(args):
             "mixed_vs_fp64": res["mixed"]["value"] / res["fp64"]["value"],
             "mixed_error_vs_fp64": err,
             "pairs": {"coulomb": nc, "dispersion": nd}, "terms": counts, "clocks": main["clocks"]}
+    if mols:
+        line["per_molecule_loop_fp64"] = loop
+        line["batch_vs_loop"] = main["value"] / loop["value"]
     if world == 1 and not args.no_cpu_baseline:
         rate, dt = cpu_oracle_rate(Z, X, 2 if n >= 2000 else 5, 1)
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",

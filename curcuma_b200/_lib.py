@@ -20,7 +20,8 @@ EXPORTED = ["gfnff_default_options", "gfnff_create", "gfnff_setup", "gfnff_energ
             "gfnff_energy_and_gradient_device", "gfnff_stream", "gfnff_charges",
             "gfnff_coordination_numbers", "gfnff_get_topology", "gfnff_sizes", "gfnff_last_error",
             "gfnff_destroy", "gfnff_set_phase_timing", "gfnff_phase_times", "gfnff_fma_peak_tflops",
-            "gfnff_eeq_charges_noalloc", "gfnff_eeq_solver", "gfnff_eeq_iterations"]
+            "gfnff_eeq_charges_noalloc", "gfnff_eeq_solver", "gfnff_eeq_iterations", "gfnff_setup_batch",
+            "gfnff_energy_and_gradient_batch"]
 PHASES = ["positions", "cn", "d4_weights", "eeq_matrix", "eeq_rhs", "eeq_solve", "bonded",
           "hbonds", "repulsion", "pairs", "post_chain", "finish"]
 
@@ -66,6 +67,8 @@ def load():
     lib.gfnff_eeq_solver.argtypes = [c_v]
     lib.gfnff_eeq_solver.restype = ctypes.c_char_p
     lib.gfnff_eeq_iterations.argtypes = [c_v]
+    lib.gfnff_setup_batch.argtypes = [c_v, c_i, P(c_i), P(c_i), P(c_d), P(c_i)]
+    lib.gfnff_energy_and_gradient_batch.argtypes = [c_v, P(c_d), P(c_d), P(c_d), P(c_i)]
     for name in EXPORTED:
         if name not in ("gfnff_default_options", "gfnff_stream", "gfnff_last_error", "gfnff_fma_peak_tflops",
                         "gfnff_eeq_solver"):

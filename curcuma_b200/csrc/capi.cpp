@@ -21,6 +21,10 @@ struct gfnff_handle {
     gfnff_options opt{};
     std::unique_ptr<Engine> eng;
     Model model;
+    std::vector<Model> batch;       // models of a batch handle (gfnff_setup_batch)
+    int nmol = 0;                   // 0: single molecule
+    int natoms = 0;                 // all atoms of the handle
+    std::vector<double> pin_terms;  // 16 per molecule
     bool ready = false;
     std::string err;
     std::vector<double> hb_ref;    // bohr, geometry of the last HB/XB detection
@@ -105,7 +109,95 @@ gfnff_status gfnff_setup(gfnff_handle* h, int n, const int* Z, const double* xyz
         return fail(h, GFNFF_CUDA_ERROR, e.what());
     }
     h->hb_ref = h->model.xyz_setup;
+    h->nmol = 0;
+    h->natoms = n;
+    h->batch.clear();
     h->ready = true;
+    return GFNFF_OK;
+}
+
+gfnff_status gfnff_setup_batch(gfnff_handle* h, int nmol, const int* natoms, const int* Z, const double* xyz,
+                               const int* charges)
+{
+    if (!h) return fail(nullptr, GFNFF_INVALID_ARG, "handle is NULL");
+    if (nmol <= 0 || !natoms || !Z || !xyz) return fail(h, GFNFF_INVALID_ARG, "invalid batch");
+    std::vector<long> off(nmol + 1, 0);
+    for (int m = 0; m < nmol; ++m) {
+        if (natoms[m] <= 0) return fail(h, GFNFF_INVALID_ARG, "molecule without atoms");
+        off[m + 1] = off[m] + natoms[m];
+    }
+    if (off[nmol] > (1l << 30)) return fail(h, GFNFF_INVALID_ARG, "batch too large");
+    h->ready = false;
+    std::vector<Model> models(nmol);
+    std::vector<std::string> errs(nmol);
+    SetupOptions so;
+    so.hbond = h->opt.hbond != 0;
+#pragma omp parallel for schedule(dynamic)
+    for (int m = 0; m < nmol; ++m) {
+        try {
+            models[m] = build_model(natoms[m], Z + off[m], xyz + 3 * off[m], charges ? charges[m] : 0, so);
+        } catch (const std::exception& e) {
+            errs[m] = e.what();
+        }
+    }
+    for (int m = 0; m < nmol; ++m)
+        if (!errs[m].empty()) return fail(h, GFNFF_SETUP_FAILED, "molecule " + std::to_string(m) + ": " + errs[m]);
+    const int n = (int)off[nmol];
+    try {
+        std::vector<const Model*> ptr(nmol);
+        for (int m = 0; m < nmol; ++m) ptr[m] = &models[m];
+        h->eng->upload_batch(ptr);
+        if (h->pin_xyz) cudaFreeHost(h->pin_xyz);
+        if (h->pin_grad) cudaFreeHost(h->pin_grad);
+        h->pin_xyz = h->pin_grad = nullptr;
+        if (!h->pin_out && cudaMallocHost(&h->pin_out, 32 * sizeof(double)) != cudaSuccess)
+            throw std::runtime_error("cudaMallocHost failed");
+        if (!h->pin_status && cudaMallocHost(&h->pin_status, sizeof(int)) != cudaSuccess)
+            throw std::runtime_error("cudaMallocHost failed");
+        if (cudaMallocHost(&h->pin_xyz, 3 * (size_t)n * sizeof(double)) != cudaSuccess ||
+            cudaMallocHost(&h->pin_grad, 3 * (size_t)n * sizeof(double)) != cudaSuccess)
+            throw std::runtime_error("cudaMallocHost failed");
+    } catch (const std::exception& e) {
+        return fail(h, GFNFF_CUDA_ERROR, e.what());
+    }
+    h->batch = std::move(models);
+    h->nmol = nmol;
+    h->natoms = n;
+    h->pin_terms.assign(16 * (size_t)nmol, 0.0);
+    h->ready = true;
+    return GFNFF_OK;
+}
+
+gfnff_status gfnff_energy_and_gradient_batch(gfnff_handle* h, const double* xyz, double* energies, double* grad,
+                                             int* status)
+{
+    if (!h) return fail(nullptr, GFNFF_INVALID_ARG, "handle is NULL");
+    if (!h->ready) return fail(h, GFNFF_NOT_READY, "gfnff_setup_batch has not been called");
+    if (h->nmol == 0) return fail(h, GFNFF_INVALID_ARG, "not a batch handle (use gfnff_energy_and_gradient)");
+    if (!xyz || !energies) return fail(h, GFNFF_INVALID_ARG, "NULL coordinates or energies");
+    const int n = h->natoms, nm = h->nmol;
+    for (long k = 0; k < 3l * n; ++k)
+        if (!std::isfinite(xyz[k])) return fail(h, GFNFF_NONFINITE, "non-finite coordinate");
+    std::vector<int> st(nm, 0);
+    try {
+        std::memcpy(h->pin_xyz, xyz, 3 * (size_t)n * sizeof(double));
+        cudaStream_t s = (cudaStream_t)h->eng->stream();
+        if (cudaMemcpyAsync(h->eng->d_xyz_scratch(), h->pin_xyz, 3 * (size_t)n * sizeof(double),
+                            cudaMemcpyHostToDevice, s) != cudaSuccess)
+            throw std::runtime_error("H2D copy failed");
+        h->eng->enqueue(h->eng->d_xyz_scratch(), false);
+        h->eng->fetch_batch(h->pin_terms.data(), h->pin_grad, st.data());
+    } catch (const std::exception& e) {
+        return fail(h, GFNFF_CUDA_ERROR, e.what());
+    }
+    gfnff_status first = GFNFF_OK;
+    for (int m = 0; m < nm; ++m) {
+        energies[m] = st[m] == GFNFF_OK ? h->pin_terms[16 * (size_t)m + GFNFF_E_TOTAL] : 0.0;
+        if (status) status[m] = st[m];
+        if (st[m] != GFNFF_OK && first == GFNFF_OK) first = (gfnff_status)st[m];
+    }
+    if (grad) std::memcpy(grad, h->pin_grad, 3 * (size_t)n * sizeof(double));
+    if (first != GFNFF_OK) return fail(h, first, "at least one molecule failed (see status)");
     return GFNFF_OK;
 }
 
@@ -115,6 +207,7 @@ gfnff_status gfnff_energy_and_gradient(gfnff_handle* h, const double* xyz, doubl
     if (!h) return fail(nullptr, GFNFF_INVALID_ARG, "handle is NULL");
     if (!h->ready) return fail(h, GFNFF_NOT_READY, "gfnff_setup has not been called");
     if (!xyz || !energy) return fail(h, GFNFF_INVALID_ARG, "NULL coordinates or energy");
+    if (h->nmol) return fail(h, GFNFF_INVALID_ARG, "batch handle (use gfnff_energy_and_gradient_batch)");
     const int n = h->model.n;
     for (int k = 0; k < 3 * n; ++k)
         if (!std::isfinite(xyz[k])) return fail(h, GFNFF_NONFINITE, "non-finite coordinate");
@@ -175,17 +268,14 @@ gfnff_status gfnff_energy_and_gradient_device(gfnff_handle* h, const double* d_x
     if (!h->ready) return fail(h, GFNFF_NOT_READY, "gfnff_setup has not been called");
     if (!d_xyz) return fail(h, GFNFF_INVALID_ARG, "NULL coordinates");
     try {
-        h->eng->enqueue(d_xyz, true);
+        h->eng->enqueue(d_xyz, true, d_energy);
         cudaStream_t s = (cudaStream_t)h->eng->stream();
-        const int n = h->model.n;
-        if (d_energy &&
-            cudaMemcpyAsync(d_energy, h->eng->d_terms() + GFNFF_E_TOTAL, sizeof(double), cudaMemcpyDeviceToDevice, s) != cudaSuccess)
-            throw std::runtime_error("D2D copy failed");
+        const int n = h->natoms;
         if (d_grad &&
             cudaMemcpyAsync(d_grad, h->eng->d_grad(), 3 * (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, s) != cudaSuccess)
             throw std::runtime_error("D2D copy failed");
-        if (d_status &&
-            cudaMemcpyAsync(d_status, h->eng->d_status(), sizeof(int), cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+        if (d_status && cudaMemcpyAsync(d_status, h->eng->d_status(), sizeof(int) * std::max(1, h->nmol),
+                                        cudaMemcpyDeviceToDevice, s) != cudaSuccess)
             throw std::runtime_error("D2D copy failed");
     } catch (const std::exception& e) {
         return fail(h, GFNFF_CUDA_ERROR, e.what());
@@ -201,7 +291,7 @@ static gfnff_status copy_atoms(gfnff_handle* h, const double* dsrc, double* out)
     if (!h->ready) return fail(h, GFNFF_NOT_READY, "gfnff_setup has not been called");
     if (!out) return fail(h, GFNFF_INVALID_ARG, "NULL output");
     cudaStream_t s = (cudaStream_t)h->eng->stream();
-    if (cudaMemcpyAsync(out, dsrc, (size_t)h->model.n * sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+    if (cudaMemcpyAsync(out, dsrc, (size_t)h->natoms * sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
         cudaStreamSynchronize(s) != cudaSuccess)
         return fail(h, GFNFF_CUDA_ERROR, "D2H copy failed");
     return GFNFF_OK;
@@ -214,6 +304,7 @@ gfnff_status gfnff_get_topology(gfnff_handle* h, int kind, int* out, long cap, l
 {
     if (!h) return fail(nullptr, GFNFF_INVALID_ARG, "handle is NULL");
     if (!h->ready) return fail(h, GFNFF_NOT_READY, "gfnff_setup has not been called");
+    if (h->nmol && kind != 4) return fail(h, GFNFF_INVALID_ARG, "topology lists of batch handles: kind 4 only");
     const Model& m = h->model;
     std::vector<int> v;
     long cnt = 0;
@@ -247,8 +338,13 @@ gfnff_status gfnff_sizes(gfnff_handle* h, int* natoms, int* nfrag)
 {
     if (!h) return fail(nullptr, GFNFF_INVALID_ARG, "handle is NULL");
     if (!h->ready) return fail(h, GFNFF_NOT_READY, "gfnff_setup has not been called");
-    if (natoms) *natoms = h->model.n;
-    if (nfrag) *nfrag = h->model.nfrag;
+    int nf = h->model.nfrag;
+    if (h->nmol) {
+        nf = 0;
+        for (const auto& m : h->batch) nf += m.nfrag;
+    }
+    if (natoms) *natoms = h->natoms;
+    if (nfrag) *nfrag = nf;
     return GFNFF_OK;
 }
 

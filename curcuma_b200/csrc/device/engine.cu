@@ -183,6 +183,10 @@ struct Engine::Impl {
     DBuf<double> q0;
     int nq = 0;
     long long msize = 0;
+    // batched EEQ (k_eeq_batch): molecules by decreasing size, work counter, launch shape
+    DBuf<int> border, bnext;
+    int batch_smem_max = 0, batch_grid = 1;
+    size_t batch_smem = 0;
     // bonded lists
     DBuf<int> b_i, b_j, b_h, b_off, b_hb;
     DBuf<double> b_fc, b_al, b_r0i, b_r0j, b_cki, b_ckj, b_sh, b_ff;
@@ -510,7 +514,7 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
             }
             const int nr = (int)r2a.size() - roff.back();
             moff.push_back(ms);
-            ms += (long long)nr * nr;
+            ms += (long long)(nr + 1) * nr;   // only used by molecules beyond the shared-memory path
             roff.push_back((int)r2a.size());
         }
         std::vector<int> off(nf + 1, 0), fa(n);
@@ -523,6 +527,43 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
         P.anchor.upload(anchor); P.atom2red.upload(a2r); P.red2atom.upload(r2a);
         P.frag_off.upload(off); P.frag_atoms.upload(fa); P.q0.upload(q0); P.qlist.upload(ql);
         P.roff.upload(roff); P.moff.upload(moff);
+        if (nm > 1) {
+            std::vector<int> ord(nm);
+            std::iota(ord.begin(), ord.end(), 0);
+            std::stable_sort(ord.begin(), ord.end(),
+                             [&](int x, int y) { return roff[x + 1] - roff[x] > roff[y + 1] - roff[y]; });
+            P.border.upload(ord);
+            P.bnext.alloc(1);
+            // shared-memory path: staged atoms + packed (nr+1) x nr matrix + two vectors
+            // within ~210 KB
+            const long long budget = 210 * 1024 / 8 - kStageDoubles - kStageInts / 2;
+            int smax = 0;
+            while ((long long)(smax + 1) * (smax + 4) / 2 + 2 * (smax + 1) + 1 <= budget) ++smax;
+            int big = 0;
+            for (int m = 0; m < nm; ++m) big = std::max(big, roff[m + 1] - roff[m]);
+            const int fit = std::min(big, smax);
+            P.batch_smem_max = smax;
+            int bigatoms = 0;
+            for (int m = 0; m < nm; ++m) bigatoms = std::max(bigatoms, mols[m]->n);
+            if (bigatoms > kStageAtoms)
+                throw std::runtime_error("batch: molecules of at most " + std::to_string(kStageAtoms) + " atoms");
+            // the two-stage path for larger molecules holds its first s = nr - smax columns
+            // (rows c..nr) and later the trailing block in turn; both must fit the budget
+            if (big > smax) {
+                const long long sp = big - smax;
+                if (sp * (big + 1) - sp * (sp - 1) / 2 > budget)
+                    throw std::runtime_error("batch: molecule too large for the batched EEQ");
+            }
+            P.batch_smem = ((size_t)kStageDoubles + kStageInts / 2 +
+                            (big > smax ? (size_t)budget : (size_t)fit * (fit + 3) / 2 + 2 * (size_t)(fit + 1) + 2)) *
+                           8;
+            CK(cudaFuncSetAttribute((const void*)k_eeq_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)P.batch_smem));
+            int per_sm = 0, nsm = 0;
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)k_eeq_batch, 512, P.batch_smem));
+            CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, P.opt.device));
+            P.batch_grid = std::max(1, std::min(nm, per_sm * nsm));
+        }
     }
     // ---- term lists (internal indices) ----
     {
@@ -874,7 +915,7 @@ int Engine::eeq_iterations()
     return it;
 }
 
-void Engine::enqueue(const double* d_xyz, bool bohr)
+void Engine::enqueue(const double* d_xyz, bool bohr, double* d_energies)
 {
     Impl& P = *p_;
     cudaStream_t s = P.stream;
@@ -929,8 +970,10 @@ void Engine::enqueue(const double* d_xyz, bool bohr)
     } else {
         P.mark(4);
         P.mark(5);
-        EEQBatch B{P.roff.p, P.moff.p, P.red2atom.p, P.anchor.p, P.qlist.p, P.nq, P.q0.p, P.M.p, P.bvec.p, P.info.p};
-        k_eeq_batch<<<P.nmol, 256, 0, s>>>(V, B);
+        CK(cudaMemsetAsync(P.bnext.p, 0, sizeof(int), s));
+        EEQBatch B{P.roff.p, P.moff.p, P.border.p, P.nmol, P.bnext.p, P.batch_smem_max, P.red2atom.p, P.anchor.p,
+                   P.qlist.p, P.nq, P.q0.p, P.M.p, P.bvec.p, P.info.p};
+        k_eeq_batch<<<P.batch_grid, 512, P.batch_smem, s>>>(V, B);
     }
     const double* ysol = P.bvec.p;
     if (P.nmol == 1 && !P.use_lu && P.solver == Impl::SOLVE_TILED) ysol = P.ysol.p;
@@ -966,7 +1009,7 @@ void Engine::enqueue(const double* d_xyz, bool bohr)
     k_cn_chain<double><<<tgrid, kTile, 0, s>>>(V, P.nsplit);
     P.mark(11);
     k_outputs<<<nblk(n), kBlock, 0, s>>>(V, P.gout.p, P.qout.p, P.cnout.p, P.bad.p);
-    k_finish<<<nblk(P.nmol), kBlock, 0, s>>>(V, (P.nred > 0 || P.nmol > 1) ? P.info.p : nullptr, P.bad.p, P.e0.p, nullptr);
+    k_finish<<<nblk(P.nmol), kBlock, 0, s>>>(V, (P.nred > 0 || P.nmol > 1) ? P.info.p : nullptr, P.bad.p, P.e0.p, d_energies);
     P.mark(12);
     CK(cudaGetLastError());
 }

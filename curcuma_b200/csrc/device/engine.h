@@ -34,7 +34,8 @@ public:
     // Enqueues one energy+gradient evaluation.  xyz is N*3 doubles (all atoms of the
     // batch in upload order), device pointer, in bohr when bohr=true else Angstrom.
     // Results stay on the device (below), in the caller's atom order.
-    void enqueue(const double* d_xyz, bool bohr);
+    // d_energies (optional, device): total energy of every molecule (nmol doubles).
+    void enqueue(const double* d_xyz, bool bohr, double* d_energies = nullptr);
 
     // device result buffers of the last enqueue
     const double* d_terms() const;     // 16 doubles per molecule (kNumTerms used)

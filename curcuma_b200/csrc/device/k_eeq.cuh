@@ -96,90 +96,268 @@ __global__ void k_eeq_expand(View V, const double* q0, const int* atom2red, cons
 }
 
 // ------------------------------------------------------------------------------------
-// Batched block-diagonal EEQ: one block per molecule builds its reduced matrix (column-
-// major lower triangle at M + moff[m]), factors it (right-looking Cholesky) and solves
-// for y in place of b.  info[m] = 1 when the molecule's matrix is not positive definite.
+// Batched block-diagonal EEQ.  One block per SM takes molecules from a work queue
+// (largest first, so the long factorisations start early) and solves each molecule's
+// reduced system on its own:
+//   * the matrix with the right-hand side appended as row nr is built from the geometry
+//     straight into shared memory, packed by columns (column c holds rows c..nr), so
+//     factoring it also yields z = L^-1 b in row nr;
+//   * right-looking Cholesky with two block barriers per column: every thread computes
+//     the pivot 1/sqrt(a_kk) itself, scales its share of column k, then the trailing
+//     triangle is updated;
+//   * back substitution L^T y = z by one warp.
+// Molecules too large for shared memory use the same steps on a global-memory copy
+// (column-major, lda = nr + 1).  info[m] = 1 when a pivot is not positive.
 // ------------------------------------------------------------------------------------
 struct EEQBatch {
     const int* roff;        // nmol+1 reduced-index offsets
-    const long long* moff;  // nmol matrix offsets (doubles)
+    const long long* moff;  // nmol offsets of the global-memory copies (doubles)
+    const int* order;       // molecules by decreasing size
+    int nmol;
+    int* next;              // work counter (zeroed before the launch)
+    int smem_max;           // largest nr that fits the shared-memory path
     const int* red2atom;
     const int* anchor;
     const int* qlist;
     int nq;
     const double* q0;
-    double* M;
-    double* b;
+    double* M;              // global copies for the large molecules
+    double* y;              // solution (reduced index space)
     int* info;
 };
 
-__global__ void __launch_bounds__(256) k_eeq_batch(View V, EEQBatch P)
+// one molecule's atoms staged in shared memory: positions, alpha, EEQ diagonal, the
+// reduced index maps (local atom indices) and the rhs row
+struct MolStage {
+    double *x, *y, *z, *al, *ad, *rhs;
+    int *red, *anc;
+};
+constexpr int kStageAtoms = 320;                       // largest molecule of the batch path
+constexpr int kStageDoubles = 5 * kStageAtoms + kStageAtoms;  // + rhs (nr <= atoms)
+constexpr int kStageInts = 2 * kStageAtoms;
+
+__device__ MolStage stage_molecule(const View& V, const EEQBatch& P, int r0, int nr, double* base, int* ibase)
 {
-    const int m = blockIdx.x;
-    const int r0 = P.roff[m], nr = P.roff[m + 1] - r0;
-    double* M = P.M + P.moff[m];
-    double* b = P.b + r0;
-    const int tid = threadIdx.x, nt = blockDim.x, warp = tid >> 5, lane = tid & 31, nw = nt >> 5;
-    __shared__ double inv;
-    __shared__ int bad;
-    if (tid == 0) bad = 0;
-    // build
-    for (long long e = tid; e < (long long)nr * nr; e += nt) {
-        const int c = (int)(e / nr), r = (int)(e % nr);
-        if (r < c) continue;
-        const int k = P.red2atom[r0 + r], l = P.red2atom[r0 + c];
-        const int ak = P.anchor[k], al = P.anchor[l];
-        M[(size_t)c * nr + r] = eeq_a(V, k, l) - eeq_a(V, k, al) - eeq_a(V, ak, l) + eeq_a(V, ak, al);
+    MolStage M{base, base + kStageAtoms, base + 2 * kStageAtoms, base + 3 * kStageAtoms, base + 4 * kStageAtoms,
+               base + 5 * kStageAtoms, ibase, ibase + kStageAtoms};
+    const int2 rg = V.jr[P.red2atom[r0]];
+    for (int i = threadIdx.x; i < rg.y - rg.x; i += blockDim.x) {
+        const double4 p = V.pos[rg.x + i];
+        M.x[i] = p.x; M.y[i] = p.y; M.z[i] = p.z;
+        M.al[i] = V.alpeeq[rg.x + i];
+        M.ad[i] = V.adiag[rg.x + i];
     }
-    for (int r = tid; r < nr; r += nt) {
-        const int k = P.red2atom[r0 + r];
-        b[r] = eeq_rhs_atom(V, k, P.qlist, P.nq, P.q0) - eeq_rhs_atom(V, P.anchor[k], P.qlist, P.nq, P.q0);
+    for (int r = threadIdx.x; r < nr; r += blockDim.x) {
+        const int k = P.red2atom[r0 + r], ak = P.anchor[k];
+        M.red[r] = k - rg.x;
+        M.anc[r] = ak - rg.x;
+        M.rhs[r] = eeq_rhs_atom(V, k, P.qlist, P.nq, P.q0) - eeq_rhs_atom(V, ak, P.qlist, P.nq, P.q0);
     }
     __syncthreads();
-    // factor: column k of L below the diagonal lives at M[k*nr + r], r > k
+    return M;
+}
+
+__device__ __forceinline__ double eeq_a_s(const MolStage& M, int a, int b)
+{
+    if (a == b) return M.ad[a];
+    const double dx = M.x[a] - M.x[b], dy = M.y[a] - M.y[b], dz = M.z[a] - M.z[b];
+    const double d2 = dx * dx + dy * dy + dz * dz;
+    const double s = M.al[a] + M.al[b];
+    if (d2 >= 36.0 * s) return rsqrt(d2);
+    const double r = sqrt(d2);
+    return erf(r / sqrt(s)) / r;
+}
+
+// element (r, c) of [[M, .], [b^T, .]]; r == nr is the rhs row
+__device__ __forceinline__ double eeq_aug(const MolStage& M, int nr, int r, int c)
+{
+    if (r == nr) return M.rhs[c];
+    const int k = M.red[r], ak = M.anc[r], l = M.red[c], al = M.anc[c];
+    return eeq_a_s(M, k, l) - eeq_a_s(M, k, al) - eeq_a_s(M, ak, l) + eeq_a_s(M, ak, al);
+}
+
+// Cholesky + back substitution of an augmented matrix whose column c starts at S + co(c)
+// (element (r, c) at S[co(c) + r - c]); y receives the solution.  Returns false when a
+// pivot is not positive.
+template <class Off>
+__device__ bool chol_aug_solve(double* S, int nr, Off co, double* y, double* lk)
+{
+    __shared__ int bad;
+    if (threadIdx.x == 0) bad = 0;
+    __syncthreads();
+    const int tid = threadIdx.x, nt = blockDim.x, warp = tid >> 5, lane = tid & 31, nw = nt >> 5;
     for (int k = 0; k < nr; ++k) {
-        if (tid == 0) {
-            const double d = M[(size_t)k * nr + k];
-            if (!(d > 0.0)) {
-                bad = 1;
-            } else {
-                const double L = sqrt(d);
-                M[(size_t)k * nr + k] = L;
-                inv = 1.0 / L;
-            }
+        const double d = S[co(k)];
+        if (!(d > 0.0)) {
+            if (tid == 0) bad = 1;
+            break;   // every thread reads the same d: uniform exit
+        }
+        const double inv = 1.0 / sqrt(d);
+        double* ck = S + co(k);
+        for (int r = k + 1 + tid; r <= nr; r += nt) {
+            const double v = ck[r - k] * inv;
+            ck[r - k] = v;
+            lk[r] = v;
         }
         __syncthreads();
-        if (bad) break;
-        for (int r = k + 1 + tid; r < nr; r += nt) M[(size_t)k * nr + r] *= inv;
-        __syncthreads();
+        if (tid == 0) ck[0] = d * inv;
+        // trailing update, one warp per column
         for (int c = k + 1 + warp; c < nr; c += nw) {
-            const double lc = M[(size_t)k * nr + c];
-            for (int r = c + lane; r < nr; r += 32) M[(size_t)c * nr + r] -= M[(size_t)k * nr + r] * lc;
+            const double lc = lk[c];
+            double* cc = S + co(c);
+            for (int r = c + lane; r <= nr; r += 32) cc[r - c] -= lk[r] * lc;
         }
         __syncthreads();
     }
-    if (bad) {
-        if (tid == 0) P.info[m] = 1;
-        return;
-    }
-    // L z = b (column sweep), then L^T y = z (row sweep over the columns of L)
-    for (int k = 0; k < nr; ++k) {
-        if (tid == 0) b[k] /= M[(size_t)k * nr + k];
-        __syncthreads();
-        const double zk = b[k];
-        for (int r = k + 1 + tid; r < nr; r += nt) b[r] -= M[(size_t)k * nr + r] * zk;
-        __syncthreads();
-    }
-    for (int k = nr - 1; k >= 0; --k) {
-        if (warp == 0) {
+    __syncthreads();
+    if (bad) return false;
+    // L^T y = z, z_k = element (nr, k)
+    if (warp == 0) {
+        for (int k = nr - 1; k >= 0; --k) {
+            const double* ck = S + co(k);
             double s = 0.0;
-            for (int r = k + 1 + lane; r < nr; r += 32) s += M[(size_t)k * nr + r] * b[r];
-            for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-            if (lane == 0) b[k] = (b[k] - s) / M[(size_t)k * nr + k];
+            for (int r = k + 1 + lane; r < nr; r += 32) s += ck[r - k] * y[r];
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+            if (lane == 0) y[k] = (ck[nr - k] - s) / ck[0];
+            __syncwarp();
+        }
+    }
+    __syncthreads();
+    return true;
+}
+
+struct PackedCols {   // column c of an (nr+1) x nr packed lower matrix
+    int n1;           // nr + 1
+    __device__ __forceinline__ long long operator()(int c) const { return (long long)c * n1 - (long long)c * (c - 1) / 2; }
+};
+struct DenseCols {    // column c of a column-major matrix with leading dimension lda, from row c
+    int lda;
+    __device__ __forceinline__ long long operator()(int c) const { return (long long)c * lda + c; }
+};
+
+// Molecules beyond the shared-memory path, in two stages (s = nr - smem_max):
+//  1. the first s columns (all rows and the rhs row) are built and factored in shared
+//     memory (packed by columns) and copied to the molecule's global scratch G
+//     (column-major, lda = nr + 1);
+//  2. the trailing block, A22 - L21 L21^T with its rhs row, is written to G, read back
+//     into shared memory, factored and back-substituted (y for rows s..nr-1);
+//  3. y for rows 0..s-1: w = z1 - L21^T y2 (parallel), then L11^T y1 = w by one warp.
+__device__ bool chol_two_stage(const EEQBatch& P, const MolStage& MS, int m, int nr, double* S, double* y)
+{
+    const int s = nr - P.smem_max;
+    const int tid = threadIdx.x, nt = blockDim.x, warp = tid >> 5, lane = tid & 31, nw = nt >> 5;
+    double* G = P.M + P.moff[m];
+    const int lda = nr + 1;
+    __shared__ int bad;
+    if (tid == 0) bad = 0;
+    // ---- stage 1: panel columns [0, s), rows c..nr, packed
+    auto po = [&](int c) { return (long long)c * (nr + 1) - (long long)c * (c - 1) / 2; };
+    for (int c = warp; c < s; c += nw)
+        for (int r = c + lane; r <= nr; r += 32) S[po(c) + r - c] = eeq_aug(MS, nr, r, c);
+    __syncthreads();
+    for (int k = 0; k < s; ++k) {
+        const double d = S[po(k)];
+        if (!(d > 0.0)) {
+            if (tid == 0) bad = 1;
+            break;
+        }
+        const double inv = 1.0 / sqrt(d);
+        double* ck = S + po(k);
+        for (int r = k + 1 + tid; r <= nr; r += nt) ck[r - k] *= inv;
+        __syncthreads();
+        if (tid == 0) ck[0] = d * inv;
+        for (int c = k + 1 + warp; c < s; c += nw) {
+            const double lc = ck[c - k];
+            double* cc = S + po(c);
+            for (int r = c + lane; r <= nr; r += 32) cc[r - c] -= ck[r - k] * lc;
         }
         __syncthreads();
     }
-    if (tid == 0) P.info[m] = 0;
+    __syncthreads();
+    if (bad) return false;
+    for (int c = 0; c < s; ++c)
+        for (int r = c + tid; r <= nr; r += nt) G[(size_t)c * lda + r] = S[po(c) + r - c];
+    // ---- stage 2: trailing block A22 - L21 L21^T (rows c..nr of columns c >= s)
+    for (int c = s + warp; c < nr; c += nw)
+        for (int r = c + lane; r <= nr; r += 32) {
+            double a = eeq_aug(MS, nr, r, c);
+            for (int p = 0; p < s; ++p) a -= S[po(p) + r - p] * S[po(p) + c - p];
+            G[(size_t)c * lda + r] = a;
+        }
+    __syncthreads();
+    const int mt = nr - s;
+    const PackedCols co{mt + 1};
+    for (int c = 0; c < mt; ++c)
+        for (int r = c + tid; r <= mt; r += nt) S[co(c) + r - c] = G[(size_t)(s + c) * lda + s + r];
+    __syncthreads();
+    double* lk = S + co(mt);
+    double* ys = lk + mt + 1;
+    if (!chol_aug_solve(S, mt, co, ys, lk)) return false;
+    for (int k = tid; k < mt; k += nt) y[s + k] = ys[k];
+    // ---- stage 3: w_k = z_k - sum_{r >= s} L_rk y_r, then L11^T y1 = w
+    double* w = S;                     // s entries (the trailing factor is no longer needed)
+    double* yt = S + s;                // copy of y[s..nr)
+    for (int k = tid; k < mt; k += nt) yt[k] = ys[k];
+    __syncthreads();
+    for (int k = warp; k < s; k += nw) {
+        double a = 0.0;
+        for (int r = s + lane; r < nr; r += 32) a += G[(size_t)k * lda + r] * yt[r - s];
+        for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+        if (lane == 0) w[k] = G[(size_t)k * lda + nr] - a;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        for (int k = s - 1; k >= 0; --k) {
+            double a = 0.0;
+            for (int r = k + 1 + lane; r < s; r += 32) a += G[(size_t)k * lda + r] * w[r];
+            for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+            if (lane == 0) w[k] = (w[k] - a) / G[(size_t)k * lda + k];
+            __syncwarp();
+        }
+    }
+    __syncthreads();
+    for (int k = tid; k < s; k += nt) y[k] = w[k];
+    return true;
+}
+
+__global__ void __launch_bounds__(512) k_eeq_batch(View V, EEQBatch P)
+{
+    extern __shared__ double S[];
+    __shared__ int mol;
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const int w = atomicAdd(P.next, 1);
+            mol = w < P.nmol ? P.order[w] : -1;
+        }
+        __syncthreads();
+        const int m = mol;
+        if (m < 0) return;
+        const int r0 = P.roff[m], nr = P.roff[m + 1] - r0;
+        double* y = P.y + r0;
+        if (nr == 0) {
+            if (threadIdx.x == 0) P.info[m] = 0;
+            continue;
+        }
+        bool ok;
+        const MolStage MS = stage_molecule(V, P, r0, nr, S, reinterpret_cast<int*>(S + kStageDoubles));
+        double* W = S + kStageDoubles + kStageInts / 2;   // matrix work area
+        if (nr <= P.smem_max) {
+            const PackedCols co{nr + 1};
+            const long long tot = co(nr);   // all entries incl. the rhs row
+            double* lk = W + tot;
+            double* ys = lk + nr + 1;
+            const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+            for (int c = warp; c < nr; c += nw)
+                for (int r = c + lane; r <= nr; r += 32) W[co(c) + r - c] = eeq_aug(MS, nr, r, c);
+            __syncthreads();
+            ok = chol_aug_solve(W, nr, co, ys, lk);
+            for (int k = threadIdx.x; k < nr; k += blockDim.x) y[k] = ys[k];
+        } else {
+            ok = chol_two_stage(P, MS, m, nr, W, y);
+        }
+        if (threadIdx.x == 0) P.info[m] = ok ? 0 : 1;
+    }
 }
 
 }  // namespace

@@ -37,6 +37,7 @@ class GFNFF:
         self._xyz = None
         self._grad = None
         self._terms = np.zeros(_lib.NTERMS)
+        self._nmol = 0
         self._err = ""
 
     # -- ComputationalMethod interface ---------------------------------------------
@@ -75,6 +76,39 @@ class GFNFF:
             return 0.0
         self._err = ""
         return e.value
+
+    # -- batches of independent molecules ----------------------------------------
+    def setMoleculeBatch(self, molecules, charges=None) -> bool:
+        """molecules: sequence of (Z, xyz_angstrom); charges: per molecule or None."""
+        nat = np.array([len(z) for z, _ in molecules], dtype=np.int32)
+        Z = np.ascontiguousarray(np.concatenate([np.asarray(z) for z, _ in molecules]), dtype=np.int32)
+        X = np.ascontiguousarray(np.concatenate([np.asarray(x, dtype=np.float64).reshape(-1, 3)
+                                                 for _, x in molecules]))
+        ch = None if charges is None else np.ascontiguousarray(charges, dtype=np.int32)
+        IP, DP = ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)
+        st = self._lib.gfnff_setup_batch(self._h, len(nat), nat.ctypes.data_as(IP), Z.ctypes.data_as(IP),
+                                         X.ctypes.data_as(DP), None if ch is None else ch.ctypes.data_as(IP))
+        if st != _lib.GFNFF_OK:
+            self._err = self._lib.gfnff_last_error(self._h).decode()
+            return False
+        self._n = len(Z)
+        self._nmol = len(nat)
+        self._xyz = X.copy()
+        self._grad = np.zeros((self._n, 3))
+        self._err = ""
+        return True
+
+    def calculateEnergyBatch(self):
+        """Energies of all molecules (0.0 where a molecule failed) and their status codes."""
+        e = np.zeros(self._nmol)
+        st = np.zeros(self._nmol, dtype=np.int32)
+        DP = ctypes.POINTER(ctypes.c_double)
+        rc = self._lib.gfnff_energy_and_gradient_batch(self._h, self._xyz.ctypes.data_as(DP), e.ctypes.data_as(DP),
+                                                       self._grad.ctypes.data_as(DP),
+                                                       st.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
+        self._err = "" if rc == _lib.GFNFF_OK else \
+            f"{_lib.STATUS_NAMES.get(rc)}: {self._lib.gfnff_last_error(self._h).decode()}"
+        return e, st
 
     def getGradient(self) -> np.ndarray:
         return self._grad.copy()

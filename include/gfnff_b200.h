@@ -66,12 +66,29 @@ gfnff_status gfnff_setup(gfnff_handle* h, int natoms, const int* Z, const double
 gfnff_status gfnff_energy_and_gradient(gfnff_handle* h, const double* xyz_angstrom, double* energy,
                                        double* grad, double* terms);
 
-/* Device-resident variant for MD/optimisation loops and CUDA-graph capture:
- * d_xyz_bohr (N*3 doubles, bohr) and the outputs are device pointers; the call only
- * enqueues work on the handle's stream (no host synchronisation).  d_status receives
- * a gfnff_status code. */
+/* Device-resident variant for MD/optimisation loops: d_xyz_bohr (N*3 doubles, bohr) and
+ * the outputs are device pointers; the call only enqueues work on the handle's stream
+ * (no host synchronisation, no HB/XB list refresh).  d_energy and d_status receive one
+ * value per molecule (nmol of a batch handle, else 1). */
 gfnff_status gfnff_energy_and_gradient_device(gfnff_handle* h, const double* d_xyz_bohr,
                                               double* d_energy, double* d_grad, int* d_status);
+
+/* Batched set-up of nmol independent molecules (conformer batches, the uneven-size
+ * batches curcuma evaluates one molecule at a time in its conformer tools):
+ * natoms[m] atoms each, Z and xyz_angstrom concatenated in molecule order, charges[m]
+ * (NULL = all neutral).  Each molecule gets the full single-molecule set-up
+ * (gfnff_setup), run in parallel on the host; the molecules do not interact.  Replaces
+ * nmol calls of ComputationalMethod::setMolecule. */
+gfnff_status gfnff_setup_batch(gfnff_handle* h, int nmol, const int* natoms, const int* Z,
+                               const double* xyz_angstrom, const int* charges);
+
+/* Energy + gradient of every molecule of a batch handle in one pass (nmol calls of
+ * calculateEnergy + copyGradientTo).  energies: nmol doubles; grad: N*3 (may be NULL);
+ * status: nmol gfnff_status values (may be NULL).  Returns the first failing status (the
+ * failing molecules' energies are 0.0), else GFNFF_OK.  HB/XB lists stay those of the
+ * set-up geometry. */
+gfnff_status gfnff_energy_and_gradient_batch(gfnff_handle* h, const double* xyz_angstrom, double* energies,
+                                             double* grad, int* status);
 
 /* The handle's CUDA stream (a cudaStream_t). */
 void* gfnff_stream(gfnff_handle* h);
