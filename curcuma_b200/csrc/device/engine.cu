@@ -185,6 +185,8 @@ struct Engine::Impl {
     long long msize = 0;
     // batched EEQ (k_eeq_batch): molecules by decreasing size, work counter, launch shape
     DBuf<int> border, bnext;
+    DBuf<int4> bitems;
+    int nbitems = 0;
     int batch_smem_max = 0, batch_grid = 1;
     size_t batch_smem = 0;
     // bonded lists
@@ -534,6 +536,22 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
                              [&](int x, int y) { return roff[x + 1] - roff[x] > roff[y + 1] - roff[y]; });
             P.border.upload(ord);
             P.bnext.alloc(1);
+            // work items: large molecules one per block, small ones in packs of kWarpMols
+            // (one warp each)
+            std::vector<int4> items;
+            for (int k = 0; k < nm;) {
+                const int nr = roff[ord[k] + 1] - roff[ord[k]];
+                if (nr > kWarpMaxRed || mols[ord[k]]->n > kWarpAtoms) {
+                    items.push_back(make_int4(k, 1, 0, 0));
+                    ++k;
+                } else {
+                    const int cnt = std::min(kWarpMols, nm - k);
+                    items.push_back(make_int4(k, cnt, 1, 0));
+                    k += cnt;
+                }
+            }
+            P.bitems.upload(items);
+            P.nbitems = (int)items.size();
             // shared-memory path: staged atoms + packed (nr+1) x nr matrix + two vectors
             // within ~210 KB
             const long long budget = 210 * 1024 / 8 - kStageDoubles - kStageInts / 2;
@@ -557,6 +575,7 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
             P.batch_smem = ((size_t)kStageDoubles + kStageInts / 2 +
                             (big > smax ? (size_t)budget : (size_t)fit * (fit + 3) / 2 + 2 * (size_t)(fit + 1) + 2)) *
                            8;
+            P.batch_smem = std::max<size_t>(P.batch_smem, (size_t)kWarpMols * kWarpRegion * 8);
             CK(cudaFuncSetAttribute((const void*)k_eeq_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)P.batch_smem));
             int per_sm = 0, nsm = 0;
@@ -971,8 +990,8 @@ void Engine::enqueue(const double* d_xyz, bool bohr, double* d_energies)
         P.mark(4);
         P.mark(5);
         CK(cudaMemsetAsync(P.bnext.p, 0, sizeof(int), s));
-        EEQBatch B{P.roff.p, P.moff.p, P.border.p, P.nmol, P.bnext.p, P.batch_smem_max, P.red2atom.p, P.anchor.p,
-                   P.qlist.p, P.nq, P.q0.p, P.M.p, P.bvec.p, P.info.p};
+        EEQBatch B{P.roff.p, P.moff.p, P.border.p, P.bitems.p, P.nbitems, P.bnext.p, P.batch_smem_max, P.red2atom.p,
+                   P.anchor.p, P.qlist.p, P.nq, P.q0.p, P.M.p, P.bvec.p, P.info.p};
         k_eeq_batch<<<P.batch_grid, 512, P.batch_smem, s>>>(V, B);
     }
     const double* ysol = P.bvec.p;

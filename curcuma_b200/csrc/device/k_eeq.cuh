@@ -113,7 +113,8 @@ struct EEQBatch {
     const int* roff;        // nmol+1 reduced-index offsets
     const long long* moff;  // nmol offsets of the global-memory copies (doubles)
     const int* order;       // molecules by decreasing size
-    int nmol;
+    const int4* items;      // work items {first position in order, count, warp mode, 0}
+    int nitems;
     int* next;              // work counter (zeroed before the launch)
     int smem_max;           // largest nr that fits the shared-memory path
     const int* red2atom;
@@ -320,19 +321,100 @@ __device__ bool chol_two_stage(const EEQBatch& P, const MolStage& MS, int m, int
     return true;
 }
 
+// ---- small molecules: one warp each, __syncwarp only --------------------------------
+constexpr int kWarpMols = 8;          // molecules per warp-mode work item
+constexpr int kWarpMaxRed = 70;       // largest reduced system of the warp path
+constexpr int kWarpAtoms = kWarpMaxRed + 1;
+constexpr int kWarpRegion = 7 * kWarpAtoms + kWarpMaxRed * (kWarpMaxRed + 3) / 2 + 2 * kWarpMaxRed + 2;
+
+__device__ void warp_solve(const View& V, const EEQBatch& P, int m, double* R)
+{
+    const int lane = threadIdx.x & 31;
+    const int r0 = P.roff[m], nr = P.roff[m + 1] - r0;
+    if (nr == 0) {
+        if (lane == 0) P.info[m] = 0;
+        return;
+    }
+    MolStage M{R, R + kWarpAtoms, R + 2 * kWarpAtoms, R + 3 * kWarpAtoms, R + 4 * kWarpAtoms, R + 5 * kWarpAtoms,
+               reinterpret_cast<int*>(R + 6 * kWarpAtoms), reinterpret_cast<int*>(R + 6 * kWarpAtoms) + kWarpAtoms};
+    const int2 rg = V.jr[P.red2atom[r0]];
+    for (int i = lane; i < rg.y - rg.x; i += 32) {
+        const double4 p = V.pos[rg.x + i];
+        M.x[i] = p.x; M.y[i] = p.y; M.z[i] = p.z;
+        M.al[i] = V.alpeeq[rg.x + i];
+        M.ad[i] = V.adiag[rg.x + i];
+    }
+    for (int r = lane; r < nr; r += 32) {
+        const int k = P.red2atom[r0 + r], ak = P.anchor[k];
+        M.red[r] = k - rg.x;
+        M.anc[r] = ak - rg.x;
+        M.rhs[r] = eeq_rhs_atom(V, k, P.qlist, P.nq, P.q0) - eeq_rhs_atom(V, ak, P.qlist, P.nq, P.q0);
+    }
+    __syncwarp();
+    double* S = R + 7 * kWarpAtoms;
+    const PackedCols co{nr + 1};
+    double* lk = S + co(nr);
+    double* ys = lk + nr + 1;
+    for (int c = 0; c < nr; ++c)
+        for (int r = c + lane; r <= nr; r += 32) S[co(c) + r - c] = eeq_aug(M, nr, r, c);
+    __syncwarp();
+    bool ok = true;
+    for (int k = 0; k < nr; ++k) {
+        const double d = S[co(k)];
+        if (!(d > 0.0)) {
+            ok = false;
+            break;
+        }
+        const double inv = 1.0 / sqrt(d);
+        double* ck = S + co(k);
+        for (int r = k + 1 + lane; r <= nr; r += 32) {
+            const double v = ck[r - k] * inv;
+            ck[r - k] = v;
+            lk[r] = v;
+        }
+        __syncwarp();
+        if (lane == 0) ck[0] = d * inv;
+        for (int c = k + 1; c < nr; ++c) {
+            const double lc = lk[c];
+            double* cc = S + co(c);
+            for (int r = c + lane; r <= nr; r += 32) cc[r - c] -= lk[r] * lc;
+        }
+        __syncwarp();
+    }
+    if (ok) {
+        for (int k = nr - 1; k >= 0; --k) {
+            const double* ck = S + co(k);
+            double sum = 0.0;
+            for (int r = k + 1 + lane; r < nr; r += 32) sum += ck[r - k] * ys[r];
+            for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+            if (lane == 0) ys[k] = (ck[nr - k] - sum) / ck[0];
+            __syncwarp();
+        }
+        for (int k = lane; k < nr; k += 32) P.y[r0 + k] = ys[k];
+    }
+    if (lane == 0) P.info[m] = ok ? 0 : 1;
+    __syncwarp();
+}
+
 __global__ void __launch_bounds__(512) k_eeq_batch(View V, EEQBatch P)
 {
     extern __shared__ double S[];
-    __shared__ int mol;
+    __shared__ int4 item;
     for (;;) {
         __syncthreads();
         if (threadIdx.x == 0) {
             const int w = atomicAdd(P.next, 1);
-            mol = w < P.nmol ? P.order[w] : -1;
+            item = w < P.nitems ? P.items[w] : make_int4(-1, 0, 0, 0);
         }
         __syncthreads();
-        const int m = mol;
-        if (m < 0) return;
+        const int4 it = item;
+        if (it.x < 0) return;
+        if (it.z) {   // warp mode: warp w solves molecule order[first + w]
+            const int w = threadIdx.x >> 5;
+            if (w < it.y) warp_solve(V, P, P.order[it.x + w], S + (size_t)w * kWarpRegion);
+            continue;
+        }
+        const int m = P.order[it.x];
         const int r0 = P.roff[m], nr = P.roff[m + 1] - r0;
         double* y = P.y + r0;
         if (nr == 0) {
