@@ -261,6 +261,19 @@ struct Engine::Impl {
         CK(cudaLaunchCooperativeKernel((const void*)k_pcg, dim3(pcg_grid), dim3(kPcgThreads), args, pcg_smem, stream));
     }
     bool timing = false;
+    // One evaluation is ~20 kernels and memsets.  Everything after the positions is
+    // captured once as a CUDA graph and replayed while the model and the solver choice
+    // stay the same (removing the per-launch host cost).  Phase timing (events between
+    // phases, which cannot be timed inside a graph) and GFNFF_GRAPHS=0 use direct
+    // launches, and a capture that fails falls back to them for good.
+    cudaGraphExec_t graph = nullptr;
+    bool graphs_ok = true;
+    DBuf<double> etot;   // molecule totals of the last evaluation
+    void drop_graphs()
+    {
+        if (graph) cudaGraphExecDestroy(graph);
+        graph = nullptr;
+    }
     cudaEvent_t ev[Engine::kNumPhases + 1] = {};
     void mark(int k)
     {
@@ -321,6 +334,7 @@ std::vector<double> Engine::phase_ms()
 
 Engine::~Engine()
 {
+    p_->drop_graphs();
     for (auto& e : p_->ev)
         if (e) cudaEventDestroy(e);
     if (p_->sol) cusolverDnDestroy(p_->sol);
@@ -329,6 +343,7 @@ Engine::~Engine()
 
 void Engine::upload_hbxb(const Model& m)
 {
+    p_->drop_graphs();
     if (p_->nmol != 1) throw std::runtime_error("upload_hbxb: single-molecule engines only");
     Impl& P = *p_;
     auto X = [&](int a) { return P.ix(0, a); };
@@ -398,6 +413,11 @@ void Engine::upload(const Model& m) { upload_batch({&m}); }
 void Engine::upload_batch(const std::vector<const Model*>& mols)
 {
     Impl& P = *p_;
+    P.drop_graphs();
+    {
+        const char* env = std::getenv("GFNFF_GRAPHS");
+        P.graphs_ok = !(env && env[0] == '0');
+    }
     CK(cudaSetDevice(P.opt.device));
     if (mols.empty()) throw std::runtime_error("upload: no molecules");
     const int nm = (int)mols.size();
@@ -745,6 +765,7 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
     // ---- per-step buffers ----
     P.cnraw.alloc(n); P.cn.alloc(n); P.dlog.alloc(n); P.w.alloc((size_t)n * 7); P.dw.alloc((size_t)n * 7);
     P.hg.alloc((size_t)n * K * 7); P.hdg.alloc((size_t)n * K * 7);
+    P.etot.alloc(nm);
     P.q.alloc(n); P.dEdcn.alloc(n); P.v.alloc(n); P.grad.alloc(3 * (size_t)n); P.E.alloc(16 * (size_t)nm);
     P.gout.alloc(3 * (size_t)n); P.qout.alloc(n); P.cnout.alloc(n);
     P.lda = (P.nred + 2) & ~1;   // >= nred + 1 and even: 16-byte aligned columns
@@ -847,6 +868,8 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
     // (eeq_solver.cpp:1448-2086).  Probe once at the setup geometry and keep the
     // choice for this molecule; the host entry point switches later if a geometry
     // turns it.
+    const bool graphs_setting = P.graphs_ok;
+    P.graphs_ok = false;   // probes below run direct (their buffers are temporary)
     if (nm == 1 && P.nred > 0) {
         DBuf<double> x;
         std::vector<double> h(mols[0]->xyz_setup);
@@ -902,11 +925,13 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
             }
         }
     }
+    P.graphs_ok = graphs_setting;
 }
 
 bool Engine::switch_to_lu()
 {
     if (p_->use_lu || p_->nred == 0 || p_->nmol != 1) return false;
+    p_->drop_graphs();
     p_->use_lu = true;
     return true;
 }
@@ -914,6 +939,7 @@ bool Engine::switch_to_lu()
 bool Engine::switch_to_direct()
 {
     if (p_->nmol != 1 || p_->solver != Impl::SOLVE_PCG) return false;
+    p_->drop_graphs();
     p_->solver = Impl::SOLVE_LIBRARY;
     return true;
 }
@@ -934,7 +960,61 @@ int Engine::eeq_iterations()
     return it;
 }
 
+// One evaluation is ~20 kernels and memsets; replaying them as a CUDA graph removes the
+// per-launch host overhead.  A graph is captured per (coordinate buffer, energy buffer,
+// unit) combination and replayed while the model and the solver choice stay the same;
+// phase timing (events between phases) and GFNFF_GRAPHS=0 use direct launches, and a
+// capture that fails falls back to them for good.
 void Engine::enqueue(const double* d_xyz, bool bohr, double* d_energies)
+{
+    Impl& P = *p_;
+    launch_positions(d_xyz, bohr);
+    if (P.timing || !P.graphs_ok) {   // phase events cannot be timed inside a graph
+        launch_body();
+    } else {
+        if (!P.graph) {
+            cudaGraph_t graph = nullptr;
+            bool ok = cudaStreamBeginCapture(P.stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+            if (ok) {
+                try {
+                    launch_body();
+                } catch (const std::exception&) {
+                    ok = false;
+                }
+                const cudaError_t e = cudaStreamEndCapture(P.stream, &graph);
+                ok = ok && e == cudaSuccess && graph;
+                if (ok) ok = cudaGraphInstantiate(&P.graph, graph, 0) == cudaSuccess;
+                if (graph) cudaGraphDestroy(graph);
+            }
+            if (!ok) {
+                cudaGetLastError();   // clear the capture error, stay with direct launches
+                P.graph = nullptr;
+                P.graphs_ok = false;
+            }
+        }
+        if (P.graph) CK(cudaGraphLaunch(P.graph, P.stream));
+        else launch_body();
+    }
+    if (d_energies)
+        CK(cudaMemcpyAsync(d_energies, P.etot.p, (size_t)P.nmol * sizeof(double), cudaMemcpyDeviceToDevice, P.stream));
+    P.mark(12);
+    CK(cudaGetLastError());
+}
+
+// geometry in: caller order -> internal order, the HB refresh metric (direct launches;
+// the only part of an evaluation that touches the caller's coordinate buffer)
+void Engine::launch_positions(const double* d_xyz, bool bohr)
+{
+    Impl& P = *p_;
+    P.mark(0);
+    CK(cudaMemsetAsync(P.msd.p, 0, sizeof(double), P.stream));
+    k_positions<<<nblk(P.n), kBlock, 0, P.stream>>>(P.n, P.perm.p, d_xyz, bohr ? 1.0 : kAngToBohr, P.pos.p,
+                                                   P.hbref.p, P.msd.p);
+}
+
+// everything after the positions, reading and writing engine buffers only, so that it
+// can be captured once as a graph; molecule totals go to etot
+void Engine::launch_body()
 {
     Impl& P = *p_;
     cudaStream_t s = P.stream;
@@ -945,15 +1025,11 @@ void Engine::enqueue(const double* d_xyz, bool bohr, double* d_energies)
     // everywhere else (per-pair float<->double conversions cost more than FP32 saves in
     // the pair and CN-chain kernels) and in every accumulation
     const bool mixed = P.opt.precision == 1;
-    P.mark(0);
     CK(cudaMemsetAsync(P.grad.p, 0, 3 * (size_t)n * sizeof(double), s));
     CK(cudaMemsetAsync(P.dEdcn.p, 0, (size_t)n * sizeof(double), s));
     CK(cudaMemsetAsync(P.cnraw.p, 0, (size_t)n * sizeof(double), s));
-    CK(cudaMemsetAsync(P.msd.p, 0, sizeof(double), s));
     CK(cudaMemsetAsync(P.E.p, 0, 16 * (size_t)P.nmol * sizeof(double), s));
     CK(cudaMemsetAsync(P.bad.p, 0, (size_t)P.nmol * sizeof(int), s));
-    const double scale = bohr ? 1.0 : kAngToBohr;
-    k_positions<<<nblk(n), kBlock, 0, s>>>(n, P.perm.p, d_xyz, scale, P.pos.p, P.hbref.p, P.msd.p);
     P.mark(1);
     (mixed ? k_cn<float> : k_cn<double>)<<<tgrid, kTile, 0, s>>>(V, P.nsplit);
     P.mark(2);
@@ -1028,9 +1104,8 @@ void Engine::enqueue(const double* d_xyz, bool bohr, double* d_energies)
     k_cn_chain<double><<<tgrid, kTile, 0, s>>>(V, P.nsplit);
     P.mark(11);
     k_outputs<<<nblk(n), kBlock, 0, s>>>(V, P.gout.p, P.qout.p, P.cnout.p, P.bad.p);
-    k_finish<<<nblk(P.nmol), kBlock, 0, s>>>(V, (P.nred > 0 || P.nmol > 1) ? P.info.p : nullptr, P.bad.p, P.e0.p, d_energies);
-    P.mark(12);
-    CK(cudaGetLastError());
+    k_finish<<<nblk(P.nmol), kBlock, 0, s>>>(V, (P.nred > 0 || P.nmol > 1) ? P.info.p : nullptr, P.bad.p, P.e0.p,
+                                             P.etot.p);
 }
 
 const double* Engine::d_terms() const { return p_->E.p; }

@@ -76,6 +76,8 @@ public:
     static constexpr int kNumTerms = 14;
 
 private:
+    void launch_positions(const double* d_xyz, bool bohr);
+    void launch_body();
     struct Impl;
     std::unique_ptr<Impl> p_;
 };

@@ -146,3 +146,26 @@ def test_eeq_solvers(solver, system, monkeypatch):
             "peptide": lambda: workloads.solvated_peptide(8, 60, 12)}[system]()
     gpu, _ = _compare(Z, X)
     assert gpu.eeqSolver() == solver
+
+
+@pytest.mark.parametrize("system", ["water200", "alkane"])
+def test_graph_replay_matches_direct_launches(system, monkeypatch):
+    """The step replayed as a captured CUDA graph gives the same results as direct
+    launches (GFNFF_GRAPHS=0), over several geometries."""
+    Z, X = {"water200": lambda: workloads.water_cluster(200, 10),
+            "alkane": lambda: workloads.alkane(64, 1001)}[system]()
+    res = {}
+    for flag in ("1", "0"):
+        monkeypatch.setenv("GFNFF_GRAPHS", flag)
+        g = GFNFF()
+        assert g.setMolecule(Z, X)
+        out = []
+        for k in range(3):
+            g.updateGeometry(X + 0.002 * k)
+            e = g.calculateEnergy(True)
+            assert not g.hasError(), g.getErrorMessage()
+            out.append((e, g.getGradient()))
+        res[flag] = out
+    for (e1, g1), (e0, g0) in zip(res["1"], res["0"]):
+        assert abs(e1 - e0) < 1e-10
+        assert np.abs(g1 - g0).max() < 1e-10
