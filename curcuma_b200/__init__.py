@@ -4,6 +4,6 @@ A drop-in for curcuma's ``-method gfnff -gpu cuda`` path: host setup (topology a
 parameters) once per molecule, then energy + gradient per geometry on the GPU through the
 C ABI declared in ``include/gfnff_b200.h``.
 """
-from .gfnff import FP64, MIXED, GFNFF  # noqa: F401
+from .gfnff import FP64, MIXED, GFNFF, atomic_masses, maxwell_boltzmann  # noqa: F401
 
-__all__ = ["GFNFF", "FP64", "MIXED"]
+__all__ = ["GFNFF", "FP64", "MIXED", "atomic_masses", "maxwell_boltzmann"]

@@ -21,14 +21,14 @@ EXPORTED = ["gfnff_default_options", "gfnff_create", "gfnff_setup", "gfnff_energ
             "gfnff_coordination_numbers", "gfnff_get_topology", "gfnff_sizes", "gfnff_last_error",
             "gfnff_destroy", "gfnff_set_phase_timing", "gfnff_phase_times", "gfnff_fma_peak_tflops",
             "gfnff_eeq_charges_noalloc", "gfnff_eeq_solver", "gfnff_eeq_iterations", "gfnff_setup_batch",
-            "gfnff_energy_and_gradient_batch"]
+            "gfnff_energy_and_gradient_batch", "gfnff_md_nve"]
 PHASES = ["positions", "cn", "d4_weights", "eeq_matrix", "eeq_rhs", "eeq_solve", "bonded",
           "hbonds", "repulsion", "pairs", "post_chain", "finish"]
 
 
 class Options(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int), ("device", ctypes.c_int), ("hbond", ctypes.c_int),
-                ("hb_rmsd_bohr", ctypes.c_double)]
+                ("hb_rmsd_bohr", ctypes.c_double), ("gradient", ctypes.c_int)]
 
 
 _lib = None
@@ -69,6 +69,7 @@ def load():
     lib.gfnff_eeq_iterations.argtypes = [c_v]
     lib.gfnff_setup_batch.argtypes = [c_v, c_i, P(c_i), P(c_i), P(c_d), P(c_i)]
     lib.gfnff_energy_and_gradient_batch.argtypes = [c_v, P(c_d), P(c_d), P(c_d), P(c_i)]
+    lib.gfnff_md_nve.argtypes = [c_v, c_i, c_d, P(c_d), P(c_d), P(c_d), P(c_d), P(c_d)]
     for name in EXPORTED:
         if name not in ("gfnff_default_options", "gfnff_stream", "gfnff_last_error", "gfnff_fma_peak_tflops",
                         "gfnff_eeq_solver"):

@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "device/engine.h"
+#include "device/md.h"
 #include "setup/model.h"
 
 using namespace gfnff;
@@ -59,6 +60,7 @@ void gfnff_default_options(gfnff_options* o)
     o->device = 0;
     o->hbond = 1;
     o->hb_rmsd_bohr = 0.3;
+    o->gradient = GFNFF_GRADIENT_REFERENCE;
 }
 
 gfnff_status gfnff_create(const gfnff_options* opts, gfnff_handle** out)
@@ -70,10 +72,13 @@ gfnff_status gfnff_create(const gfnff_options* opts, gfnff_handle** out)
     else gfnff_default_options(&h->opt);
     if (h->opt.precision != GFNFF_FP64 && h->opt.precision != GFNFF_MIXED)
         return fail(nullptr, GFNFF_INVALID_ARG, "unknown precision");
+    if (h->opt.gradient != GFNFF_GRADIENT_REFERENCE && h->opt.gradient != GFNFF_GRADIENT_EXACT)
+        return fail(nullptr, GFNFF_INVALID_ARG, "unknown gradient mode");
     try {
         EngineOptions eo;
         eo.precision = h->opt.precision;
         eo.device = h->opt.device;
+        eo.exact_gradient = h->opt.gradient == GFNFF_GRADIENT_EXACT;
         h->eng = std::make_unique<Engine>(eo);
     } catch (const std::exception& e) {
         return fail(nullptr, GFNFF_CUDA_ERROR, e.what());
@@ -371,6 +376,56 @@ int gfnff_phase_times(gfnff_handle* h, double* ms, int cap)
         fail(h, GFNFF_CUDA_ERROR, e.what());
         return -1;
     }
+}
+
+gfnff_status gfnff_md_nve(gfnff_handle* h, int nsteps, double dt_fs, double* xyz, double* vel, const double* mass,
+                          double* epot, double* ekin)
+{
+    if (!h) return fail(nullptr, GFNFF_INVALID_ARG, "handle is NULL");
+    if (!h->ready) return fail(h, GFNFF_NOT_READY, "gfnff_setup has not been called");
+    if (nsteps < 0 || !(dt_fs > 0.0) || !xyz || !vel || !mass || !epot || !ekin)
+        return fail(h, GFNFF_INVALID_ARG, "invalid MD arguments");
+    const int n = h->natoms;
+    for (int i = 0; i < n; ++i)
+        if (!(mass[i] > 0.0)) return fail(h, GFNFF_INVALID_ARG, "non-positive mass");
+    try {
+        // chunks of 100 steps; between chunks the HB/XB lists are re-detected when the
+        // RMSD-like measure sqrt(sum d^2)/N exceeds the threshold (single molecules)
+        int done = 0, worst = 0;
+        std::vector<double> ep, ek;
+        while (done < nsteps && worst == 0) {
+            const int chunk = std::min(100, nsteps - done);
+            ep.assign(chunk + 1, 0.0);
+            ek.assign(chunk + 1, 0.0);
+            md_nve(*h->eng, chunk, dt_fs, xyz, vel, mass, ep.data(), ek.data(), &worst);
+            if (done == 0) {
+                epot[0] = ep[0];
+                ekin[0] = ek[0];
+            }
+            for (int t = 1; t <= chunk; ++t) {
+                epot[done + t] = ep[t];
+                ekin[done + t] = ek[t];
+            }
+            done += chunk;
+            if (h->nmol == 0 && h->opt.hbond && worst == 0) {
+                double msd = 0.0;
+                h->eng->fetch(nullptr, nullptr, nullptr, &msd);
+                if (std::sqrt(msd) / (double)n > h->opt.hb_rmsd_bohr) {
+                    std::vector<double> xb(3 * (size_t)n);
+                    for (int k = 0; k < 3 * n; ++k) xb[k] = xyz[k] * kAngToBohr;
+                    redetect_hbxb(h->model, xb.data());
+                    h->eng->upload_hbxb(h->model);
+                    h->eng->set_hb_reference(xb.data());
+                    h->hb_ref = xb;
+                }
+            }
+        }
+        for (int t = done + 1; t <= nsteps; ++t) epot[t] = ekin[t] = 0.0;
+        if (worst != 0) return fail(h, (gfnff_status)worst, "MD stopped: evaluation failed");
+    } catch (const std::exception& e) {
+        return fail(h, GFNFF_CUDA_ERROR, e.what());
+    }
+    return GFNFF_OK;
 }
 
 const char* gfnff_eeq_solver(gfnff_handle* h)

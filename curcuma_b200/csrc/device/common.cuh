@@ -240,6 +240,10 @@ struct View {
     double* grad;
     double* E;                // nmol*16 term energies
     int* status;              // nmol
+    // exact-gradient mode (see the gradient options of the C ABI)
+    int exact;                // drop the D4 dC6/dCN term
+    double* cfar;             // n: potential of the Coulomb pairs beyond 100 bohr, or null
+    const double* u;          // n: EEQ charge response, or null
 };
 
 // Adds v to term `term` of molecule `mol` (mol < 0: nothing to add).  Every thread of

@@ -250,13 +250,13 @@ struct Engine::Impl {
     int pcg_grid = 0, pcg_max_iter = 200, pcg_maxrows = 1, pcg_maxinv = 1;
     size_t pcg_smem = 0;
     bool pcg_ready = false;
-    void pcg_launch()
+    void pcg_launch(const double* rhs, double* x, int* inf)
     {
         CK(cudaMemsetAsync(pbar.p, 0, sizeof(unsigned int), stream));
         PCGArgs A;
-        A.M = M.p; A.lda = lda; A.n = nred; A.b = bvec.p; A.x = px.p; A.z = pz.p;
+        A.M = M.p; A.lda = lda; A.n = nred; A.b = rhs; A.x = x; A.z = pz.p;
         A.blocks = pblocks.p; A.boff = pboff.p; A.maxrows = pcg_maxrows; A.maxinv = pcg_maxinv; A.part = ppart.p; A.rblk = prblk.p; A.partial = ppartial.p;
-        A.bar = pbar.p; A.info = info.p; A.iters = piters.p; A.max_iter = pcg_max_iter; A.tol = 1e-12;
+        A.bar = pbar.p; A.info = inf; A.iters = piters.p; A.max_iter = pcg_max_iter; A.tol = 1e-12;
         void* args[] = {&A};
         CK(cudaLaunchCooperativeKernel((const void*)k_pcg, dim3(pcg_grid), dim3(kPcgThreads), args, pcg_smem, stream));
     }
@@ -269,6 +269,10 @@ struct Engine::Impl {
     cudaGraphExec_t graph = nullptr;
     bool graphs_ok = true;
     DBuf<double> etot;   // molecule totals of the last evaluation
+    // exact-gradient mode: EEQ charge response of the Coulomb pairs cut at 100 bohr
+    bool resp_on = false;
+    DBuf<double> cfar, ures, bres, xres;
+    DBuf<int> info3;
     void drop_graphs()
     {
         if (graph) cudaGraphExecDestroy(graph);
@@ -293,6 +297,9 @@ struct Engine::Impl {
         V.zeta = zeta.p; V.szr = szr.p;
         V.cnraw = cnraw.p; V.cn = cn.p; V.dlog = dlog.p; V.w = w.p; V.dw = dw.p; V.hg = hg.p; V.hdg = hdg.p;
         V.q = q.p; V.dEdcn = dEdcn.p; V.v = v.p; V.grad = grad.p; V.E = E.p; V.status = status.p;
+        V.exact = opt.exact_gradient ? 1 : 0;
+        V.cfar = resp_on ? cfar.p : nullptr;
+        V.u = resp_on ? ures.p : nullptr;
         return V;
     }
     // caller index (molecule m, local atom a) -> internal index
@@ -766,6 +773,21 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
     P.cnraw.alloc(n); P.cn.alloc(n); P.dlog.alloc(n); P.w.alloc((size_t)n * 7); P.dw.alloc((size_t)n * 7);
     P.hg.alloc((size_t)n * K * 7); P.hdg.alloc((size_t)n * K * 7);
     P.etot.alloc(nm);
+    {   // charge response only where a pair can exceed the 100 bohr Coulomb cut
+        double ext = 0.0;
+        if (nm == 1) {
+            double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+            for (const auto& p : p0) {
+                const double c[3] = {p.x, p.y, p.z};
+                for (int d = 0; d < 3; ++d) { lo[d] = std::min(lo[d], c[d]); hi[d] = std::max(hi[d], c[d]); }
+            }
+            for (int d = 0; d < 3; ++d) ext += (hi[d] - lo[d]) * (hi[d] - lo[d]);
+        }
+        P.resp_on = P.opt.exact_gradient && nm == 1 && P.nred > 0 && std::sqrt(ext) > 90.0;
+        if (P.resp_on) {
+            P.cfar.alloc(n); P.ures.alloc(n); P.bres.alloc(P.nred); P.xres.alloc(P.nred); P.info3.alloc(1);
+        }
+    }
     P.q.alloc(n); P.dEdcn.alloc(n); P.v.alloc(n); P.grad.alloc(3 * (size_t)n); P.E.alloc(16 * (size_t)nm);
     P.gout.alloc(3 * (size_t)n); P.qout.alloc(n); P.cnout.alloc(n);
     P.lda = (P.nred + 2) & ~1;   // >= nred + 1 and even: 16-byte aligned columns
@@ -1030,6 +1052,7 @@ void Engine::launch_body()
     CK(cudaMemsetAsync(P.cnraw.p, 0, (size_t)n * sizeof(double), s));
     CK(cudaMemsetAsync(P.E.p, 0, 16 * (size_t)P.nmol * sizeof(double), s));
     CK(cudaMemsetAsync(P.bad.p, 0, (size_t)P.nmol * sizeof(int), s));
+    if (P.resp_on) CK(cudaMemsetAsync(P.cfar.p, 0, (size_t)n * sizeof(double), s));
     P.mark(1);
     (mixed ? k_cn<float> : k_cn<double>)<<<tgrid, kTile, 0, s>>>(V, P.nsplit);
     P.mark(2);
@@ -1053,7 +1076,7 @@ void Engine::launch_body()
             if (sv == Impl::SOLVE_TILED) {
                 P.chol_launch();
             } else if (sv == Impl::SOLVE_PCG) {
-                P.pcg_launch();
+                P.pcg_launch(P.bvec.p, P.px.p, P.info.p);
             } else if (sv == Impl::SOLVE_LIBRARY) {
                 CS(cusolverDnDpotrf(P.sol, CUBLAS_FILL_MODE_LOWER, P.nred, P.M.p, P.lda, P.work.p, P.lwork, P.info.p));
                 CS(cusolverDnDpotrs(P.sol, CUBLAS_FILL_MODE_LOWER, P.nred, 1, P.M.p, P.lda, P.bvec.p, P.nred, P.info2.p));
@@ -1073,7 +1096,7 @@ void Engine::launch_body()
     const double* ysol = P.bvec.p;
     if (P.nmol == 1 && !P.use_lu && P.solver == Impl::SOLVE_TILED) ysol = P.ysol.p;
     if (P.nmol == 1 && !P.use_lu && P.solver == Impl::SOLVE_PCG) ysol = P.px.p;
-    k_eeq_expand<<<nblk(n), kBlock, 0, s>>>(V, P.q0.p, P.atom2red.p, P.frag_off.p, P.frag_atoms.p, ysol);
+    k_eeq_expand<<<nblk(n), kBlock, 0, s>>>(V, P.q0.p, P.atom2red.p, P.frag_off.p, P.frag_atoms.p, ysol, P.q.p);
     P.mark(6);
     if (P.nb) {
         BondSoA B{P.nb, P.b_i.p, P.b_j.p, P.b_h.p, P.b_off.p, P.b_hb.p, P.b_fc.p, P.b_al.p,
@@ -1099,6 +1122,22 @@ void Engine::launch_body()
     k_repulsion<double><<<nblk((long)n * 32), kBlock, 0, s>>>(V, P.r_off.p, P.r_j.p, P.r_al.p, P.r_ab.p, P.r_kind.p);
     P.mark(9);
     k_pairs<double><<<tgrid, kTile, 0, s>>>(V, P.nsplit);
+    if (P.resp_on) {
+        // u = B M^-1 B^T w with the factor (or the iteration) of this step's EEQ matrix
+        k_resp_rhs<<<nblk(P.nred), kBlock, 0, s>>>(V, P.red2atom.p, P.anchor.p, P.bres.p);
+        const double* y = P.bres.p;
+        if (P.use_lu) {
+            CS(cusolverDnDgetrs(P.sol, CUBLAS_OP_N, P.nred, 1, P.M.p, P.lda, P.ipiv.p, P.bres.p, P.nred, P.info2.p));
+        } else if (P.solver == Impl::SOLVE_PCG) {
+            P.pcg_launch(P.bres.p, P.xres.p, P.info3.p);
+            k_merge_info<<<1, 1, 0, s>>>(P.info.p, P.info3.p);
+            y = P.xres.p;
+        } else {   // the Cholesky factor (cuSOLVER or the tiled kernel) is in M
+            CS(cusolverDnDpotrs(P.sol, CUBLAS_FILL_MODE_LOWER, P.nred, 1, P.M.p, P.lda, P.bres.p, P.nred, P.info2.p));
+        }
+        k_eeq_expand<<<nblk(n), kBlock, 0, s>>>(V, nullptr, P.atom2red.p, P.frag_off.p, P.frag_atoms.p, y, P.ures.p);
+        k_resp_pairs<<<tgrid, kTile, 0, s>>>(V, P.nsplit);
+    }
     P.mark(10);
     k_post<<<nblk(n), kBlock, 0, s>>>(V);
     k_cn_chain<double><<<tgrid, kTile, 0, s>>>(V, P.nsplit);

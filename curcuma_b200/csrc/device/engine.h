@@ -14,6 +14,7 @@ namespace gfnff {
 struct EngineOptions {
     int precision = 0;      // 0 = FP64, 1 = mixed
     int device = 0;
+    bool exact_gradient = false;   // derivative of the energy instead of curcuma's gradient
 };
 
 class Engine {

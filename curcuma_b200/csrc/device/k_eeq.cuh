@@ -67,6 +67,12 @@ __global__ void k_eeq_rhs(View V, const int* __restrict__ red2atom, const int* _
     if (aug) aug[(size_t)r * lda] = v;
 }
 
+// info = max(info, other) (status of a second solve in the same evaluation)
+__global__ void k_merge_info(int* info, const int* other)
+{
+    if (*other > *info) *info = *other;
+}
+
 // status of the persistent Cholesky: info = 1 not positive definite, 2 a wait gave up
 __global__ void k_chol_info(const int* err, int* info)
 {
@@ -74,15 +80,16 @@ __global__ void k_chol_info(const int* err, int* info)
     *info = (e & 2) ? 2 : ((e & 1) ? 1 : 0);
 }
 
-// q = q0 + B y
+// out = q0 + B y (q0 null: B y)
 __global__ void k_eeq_expand(View V, const double* q0, const int* atom2red, const int* frag_off,
-                             const int* frag_atoms, const double* y)
+                             const int* frag_atoms, const double* y, double* out)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= V.n) return;
+    const double base = q0 ? q0[i] : 0.0;
     const int rr = atom2red[i];
     if (rr >= 0) {
-        V.q[i] = q0[i] + y[rr];
+        out[i] = base + y[rr];
     } else {
         // anchor: minus the sum of its fragment's reduced variables
         const int f = -rr - 1;
@@ -91,8 +98,17 @@ __global__ void k_eeq_expand(View V, const double* q0, const int* atom2red, cons
             const int ra = atom2red[frag_atoms[p]];
             if (ra >= 0) s += y[ra];
         }
-        V.q[i] = q0[i] - s;
+        out[i] = base - s;
     }
+}
+
+// rhs of the charge-response solve, B^T w with w_i = -cfar_i
+__global__ void k_resp_rhs(View V, const int* __restrict__ red2atom, const int* __restrict__ anchor, double* b)
+{
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= V.nred) return;
+    const int k = red2atom[r];
+    b[r] = V.cfar[anchor[k]] - V.cfar[k];
 }
 
 // ------------------------------------------------------------------------------------

@@ -242,7 +242,7 @@ __global__ void __launch_bounds__(kTile) k_pairs(View V, int nsplit)
     const double* g0i = V.g0 + (size_t)ic * V.K * 7;
     const double* dgi = V.hdg + (size_t)ic * V.K * 7;
     const double tsp = 2.0 / 1.772453850905516;
-    double ec = 0.0, ed = 0.0, gx = 0.0, gy = 0.0, gz = 0.0, dcn = 0.0;
+    double ec = 0.0, ed = 0.0, gx = 0.0, gy = 0.0, gz = 0.0, dcn = 0.0, cfar = 0.0;
     for (int t0 = jb; t0 < je; t0 += kTile) {
         __syncthreads();
         const int jl = t0 + threadIdx.x;
@@ -285,6 +285,8 @@ __global__ void __launch_bounds__(kTile) k_pairs(View V, int nsplit)
                     ec += qq * ef / r;
                     f += qq * ((g * exp(-gr * gr) * tsp) / r - ef / d2) / r;
                 }
+            } else if (V.cfar) {
+                cfar += sq[jj] * rsqrt(d2);   // cut pair: its EEQ element is 1/r
             }
             if (d2 <= 2500.0 &&
                 d2_exact(p0i, make_double4(s0x[jj], s0y[jj], s0z[jj], 0.0)) <= 3600.0) {
@@ -299,7 +301,7 @@ __global__ void __launch_bounds__(kTile) k_pairs(View V, int nsplit)
                     d4_pair<R>(d2, g0, dg, sw0, sw, jj, nr, szi, ssz[jj], zi * sze[jj], e, dedr, dc);
                 ed += e;
                 f += dedr;
-                dcn += dc;
+                if (!V.exact) dcn += dc;
             }
             gx += f * dx; gy += f * dy; gz += f * dz;
         }
@@ -309,10 +311,65 @@ __global__ void __launch_bounds__(kTile) k_pairs(View V, int nsplit)
         if (gy != 0.0) atomicAdd(V.grad + 3 * i + 1, gy);
         if (gz != 0.0) atomicAdd(V.grad + 3 * i + 2, gz);
         if (dcn != 0.0) atomicAdd(V.dEdcn + i, dcn);
+        if (cfar != 0.0) atomicAdd(V.cfar + i, cfar);
     }
     const int m = act ? V.mol[i] : -1;
     eadd(V, 0.5 * ec, m, T_COUL);
     eadd(V, 0.5 * ed, m, T_DISP);
+}
+
+// ------------------------------------------------------------------------------------
+// EEQ charge response (exact-gradient mode): with u = B M^-1 B^T w and w = dE/dq of the
+// Coulomb pairs cut at 100 bohr, the gradient gains -sum_ij u_i q_j dA_ij/dr over all
+// pairs (A is the uncut EEQ matrix) and u_i dx_i/dCN_i through the CN chain (k_post).
+// ------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(kTile) k_resp_pairs(View V, int nsplit)
+{
+    __shared__ double sx[kTile], sy[kTile], sz[kTile], sq[kTile], su[kTile], sa[kTile];
+    const int i0 = blockIdx.x * kTile, i = i0 + threadIdx.x;
+    int jb, je;
+    tile_range(V, i0, nsplit, jb, je);
+    const bool act = i < V.n;
+    const int ic = act ? i : i0;
+    const double4 pi = V.pos[ic];
+    const double qi = V.q[ic], ui = V.u[ic], ai = V.alpeeq[ic];
+    const int2 rg = act ? V.jr[i] : make_int2(0, 0);
+    const double tsp = 2.0 / 1.772453850905516;
+    double gx = 0.0, gy = 0.0, gz = 0.0;
+    for (int t0 = jb; t0 < je; t0 += kTile) {
+        __syncthreads();
+        const int jl = t0 + threadIdx.x;
+        if (jl < je) {
+            const double4 p = V.pos[jl];
+            sx[threadIdx.x] = p.x; sy[threadIdx.x] = p.y; sz[threadIdx.x] = p.z;
+            sq[threadIdx.x] = V.q[jl]; su[threadIdx.x] = V.u[jl]; sa[threadIdx.x] = V.alpeeq[jl];
+        }
+        __syncthreads();
+        const int cnt = min(kTile, je - t0);
+        if (!act) continue;
+        for (int jj = 0; jj < cnt; ++jj) {
+            const int j = t0 + jj;
+            if (j == i || j < rg.x || j >= rg.y) continue;
+            const double dx = pi.x - sx[jj], dy = pi.y - sy[jj], dz = pi.z - sz[jj];
+            const double d2 = dx * dx + dy * dy + dz * dz;
+            const double s = ai + sa[jj];
+            double dadr_r;   // dA/dr / r
+            if (d2 >= 36.0 * s) {
+                const double ir = rsqrt(d2);
+                dadr_r = -ir * ir * ir;
+            } else {
+                const double r = sqrt(d2), g = 1.0 / sqrt(s), gr = g * r;
+                dadr_r = ((g * exp(-gr * gr) * tsp) / r - erf(gr) / d2) / r;
+            }
+            const double f = -(ui * sq[jj] + su[jj] * qi) * dadr_r;
+            gx += f * dx; gy += f * dy; gz += f * dz;
+        }
+    }
+    if (act) {
+        if (gx != 0.0) atomicAdd(V.grad + 3 * i, gx);
+        if (gy != 0.0) atomicAdd(V.grad + 3 * i + 1, gy);
+        if (gz != 0.0) atomicAdd(V.grad + 3 * i + 2, gz);
+    }
 }
 
 // ------------------------------------------------------------------------------------
@@ -330,7 +387,9 @@ __global__ void k_post(View V)
             const double chi = V.chi_base[i] + V.cnf[i] * sqrt(cn);
             e = -q * chi + 0.5 * q * q * V.adiag[i];
         }
-        V.v[i] = V.dlog[i] * (V.dEdcn[i] - q * V.cnf[i] / (2.0 * sqrt(cn) + 1e-16));
+        // the EEQ charge response u adds u dx/dCN (exact-gradient mode)
+        const double qe = V.u ? q - V.u[i] : q;
+        V.v[i] = V.dlog[i] * (V.dEdcn[i] - qe * V.cnf[i] / (2.0 * sqrt(cn) + 1e-16));
     }
     eadd(V, e, i < V.n ? V.mol[i] : -1, T_COUL);
 }

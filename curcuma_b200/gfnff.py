@@ -13,13 +13,32 @@ import numpy as np
 
 from . import _lib
 
+# standard atomic weights (amu) of H..Ar, for MD when no masses are given
+_MASS = [1.008, 4.0026, 6.94, 9.0122, 10.81, 12.011, 14.007, 15.999, 18.998, 20.180, 22.990, 24.305, 26.982,
+         28.085, 30.974, 32.06, 35.45, 39.948]
+
+
+def atomic_masses(Z):
+    return np.array([_MASS[z - 1] if 1 <= z <= len(_MASS) else 2.0 * z for z in np.asarray(Z)], dtype=np.float64)
+
+
+def maxwell_boltzmann(masses_amu, temperature_k, seed):
+    """Seeded Maxwell-Boltzmann velocities (Angstrom/fs) without centre-of-mass motion."""
+    rng = np.random.default_rng(seed)
+    kt = 3.166811563e-6 * temperature_k                      # Hartree
+    m = np.asarray(masses_amu, dtype=np.float64) * 1822.888486209  # electron masses
+    v = rng.normal(size=(len(m), 3)) * np.sqrt(kt / m)[:, None]    # bohr / atomic time unit
+    v -= (m[:, None] * v).sum(axis=0) / m.sum()
+    return v * 0.529177210903 * 41.341373335                 # Angstrom / fs
+
+
 FP64 = 0
 MIXED = 1
 
 
 class GFNFF:
     def __init__(self, precision: int = FP64, device: int = 0, hbond: bool = True,
-                 hb_rmsd_bohr: float = 0.3):
+                 hb_rmsd_bohr: float = 0.3, exact_gradient: bool = False):
         self._lib = _lib.load()
         opts = _lib.Options()
         self._lib.gfnff_default_options(ctypes.byref(opts))
@@ -27,6 +46,7 @@ class GFNFF:
         opts.device = device
         opts.hbond = 1 if hbond else 0
         opts.hb_rmsd_bohr = hb_rmsd_bohr
+        opts.gradient = 1 if exact_gradient else 0
         h = ctypes.c_void_p()
         st = self._lib.gfnff_create(ctypes.byref(opts), ctypes.byref(h))
         if st != _lib.GFNFF_OK:
@@ -54,6 +74,7 @@ class GFNFF:
         self._n = len(Z)
         self._xyz = X.copy()
         self._grad = np.zeros((self._n, 3))
+        self._masses = atomic_masses(Z)
         self._err = ""
         return True
 
@@ -109,6 +130,27 @@ class GFNFF:
         self._err = "" if rc == _lib.GFNFF_OK else \
             f"{_lib.STATUS_NAMES.get(rc)}: {self._lib.gfnff_last_error(self._h).decode()}"
         return e, st
+
+    # -- molecular dynamics ------------------------------------------------------
+    def runMD(self, nsteps: int, dt_fs: float, velocities_ang_fs, masses_amu=None):
+        """NVE velocity Verlet from the current geometry; returns (epot, ekin) traces of
+        nsteps + 1 values and updates the geometry and velocities (see velocities())."""
+        X = np.ascontiguousarray(self._xyz, dtype=np.float64).copy()
+        V = np.ascontiguousarray(velocities_ang_fs, dtype=np.float64).reshape(-1, 3).copy()
+        m = np.ascontiguousarray(masses_amu if masses_amu is not None else self._masses, dtype=np.float64)
+        ep = np.zeros(nsteps + 1)
+        ek = np.zeros(nsteps + 1)
+        DP = ctypes.POINTER(ctypes.c_double)
+        st = self._lib.gfnff_md_nve(self._h, int(nsteps), float(dt_fs), X.ctypes.data_as(DP), V.ctypes.data_as(DP),
+                                    m.ctypes.data_as(DP), ep.ctypes.data_as(DP), ek.ctypes.data_as(DP))
+        self._err = "" if st == _lib.GFNFF_OK else \
+            f"{_lib.STATUS_NAMES.get(st)}: {self._lib.gfnff_last_error(self._h).decode()}"
+        self._xyz = X
+        self._vel = V
+        return ep, ek
+
+    def velocities(self) -> np.ndarray:
+        return self._vel.copy()
 
     def getGradient(self) -> np.ndarray:
         return self._grad.copy()

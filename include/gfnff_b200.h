@@ -42,7 +42,17 @@ typedef struct {
     int device;             /* CUDA device ordinal */
     int hbond;              /* 1: hydrogen/halogen bonds on (default) */
     double hb_rmsd_bohr;    /* HB/XB list refresh threshold, default 0.3 */
+    int gradient;           /* GFNFF_GRADIENT_REFERENCE (default) or GFNFF_GRADIENT_EXACT */
 } gfnff_options;
+
+/* Gradient definition.  REFERENCE reproduces curcuma's analytic gradient: it adds the
+ * D4 dC6/dCN chain term although the dispersion energy uses the C6 of the set-up
+ * geometry (ff_workspace_gfnff.cpp:715-772, gfnff_method.cpp:1333-1345), and it treats
+ * the EEQ charges as stationary although the Coulomb pair energy is cut at 100 bohr
+ * while the EEQ matrix is not.  EXACT is the derivative of the same energy: no dC6/dCN
+ * term, plus the charge response of the cut pairs (one extra solve with the EEQ matrix
+ * and one extra pair pass, only when a pair exceeds the cut).  The energy is the same. */
+enum { GFNFF_GRADIENT_REFERENCE = 0, GFNFF_GRADIENT_EXACT = 1 };
 
 typedef struct gfnff_handle gfnff_handle;
 
@@ -89,6 +99,16 @@ gfnff_status gfnff_setup_batch(gfnff_handle* h, int nmol, const int* natoms, con
  * set-up geometry. */
 gfnff_status gfnff_energy_and_gradient_batch(gfnff_handle* h, const double* xyz_angstrom, double* energies,
                                              double* grad, int* status);
+
+/* NVE velocity-Verlet molecular dynamics on the device, the loop of curcuma's SimpleMD
+ * (capabilities/simplemd.cpp:2580-2674) with the energy + gradient step replayed as a
+ * CUDA graph: nsteps steps of dt_fs femtoseconds.  xyz_angstrom and vel (Angstrom/fs,
+ * N*3) are updated in place; mass (N, amu); epot and ekin receive nsteps + 1 energies
+ * (Hartree, entry 0 = start).  The HB/XB lists are re-detected every 100 steps when
+ * sqrt(sum d^2)/N exceeds hb_rmsd_bohr, as in gfnff_energy_and_gradient.  Returns the
+ * first failing evaluation status (the run stops there). */
+gfnff_status gfnff_md_nve(gfnff_handle* h, int nsteps, double dt_fs, double* xyz_angstrom, double* vel,
+                          const double* mass, double* epot, double* ekin);
 
 /* The handle's CUDA stream (a cudaStream_t). */
 void* gfnff_stream(gfnff_handle* h);
