@@ -1,9 +1,9 @@
 #!/usr/bin/env python3
 """GFN-FF energy + gradient throughput on B200.
 
-Default workload: BASELINE config 2, a seeded 1000-water cluster (3000 atoms, 1000
-fragments, 1.0 g/cm^3), FP64 form.  One step = one energy + analytic gradient
-evaluation of a fresh geometry (MD-like perturbation of the cluster).
+Default workload: a seeded 1000-water cluster (3000 atoms, 1000 fragments, 1.0 g/cm^3),
+mixed form, with the FP64 form measured beside it.  One step = one energy + analytic
+gradient evaluation of a fresh geometry (MD-like perturbation of the cluster).
 
 * ``value``: evaluations/s with coordinates resident in HBM, through the device entry
   point ``gfnff_energy_and_gradient_device``; each step timed with CUDA events on the
@@ -47,6 +47,9 @@ def parse():
     ap.add_argument("--config", type=int, default=2)
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", action="store_true",
+                    help="only set up the workload and run warmup + steps evaluations through the "
+                         "public API (a short command for ncu captures); prints one line")
     return ap.parse_args()
 
 
@@ -494,8 +497,37 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_profile(args):
+    """Set-up plus warmup + steps evaluations of the workload and nothing else: the launch
+    sequence a profiler should see (set-up's solver probes, then the evaluations)."""
+    import torch
+
+    from curcuma_b200 import GFNFF
+
+    torch.cuda.set_device(0)
+    wl = workload(args.config)
+    desc, Z, X = wl[:3]
+    mols = wl[3] if len(wl) > 3 else None
+    g = GFNFF(precision=0 if args.precision == "fp64" else 1, device=0)
+    if not (g.setMoleculeBatch(mols) if mols else g.setMolecule(Z, X)):
+        raise SystemExit(g.getErrorMessage())
+    for k in range(args.warmup + args.steps):
+        g.updateGeometry(perturbed(X, k))
+        if mols:
+            g.calculateEnergyBatch()
+        else:
+            g.calculateEnergy(True)
+        if g.hasError():
+            raise SystemExit(g.getErrorMessage())
+    print(json.dumps({"profile": f"config {args.config}: {desc}", "precision": args.precision,
+                      "evals": args.warmup + args.steps, "eeq_solver": g.eeqSolver()}), flush=True)
+
+
 def main():
     args = parse()
+    if args.profile:
+        run_profile(args)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:

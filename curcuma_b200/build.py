@@ -40,7 +40,8 @@ def _stale(target: Path, deps) -> bool:
 
 
 def _headers():
-    return list(CSRC.rglob("*.h")) + list(CSRC.rglob("*.inc")) + [ROOT / "include" / "gfnff_b200.h"]
+    return (list(CSRC.rglob("*.h")) + list(CSRC.rglob("*.cuh")) + list(CSRC.rglob("*.inc"))
+            + [ROOT / "include" / "gfnff_b200.h"])
 
 
 def build_library(force: bool = False) -> Path:
