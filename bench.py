@@ -314,7 +314,7 @@ def measure(args, precision, Z, X, torch, dist, world, local, mols=None):
             "phase_avg": {k: v / steps for k, v in zip(_lib.PHASES, phases)}, "status": worst,
             "e2e": {"value": world * nmol * steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 3 * n * 8,
                     "d2h_bytes_per_step": (3 * n + 16 * nmol) * 8 + 4 * nmol},
-            "clocks": clk, "setup_s": setup_s, "solver": gpu.eeqSolver()}
+            "clocks": clk, "setup_s": setup_s, "solver": gpu.eeqSolver(), "iters": gpu.eeqIterations()}
 
 
 def per_molecule_loop(mols, local):
@@ -458,6 +458,7 @@ def run_ours(args):
             "data": "synthetic",
             "config": {"workload": f"config {args.config}: {desc}", "natoms": natoms, "nfrag": nfrag,
                        "precision": args.precision, "eeq_solver": main["solver"],
+                       "eeq_iterations_last_step": main["iters"],
                        "l2": "flushed before every timed step (256 MiB write)",
                        "parallelism": f"replicas x{world}", "setup_s": round(main["setup_s"], 3)},
             "e2e": main["e2e"], "gpu_launches": launches * steps, "roofline": roof,

@@ -166,6 +166,11 @@ int pair_splits(int n, int max_range)
 struct Engine::Impl {
     EngineOptions opt;
     cudaStream_t stream = nullptr;
+    // second stream of the evaluation: the terms that do not depend on the charges (HB,
+    // XB, repulsion after the positions; bonded and ATM after the CN) run beside the EEQ
+    // chain and join before the CN chain rule.  GFNFF_STREAMS=1 keeps one stream.
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork0 = nullptr, ev_fork1 = nullptr, ev_join = nullptr;
     cusolverDnHandle_t sol = nullptr;
     int n = 0, nfrag = 0, K = 0, nred = 0, nmol = 0, nsplit = 1;
     // molecule structure and atom order
@@ -250,13 +255,18 @@ struct Engine::Impl {
     int pcg_grid = 0, pcg_max_iter = 200, pcg_maxrows = 1, pcg_maxinv = 1;
     size_t pcg_smem = 0;
     bool pcg_ready = false;
-    void pcg_launch(const double* rhs, double* x, int* inf)
+    // warm[0]: px holds the last converged solution of the main solve, warm[1]: xres of the
+    // response solve; probes (pcg_warm false) start from zero so that their timing is fair
+    DBuf<int> pwarm;
+    bool pcg_warm = false;
+    void pcg_launch(const double* rhs, double* x, int* inf, int slot)
     {
         CK(cudaMemsetAsync(pbar.p, 0, sizeof(unsigned int), stream));
         PCGArgs A;
         A.M = M.p; A.lda = lda; A.n = nred; A.b = rhs; A.x = x; A.z = pz.p;
         A.blocks = pblocks.p; A.boff = pboff.p; A.maxrows = pcg_maxrows; A.maxinv = pcg_maxinv; A.part = ppart.p; A.rblk = prblk.p; A.partial = ppartial.p;
         A.bar = pbar.p; A.info = inf; A.iters = piters.p; A.max_iter = pcg_max_iter; A.tol = 1e-12;
+        A.warm = pcg_warm ? pwarm.p + slot : nullptr;
         void* args[] = {&A};
         CK(cudaLaunchCooperativeKernel((const void*)k_pcg, dim3(pcg_grid), dim3(kPcgThreads), args, pcg_smem, stream));
     }
@@ -310,7 +320,17 @@ Engine::Engine(const EngineOptions& opt) : p_(new Impl)
 {
     p_->opt = opt;
     CK(cudaSetDevice(opt.device));
-    CK(cudaStreamCreateWithFlags(&p_->stream, cudaStreamNonBlocking));
+    int lo = 0, hi = 0;
+    CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+    // the EEQ chain is the critical path: its stream gets the higher priority
+    CK(cudaStreamCreateWithPriority(&p_->stream, cudaStreamNonBlocking, hi));
+    const char* st = std::getenv("GFNFF_STREAMS");
+    if (!(st && !std::strcmp(st, "1"))) {
+        CK(cudaStreamCreateWithPriority(&p_->side, cudaStreamNonBlocking, lo));
+        CK(cudaEventCreateWithFlags(&p_->ev_fork0, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&p_->ev_fork1, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&p_->ev_join, cudaEventDisableTiming));
+    }
     CS(cusolverDnCreate(&p_->sol));
     CS(cusolverDnSetStream(p_->sol, p_->stream));
 }
@@ -345,6 +365,9 @@ Engine::~Engine()
     for (auto& e : p_->ev)
         if (e) cudaEventDestroy(e);
     if (p_->sol) cusolverDnDestroy(p_->sol);
+    for (cudaEvent_t e : {p_->ev_fork0, p_->ev_fork1, p_->ev_join})
+        if (e) cudaEventDestroy(e);
+    if (p_->side) cudaStreamDestroy(p_->side);
     if (p_->stream) cudaStreamDestroy(p_->stream);
 }
 
@@ -820,23 +843,40 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
             CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)k_chol, kCholThreads, P.chol_smem));
             P.chol_grid = std::max(1, std::min(per_sm * nsm, P.chol_ntasks));
         }
-        // block-Jacobi PCG: each fragment's contiguous reduced range in blocks of <= 64
+        // block-Jacobi PCG: one block per fragment (blocks of <= 64 for larger ones).
+        // GFNFF_PCG_BLOCK=g merges runs of consecutive fragments (neighbours in space:
+        // fragments are Morton-ordered) into blocks of up to g unknowns; measured on water
+        // clusters this leaves the iteration count unchanged, so it is off by default.
         P.pcg_ready = false;
         std::vector<int2> blocks;
         {
+            int group = 0;
+            if (const char* e = std::getenv("GFNFF_PCG_BLOCK")) group = std::max(0, std::min(kPcgWarpMax, std::atoi(e)));
             std::vector<int> fr(n);
             const Model& M0 = *mols[0];
             for (int a = 0; a < n; ++a) fr[P.ix(0, a)] = M0.frag[a];
-            int r = 0, i = 0;
+            int r = 0, i = 0, cur0 = 0, cur = 0;
+            auto flush = [&]() {
+                if (cur > 0) blocks.push_back(make_int2(cur0, cur));
+                cur = 0;
+            };
             while (i < n) {
                 int j = i;
                 while (j < n && fr[j] == fr[i]) ++j;
                 const int nr = j - i - 1;   // the fragment's anchor is its first atom
-                for (int c = 0; c < nr; c += kPcgMaxBlock)
-                    blocks.push_back(make_int2(r + c, std::min(kPcgMaxBlock, nr - c)));
+                if (nr > group) {
+                    flush();
+                    for (int c = 0; c < nr; c += kPcgMaxBlock)
+                        blocks.push_back(make_int2(r + c, std::min(kPcgMaxBlock, nr - c)));
+                } else if (nr > 0) {
+                    if (cur + nr > group) flush();
+                    if (cur == 0) cur0 = r;
+                    cur += nr;
+                }
                 r += nr;
                 i = j;
             }
+            flush();
             if (r != P.nred) blocks.clear();   // fragments not contiguous: no PCG
         }
         if (!blocks.empty()) {
@@ -872,7 +912,8 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
                 P.px.alloc(P.nred); P.pz.alloc(P.nred);
                 P.pcg_maxrows = maxrows;
                 P.pcg_maxinv = (int)maxinv;
-                P.ppartial.alloc(4 * (size_t)G); P.pbar.alloc(2 * kBarGen); P.piters.alloc(1);
+                P.ppartial.alloc(4 * (size_t)G); P.pbar.alloc(2 * kBarGen); P.piters.alloc(1); P.pwarm.alloc(2);
+                CK(cudaMemset(P.pwarm.p, 0, 2 * sizeof(int)));
                 CK(cudaMemset(P.pbar.p, 0, 2 * kBarGen * sizeof(unsigned int)));
                 CK(cudaMemset(P.piters.p, 0, sizeof(int)));
                 P.pcg_grid = G;
@@ -892,6 +933,7 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
     // turns it.
     const bool graphs_setting = P.graphs_ok;
     P.graphs_ok = false;   // probes below run direct (their buffers are temporary)
+    P.pcg_warm = false;    // and PCG probes start from zero
     if (nm == 1 && P.nred > 0) {
         DBuf<double> x;
         std::vector<double> h(mols[0]->xyz_setup);
@@ -948,6 +990,9 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
         }
     }
     P.graphs_ok = graphs_setting;
+    // from here on PCG starts from the previous step's solution (GFNFF_PCG_WARM=0: from zero)
+    const char* warm_env = std::getenv("GFNFF_PCG_WARM");
+    P.pcg_warm = !(warm_env && !std::strcmp(warm_env, "0"));
 }
 
 bool Engine::switch_to_lu()
@@ -1053,10 +1098,50 @@ void Engine::launch_body()
     CK(cudaMemsetAsync(P.E.p, 0, 16 * (size_t)P.nmol * sizeof(double), s));
     CK(cudaMemsetAsync(P.bad.p, 0, (size_t)P.nmol * sizeof(int), s));
     if (P.resp_on) CK(cudaMemsetAsync(P.cfar.p, 0, (size_t)n * sizeof(double), s));
+    // terms without a charge dependence: on the side stream when forking, else in phase order
+    const bool fork = P.side && !P.timing;
+    cudaStream_t s2 = fork ? P.side : s;
+    auto hb_rep_terms = [&]() {
+    if (P.nhb) {
+        HBSoA H{P.nhb, P.h_a.p, P.h_h.p, P.h_b.p, P.h_c.p, P.h_pc.p, P.h_nbo.p, P.h_nb.p, P.h_nco.p, P.h_nc.p,
+                P.h_ba.p, P.h_bb.p, P.h_aa.p, P.h_ab.p, P.h_QH.p, P.h_QA.p, P.h_QB.p, P.h_rv.p, P.h_zlp.p, P.h_nfl.p};
+        const int split = mixed ? P.nhb_near : P.nhb;
+        if (split > 0) k_hbonds<double><<<nblk(split), kBlock, 0, s2>>>(V, H, 0, split);
+        if (P.nhb > split) k_hbonds<float><<<nblk(P.nhb - split), kBlock, 0, s2>>>(V, H, split, P.nhb);
+    }
+    if (P.nxb) k_xbonds<<<nblk(P.nxb), kBlock, 0, s2>>>(V, XBSoA{P.nxb, P.x_a.p, P.x_x.p, P.x_b.p, P.x_pre.p, P.x_rv.p});
+    P.mark(8);
+    k_repulsion<double><<<nblk((long)n * 32), kBlock, 0, s2>>>(V, P.r_off.p, P.r_j.p, P.r_al.p, P.r_ab.p, P.r_kind.p);
+    P.mark(9);
+    };
+    auto bonded_terms = [&]() {
+    if (P.nb) {
+        BondSoA B{P.nb, P.b_i.p, P.b_j.p, P.b_h.p, P.b_off.p, P.b_hb.p, P.b_fc.p, P.b_al.p,
+                  P.b_r0i.p, P.b_r0j.p, P.b_cki.p, P.b_ckj.p, P.b_sh.p, P.b_ff.p};
+        k_bonds<<<nblk((long)P.nb * 32), kBlock, 0, s2>>>(V, B);
+    }
+    if (P.na) k_angles<<<nblk(P.na), kBlock, 0, s2>>>(V, AngleSoA{P.na, P.a_i.p, P.a_j.p, P.a_k.p, P.a_fc.p, P.a_th.p});
+    if (P.nt) k_torsions<<<nblk(P.nt), kBlock, 0, s2>>>(V, TorsSoA{P.nt, P.t_i.p, P.t_j.p, P.t_k.p, P.t_l.p, P.t_V.p, P.t_n.p, P.t_p.p}, 0);
+    if (P.ns) k_torsions<<<nblk(P.ns), kBlock, 0, s2>>>(V, TorsSoA{P.ns, P.s_i.p, P.s_j.p, P.s_k.p, P.s_l.p, P.s_e.p, nullptr, nullptr}, 1);
+    if (P.ninv) k_inversions<<<nblk(P.ninv), kBlock, 0, s2>>>(V, InvSoA{P.ninv, P.v_i.p, P.v_j.p, P.v_k.p, P.v_l.p, P.v_t.p, P.v_fc.p, P.v_om.p});
+    if (P.natm) k_atm<<<nblk(P.natm), kBlock, 0, s2>>>(V, TripSoA{P.natm, P.at_i.p, P.at_j.p, P.at_k.p, P.at_c9.p, P.at_r0ij.p, P.at_r0ik.p, P.at_r0jk.p, P.at_sc.p});
+    if (P.nbatm) k_batm<<<nblk(P.nbatm), kBlock, 0, s2>>>(V, TripSoA{P.nbatm, P.ba_i.p, P.ba_j.p, P.ba_k.p, P.ba_c9.p, nullptr, nullptr, nullptr, nullptr});
+    };
+    if (fork) {
+        CK(cudaEventRecord(P.ev_fork0, s));
+        CK(cudaStreamWaitEvent(s2, P.ev_fork0, 0));
+        hb_rep_terms();
+    }
     P.mark(1);
     (mixed ? k_cn<float> : k_cn<double>)<<<tgrid, kTile, 0, s>>>(V, P.nsplit);
     P.mark(2);
     k_d4_weights<<<nblk(n), kBlock, 0, s>>>(V);
+    if (fork) {
+        CK(cudaEventRecord(P.ev_fork1, s));
+        CK(cudaStreamWaitEvent(s2, P.ev_fork1, 0));
+        bonded_terms();
+        CK(cudaEventRecord(P.ev_join, s2));
+    }
     // EEQ
     P.mark(3);
     if (P.nmol == 1) {
@@ -1064,8 +1149,9 @@ void Engine::launch_body()
         const bool full = sv == -1 || sv == Impl::SOLVE_PCG;
         const bool aug = sv == Impl::SOLVE_TILED;
         if (P.nred > 0) {
-            dim3 g(nblk(P.nred), std::min(P.nred, 128));
-            k_eeq_M<<<g, kBlock, 0, s>>>(V, P.red2atom.p, P.anchor.p, P.M.p, P.lda, full ? 1 : 0);
+            const long long nt = (P.nred + kMT - 1) / kMT;
+            k_eeq_M_tiles<<<(unsigned)(nt * (nt + 1) / 2), 256, 0, s>>>(V, P.red2atom.p, P.anchor.p, P.M.p, P.lda,
+                                                                      full ? 1 : 0);
         }
         P.mark(4);
         if (P.nred > 0)
@@ -1076,7 +1162,7 @@ void Engine::launch_body()
             if (sv == Impl::SOLVE_TILED) {
                 P.chol_launch();
             } else if (sv == Impl::SOLVE_PCG) {
-                P.pcg_launch(P.bvec.p, P.px.p, P.info.p);
+                P.pcg_launch(P.bvec.p, P.px.p, P.info.p, 0);
             } else if (sv == Impl::SOLVE_LIBRARY) {
                 CS(cusolverDnDpotrf(P.sol, CUBLAS_FILL_MODE_LOWER, P.nred, P.M.p, P.lda, P.work.p, P.lwork, P.info.p));
                 CS(cusolverDnDpotrs(P.sol, CUBLAS_FILL_MODE_LOWER, P.nred, 1, P.M.p, P.lda, P.bvec.p, P.nred, P.info2.p));
@@ -1098,29 +1184,11 @@ void Engine::launch_body()
     if (P.nmol == 1 && !P.use_lu && P.solver == Impl::SOLVE_PCG) ysol = P.px.p;
     k_eeq_expand<<<nblk(n), kBlock, 0, s>>>(V, P.q0.p, P.atom2red.p, P.frag_off.p, P.frag_atoms.p, ysol, P.q.p);
     P.mark(6);
-    if (P.nb) {
-        BondSoA B{P.nb, P.b_i.p, P.b_j.p, P.b_h.p, P.b_off.p, P.b_hb.p, P.b_fc.p, P.b_al.p,
-                  P.b_r0i.p, P.b_r0j.p, P.b_cki.p, P.b_ckj.p, P.b_sh.p, P.b_ff.p};
-        k_bonds<<<nblk((long)P.nb * 32), kBlock, 0, s>>>(V, B);
+    if (!fork) {
+        bonded_terms();
+        P.mark(7);
+        hb_rep_terms();
     }
-    if (P.na) k_angles<<<nblk(P.na), kBlock, 0, s>>>(V, AngleSoA{P.na, P.a_i.p, P.a_j.p, P.a_k.p, P.a_fc.p, P.a_th.p});
-    if (P.nt) k_torsions<<<nblk(P.nt), kBlock, 0, s>>>(V, TorsSoA{P.nt, P.t_i.p, P.t_j.p, P.t_k.p, P.t_l.p, P.t_V.p, P.t_n.p, P.t_p.p}, 0);
-    if (P.ns) k_torsions<<<nblk(P.ns), kBlock, 0, s>>>(V, TorsSoA{P.ns, P.s_i.p, P.s_j.p, P.s_k.p, P.s_l.p, P.s_e.p, nullptr, nullptr}, 1);
-    if (P.ninv) k_inversions<<<nblk(P.ninv), kBlock, 0, s>>>(V, InvSoA{P.ninv, P.v_i.p, P.v_j.p, P.v_k.p, P.v_l.p, P.v_t.p, P.v_fc.p, P.v_om.p});
-    if (P.natm) k_atm<<<nblk(P.natm), kBlock, 0, s>>>(V, TripSoA{P.natm, P.at_i.p, P.at_j.p, P.at_k.p, P.at_c9.p, P.at_r0ij.p, P.at_r0ik.p, P.at_r0jk.p, P.at_sc.p});
-    if (P.nbatm) k_batm<<<nblk(P.nbatm), kBlock, 0, s>>>(V, TripSoA{P.nbatm, P.ba_i.p, P.ba_j.p, P.ba_k.p, P.ba_c9.p, nullptr, nullptr, nullptr, nullptr});
-    P.mark(7);
-    if (P.nhb) {
-        HBSoA H{P.nhb, P.h_a.p, P.h_h.p, P.h_b.p, P.h_c.p, P.h_pc.p, P.h_nbo.p, P.h_nb.p, P.h_nco.p, P.h_nc.p,
-                P.h_ba.p, P.h_bb.p, P.h_aa.p, P.h_ab.p, P.h_QH.p, P.h_QA.p, P.h_QB.p, P.h_rv.p, P.h_zlp.p, P.h_nfl.p};
-        const int split = mixed ? P.nhb_near : P.nhb;
-        if (split > 0) k_hbonds<double><<<nblk(split), kBlock, 0, s>>>(V, H, 0, split);
-        if (P.nhb > split) k_hbonds<float><<<nblk(P.nhb - split), kBlock, 0, s>>>(V, H, split, P.nhb);
-    }
-    if (P.nxb) k_xbonds<<<nblk(P.nxb), kBlock, 0, s>>>(V, XBSoA{P.nxb, P.x_a.p, P.x_x.p, P.x_b.p, P.x_pre.p, P.x_rv.p});
-    P.mark(8);
-    k_repulsion<double><<<nblk((long)n * 32), kBlock, 0, s>>>(V, P.r_off.p, P.r_j.p, P.r_al.p, P.r_ab.p, P.r_kind.p);
-    P.mark(9);
     k_pairs<double><<<tgrid, kTile, 0, s>>>(V, P.nsplit);
     if (P.resp_on) {
         // u = B M^-1 B^T w with the factor (or the iteration) of this step's EEQ matrix
@@ -1129,7 +1197,7 @@ void Engine::launch_body()
         if (P.use_lu) {
             CS(cusolverDnDgetrs(P.sol, CUBLAS_OP_N, P.nred, 1, P.M.p, P.lda, P.ipiv.p, P.bres.p, P.nred, P.info2.p));
         } else if (P.solver == Impl::SOLVE_PCG) {
-            P.pcg_launch(P.bres.p, P.xres.p, P.info3.p);
+            P.pcg_launch(P.bres.p, P.xres.p, P.info3.p, 1);
             k_merge_info<<<1, 1, 0, s>>>(P.info.p, P.info3.p);
             y = P.xres.p;
         } else {   // the Cholesky factor (cuSOLVER or the tiled kernel) is in M
@@ -1138,6 +1206,7 @@ void Engine::launch_body()
         k_eeq_expand<<<nblk(n), kBlock, 0, s>>>(V, nullptr, P.atom2red.p, P.frag_off.p, P.frag_atoms.p, y, P.ures.p);
         k_resp_pairs<<<tgrid, kTile, 0, s>>>(V, P.nsplit);
     }
+    if (fork) CK(cudaStreamWaitEvent(s, P.ev_join, 0));
     P.mark(10);
     k_post<<<nblk(n), kBlock, 0, s>>>(V);
     k_cn_chain<double><<<tgrid, kTile, 0, s>>>(V, P.nsplit);

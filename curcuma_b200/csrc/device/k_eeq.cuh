@@ -41,6 +41,64 @@ __global__ void k_eeq_M(View V, const int* __restrict__ red2atom, const int* __r
     }
 }
 
+// Reduced matrix by 32 x 32 tiles of the lower triangle (block (tr, tc), tr >= tc): the
+// tile's row and column atoms (and their anchors) are staged in shared memory, every
+// entry is computed once and written to (r, c) and, when full, to (c, r) through a
+// shared-memory transpose so that both writes are coalesced.
+constexpr int kMT = 32;
+__global__ void __launch_bounds__(256) k_eeq_M_tiles(View V, const int* __restrict__ red2atom,
+                                                    const int* __restrict__ anchor, double* M, int lda, int full)
+{
+    __shared__ double px[4][kMT], py[4][kMT], pz[4][kMT], pa[4][kMT];   // rows k, rows ak, cols l, cols al
+    __shared__ int pid[4][kMT];
+    __shared__ double T[kMT][kMT + 1];
+    // triangular block index -> (tr, tc)
+    const long long b = blockIdx.x;
+    int tr = (int)((sqrt(8.0 * (double)b + 1.0) - 1.0) * 0.5);
+    while ((long long)(tr + 1) * (tr + 2) / 2 <= b) ++tr;
+    while ((long long)tr * (tr + 1) / 2 > b) --tr;
+    const int tc = (int)(b - (long long)tr * (tr + 1) / 2);
+    const int r0 = tr * kMT, c0 = tc * kMT, n = V.nred;
+    if (threadIdx.x < 4 * kMT) {
+        const int w = threadIdx.x / kMT, t = threadIdx.x % kMT;
+        const int idx = (w < 2 ? r0 : c0) + t;
+        int a = -1;
+        if (idx < n) {
+            const int k = red2atom[idx];
+            a = (w & 1) ? anchor[k] : k;
+        }
+        pid[w][t] = a;
+        if (a >= 0) {
+            const double4 p = V.pos[a];
+            px[w][t] = p.x; py[w][t] = p.y; pz[w][t] = p.z; pa[w][t] = V.alpeeq[a];
+        }
+    }
+    __syncthreads();
+    auto el = [&](int wa, int ia, int wb, int ib) {
+        if (pid[wa][ia] == pid[wb][ib]) return V.adiag[pid[wa][ia]];
+        const double dx = px[wa][ia] - px[wb][ib], dy = py[wa][ia] - py[wb][ib], dz = pz[wa][ia] - pz[wb][ib];
+        const double d2 = dx * dx + dy * dy + dz * dz;
+        const double s = pa[wa][ia] + pa[wb][ib];
+        if (d2 >= 36.0 * s) return rsqrt(d2);
+        const double r = sqrt(d2);
+        return erf(r / sqrt(s)) / r;
+    };
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;   // 32 x 8
+    for (int cc = ty; cc < kMT; cc += 8) {
+        const int r = r0 + tx, c = c0 + cc;
+        double v = 0.0;
+        if (r < n && c < n) v = el(0, tx, 2, cc) - el(0, tx, 3, cc) - el(1, tx, 2, cc) + el(1, tx, 3, cc);
+        T[cc][tx] = v;
+        if (r < n && c < n && (full || r >= c)) M[(size_t)c * lda + r] = v;
+    }
+    if (!full || tr == tc) return;
+    __syncthreads();
+    for (int rr = ty; rr < kMT; rr += 8) {   // (c, r) entries: row c0 + tx of column r0 + rr
+        const int r = r0 + rr, c = c0 + tx;
+        if (r < n && c < n) M[(size_t)r * lda + c] = T[tx][rr];
+    }
+}
+
 // x_i - sum_j A_ij q0_j over the atoms of charged fragments of i's molecule
 __device__ __forceinline__ double eeq_rhs_atom(const View& V, int i, const int* qlist, int nq, const double* q0)
 {
@@ -193,42 +251,126 @@ __device__ __forceinline__ double eeq_aug(const MolStage& M, int nr, int r, int 
     return eeq_a_s(M, k, l) - eeq_a_s(M, k, al) - eeq_a_s(M, ak, l) + eeq_a_s(M, ak, al);
 }
 
-// Cholesky + back substitution of an augmented matrix whose column c starts at S + co(c)
-// (element (r, c) at S[co(c) + r - c]); y receives the solution.  Returns false when a
-// pivot is not positive.
+// Rank-(k1 - k0) update of the trailing columns [k1, ccap) (rows c..nr) with the factored
+// panel columns [k0, k1): a warp owns 4 columns x 32*RPL rows, each lane RPL rows x 4
+// columns in registers; rows are read conflict-free along the packed columns, the column
+// values as shared-memory broadcasts.
+template <int RPL, class Off>
+__device__ void chol_trailing(double* S, int nr, int ccap, int k0, int k1, Off co)
+{
+    constexpr int RB = 32 * RPL;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const int m = ccap - k1;
+    const int ncg = (m + 3) >> 2, nrb = (nr + 1 - k1 + RB - 1) / RB;
+    for (int task = warp; task < ncg * nrb; task += nw) {
+        const int cg = task / nrb, rb = task % nrb;
+        const int c0 = k1 + 4 * cg, rbase = k1 + RB * rb;
+        if (rbase + RB - 1 < c0) continue;
+        double acc[RPL][4];
+#pragma unroll
+        for (int i = 0; i < RPL; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+        for (int p = k0; p < k1; ++p) {
+            const double* cp = S + co(p) - p;   // element (r, p) at cp[r]
+            double lr[RPL], lc[4];
+#pragma unroll
+            for (int i = 0; i < RPL; ++i) {
+                const int r = rbase + lane + 32 * i;
+                lr[i] = r <= nr ? cp[r] : 0.0;
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) lc[j] = c0 + j < ccap ? cp[c0 + j] : 0.0;
+#pragma unroll
+            for (int i = 0; i < RPL; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][j] = fma(lr[i], lc[j], acc[i][j]);
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int c = c0 + j;
+            if (c >= ccap) break;
+            double* cc = S + co(c) - c;
+#pragma unroll
+            for (int i = 0; i < RPL; ++i) {
+                const int r = rbase + lane + 32 * i;
+                if (r >= c && r <= nr) cc[r] -= acc[i][j];
+            }
+        }
+    }
+}
+
+// Blocked right-looking Cholesky of the first ccap columns of an augmented matrix with
+// nr + 1 rows whose column c starts at S + co(c) (element (r, c) at S[co(c) + r - c]);
+// updates reach columns < ccap only.  A panel of kCholNB columns is factored with one
+// block barrier per column: column k stays unscaled during the panel (the update of the
+// later panel columns uses u_r u_c / d_k with u the unscaled entries), so a step only
+// reads column k and only writes columns > k, each thread in the rows it owns (r = tid
+// mod blockDim); the panel is scaled by 1/sqrt(d_k) at its end.  The trailing columns
+// then take the panel's rank-kCholNB update (chol_trailing).  Returns false (uniformly)
+// when a pivot is not positive.
+constexpr int kCholNB = 8;
+template <class Off>
+__device__ bool chol_factor(double* S, int nr, int ccap, Off co)
+{
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int k0 = 0; k0 < ccap; k0 += kCholNB) {
+        const int k1 = min(k0 + kCholNB, ccap);
+        double isq[kCholNB];
+#pragma unroll
+        for (int j = 0; j < kCholNB; ++j) isq[j] = 0.0;
+#pragma unroll
+        for (int kk = 0; kk < kCholNB; ++kk) {
+            const int k = k0 + kk;
+            if (k >= k1) break;
+            const double d = S[co(k)];
+            if (!(d > 0.0)) return false;   // every thread reads the same d after a barrier
+            isq[kk] = 1.0 / sqrt(d);
+            const double id = 1.0 / d;
+            const double* ck = S + co(k) - k;   // element (r, k) at ck[r]
+            double uc[kCholNB - 1];
+#pragma unroll
+            for (int j = 0; j < kCholNB - 1; ++j) {
+                const int c = k + 1 + j;
+                uc[j] = c < k1 ? ck[c] * id : 0.0;
+            }
+            for (int r = k + 1 + tid; r <= nr; r += nt) {
+                const double ur = ck[r];
+#pragma unroll
+                for (int j = 0; j < kCholNB - 1; ++j) {
+                    const int c = k + 1 + j;
+                    if (c < k1 && r >= c) S[co(c) + r - c] -= ur * uc[j];
+                }
+            }
+            __syncthreads();
+        }
+        // scale the panel: L(r, k) = u_r / sqrt(d_k), L(k, k) = sqrt(d_k)
+#pragma unroll
+        for (int kk = 0; kk < kCholNB; ++kk) {
+            const int k = k0 + kk;
+            if (k >= k1) break;
+            double* ck = S + co(k) - k;
+            for (int r = k + tid; r <= nr; r += nt) ck[r] *= isq[kk];   // r == k: d / sqrt(d)
+        }
+        __syncthreads();
+        if (k1 >= ccap) continue;
+        if (nr + 1 - k1 <= 96) chol_trailing<2>(S, nr, ccap, k0, k1, co);
+        else chol_trailing<4>(S, nr, ccap, k0, k1, co);
+        __syncthreads();
+    }
+    return true;
+}
+
+// Cholesky + back substitution L^T y = z of the augmented matrix (z_k = element (nr, k));
+// y receives the solution.  Returns false when a pivot is not positive.
 template <class Off>
 __device__ bool chol_aug_solve(double* S, int nr, Off co, double* y, double* lk)
 {
-    __shared__ int bad;
-    if (threadIdx.x == 0) bad = 0;
+    (void)lk;
+    const bool ok = chol_factor(S, nr, nr, co);
     __syncthreads();
-    const int tid = threadIdx.x, nt = blockDim.x, warp = tid >> 5, lane = tid & 31, nw = nt >> 5;
-    for (int k = 0; k < nr; ++k) {
-        const double d = S[co(k)];
-        if (!(d > 0.0)) {
-            if (tid == 0) bad = 1;
-            break;   // every thread reads the same d: uniform exit
-        }
-        const double inv = 1.0 / sqrt(d);
-        double* ck = S + co(k);
-        for (int r = k + 1 + tid; r <= nr; r += nt) {
-            const double v = ck[r - k] * inv;
-            ck[r - k] = v;
-            lk[r] = v;
-        }
-        __syncthreads();
-        if (tid == 0) ck[0] = d * inv;
-        // trailing update, one warp per column
-        for (int c = k + 1 + warp; c < nr; c += nw) {
-            const double lc = lk[c];
-            double* cc = S + co(c);
-            for (int r = c + lane; r <= nr; r += 32) cc[r - c] -= lk[r] * lc;
-        }
-        __syncthreads();
-    }
-    __syncthreads();
-    if (bad) return false;
-    // L^T y = z, z_k = element (nr, k)
+    if (!ok) return false;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (warp == 0) {
         for (int k = nr - 1; k >= 0; --k) {
             const double* ck = S + co(k);
@@ -265,33 +407,14 @@ __device__ bool chol_two_stage(const EEQBatch& P, const MolStage& MS, int m, int
     const int tid = threadIdx.x, nt = blockDim.x, warp = tid >> 5, lane = tid & 31, nw = nt >> 5;
     double* G = P.M + P.moff[m];
     const int lda = nr + 1;
-    __shared__ int bad;
-    if (tid == 0) bad = 0;
     // ---- stage 1: panel columns [0, s), rows c..nr, packed
     auto po = [&](int c) { return (long long)c * (nr + 1) - (long long)c * (c - 1) / 2; };
     for (int c = warp; c < s; c += nw)
         for (int r = c + lane; r <= nr; r += 32) S[po(c) + r - c] = eeq_aug(MS, nr, r, c);
     __syncthreads();
-    for (int k = 0; k < s; ++k) {
-        const double d = S[po(k)];
-        if (!(d > 0.0)) {
-            if (tid == 0) bad = 1;
-            break;
-        }
-        const double inv = 1.0 / sqrt(d);
-        double* ck = S + po(k);
-        for (int r = k + 1 + tid; r <= nr; r += nt) ck[r - k] *= inv;
-        __syncthreads();
-        if (tid == 0) ck[0] = d * inv;
-        for (int c = k + 1 + warp; c < s; c += nw) {
-            const double lc = ck[c - k];
-            double* cc = S + po(c);
-            for (int r = c + lane; r <= nr; r += 32) cc[r - c] -= ck[r - k] * lc;
-        }
-        __syncthreads();
-    }
+    const bool ok1 = chol_factor(S, nr, s, PackedCols{nr + 1});
     __syncthreads();
-    if (bad) return false;
+    if (!ok1) return false;
     for (int c = 0; c < s; ++c)
         for (int r = c + tid; r <= nr; r += nt) G[(size_t)c * lda + r] = S[po(c) + r - c];
     // ---- stage 2: trailing block A22 - L21 L21^T (rows c..nr of columns c >= s)

@@ -39,6 +39,8 @@ struct PCGArgs {
     unsigned int* bar;    // arrival count at [0], generation at [kBarGen]
     int* info;
     int* iters;
+    int* warm;            // when non-null and *warm != 0, x holds the previous solution of the
+                          // same system and is the initial guess; set to 1 on convergence
     int max_iter;
     double tol;           // converged when max|b - M x| <= tol * max|b|
 };
@@ -241,6 +243,36 @@ __device__ void invert_small(const PCGArgs& A, int bk, double* I)
         for (int j = 0; j < s; ++j) I[i * s + j] = inv[i][j];
 }
 
+// in-place Gauss-Jordan inverse of a preconditioner block of kPcgSmall < s <= 32 rows by
+// one warp: lane j owns column j, column c of the pivot step is staged in colc (32
+// doubles per warp), __syncwarp only.  M is stored in full and symmetric, so row i of
+// the block is read from column i of M (coalesced).
+constexpr int kPcgWarpMax = 32;
+__device__ void invert_warp(const PCGArgs& A, int bk, double* I, double* colc)
+{
+    const int lane = threadIdx.x & 31;
+    const int2 bl = A.blocks[bk];
+    const int s = bl.y;
+    if (lane < s)
+        for (int i = 0; i < s; ++i) I[i * s + lane] = A.M[(size_t)(bl.x + i) * A.lda + bl.x + lane];
+    __syncwarp();
+    for (int c = 0; c < s; ++c) {
+        colc[lane] = lane < s ? I[lane * s + c] : 0.0;
+        __syncwarp();
+        const double inv = 1.0 / colc[c];
+        if (lane < s) {
+            const int j = lane;
+            const double rc = (j == c ? 1.0 : I[c * s + j]) * inv;
+            I[c * s + j] = rc;
+            for (int i = 0; i < s; ++i) {
+                if (i == c) continue;
+                I[i * s + j] = (j == c ? 0.0 : I[i * s + j]) - colc[i] * rc;
+            }
+        }
+        __syncwarp();
+    }
+}
+
 __global__ void __launch_bounds__(kPcgThreads) k_pcg(PCGArgs A)
 {
     extern __shared__ double sm[];
@@ -264,10 +296,18 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(PCGArgs A)
     // no pivoting); small blocks one per thread, larger ones by the whole grid block
     for (int bk = pt.z + threadIdx.x; bk < pt.w; bk += blockDim.x)
         if (A.blocks[bk].y <= kPcgSmall) invert_small(A, bk, Bs + (A.boff[bk] - boff0));
+    {
+        __shared__ double colc[kPcgThreads / 32][32];
+        const int warp = threadIdx.x >> 5;
+        for (int bk = pt.z + warp; bk < pt.w; bk += kPcgThreads / 32) {
+            const int s = A.blocks[bk].y;
+            if (s > kPcgSmall && s <= kPcgWarpMax) invert_warp(A, bk, Bs + (A.boff[bk] - boff0), colc[warp]);
+        }
+    }
     for (int bk = pt.z; bk < pt.w; ++bk) {
         const int2 bl = A.blocks[bk];
         const int s = bl.y;
-        if (s <= kPcgSmall) continue;
+        if (s <= kPcgWarpMax) continue;
         double* I = Bs + (A.boff[bk] - boff0);
         __syncthreads();
         for (int e = threadIdx.x; e < s * s; e += blockDim.x) {
@@ -305,12 +345,20 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(PCGArgs A)
         const int2 bl = A.blocks[bk];
         meta[k] = make_int4(bl.x - row0, bl.y, (int)(A.boff[bk] - boff0) + (rr - bl.x) * bl.y, 0);
     }
-    // ---- x = 0, r = b, z = P^-1 r
+    // ---- x = x0 (the previous solution, or 0), r = b - M x0, z = P^-1 r.  x0 is complete
+    // in global memory since the previous launch, so no grid barrier is needed here.
+    const bool warm = A.warm != nullptr && *A.warm != 0;
+    if (warm) {
+        update_p(p, A.x, A.n, 0.0);
+        __syncthreads();
+        matvec_rows(A, p, row0, row1, Ap);
+        __syncthreads();
+    }
     double bmax_t = 0.0;
     for (int k = threadIdx.x; k < nrow; k += blockDim.x) {
         const double bv = A.b[row0 + k];
-        xs[k] = 0.0;
-        rs[k] = bv;
+        xs[k] = warm ? p[row0 + k] : 0.0;
+        rs[k] = warm ? bv - Ap[k] : bv;
         bmax_t = fmax(bmax_t, fabs(bv));
     }
     __syncthreads();
@@ -385,6 +433,7 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(PCGArgs A)
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         *A.info = !ok ? 2 : (conv ? 0 : 3);
         *A.iters = it;
+        if (A.warm) *A.warm = (ok && conv) ? 1 : 0;
     }
 }
 

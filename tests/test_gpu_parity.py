@@ -169,3 +169,33 @@ def test_graph_replay_matches_direct_launches(system, monkeypatch):
     for (e1, g1), (e0, g0) in zip(res["1"], res["0"]):
         assert abs(e1 - e0) < 1e-10
         assert np.abs(g1 - g0).max() < 1e-10
+
+
+@pytest.mark.parametrize("system", ["water200", "alkane"])
+def test_pcg_warm_start(system, monkeypatch):
+    """PCG started from the previous geometry's solution reaches the same charges and
+    energies as the oracle on every geometry of a short sequence, in fewer iterations than
+    a start from zero."""
+    monkeypatch.setenv("GFNFF_EEQ_SOLVER", "pcg")
+    Z, X = {"water200": lambda: workloads.water_cluster(200, 10),
+            "alkane": lambda: workloads.alkane(64, 1001)}[system]()
+    rng = np.random.default_rng(5)
+    geoms = [X + rng.normal(scale=0.01, size=X.shape) for _ in range(4)]
+    iters = {}
+    o = Oracle(Z, X)
+    for flag in ("1", "0"):
+        monkeypatch.setenv("GFNFF_PCG_WARM", flag)
+        g = GFNFF()
+        assert g.setMolecule(Z, X)
+        iters[flag] = []
+        for Xk in geoms:
+            g.updateGeometry(Xk)
+            e = g.calculateEnergy(True)
+            assert not g.hasError(), g.getErrorMessage()
+            iters[flag].append(g.eeqIterations())
+            if flag == "1":
+                T, G, q, _ = o.engrad(Xk)
+                assert abs(e - T["total"]) < E_TOL
+                assert np.abs(g.getGradient() - G).max() < G_TOL
+                assert np.abs(g.getCharges() - q).max() < 1e-9
+    assert sum(iters["1"][1:]) < sum(iters["0"][1:]), iters
