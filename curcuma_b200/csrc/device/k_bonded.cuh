@@ -338,6 +338,26 @@ struct HBSoA {
     const int* nflag;   // acceptor is N with a single neighbour: neighbour cutoff 2.0
 };
 
+// Arithmetic of the HB kernel.  FP64 keeps IEEE operations but divides by reciprocals
+// computed once per distance; FP32 (only the weak, strongly damped terms of the mixed
+// form) uses the hardware approximations of 1/x, exp and 1/sqrt (relative error ~1e-7).
+template <class R>
+__device__ __forceinline__ R hb_rcp(R x) { return R(1.0) / x; }
+template <>
+__device__ __forceinline__ float hb_rcp<float>(float x) { return __fdividef(1.0f, x); }
+template <class R>
+__device__ __forceinline__ R hb_exp(R x) { return exp(x); }
+template <>
+__device__ __forceinline__ float hb_exp<float>(float x) { return __expf(x); }
+// |v| and 1/|v| from one reciprocal square root
+template <class R>
+__device__ __forceinline__ R hb_len(V3<R> v, R& inv)
+{
+    const R d2 = dot(v, v);
+    inv = rsqrt(d2);
+    return d2 * inv;
+}
+
 // hydrogen bonds, cases 1-4 (ff_workspace_gfnff.cpp:938-1409).  R = double is the FP64
 // form; R = float evaluates the term in FP32 relative to the H atom (the FP64 position
 // differences are taken first), energies and gradients accumulate in FP64.  The damping
@@ -356,41 +376,46 @@ __global__ void __launch_bounds__(kBlock, GFNFF_HB_MINBLOCKS) k_hbonds(View V, H
     if (t < t1) {
         using P3 = V3<R>;
         const double4 org = V.pos[S.h[t]];   // H as the local origin
-        const R HB_BACUT = R(49.0), HB_SCUT = R(22.0), HB_ALP = R(6.0), HB_LONGCUT = R(85.0), HB_NBCUT = R(11.20);
+        const R HB_BACUT = R(49.0), HB_SCUT = R(22.0), HB_ALP = R(6.0), HB_NBCUT = R(11.20);
         const R TORS_HB = R(0.94), BEND_HB = R(0.20), HBLPCUT = R(56.0);
         const int A = S.a[t], H = S.h[t], Bq = S.b[t], cs = S.cas[t];
         P3 pA = ldr<R>(V.pos, A, org), pH = ldr<R>(V.pos, H, org), pB = ldr<R>(V.pos, Bq, org);
-        const R rAH = nrm(pH - pA), rHB = nrm(pB - pH), rAB = nrm(pB - pA);
+        R irAH, irHB, irAB;
+        const R rAH = hb_len(pH - pA, irAH), rHB = hb_len(pB - pH, irHB), rAB = hb_len(pB - pA, irAB);
         if (rAB <= R(50.0)) {
             const R rAH4 = rAH * rAH * rAH * rAH, rHB4 = rHB * rHB * rHB * rHB;
-            const R den = R(1.0) / (rAH4 + rHB4);
+            const R den = hb_rcp(rAH4 + rHB4);
             const R QH = S.QH[t], QA = S.QA[t], QB = S.QB[t];
             const R bas = (QA * S.bas_a[t] * rAH4 + QB * S.bas_b[t] * rHB4) * den;
             const R aci = (S.aci_b[t] * rAH4 + S.aci_a[t] * rHB4) * den;
             const R rv = S.rv[t];
+            const R irv = hb_rcp(rv);
+            const R rab2 = rAB * rAB, irab2 = irAB * irAB;
             // HB_ALP = 6: integer powers
-            const R ratio1 = pow6<R>(rAB * rAB / HB_LONGCUT);
-            const R ratio3 = pow6<R>(HB_SCUT * rv / (rAB * rAB));
-            const R dsh = R(1.0) / (R(1.0) + ratio3);
-            const R dlg = R(1.0) / (R(1.0) + ratio1);
+            const R ratio1 = pow6<R>(rab2 * R(1.0 / 85.0));   // (r_AB^2 / HB_LONGCUT)^6
+            const R ratio3 = pow6<R>(HB_SCUT * rv * irab2);
+            const R dsh = hb_rcp(R(1.0) + ratio3);
+            const R dlg = hb_rcp(R(1.0) + ratio1);
             const R denv = dsh * dlg;
+            const R bacut = HB_BACUT * irv;
             R doutl;
             {
-                const R ex = (HB_BACUT / rv) * ((rAH + rHB) / rAB - R(1.0));
-                doutl = ex > R(15.0) ? R(0.0) : R(2.0) / (R(1.0) + exp(ex));
+                const R ex = bacut * ((rAH + rHB) * irAB - R(1.0));
+                doutl = ex > R(15.0) ? R(0.0) : R(2.0) * hb_rcp(R(1.0) + hb_exp(ex));
             }
             const int nb0 = S.nbb_off[t], nb1 = S.nbb_off[t + 1];
-            const R nbcut = S.nflag[t] ? R(2.0) : HB_NBCUT;
+            const R nbc = (S.nflag[t] ? R(2.0) : HB_NBCUT) * irv;
             R onb = R(1.0);
             if (cs >= 2)
                 for (int p = nb0; p < nb1; ++p) {
                     P3 pn = ldr<R>(V.pos, S.nbb[p], org);
-                    const R ra = nrm(pn - pA), rb = nrm(pn - pB);
-                    const R ex = (nbcut / rv) * ((ra + rb) / rAB - R(1.0));
-                    onb *= (R(2.0) / (R(1.0) + exp(-ex)) - R(1.0));
+                    R ia, ib;
+                    const R ra = hb_len(pn - pA, ia), rb = hb_len(pn - pB, ib);
+                    const R ex = nbc * ((ra + rb) * irAB - R(1.0));
+                    onb *= (R(2.0) * hb_rcp(R(1.0) + hb_exp(-ex)) - R(1.0));
                 }
-            const R rdamp = cs >= 2 ? denv * (R(1.8) / (rHB * rHB * rHB) - R(0.8) / (rAB * rAB * rAB))
-                                         : denv / (rAB * rAB * rAB);
+            const R irHB3 = irHB * irHB * irHB, irAB3 = irAB * irAB * irAB;
+            const R rdamp = cs >= 2 ? denv * (R(1.8) * irHB3 - R(0.8) * irAB3) : denv * irAB3;
             R olp = R(1.0), lpd = R(0.0);
             int nlp = 0;
             P3 lpv = P3{0, 0, 0}, lpp = pB;
@@ -400,10 +425,10 @@ __global__ void __launch_bounds__(kBlock, GFNFF_HB_MINBLOCKS) k_hbonds(View V, H
                 for (int p = nb0; p < nb1; ++p) lpv = lpv + (ldr<R>(V.pos, S.nbb[p], org) - pB);
                 const R vn = nrm(lpv);
                 if (vn > R(1e-10) && nlp > 0) {
-                    lpp = pB + (-lpd) * ((R(1.0) / vn) * lpv);
+                    lpp = pB + (-lpd) * (hb_rcp(vn) * lpv);
                     const R ral = nrm(pA - lpp);
-                    const R ex = (HBLPCUT / rv) * ((ral + lpd + R(1e-12)) / rAB - R(1.0));
-                    olp = R(2.0) / (R(1.0) + exp(ex));
+                    const R ex = (HBLPCUT * irv) * ((ral + lpd + R(1e-12)) * irAB - R(1.0));
+                    olp = R(2.0) * hb_rcp(R(1.0) + hb_exp(ex));
                 } else {
                     nlp = 0;
                     olp = R(1.0);
@@ -419,16 +444,16 @@ __global__ void __launch_bounds__(kBlock, GFNFF_HB_MINBLOCKS) k_hbonds(View V, H
                 const R kijk = (R(1.0) - BEND_HB) / ((cos(R(0.0)) - cos(c0)) * (cos(R(0.0)) - cos(c0)));
                 P3 va = ldr<R>(V.pos, Ci, org), vb = pB, vc = pH;
                 P3 vab = va - vb, vcb = vc - vb;
-                const R rab2 = dot(vab, vab), rcb2 = dot(vcb, vcb);
+                const R rab2c = dot(vab, vab), rcb2 = dot(vcb, vcb);
                 P3 vp = cross(vcb, vab);
                 const R rp = nrm(vp) + R(1e-14);
-                R ca = dot(vab, vcb) / (sqrt(rab2) * sqrt(rcb2) + R(1e-14));
+                R ca = dot(vab, vcb) / (sqrt(rab2c) * sqrt(rcb2) + R(1e-14));
                 ca = fmax(-R(1.0), fmin(R(1.0), ca));
                 const R th = acos(ca);
                 const R ea = kijk * (ca - cos(c0)) * (ca - cos(c0));
                 const R deddt = R(2.0) * kijk * sin(th) * (cos(c0) - ca);
                 eangl = R(1.0) - ea;
-                P3 deda = (-deddt / (rab2 * rp)) * cross(vab, vp);
+                P3 deda = (-deddt / (rab2c * rp)) * cross(vab, vp);
                 P3 dedc = (deddt / (rcb2 * rp)) * cross(vcb, vp);
                 ga3[0] = deda + dedc;
                 ga3[1] = -R(1.0) * deda;
@@ -451,35 +476,36 @@ __global__ void __launch_bounds__(kBlock, GFNFF_HB_MINBLOCKS) k_hbonds(View V, H
             etot = E;
 
             P3 drab = pA - pB, drah = pA - pH, drbh = pB - pH;
-            const R rab2 = rAB * rAB, rbh2 = rHB * rHB, rah2 = rAH * rAH;
             const R rahprbh = rAH + rHB + R(1e-12);
-            const R ddamp = (-R(2.0) * HB_ALP * ratio1 / (R(1.0) + ratio1)) + (R(2.0) * HB_ALP * ratio3 / (R(1.0) + ratio3));
-            const R expo = (HB_BACUT / rv) * (rahprbh / rAB - R(1.0));
+            const R ddamp = (-R(2.0) * HB_ALP * ratio1 * dlg) + (R(2.0) * HB_ALP * ratio3 * dsh);
+            const R expo = bacut * (rahprbh * irAB - R(1.0));
             if (expo <= R(15.0)) {
-                const R ratio2 = exp(expo);
+                const R ratio2 = hb_exp(expo);
+                const R i1r2 = hb_rcp(R(1.0) + ratio2);
+                const R dsig = ratio2 * bacut * irAB * i1r2 * i1r2;   // ratio2 (cut/rv) / rAB / (1 + ratio2)^2
                 P3 ga = P3{0, 0, 0}, gb = P3{0, 0, 0}, gh = P3{0, 0, 0};
                 if (cs >= 2) {
-                    const R rbhdamp = denv * R(1.8) / (rbh2 * rHB);
-                    const R rabdamp = denv * (-R(0.8)) / (rab2 * rAB);
+                    const R rbhdamp = denv * R(1.8) * irHB3;
+                    const R rabdamp = denv * (-R(0.8)) * irAB3;
                     const R dterm = -qhoutl * eangl * etors * cst;
                     const R aterm = -rdamp * QH * onb * olp * eangl * etors * cst;
                     const R nbterm = -rdamp * QH * doutl * olp * eangl * etors * cst;
-                    R gi = ((rabdamp + rbhdamp) * ddamp - R(3.0) * rabdamp) / rab2;
+                    R gi = ((rabdamp + rbhdamp) * ddamp - R(3.0) * rabdamp) * irab2;
                     gi *= dterm;
                     P3 dg = gi * drab;
                     ga = dg;
                     gb = -R(1.0) * dg;
-                    gi = -R(3.0) * rbhdamp / rbh2;
+                    gi = -R(3.0) * rbhdamp * (irHB * irHB);
                     gi *= dterm;
                     dg = gi * drbh;
                     gb = gb + dg;
                     gh = -R(1.0) * dg;
-                    const R tmp1 = -R(2.0) * aterm * ratio2 * (HB_BACUT / rv) / rAB / ((R(1.0) + ratio2) * (R(1.0) + ratio2));
-                    gi = -tmp1 * rahprbh / rab2;
+                    const R tmp1 = -R(2.0) * aterm * dsig;
+                    gi = -tmp1 * rahprbh * irab2;
                     dg = gi * drab;
                     ga = ga + dg;
                     gb = gb - dg;
-                    P3 dgao = (tmp1 / rAH) * drah, dgbo = (tmp1 / rHB) * drbh;
+                    P3 dgao = (tmp1 * irAH) * drah, dgbo = (tmp1 * irHB) * drbh;
                     ga = ga + dgao;
                     gb = gb + dgbo;
                     gh = gh - dgao - dgbo;
@@ -487,17 +513,19 @@ __global__ void __launch_bounds__(kBlock, GFNFF_HB_MINBLOCKS) k_hbonds(View V, H
                         const int nb = S.nbb[p];
                         P3 pn = ldr<R>(V.pos, nb, org);
                         P3 dranb = pA - pn, drbnb = pB - pn;
-                        const R ranb = nrm(dranb), rbnb = nrm(drbnb);
+                        R ia, ib;
+                        const R ranb = hb_len(dranb, ia), rbnb = hb_len(drbnb, ib);
                         const R sum = ranb + rbnb + R(1e-12);
-                        const R ex = (nbcut / rv) * (sum / rAB - R(1.0));
-                        const R r2n = exp(-ex);
-                        const R oi = R(2.0) / (R(1.0) + r2n) - R(1.0);
-                        const R others = fabs(oi) > R(1e-12) ? onb / oi : R(1.0);
-                        const R tmp2 = R(2.0) * nbterm * others * r2n * (nbcut / rv) / rAB / ((R(1.0) + r2n) * (R(1.0) + r2n));
-                        dg = (-tmp2 * sum / rab2) * drab;
+                        const R ex = nbc * (sum * irAB - R(1.0));
+                        const R r2n = hb_exp(-ex);
+                        const R i1 = hb_rcp(R(1.0) + r2n);
+                        const R oi = R(2.0) * i1 - R(1.0);
+                        const R others = fabs(oi) > R(1e-12) ? onb * hb_rcp(oi) : R(1.0);
+                        const R tmp2 = R(2.0) * nbterm * others * r2n * nbc * irAB * i1 * i1;
+                        dg = (-tmp2 * sum * irab2) * drab;
                         ga = ga + dg;
                         gb = gb - dg;
-                        P3 dgan = (tmp2 / ranb) * dranb, dgbn = (tmp2 / rbnb) * drbnb;
+                        P3 dgan = (tmp2 * ia) * dranb, dgbn = (tmp2 * ib) * drbnb;
                         ga = ga + dgan;
                         gb = gb + dgbn;
                         agrad(V.grad, nb, -R(1.0) * dgan - dgbn);
@@ -506,14 +534,16 @@ __global__ void __launch_bounds__(kBlock, GFNFF_HB_MINBLOCKS) k_hbonds(View V, H
                         const R lpterm = -rdamp * QH * doutl * onb * cst;
                         const R ral = nrm(pA - lpp);
                         const R sum = ral + lpd + R(1e-12);
-                        const R ex = (HBLPCUT / rv) * (sum / rAB - R(1.0));
-                        const R r2l = exp(fmin(ex, R(80.0)));   // e^-80: the term vanishes, no overflow
-                        const R tmp3 = -R(2.0) * lpterm * r2l * (HBLPCUT / rv) / rAB / ((R(1.0) + r2l) * (R(1.0) + r2l));
-                        P3 dgl = (-tmp3 * sum / rab2) * drab;
+                        const R lpc = HBLPCUT * irv;
+                        const R ex = lpc * (sum * irAB - R(1.0));
+                        const R r2l = hb_exp(fmin(ex, R(80.0)));   // e^-80: the term vanishes, no overflow
+                        const R i1 = hb_rcp(R(1.0) + r2l);
+                        const R tmp3 = -R(2.0) * lpterm * r2l * lpc * irAB * i1 * i1;
+                        P3 dgl = (-tmp3 * sum * irab2) * drab;
                         ga = ga + dgl;
                         gb = gb - dgl;
                         P3 dral = pA - lpp;
-                        P3 dgal = (tmp3 / (ral + R(1e-12))) * dral;
+                        P3 dgal = (tmp3 * hb_rcp(ral + R(1e-12))) * dral;
                         ga = ga + dgal;
                         gb = gb - dgal;
                         P3 glp = -R(1.0) * dgal;
@@ -521,11 +551,12 @@ __global__ void __launch_bounds__(kBlock, GFNFF_HB_MINBLOCKS) k_hbonds(View V, H
                         if (vn > R(1e-10)) {
                             const R lv[3] = {lpv.x, lpv.y, lpv.z}, gl3[3] = {glp.x, glp.y, glp.z};
                             R out[3] = {0, 0, 0};
-                            const R vn3 = vn * vn * vn;
+                            const R ivn = hb_rcp(vn);
+                            const R ivn3 = ivn * ivn * ivn;
                             for (int col = 0; col < 3; ++col)
                                 for (int row = 0; row < 3; ++row) {
                                     const R unit = (row == col) ? -R(1.0) : R(0.0);
-                                    out[row] += -lpd * (R)nlp * (unit / vn + lv[row] * lv[col] / vn3) * gl3[col];
+                                    out[row] += -lpd * (R)nlp * (unit * ivn + lv[row] * lv[col] * ivn3) * gl3[col];
                                 }
                             P3 gnb = P3{out[0], out[1], out[2]};
                             gb = gb + gnb;
@@ -561,9 +592,8 @@ __global__ void __launch_bounds__(kBlock, GFNFF_HB_MINBLOCKS) k_hbonds(View V, H
                     const R caa = QA * S.bas_a[t], cbb = QB * S.bas_b[t];
                     const R rterm = -aci * rdamp * qhoutl, dterm = -aci * bas * qhoutl;
                     const R sterm = -rdamp * bas * qhoutl, aterm = -aci * bas * rdamp * QH;
-                    const R dv = R(1.0) / (rAH4 + rHB4);
-                    const R tmp = dv * dv * R(4.0);
-                    const R dd24a = rah2 * rHB4 * tmp, dd24b = rbh2 * rAH4 * tmp;
+                    const R tmp = den * den * R(4.0);
+                    const R dd24a = (rAH * rAH) * rHB4 * tmp, dd24b = (rHB * rHB) * rAH4 * tmp;
                     R gi = (caa - cbb) * dd24a * rterm;
                     ga = gi * drah;
                     gi = (cbb - caa) * dd24b * rterm;
@@ -576,16 +606,16 @@ __global__ void __launch_bounds__(kBlock, GFNFF_HB_MINBLOCKS) k_hbonds(View V, H
                     P3 dgb = (gi * sterm) * drbh;
                     gb = gb + dgb;
                     gh = gh - dga - dgb;
-                    gi = rdamp * (ddamp - R(3.0)) / rab2;
+                    gi = rdamp * (ddamp - R(3.0)) * irab2;
                     P3 dg = (gi * dterm) * drab;
                     ga = ga + dg;
                     gb = gb - dg;
-                    gi = aterm * R(2.0) * ratio2 * (HB_BACUT / rv) / rAB * rahprbh / ((R(1.0) + ratio2) * (R(1.0) + ratio2)) / rab2;
+                    gi = aterm * R(2.0) * dsig * rahprbh * irab2;
                     dg = gi * drab;
                     ga = ga + dg;
                     gb = gb - dg;
-                    const R to = -R(2.0) * aterm * ratio2 * (HB_BACUT / rv) / rAB / ((R(1.0) + ratio2) * (R(1.0) + ratio2));
-                    P3 dgao = (to / rAH) * drah, dgbo = (to / rHB) * drbh;
+                    const R to = -R(2.0) * aterm * dsig;
+                    P3 dgao = (to * irAH) * drah, dgbo = (to * irHB) * drbh;
                     ga = ga + dgao;
                     gb = gb + dgbo;
                     gh = gh - dgao - dgbo;
