@@ -162,6 +162,14 @@ def roofline(phase_avg, info, fp64_peak, hbm_peak, hbm_src):
         flops = 40.0 * info["coulomb_pairs"] + 45.0 * info["disp_pairs"]
         bound, unit, peak = "fp64", "TFLOP/s", fp64_peak
         achieved = flops / (ms * 1e-3) / 1e12
+    elif name == "eeq_solve" and info.get("solver") == "pcg":
+        # PCG: the reduced matrix is streamed once per matrix-vector product (the
+        # iterations, the warm start and the true-residual check); only its lower
+        # triangle from 4096 unknowns on
+        mbytes = 8.0 * nred * (nred + 1) / 2.0 if info["pcg_lower"] else 8.0 * nred * nred
+        bytes_ = (info["iters"] + 2) * mbytes
+        bound, unit, peak = "hbm", "GB/s", hbm_peak
+        achieved = bytes_ / (ms * 1e-3) / 1e9
     elif name == "eeq_solve":
         flops = info.get("eeq_flops", nred ** 3 / 3.0 + 2.0 * nred ** 2)
         bound, unit, peak = "fp64", "TFLOP/s", fp64_peak
@@ -443,7 +451,10 @@ def run_ours(args):
     else:
         nc, nd = pair_counts(Z, X)
         hbs = gpu.topology(6, 4)
+    sym = os.environ.get("GFNFF_PCG_SYM")
     info = {"n": n, "nred": n - nfrag, "config": args.config, "coulomb_pairs": nc, "disp_pairs": nd,
+            "solver": main["solver"], "iters": main["iters"],
+            "pcg_lower": (sym != "0") if sym is not None else (n - nfrag) >= 4096,
             "bytes_hbonds": len(hbs) * (19 * 8 + 3 * 48 + 2 * 48)}
     if mols:   # block-diagonal EEQ: one reduced system per molecule (one fragment each)
         info["eeq_flops"] = sum((len(z) - 1) ** 3 / 3.0 + 2.0 * (len(z) - 1) ** 2 for z, _ in mols)

@@ -173,6 +173,11 @@ struct Engine::Impl {
     cudaEvent_t ev_fork0 = nullptr, ev_fork1 = nullptr, ev_join = nullptr;
     cusolverDnHandle_t sol = nullptr;
     int n = 0, nfrag = 0, K = 0, nred = 0, nmol = 0, nsplit = 1;
+    // Coulomb + D4 pairs: each pair once over a tile-pair list (default), or both
+    // directions by rows (GFNFF_PAIRS=rows)
+    DBuf<int2> symtiles;
+    int nsym = 0;
+    bool pairs_sym = true;
     // molecule structure and atom order
     DBuf<int> mol, perm;
     DBuf<int2> jr;
@@ -259,6 +264,12 @@ struct Engine::Impl {
     // response solve; probes (pcg_warm false) start from zero so that their timing is fair
     DBuf<int> pwarm;
     bool pcg_warm = false;
+    // matrices beyond L2 keep only their lower triangle; the PCG multiplies by tiles
+    bool pcg_lower = false;
+    int pcg_cols = 1;   // 1: 4 columns per warp step, 2: 8 (GFNFF_PCG_COLS=8)
+    DBuf<double> pyA;
+    DBuf<int2> ptiles;
+    int pcg_ntiles = 0;
     void pcg_launch(const double* rhs, double* x, int* inf, int slot)
     {
         CK(cudaMemsetAsync(pbar.p, 0, sizeof(unsigned int), stream));
@@ -267,6 +278,7 @@ struct Engine::Impl {
         A.blocks = pblocks.p; A.boff = pboff.p; A.maxrows = pcg_maxrows; A.maxinv = pcg_maxinv; A.part = ppart.p; A.rblk = prblk.p; A.partial = ppartial.p;
         A.bar = pbar.p; A.info = inf; A.iters = piters.p; A.max_iter = pcg_max_iter; A.tol = 1e-12;
         A.warm = pcg_warm ? pwarm.p + slot : nullptr;
+        A.lower = pcg_lower ? pcg_cols : 0; A.yA = pyA.p; A.tiles = ptiles.p; A.ntiles = pcg_ntiles;
         void* args[] = {&A};
         CK(cudaLaunchCooperativeKernel((const void*)k_pcg, dim3(pcg_grid), dim3(kPcgThreads), args, pcg_smem, stream));
     }
@@ -477,6 +489,18 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
     int max_range = 0;
     for (int m = 0; m < nm; ++m) max_range = std::max(max_range, mols[m]->n);
     P.nsplit = pair_splits(n, max_range);
+    {   // tile pairs (i tile <= j tile, both within the tile's molecules) of k_pairs_sym
+        std::vector<int2> tl;
+        const int nt = (n + kST - 1) / kST;
+        for (int I = 0; I < nt; ++I) {
+            const int i0 = I * kST, hi = hjr[std::min(n, i0 + kST) - 1].y;
+            for (int J = I; J * kST < hi; ++J) tl.push_back(make_int2(i0, J * kST));
+        }
+        P.symtiles.upload(tl);
+        P.nsym = (int)tl.size();
+        const char* pe = std::getenv("GFNFF_PAIRS");
+        P.pairs_sym = !(pe && !std::strcmp(pe, "rows"));
+    }
     // ---- global element table (union of the molecules' D4 element slots) ----
     std::vector<int> gZ;
     std::vector<std::vector<int>> gslot(nm);
@@ -912,6 +936,19 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
                 P.px.alloc(P.nred); P.pz.alloc(P.nred);
                 P.pcg_maxrows = maxrows;
                 P.pcg_maxinv = (int)maxinv;
+                {
+                    const char* e = std::getenv("GFNFF_PCG_SYM");
+                    P.pcg_lower = e ? std::strcmp(e, "0") != 0 : P.nred >= 4096;
+                    const char* ec = std::getenv("GFNFF_PCG_COLS");
+                    P.pcg_cols = (ec && !std::strcmp(ec, "8")) ? 2 : 1;
+                    std::vector<int2> tl;
+                    for (int i0 = 0; i0 < P.nred; i0 += kPcgT)
+                        for (int j0 = 0; j0 <= i0; j0 += kPcgT) tl.push_back(make_int2(i0, j0));
+                    P.ptiles.upload(tl);
+                    P.pcg_ntiles = (int)tl.size();
+                    P.pyA.alloc(P.nred);
+                    CK(cudaMemset(P.pyA.p, 0, (size_t)P.nred * sizeof(double)));
+                }
                 P.ppartial.alloc(4 * (size_t)G); P.pbar.alloc(2 * kBarGen); P.piters.alloc(1); P.pwarm.alloc(2);
                 CK(cudaMemset(P.pwarm.p, 0, 2 * sizeof(int)));
                 CK(cudaMemset(P.pbar.p, 0, 2 * kBarGen * sizeof(unsigned int)));
@@ -1146,7 +1183,7 @@ void Engine::launch_body()
     P.mark(3);
     if (P.nmol == 1) {
         const int sv = P.use_lu ? -1 : P.solver;
-        const bool full = sv == -1 || sv == Impl::SOLVE_PCG;
+        const bool full = sv == -1 || (sv == Impl::SOLVE_PCG && !P.pcg_lower);
         const bool aug = sv == Impl::SOLVE_TILED;
         if (P.nred > 0) {
             const long long nt = (P.nred + kMT - 1) / kMT;
@@ -1189,7 +1226,8 @@ void Engine::launch_body()
         P.mark(7);
         hb_rep_terms();
     }
-    k_pairs<double><<<tgrid, kTile, 0, s>>>(V, P.nsplit);
+    if (P.pairs_sym) k_pairs_sym<double><<<P.nsym, kST, 0, s>>>(V, P.symtiles.p);
+    else k_pairs<double><<<tgrid, kTile, 0, s>>>(V, P.nsplit);
     if (P.resp_on) {
         // u = B M^-1 B^T w with the factor (or the iteration) of this step's EEQ matrix
         k_resp_rhs<<<nblk(P.nred), kBlock, 0, s>>>(V, P.red2atom.p, P.anchor.p, P.bres.p);

@@ -202,35 +202,18 @@ struct EEQBatch {
 };
 
 // one molecule's atoms staged in shared memory: positions, alpha, EEQ diagonal, the
-// reduced index maps (local atom indices) and the rhs row
+// reduced index maps (local atom indices) and the rhs row.  For a molecule of one
+// fragment every reduced row has the same anchor a, and va[r] = A(k_r, a) is staged too,
+// so that an entry of M costs one EEQ element instead of four (same value bit for bit:
+// A is evaluated symmetrically and the terms are combined in the same order).
 struct MolStage {
-    double *x, *y, *z, *al, *ad, *rhs;
+    double *x, *y, *z, *al, *ad, *rhs, *va;
     int *red, *anc;
+    bool single;
 };
 constexpr int kStageAtoms = 320;                       // largest molecule of the batch path
-constexpr int kStageDoubles = 5 * kStageAtoms + kStageAtoms;  // + rhs (nr <= atoms)
+constexpr int kStageDoubles = 7 * kStageAtoms;         // x y z al ad, rhs, va
 constexpr int kStageInts = 2 * kStageAtoms;
-
-__device__ MolStage stage_molecule(const View& V, const EEQBatch& P, int r0, int nr, double* base, int* ibase)
-{
-    MolStage M{base, base + kStageAtoms, base + 2 * kStageAtoms, base + 3 * kStageAtoms, base + 4 * kStageAtoms,
-               base + 5 * kStageAtoms, ibase, ibase + kStageAtoms};
-    const int2 rg = V.jr[P.red2atom[r0]];
-    for (int i = threadIdx.x; i < rg.y - rg.x; i += blockDim.x) {
-        const double4 p = V.pos[rg.x + i];
-        M.x[i] = p.x; M.y[i] = p.y; M.z[i] = p.z;
-        M.al[i] = V.alpeeq[rg.x + i];
-        M.ad[i] = V.adiag[rg.x + i];
-    }
-    for (int r = threadIdx.x; r < nr; r += blockDim.x) {
-        const int k = P.red2atom[r0 + r], ak = P.anchor[k];
-        M.red[r] = k - rg.x;
-        M.anc[r] = ak - rg.x;
-        M.rhs[r] = eeq_rhs_atom(V, k, P.qlist, P.nq, P.q0) - eeq_rhs_atom(V, ak, P.qlist, P.nq, P.q0);
-    }
-    __syncthreads();
-    return M;
-}
 
 __device__ __forceinline__ double eeq_a_s(const MolStage& M, int a, int b)
 {
@@ -243,11 +226,46 @@ __device__ __forceinline__ double eeq_a_s(const MolStage& M, int a, int b)
     return erf(r / sqrt(s)) / r;
 }
 
+// fills the staged arrays of M (x .. va, red, anc) for the molecule of reduced rows
+// [r0, r0 + nr); `lane`/`nth` stride the work (block or warp), the caller synchronises
+__device__ void fill_stage(const View& V, const EEQBatch& P, int r0, int nr, MolStage& M, int lane, int nth,
+                           bool block)
+{
+    const int2 rg = V.jr[P.red2atom[r0]];
+    for (int i = lane; i < rg.y - rg.x; i += nth) {
+        const double4 p = V.pos[rg.x + i];
+        M.x[i] = p.x; M.y[i] = p.y; M.z[i] = p.z;
+        M.al[i] = V.alpeeq[rg.x + i];
+        M.ad[i] = V.adiag[rg.x + i];
+    }
+    for (int r = lane; r < nr; r += nth) {
+        const int k = P.red2atom[r0 + r], ak = P.anchor[k];
+        M.red[r] = k - rg.x;
+        M.anc[r] = ak - rg.x;
+        M.rhs[r] = eeq_rhs_atom(V, k, P.qlist, P.nq, P.q0) - eeq_rhs_atom(V, ak, P.qlist, P.nq, P.q0);
+    }
+    M.single = P.anchor[P.red2atom[r0]] == P.anchor[P.red2atom[r0 + nr - 1]];
+    if (block) __syncthreads(); else __syncwarp();
+    if (M.single)
+        for (int r = lane; r < nr; r += nth) M.va[r] = eeq_a_s(M, M.red[r], M.anc[r]);
+}
+
+__device__ MolStage stage_molecule(const View& V, const EEQBatch& P, int r0, int nr, double* base, int* ibase)
+{
+    MolStage M{base, base + kStageAtoms, base + 2 * kStageAtoms, base + 3 * kStageAtoms, base + 4 * kStageAtoms,
+               base + 5 * kStageAtoms, base + 6 * kStageAtoms, ibase, ibase + kStageAtoms, false};
+    fill_stage(V, P, r0, nr, M, threadIdx.x, blockDim.x, true);
+    __syncthreads();
+    return M;
+}
+
 // element (r, c) of [[M, .], [b^T, .]]; r == nr is the rhs row
 __device__ __forceinline__ double eeq_aug(const MolStage& M, int nr, int r, int c)
 {
     if (r == nr) return M.rhs[c];
-    const int k = M.red[r], ak = M.anc[r], l = M.red[c], al = M.anc[c];
+    const int k = M.red[r], l = M.red[c];
+    if (M.single) return ((eeq_a_s(M, k, l) - M.va[r]) - M.va[c]) + M.ad[M.anc[r]];
+    const int ak = M.anc[r], al = M.anc[c];
     return eeq_a_s(M, k, l) - eeq_a_s(M, k, al) - eeq_a_s(M, ak, l) + eeq_a_s(M, ak, al);
 }
 
@@ -271,6 +289,7 @@ __device__ void chol_trailing(double* S, int nr, int ccap, int k0, int k1, Off c
         for (int i = 0; i < RPL; ++i)
 #pragma unroll
             for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+#pragma unroll 4
         for (int p = k0; p < k1; ++p) {
             const double* cp = S + co(p) - p;   // element (r, p) at cp[r]
             double lr[RPL], lc[4];
@@ -302,55 +321,73 @@ __device__ void chol_trailing(double* S, int nr, int ccap, int k0, int k1, Off c
 
 // Blocked right-looking Cholesky of the first ccap columns of an augmented matrix with
 // nr + 1 rows whose column c starts at S + co(c) (element (r, c) at S[co(c) + r - c]);
-// updates reach columns < ccap only.  A panel of kCholNB columns is factored with one
-// block barrier per column: column k stays unscaled during the panel (the update of the
-// later panel columns uses u_r u_c / d_k with u the unscaled entries), so a step only
-// reads column k and only writes columns > k, each thread in the rows it owns (r = tid
-// mod blockDim); the panel is scaled by 1/sqrt(d_k) at its end.  The trailing columns
-// then take the panel's rank-kCholNB update (chol_trailing).  Returns false (uniformly)
-// when a pivot is not positive.
+// updates reach columns < ccap only.  Per panel of kCholNB columns: warp 0 factors the
+// panel's diagonal block in registers (lane i holds its row, pivots broadcast by
+// shuffles) and leaves it with the inverse pivots in shared memory; after one barrier
+// every thread solves its own rows of the panel against it (forward substitution along
+// the row, no further barrier); after a second barrier the trailing columns take the
+// panel's rank-kCholNB update (chol_trailing).  Returns false (uniformly) when a pivot
+// is not positive.
 constexpr int kCholNB = 8;
 template <class Off>
 __device__ bool chol_factor(double* S, int nr, int ccap, Off co)
 {
-    const int tid = threadIdx.x, nt = blockDim.x;
+    __shared__ double sL[kCholNB][kCholNB];   // diagonal block: L(i, j) for j < i, 1/L(j, j) at [j][j]
+    __shared__ int sbad;
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31;
     for (int k0 = 0; k0 < ccap; k0 += kCholNB) {
-        const int k1 = min(k0 + kCholNB, ccap);
-        double isq[kCholNB];
+        const int kb = min(kCholNB, ccap - k0), k1 = k0 + kb;
+        if (tid < 32) {
+            double a[kCholNB];
 #pragma unroll
-        for (int j = 0; j < kCholNB; ++j) isq[j] = 0.0;
+            for (int j = 0; j < kCholNB; ++j)
+                a[j] = (lane < kb && j <= lane) ? S[co(k0 + j) + lane - j] : 0.0;
+            bool bad = false;
 #pragma unroll
-        for (int kk = 0; kk < kCholNB; ++kk) {
-            const int k = k0 + kk;
-            if (k >= k1) break;
-            const double d = S[co(k)];
-            if (!(d > 0.0)) return false;   // every thread reads the same d after a barrier
-            isq[kk] = 1.0 / sqrt(d);
-            const double id = 1.0 / d;
-            const double* ck = S + co(k) - k;   // element (r, k) at ck[r]
-            double uc[kCholNB - 1];
+            for (int j = 0; j < kCholNB; ++j) {
+                if (j >= kb) break;
+                const double d = __shfl_sync(0xffffffffu, a[j], j);
+                if (!(d > 0.0)) {
+                    bad = true;
+                    break;
+                }
+                const double is = rsqrt(d);   // 1/L(j, j); L(j, j) = d / sqrt(d)
+                if (lane == j) a[j] = d * is;
+                else if (lane > j) a[j] *= is;
+                if (lane == j) sL[j][j] = is;
 #pragma unroll
-            for (int j = 0; j < kCholNB - 1; ++j) {
-                const int c = k + 1 + j;
-                uc[j] = c < k1 ? ck[c] * id : 0.0;
-            }
-            for (int r = k + 1 + tid; r <= nr; r += nt) {
-                const double ur = ck[r];
-#pragma unroll
-                for (int j = 0; j < kCholNB - 1; ++j) {
-                    const int c = k + 1 + j;
-                    if (c < k1 && r >= c) S[co(c) + r - c] -= ur * uc[j];
+                for (int p = j + 1; p < kCholNB; ++p) {
+                    const double lpj = __shfl_sync(0xffffffffu, a[j], p < kb ? p : 0);
+                    if (p < kb && lane >= p) a[p] -= a[j] * lpj;
                 }
             }
-            __syncthreads();
-        }
-        // scale the panel: L(r, k) = u_r / sqrt(d_k), L(k, k) = sqrt(d_k)
+            if (lane < kb) {
 #pragma unroll
-        for (int kk = 0; kk < kCholNB; ++kk) {
-            const int k = k0 + kk;
-            if (k >= k1) break;
-            double* ck = S + co(k) - k;
-            for (int r = k + tid; r <= nr; r += nt) ck[r] *= isq[kk];   // r == k: d / sqrt(d)
+                for (int j = 0; j < kCholNB; ++j)
+                    if (j <= lane) {
+                        S[co(k0 + j) + lane - j] = a[j];
+                        if (j < lane) sL[lane][j] = a[j];
+                    }
+            }
+            if (lane == 0) sbad = bad ? 1 : 0;
+        }
+        __syncthreads();
+        if (sbad) return false;   // uniform: read after the barrier by every thread
+        for (int r = k1 + tid; r <= nr; r += nt) {
+            double v[kCholNB];
+#pragma unroll
+            for (int j = 0; j < kCholNB; ++j) v[j] = j < kb ? S[co(k0 + j) + r - k0 - j] : 0.0;
+#pragma unroll
+            for (int j = 0; j < kCholNB; ++j) {
+                if (j >= kb) break;
+                double x = v[j];
+#pragma unroll
+                for (int p = 0; p < j; ++p) x -= v[p] * sL[j][p];
+                v[j] = x * sL[j][j];
+            }
+#pragma unroll
+            for (int j = 0; j < kCholNB; ++j)
+                if (j < kb) S[co(k0 + j) + r - k0 - j] = v[j];
         }
         __syncthreads();
         if (k1 >= ccap) continue;
@@ -359,6 +396,41 @@ __device__ bool chol_factor(double* S, int nr, int ccap, Off co)
         __syncthreads();
     }
     return true;
+}
+
+// L^T y = z for a factored augmented matrix (z_k = element (nr, k)), by 32-row blocks
+// from the bottom: warp 0 solves the diagonal block (lane l holds row kb + l, each y_j
+// broadcast with a shuffle), then every thread takes one row above the block and
+// subtracts the block's contribution, a dot product along its packed column.
+template <class Off>
+__device__ void chol_back_subst(const double* S, int nr, Off co, double* y)
+{
+    for (int k = threadIdx.x; k < nr; k += blockDim.x) y[k] = S[co(k) + nr - k];
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int kb = ((nr - 1) >> 5) << 5; kb >= 0; kb -= 32) {
+        const int ke = min(kb + 32, nr);
+        if (warp == 0) {
+            const int r = kb + lane;
+            double z = r < ke ? y[r] : 0.0;
+            const double dinv = r < ke ? 1.0 / S[co(r)] : 0.0;
+            double yr = 0.0;
+            for (int j = ke - 1; j >= kb; --j) {
+                const double yj = __shfl_sync(0xffffffffu, z * dinv, j - kb);
+                if (r == j) yr = yj;
+                if (r < j) z -= S[co(r) + j - r] * yj;   // L(j, r)
+            }
+            if (r < ke) y[r] = yr;
+        }
+        __syncthreads();
+        for (int r = threadIdx.x; r < kb; r += blockDim.x) {
+            const double* cr = S + co(r) - r;   // element (j, r) at cr[j]
+            double a = 0.0;
+            for (int j = kb; j < ke; ++j) a += cr[j] * y[j];
+            y[r] -= a;
+        }
+        __syncthreads();
+    }
 }
 
 // Cholesky + back substitution L^T y = z of the augmented matrix (z_k = element (nr, k));
@@ -370,18 +442,7 @@ __device__ bool chol_aug_solve(double* S, int nr, Off co, double* y, double* lk)
     const bool ok = chol_factor(S, nr, nr, co);
     __syncthreads();
     if (!ok) return false;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (warp == 0) {
-        for (int k = nr - 1; k >= 0; --k) {
-            const double* ck = S + co(k);
-            double s = 0.0;
-            for (int r = k + 1 + lane; r < nr; r += 32) s += ck[r - k] * y[r];
-            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-            if (lane == 0) y[k] = (ck[nr - k] - s) / ck[0];
-            __syncwarp();
-        }
-    }
-    __syncthreads();
+    chol_back_subst(S, nr, co, y);
     return true;
 }
 
@@ -408,55 +469,85 @@ __device__ bool chol_two_stage(const EEQBatch& P, const MolStage& MS, int m, int
     double* G = P.M + P.moff[m];
     const int lda = nr + 1;
     // ---- stage 1: panel columns [0, s), rows c..nr, packed
-    auto po = [&](int c) { return (long long)c * (nr + 1) - (long long)c * (c - 1) / 2; };
+    const PackedCols po{nr + 1};
     for (int c = warp; c < s; c += nw)
         for (int r = c + lane; r <= nr; r += 32) S[po(c) + r - c] = eeq_aug(MS, nr, r, c);
     __syncthreads();
-    const bool ok1 = chol_factor(S, nr, s, PackedCols{nr + 1});
+    const bool ok1 = chol_factor(S, nr, s, po);
     __syncthreads();
     if (!ok1) return false;
-    for (int c = 0; c < s; ++c)
-        for (int r = c + tid; r <= nr; r += nt) G[(size_t)c * lda + r] = S[po(c) + r - c];
-    // ---- stage 2: trailing block A22 - L21 L21^T (rows c..nr of columns c >= s)
-    for (int c = s + warp; c < nr; c += nw)
-        for (int r = c + lane; r <= nr; r += 32) {
-            double a = eeq_aug(MS, nr, r, c);
-            for (int p = 0; p < s; ++p) a -= S[po(p) + r - p] * S[po(p) + c - p];
-            G[(size_t)c * lda + r] = a;
+    for (int c = warp; c < s; c += nw)   // a warp per column keeps many loads/stores in flight
+        for (int r = c + lane; r <= nr; r += 32) G[(size_t)c * lda + r] = S[po(c) + r - c];
+    // ---- stage 2: trailing block A22 - L21 L21^T (rows c..nr of columns c >= s) into G:
+    // a warp owns 4 columns x 128 rows, the rank-s product in registers (as chol_trailing)
+    {
+        const int m2 = nr - s;
+        const int ncg = (m2 + 3) >> 2, nrb = (nr + 1 - s + 127) >> 7;
+        for (int task = warp; task < ncg * nrb; task += nw) {
+            const int cg = task / nrb, rb = task % nrb;
+            const int c0 = s + 4 * cg, rbase = s + 128 * rb;
+            if (rbase + 127 < c0) continue;
+            double acc[4][4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+#pragma unroll 4
+            for (int p = 0; p < s; ++p) {
+                const double* cp = S + po(p) - p;
+                double lr[4], lc[4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int r = rbase + lane + 32 * i;
+                    lr[i] = r <= nr ? cp[r] : 0.0;
+                }
+#pragma unroll
+                for (int j = 0; j < 4; ++j) lc[j] = c0 + j < nr ? cp[c0 + j] : 0.0;
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) acc[i][j] = fma(lr[i], lc[j], acc[i][j]);
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int c = c0 + j;
+                if (c >= nr) break;
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int r = rbase + lane + 32 * i;
+                    if (r >= c && r <= nr) G[(size_t)c * lda + r] = eeq_aug(MS, nr, r, c) - acc[i][j];
+                }
+            }
         }
+    }
     __syncthreads();
     const int mt = nr - s;
     const PackedCols co{mt + 1};
-    for (int c = 0; c < mt; ++c)
-        for (int r = c + tid; r <= mt; r += nt) S[co(c) + r - c] = G[(size_t)(s + c) * lda + s + r];
+    for (int c = warp; c < mt; c += nw)
+        for (int r = c + lane; r <= mt; r += 32) S[co(c) + r - c] = G[(size_t)(s + c) * lda + s + r];
     __syncthreads();
     double* lk = S + co(mt);
     double* ys = lk + mt + 1;
     if (!chol_aug_solve(S, mt, co, ys, lk)) return false;
     for (int k = tid; k < mt; k += nt) y[s + k] = ys[k];
-    // ---- stage 3: w_k = z_k - sum_{r >= s} L_rk y_r, then L11^T y1 = w
-    double* w = S;                     // s entries (the trailing factor is no longer needed)
-    double* yt = S + s;                // copy of y[s..nr)
+    // ---- stage 3: w_k = z_k - sum_{r >= s} L_rk y_r, then L11^T y1 = w with L11 and w
+    // copied back into shared memory as a packed (s + 1) x s augmented matrix
+    const PackedCols c1{s + 1};
+    double* yt = S + c1(s);             // copy of y[s..nr) behind the packed L11
+    double* y1 = yt + mt;
     for (int k = tid; k < mt; k += nt) yt[k] = ys[k];
     __syncthreads();
+    for (int c = warp; c < s; c += nw)
+        for (int r = c + lane; r < s; r += 32) S[c1(c) + r - c] = G[(size_t)c * lda + r];
     for (int k = warp; k < s; k += nw) {
         double a = 0.0;
         for (int r = s + lane; r < nr; r += 32) a += G[(size_t)k * lda + r] * yt[r - s];
         for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
-        if (lane == 0) w[k] = G[(size_t)k * lda + nr] - a;
+        if (lane == 0) S[c1(k) + s - k] = G[(size_t)k * lda + nr] - a;
     }
     __syncthreads();
-    if (warp == 0) {
-        for (int k = s - 1; k >= 0; --k) {
-            double a = 0.0;
-            for (int r = k + 1 + lane; r < s; r += 32) a += G[(size_t)k * lda + r] * w[r];
-            for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
-            if (lane == 0) w[k] = (w[k] - a) / G[(size_t)k * lda + k];
-            __syncwarp();
-        }
-    }
-    __syncthreads();
-    for (int k = tid; k < s; k += nt) y[k] = w[k];
+    chol_back_subst(S, s, c1, y1);
+    for (int k = tid; k < s; k += nt) y[k] = y1[k];
     return true;
 }
 
@@ -464,7 +555,7 @@ __device__ bool chol_two_stage(const EEQBatch& P, const MolStage& MS, int m, int
 constexpr int kWarpMols = 8;          // molecules per warp-mode work item
 constexpr int kWarpMaxRed = 70;       // largest reduced system of the warp path
 constexpr int kWarpAtoms = kWarpMaxRed + 1;
-constexpr int kWarpRegion = 7 * kWarpAtoms + kWarpMaxRed * (kWarpMaxRed + 3) / 2 + 2 * kWarpMaxRed + 2;
+constexpr int kWarpRegion = 8 * kWarpAtoms + kWarpMaxRed * (kWarpMaxRed + 3) / 2 + 2 * kWarpMaxRed + 2;
 
 __device__ void warp_solve(const View& V, const EEQBatch& P, int m, double* R)
 {
@@ -475,22 +566,11 @@ __device__ void warp_solve(const View& V, const EEQBatch& P, int m, double* R)
         return;
     }
     MolStage M{R, R + kWarpAtoms, R + 2 * kWarpAtoms, R + 3 * kWarpAtoms, R + 4 * kWarpAtoms, R + 5 * kWarpAtoms,
-               reinterpret_cast<int*>(R + 6 * kWarpAtoms), reinterpret_cast<int*>(R + 6 * kWarpAtoms) + kWarpAtoms};
-    const int2 rg = V.jr[P.red2atom[r0]];
-    for (int i = lane; i < rg.y - rg.x; i += 32) {
-        const double4 p = V.pos[rg.x + i];
-        M.x[i] = p.x; M.y[i] = p.y; M.z[i] = p.z;
-        M.al[i] = V.alpeeq[rg.x + i];
-        M.ad[i] = V.adiag[rg.x + i];
-    }
-    for (int r = lane; r < nr; r += 32) {
-        const int k = P.red2atom[r0 + r], ak = P.anchor[k];
-        M.red[r] = k - rg.x;
-        M.anc[r] = ak - rg.x;
-        M.rhs[r] = eeq_rhs_atom(V, k, P.qlist, P.nq, P.q0) - eeq_rhs_atom(V, ak, P.qlist, P.nq, P.q0);
-    }
+               R + 6 * kWarpAtoms, reinterpret_cast<int*>(R + 7 * kWarpAtoms),
+               reinterpret_cast<int*>(R + 7 * kWarpAtoms) + kWarpAtoms, false};
+    fill_stage(V, P, r0, nr, M, lane, 32, false);
     __syncwarp();
-    double* S = R + 7 * kWarpAtoms;
+    double* S = R + 8 * kWarpAtoms;
     const PackedCols co{nr + 1};
     double* lk = S + co(nr);
     double* ys = lk + nr + 1;

@@ -319,6 +319,187 @@ __global__ void __launch_bounds__(kTile) k_pairs(View V, int nsplit)
 }
 
 // ------------------------------------------------------------------------------------
+// The same Coulomb + D4 pair terms with every pair evaluated once (Newton's third law).
+// Blocks take 64 x 64 tiles (i tile <= j tile, listed at set-up; only j > i within a
+// diagonal tile).  Row i keeps its sums in registers as in k_pairs; the j side of every
+// pair (gradient, dE/dCN_j from j's half contraction against i's current weights, and the
+// far-pair potential of the exact-gradient mode) is summed over the warp's 32 rows with
+// shuffles and kept per warp in shared memory, then added once per tile.
+// ------------------------------------------------------------------------------------
+constexpr int kST = 64;
+
+// one D4 pair in arithmetic type R with both CN derivatives: energy e, dE/dr / r in dedr,
+// dE/dCN_i in dci, dE/dCN_j in dcj (wi: current weights of i in registers)
+template <class R>
+__device__ __forceinline__ void d4_pair_sym(double d2, const double* g0, const double* dgi, const double* dgj,
+                                            const double (*sw0)[kST], const double (*sw)[kST], int jj, int nrj,
+                                            int nri, const double (&wi)[7], double r4r2_d, double zz_d, bool want_dc,
+                                            double& e, double& dedr, double& dci, double& dcj)
+{
+    R c6 = R(0), dc6i = R(0), dc6j = R(0);
+    for (int b = 0; b < nrj; ++b) c6 += (R)__ldg(g0 + b) * (R)sw0[b][jj];
+    if (want_dc) {
+        for (int b = 0; b < nrj; ++b) dc6i += (R)__ldg(dgi + b) * (R)sw[b][jj];
+#pragma unroll
+        for (int a = 0; a < 7; ++a)
+            if (a < nri) dc6j += (R)__ldg(dgj + a) * (R)wi[a];
+    }
+    const R q2 = (R)d2;
+    const R r4r2 = (R)r4r2_d;
+    const R t = R(0.58) * sqrt(r4r2) + R(4.80);
+    const R r0sq = t * t;
+    const R zz = (R)zz_d;
+    const R r6 = q2 * q2 * q2, r06 = r0sq * r0sq * r0sq;
+    const R t6 = R(1) / (r6 + r06);
+    const R t8 = R(1) / (r6 * q2 + r06 * r0sq);
+    const R sum = t6 + R(2) * r4r2 * t8;
+    e = -(double)(c6 * sum * zz);
+    const R d6 = R(-6) * q2 * q2 * t6 * t6, d8 = R(-8) * r6 * t8 * t8;
+    dedr = -(double)(c6 * zz * (d6 + R(2) * r4r2 * d8));
+    dci = -(double)(dc6i * sum * zz);
+    dcj = -(double)(dc6j * sum * zz);
+}
+
+template <class R>
+__global__ void __launch_bounds__(kST) k_pairs_sym(View V, const int2* __restrict__ tiles)
+{
+    __shared__ double sx[kST], sy[kST], sz[kST], s0x[kST], s0y[kST], s0z[kST];
+    __shared__ double sq[kST], sa[kST], sze[kST], ssz[kST];
+    __shared__ double sw0[7][kST], sw[7][kST];
+    __shared__ int ssl[kST], snr[kST];
+    __shared__ double jacc[kST / 32][5][kST];
+    const int2 tp = tiles[blockIdx.x];
+    const int i0 = tp.x, j0 = tp.y, i = i0 + threadIdx.x;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const bool act = i < V.n;
+    const int ic = act ? i : i0;
+    const double4 pi = V.pos[ic], p0i = V.pos0[ic];
+    const double ai = V.alpeeq[ic], qi = V.q[ic], zi = V.zeta[ic], szi = V.szr[ic];
+    const int2 rg = act ? V.jr[i] : make_int2(0, 0);
+    const int si = V.slot[ic], nri = V.nref[ic];
+    double wi[7];
+#pragma unroll
+    for (int a = 0; a < 7; ++a) wi[a] = V.w[(size_t)ic * 7 + a];
+    const double* g0i = V.g0 + (size_t)ic * V.K * 7;
+    const double* dgi = V.hdg + (size_t)ic * V.K * 7;
+    const bool want_dc = !V.exact, want_far = V.cfar != nullptr;
+    {
+        const int jl = j0 + threadIdx.x;
+        if (jl < V.n) {
+            const int u = threadIdx.x;
+            const double4 p = V.pos[jl], p0 = V.pos0[jl];
+            sx[u] = p.x; sy[u] = p.y; sz[u] = p.z;
+            s0x[u] = p0.x; s0y[u] = p0.y; s0z[u] = p0.z;
+            sq[u] = V.q[jl]; sa[u] = V.alpeeq[jl]; sze[u] = V.zeta[jl]; ssz[u] = V.szr[jl];
+            ssl[u] = V.slot[jl]; snr[u] = V.nref[jl];
+#pragma unroll
+            for (int b = 0; b < 7; ++b) {
+                sw0[b][u] = V.w0[(size_t)jl * 7 + b];
+                sw[b][u] = V.w[(size_t)jl * 7 + b];
+            }
+        }
+    }
+    __syncthreads();
+    const double tsp = 2.0 / 1.772453850905516;
+    double ec = 0.0, ed = 0.0, gx = 0.0, gy = 0.0, gz = 0.0, dcn = 0.0, cfar = 0.0;
+    const int cnt = min(kST, V.n - j0);
+    for (int jj = 0; jj < cnt; ++jj) {
+        const int j = j0 + jj;
+        double fx = 0.0, fy = 0.0, fz = 0.0, dcj = 0.0, cfj = 0.0;
+        bool valid = act && j > i && j >= rg.x && j < rg.y;
+        double dx = 0.0, dy = 0.0, dz = 0.0, d2 = 0.0;
+        if (valid) {
+            dx = pi.x - sx[jj]; dy = pi.y - sy[jj]; dz = pi.z - sz[jj];
+            d2 = dx * dx + dy * dy + dz * dz;
+            valid = d2 >= 1e-20;
+        }
+        if (valid) {
+            double f = 0.0;   // dE/dr / r
+            if (d2 <= 10000.0) {
+                const double s = ai + sa[jj];
+                const double qq = qi * sq[jj];
+                if (d2 >= 36.0 * s) {
+                    const double ir = rsqrt(d2);
+                    const double e = qq * ir;
+                    ec += e;
+                    f -= e * ir * ir;
+                } else {
+                    const double r = sqrt(d2);
+                    const double g = 1.0 / sqrt(s);
+                    const double gr = g * r;
+                    const double ef = erf(gr);
+                    ec += qq * ef / r;
+                    f += qq * ((g * exp(-gr * gr) * tsp) / r - ef / d2) / r;
+                }
+            } else if (want_far) {
+                const double ir = rsqrt(d2);   // cut pair: its EEQ element is 1/r
+                cfar += sq[jj] * ir;
+                cfj = qi * ir;
+            }
+            if (d2 <= 2500.0 && d2_exact(p0i, make_double4(s0x[jj], s0y[jj], s0z[jj], 0.0)) <= 3600.0) {
+                const int sj = ssl[jj], nrj = snr[jj];
+                const double* dgj = V.hdg + ((size_t)j * V.K + si) * 7;
+                const double r4r2 = 3.0 * szi * ssz[jj], zz = zi * sze[jj];
+                double e, dedr, dci;
+                // mixed form: pairs closer than 15 bohr (the strong ones) stay FP64
+                if (sizeof(R) == sizeof(double) || d2 < 225.0)
+                    d4_pair_sym<double>(d2, g0i + sj * 7, dgi + sj * 7, dgj, sw0, sw, jj, nrj, nri, wi, r4r2, zz,
+                                        want_dc, e, dedr, dci, dcj);
+                else
+                    d4_pair_sym<R>(d2, g0i + sj * 7, dgi + sj * 7, dgj, sw0, sw, jj, nrj, nri, wi, r4r2, zz,
+                                   want_dc, e, dedr, dci, dcj);
+                ed += e;
+                f += dedr;
+                dcn += dci;
+            }
+            gx += f * dx; gy += f * dy; gz += f * dz;
+            fx = -f * dx; fy = -f * dy; fz = -f * dz;
+        }
+        if (__any_sync(0xffffffffu, valid)) {
+            for (int o = 16; o > 0; o >>= 1) {
+                fx += __shfl_xor_sync(0xffffffffu, fx, o);
+                fy += __shfl_xor_sync(0xffffffffu, fy, o);
+                fz += __shfl_xor_sync(0xffffffffu, fz, o);
+            }
+            if (want_dc)
+                for (int o = 16; o > 0; o >>= 1) dcj += __shfl_xor_sync(0xffffffffu, dcj, o);
+            if (want_far)
+                for (int o = 16; o > 0; o >>= 1) cfj += __shfl_xor_sync(0xffffffffu, cfj, o);
+        }
+        if (lane == 0) {
+            jacc[warp][0][jj] = fx; jacc[warp][1][jj] = fy; jacc[warp][2][jj] = fz;
+            jacc[warp][3][jj] = dcj; jacc[warp][4][jj] = cfj;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < cnt) {
+        const int j = j0 + threadIdx.x;
+        double a[5];
+#pragma unroll
+        for (int k = 0; k < 5; ++k) {
+            a[k] = 0.0;
+#pragma unroll
+            for (int w = 0; w < kST / 32; ++w) a[k] += jacc[w][k][threadIdx.x];
+        }
+        if (a[0] != 0.0) atomicAdd(V.grad + 3 * j, a[0]);
+        if (a[1] != 0.0) atomicAdd(V.grad + 3 * j + 1, a[1]);
+        if (a[2] != 0.0) atomicAdd(V.grad + 3 * j + 2, a[2]);
+        if (a[3] != 0.0) atomicAdd(V.dEdcn + j, a[3]);
+        if (a[4] != 0.0) atomicAdd(V.cfar + j, a[4]);
+    }
+    if (act) {
+        if (gx != 0.0) atomicAdd(V.grad + 3 * i, gx);
+        if (gy != 0.0) atomicAdd(V.grad + 3 * i + 1, gy);
+        if (gz != 0.0) atomicAdd(V.grad + 3 * i + 2, gz);
+        if (dcn != 0.0) atomicAdd(V.dEdcn + i, dcn);
+        if (cfar != 0.0) atomicAdd(V.cfar + i, cfar);
+    }
+    const int m = act ? V.mol[i] : -1;
+    eadd(V, ec, m, T_COUL);
+    eadd(V, ed, m, T_DISP);
+}
+
+// ------------------------------------------------------------------------------------
 // EEQ charge response (exact-gradient mode): with u = B M^-1 B^T w and w = dE/dq of the
 // Coulomb pairs cut at 100 bohr, the gradient gains -sum_ij u_i q_j dA_ij/dr over all
 // pairs (A is the uncut EEQ matrix) and u_i dx_i/dCN_i through the CN chain (k_post).

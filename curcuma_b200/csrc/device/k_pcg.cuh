@@ -41,6 +41,11 @@ struct PCGArgs {
     int* iters;
     int* warm;            // when non-null and *warm != 0, x holds the previous solution of the
                           // same system and is the initial guess; set to 1 on convergence
+    int lower;            // 1 or 2: only the lower triangle of M is stored; M p by tiles
+                          // (matvec_tiles, streaming 4 or 8 columns per warp at once)
+    double* yA;           // lower: n-vector the tiles add M p into (zero between uses)
+    const int2* tiles;    // lower: tiles {first row I0, first column J0}, I0 >= J0
+    int ntiles;
     int max_iter;
     double tol;           // converged when max|b - M x| <= tol * max|b|
 };
@@ -217,6 +222,107 @@ __device__ double matvec_rows(const PCGArgs& A, const double* v, int row0, int r
     return vmv;
 }
 
+// element (r, c) of M, from the lower triangle when only that is stored
+__device__ __forceinline__ double mget(const PCGArgs& A, int r, int c)
+{
+    return (A.lower && r < c) ? A.M[(size_t)r * A.lda + c] : A.M[(size_t)c * A.lda + r];
+}
+
+// Symmetric M p from the lower triangle, for matrices too large for L2: the tiles
+// (kPcgT x kPcgT, I0 >= J0) are dealt round-robin to the grid blocks.  A warp takes
+// columns c of the tile kPcgCols at a time (independent 8-byte loads per lane in flight,
+// streamed past L2) and forms u_r += M(r, c) p_c for the tile's rows (registers) and
+// v_c = sum_r M(r, c) p_r (warp sum); the transposed part v goes to y_J, the row part u
+// (summed over the block's warps in shared memory) to y_I, both as FP64 atomics into
+// A.yA.  Diagonal tiles use r >= c for u and r > c for v.  Returns the thread's part of
+// p^T M p.  The caller reads y after a grid barrier and zeroes what it read.
+constexpr int kPcgT = 128;
+template <int kPcgCols>   // columns a warp streams at once (4 * kPcgCols loads per lane in flight)
+__device__ double matvec_tiles_c(const PCGArgs& A, const double* p, double* red)
+{
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    double pap = 0.0;
+    for (int t = blockIdx.x; t < A.ntiles; t += gridDim.x) {
+        const int2 tl = A.tiles[t];
+        const int I0 = tl.x, J0 = tl.y;
+        const bool diag = I0 == J0;
+        const int ni = min(kPcgT, A.n - I0), nj = min(kPcgT, A.n - J0);
+        double u[4], pr[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int r = lane + 32 * i;
+            u[i] = 0.0;
+            pr[i] = r < ni ? p[I0 + r] : 0.0;
+        }
+        for (int cb = warp * kPcgCols; cb < nj; cb += nw * kPcgCols) {
+            double m[kPcgCols][4], v[kPcgCols], pc[kPcgCols];
+#pragma unroll
+            for (int q = 0; q < kPcgCols; ++q) {
+                const int c = cb + q;
+                pc[q] = c < nj ? p[J0 + c] : 0.0;
+                const double* col = A.M + (size_t)(J0 + (c < nj ? c : 0)) * A.lda + I0;
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int r = lane + 32 * i;
+                    m[q][i] = (c < nj && r < ni && (!diag || r >= c)) ? __ldcs(col + r) : 0.0;
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < kPcgCols; ++q) {
+                const int c = cb + q;
+                v[q] = 0.0;
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int r = lane + 32 * i;
+                    u[i] += m[q][i] * pc[q];
+                    if (!diag || r > c) v[q] += m[q][i] * pr[i];
+                }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+                for (int q = 0; q < kPcgCols; ++q) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+            double vq = 0.0;
+#pragma unroll
+            for (int q = 0; q < kPcgCols; ++q)
+                if (lane == q) vq = v[q];
+            if (lane < kPcgCols) {
+                const int c = cb + lane;
+                if (c < nj && vq != 0.0) {
+                    atomicAdd(A.yA + J0 + c, vq);
+                    pap += p[J0 + c] * vq;
+                }
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i) red[warp * kPcgT + lane + 32 * i] = u[i];
+        __syncthreads();
+        for (int r = threadIdx.x; r < ni; r += blockDim.x) {
+            double s = 0.0;
+            for (int w = 0; w < nw; ++w) s += red[w * kPcgT + r];
+            atomicAdd(A.yA + I0 + r, s);
+            pap += p[I0 + r] * s;
+        }
+        __syncthreads();
+    }
+    return pap;
+}
+
+__device__ double matvec_tiles(const PCGArgs& A, const double* p, double* red)
+{
+    return A.lower == 2 ? matvec_tiles_c<8>(A, p, red) : matvec_tiles_c<4>(A, p, red);
+}
+
+// Ap for the owned rows after matvec_tiles and a grid barrier: read y (L2) and zero it
+__device__ void take_tiles_result(const PCGArgs& A, int row0, int nrow, double* Ap)
+{
+    for (int k = threadIdx.x; k < nrow; k += blockDim.x) {
+        Ap[k] = __ldcg(A.yA + row0 + k);
+        __stcg(A.yA + row0 + k, 0.0);
+    }
+    __syncthreads();
+}
+
 // inverse of a preconditioner block of at most kPcgSmall rows by one thread
 // (Gauss-Jordan in registers-sized local storage)
 constexpr int kPcgSmall = 4;
@@ -227,7 +333,7 @@ __device__ void invert_small(const PCGArgs& A, int bk, double* I)
     double g[kPcgSmall][kPcgSmall], inv[kPcgSmall][kPcgSmall];
     for (int i = 0; i < s; ++i)
         for (int j = 0; j < s; ++j) {
-            g[i][j] = A.M[(size_t)(bl.x + j) * A.lda + bl.x + i];
+            g[i][j] = mget(A, bl.x + i, bl.x + j);
             inv[i][j] = i == j ? 1.0 : 0.0;
         }
     for (int c = 0; c < s; ++c) {
@@ -254,7 +360,7 @@ __device__ void invert_warp(const PCGArgs& A, int bk, double* I, double* colc)
     const int2 bl = A.blocks[bk];
     const int s = bl.y;
     if (lane < s)
-        for (int i = 0; i < s; ++i) I[i * s + lane] = A.M[(size_t)(bl.x + i) * A.lda + bl.x + lane];
+        for (int i = 0; i < s; ++i) I[i * s + lane] = mget(A, bl.x + lane, bl.x + i);
     __syncwarp();
     for (int c = 0; c < s; ++c) {
         colc[lane] = lane < s ? I[lane * s + c] : 0.0;
@@ -312,7 +418,7 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(PCGArgs A)
         __syncthreads();
         for (int e = threadIdx.x; e < s * s; e += blockDim.x) {
             const int i = e / s, j = e % s;
-            G[i * GL + j] = A.M[(size_t)(bl.x + j) * A.lda + bl.x + i];
+            G[i * GL + j] = mget(A, bl.x + i, bl.x + j);
             I[e] = i == j ? 1.0 : 0.0;
         }
         __syncthreads();
@@ -348,10 +454,17 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(PCGArgs A)
     // ---- x = x0 (the previous solution, or 0), r = b - M x0, z = P^-1 r.  x0 is complete
     // in global memory since the previous launch, so no grid barrier is needed here.
     const bool warm = A.warm != nullptr && *A.warm != 0;
-    if (warm) {
+    bool ok = true;
+    if (warm) {   // uniform over the grid: every block reads the same flag
         update_p(p, A.x, A.n, 0.0);
         __syncthreads();
-        matvec_rows(A, p, row0, row1, Ap);
+        if (A.lower) {
+            matvec_tiles(A, p, G);
+            ok = grid_sync(A.bar, gen);
+            take_tiles_result(A, row0, nrow, Ap);
+        } else {
+            matvec_rows(A, p, row0, row1, Ap);
+        }
         __syncthreads();
     }
     double bmax_t = 0.0;
@@ -365,7 +478,7 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(PCGArgs A)
     double rz_t = apply_precond(nrow, meta, Bs, rs, zs);
     for (int k = threadIdx.x; k < nrow; k += blockDim.x) __stcg(A.z + row0 + k, zs[k]);
     block_sum_max(rz_t, bmax_t, A.partial + 4 * blockIdx.x);
-    bool ok = grid_sync(A.bar, gen);
+    ok = grid_sync(A.bar, gen) && ok;
     double rz = 0.0, bmax = 0.0;
     if (ok) grid_totals(A.partial, 0, rz, bmax);
     update_p(p, A.z, A.n, 0.0);
@@ -374,10 +487,11 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(PCGArgs A)
     while (ok && !conv && it < A.max_iter) {
         ++it;
         __syncthreads();
-        const double pap_t = matvec_rows(A, p, row0, row1, Ap);
+        const double pap_t = A.lower ? matvec_tiles(A, p, G) : matvec_rows(A, p, row0, row1, Ap);
         block_sum_max(pap_t, 0.0, A.partial + 4 * blockIdx.x);
         ok = grid_sync(A.bar, gen);
         if (!ok) break;
+        if (A.lower) take_tiles_result(A, row0, nrow, Ap);
         double pap, unused;
         grid_totals(A.partial, 0, pap, unused);
         const double alpha = rz / pap;
@@ -402,7 +516,14 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(PCGArgs A)
             if (!ok) break;
             update_p(p, A.x, A.n, 0.0);
             __syncthreads();
-            matvec_rows(A, p, row0, row1, Ap);
+            if (A.lower) {
+                matvec_tiles(A, p, G);
+                ok = grid_sync(A.bar, gen);
+                if (!ok) break;
+                take_tiles_result(A, row0, nrow, Ap);
+            } else {
+                matvec_rows(A, p, row0, row1, Ap);
+            }
             __syncthreads();
             rmax_t = 0.0;
             for (int k = threadIdx.x; k < nrow; k += blockDim.x) {

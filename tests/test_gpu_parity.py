@@ -133,12 +133,15 @@ def test_error_paths():
     assert gpu.calculateEnergy(True) != 0.0 and not gpu.hasError()
 
 
-@pytest.mark.parametrize("solver", ["tiled", "library", "pcg"])
+@pytest.mark.parametrize("solver", ["tiled", "library", "pcg", "pcg-lower"])
 @pytest.mark.parametrize("system", ["water64", "water200", "alkane", "peptide"])
 def test_eeq_solvers(solver, system, monkeypatch):
     """Every EEQ solver of the reduced system against the oracle; the 64-water cluster
     has 128 reduced unknowns, so the tiled Cholesky's right-hand-side row forms a tile of
-    its own, and the alkane (one fragment) exercises the PCG with 64-row blocks."""
+    its own, and the alkane (one fragment) exercises the PCG with 64-row blocks.
+    pcg-lower forces the PCG form of large systems (lower triangle only, M p by tiles)."""
+    monkeypatch.setenv("GFNFF_PCG_SYM", "1" if solver == "pcg-lower" else "0")
+    solver = "pcg" if solver == "pcg-lower" else solver
     monkeypatch.setenv("GFNFF_EEQ_SOLVER", solver)
     Z, X = {"water64": lambda: workloads.water_cluster(64, 9),
             "water200": lambda: workloads.water_cluster(200, 10),
@@ -177,6 +180,7 @@ def test_pcg_warm_start(system, monkeypatch):
     energies as the oracle on every geometry of a short sequence, in fewer iterations than
     a start from zero."""
     monkeypatch.setenv("GFNFF_EEQ_SOLVER", "pcg")
+    monkeypatch.setenv("GFNFF_PCG_SYM", "1" if system == "water200" else "0")
     Z, X = {"water200": lambda: workloads.water_cluster(200, 10),
             "alkane": lambda: workloads.alkane(64, 1001)}[system]()
     rng = np.random.default_rng(5)
