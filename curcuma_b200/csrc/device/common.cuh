@@ -244,6 +244,9 @@ struct View {
     int exact;                // drop the D4 dC6/dCN term
     double* cfar;             // n: potential of the Coulomb pairs beyond 100 bohr, or null
     const double* u;          // n: EEQ charge response, or null
+    // axis-aligned boxes of the tiles of 128 consecutive atoms (current geometry)
+    const double4* boxlo;
+    const double4* boxhi;
 };
 
 // Adds v to term `term` of molecule `mol` (mol < 0: nothing to add).  Every thread of

@@ -176,6 +176,7 @@ struct Engine::Impl {
     // Coulomb + D4 pairs: each pair once over a tile-pair list (default), or both
     // directions by rows (GFNFF_PAIRS=rows)
     DBuf<int2> symtiles;
+    DBuf<double4> boxlo, boxhi;   // per tile of kTile atoms
     int nsym = 0;
     bool pairs_sym = true;
     // molecule structure and atom order
@@ -230,7 +231,8 @@ struct Engine::Impl {
     int lda = 2;           // leading dimension of M (>= nred + 1, even; row nred holds b for k_chol)
     bool use_lu = false;   // reduced EEQ matrix not positive definite: pivoted LU instead
     // EEQ solver of a single-molecule engine (chosen at upload, see upload_batch)
-    enum { SOLVE_LIBRARY = 0, SOLVE_TILED = 1, SOLVE_PCG = 2 };
+    enum { SOLVE_LIBRARY = 0, SOLVE_TILED = 1, SOLVE_PCG = 2, SOLVE_BATCH = 3 };
+    bool batch_ready = false;   // the batched kernel's structures exist (batches, small molecules)
     int solver = SOLVE_LIBRARY;
     // persistent tiled Cholesky (k_chol)
     DBuf<int4> ctasks;
@@ -266,6 +268,10 @@ struct Engine::Impl {
     bool pcg_warm = false;
     // matrices beyond L2 keep only their lower triangle; the PCG multiplies by tiles
     bool pcg_lower = false;
+    // pipelined CG (one grid barrier per iteration; GFNFF_PCG=classic|pipelined forces one)
+    bool pcg_pipe = true;
+    size_t pcg_smem_pipe = 0;
+    DBuf<double> pz2;
     int pcg_cols = 1;   // 1: 4 columns per warp step, 2: 8 (GFNFF_PCG_COLS=8)
     DBuf<double> pyA;
     DBuf<int2> ptiles;
@@ -274,13 +280,18 @@ struct Engine::Impl {
     {
         CK(cudaMemsetAsync(pbar.p, 0, sizeof(unsigned int), stream));
         PCGArgs A;
-        A.M = M.p; A.lda = lda; A.n = nred; A.b = rhs; A.x = x; A.z = pz.p;
+        A.M = M.p; A.lda = lda; A.n = nred; A.b = rhs; A.x = x; A.z = pz.p; A.z2 = pz2.p;
         A.blocks = pblocks.p; A.boff = pboff.p; A.maxrows = pcg_maxrows; A.maxinv = pcg_maxinv; A.part = ppart.p; A.rblk = prblk.p; A.partial = ppartial.p;
         A.bar = pbar.p; A.info = inf; A.iters = piters.p; A.max_iter = pcg_max_iter; A.tol = 1e-12;
         A.warm = pcg_warm ? pwarm.p + slot : nullptr;
         A.lower = pcg_lower ? pcg_cols : 0; A.yA = pyA.p; A.tiles = ptiles.p; A.ntiles = pcg_ntiles;
         void* args[] = {&A};
-        CK(cudaLaunchCooperativeKernel((const void*)k_pcg, dim3(pcg_grid), dim3(kPcgThreads), args, pcg_smem, stream));
+        if (pcg_pipe)
+            CK(cudaLaunchCooperativeKernel((const void*)k_pcg_pipe, dim3(pcg_grid), dim3(kPcgThreads), args,
+                                           pcg_smem_pipe, stream));
+        else
+            CK(cudaLaunchCooperativeKernel((const void*)k_pcg, dim3(pcg_grid), dim3(kPcgThreads), args, pcg_smem,
+                                           stream));
     }
     bool timing = false;
     // One evaluation is ~20 kernels and memsets.  Everything after the positions is
@@ -322,6 +333,8 @@ struct Engine::Impl {
         V.exact = opt.exact_gradient ? 1 : 0;
         V.cfar = resp_on ? cfar.p : nullptr;
         V.u = resp_on ? ures.p : nullptr;
+        V.boxlo = boxlo.p;
+        V.boxhi = boxhi.p;
         return V;
     }
     // caller index (molecule m, local atom a) -> internal index
@@ -490,6 +503,7 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
     for (int m = 0; m < nm; ++m) max_range = std::max(max_range, mols[m]->n);
     P.nsplit = pair_splits(n, max_range);
     {   // tile pairs (i tile <= j tile, both within the tile's molecules) of k_pairs_sym
+        const int nt0 = (n + kTile - 1) / kTile;
         std::vector<int2> tl;
         const int nt = (n + kST - 1) / kST;
         for (int I = 0; I < nt; ++I) {
@@ -497,6 +511,8 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
             for (int J = I; J * kST < hi; ++J) tl.push_back(make_int2(i0, J * kST));
         }
         P.symtiles.upload(tl);
+        P.boxlo.alloc(nt0);
+        P.boxhi.alloc(nt0);
         P.nsym = (int)tl.size();
         const char* pe = std::getenv("GFNFF_PAIRS");
         P.pairs_sym = !(pe && !std::strcmp(pe, "rows"));
@@ -603,7 +619,10 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
         P.anchor.upload(anchor); P.atom2red.upload(a2r); P.red2atom.upload(r2a);
         P.frag_off.upload(off); P.frag_atoms.upload(fa); P.q0.upload(q0); P.qlist.upload(ql);
         P.roff.upload(roff); P.moff.upload(moff);
-        if (nm > 1) {
+        // batches, and single molecules small enough for the batched kernel's staging
+        // (a candidate EEQ solver for them)
+        P.batch_ready = nm > 1 || n <= kStageAtoms;
+        if (P.batch_ready) {
             std::vector<int> ord(nm);
             std::iota(ord.begin(), ord.end(), 0);
             std::stable_sort(ord.begin(), ord.end(),
@@ -949,7 +968,8 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
                     P.pyA.alloc(P.nred);
                     CK(cudaMemset(P.pyA.p, 0, (size_t)P.nred * sizeof(double)));
                 }
-                P.ppartial.alloc(4 * (size_t)G); P.pbar.alloc(2 * kBarGen); P.piters.alloc(1); P.pwarm.alloc(2);
+                P.ppartial.alloc(8 * (size_t)G); P.pbar.alloc(2 * kBarGen); P.piters.alloc(1); P.pwarm.alloc(2);
+                P.pz2.alloc(P.nred);
                 CK(cudaMemset(P.pwarm.p, 0, 2 * sizeof(int)));
                 CK(cudaMemset(P.pbar.p, 0, 2 * kBarGen * sizeof(unsigned int)));
                 CK(cudaMemset(P.piters.p, 0, sizeof(int)));
@@ -959,6 +979,21 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
                 int per_sm = 0;
                 CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)k_pcg, kPcgThreads, smem));
                 P.pcg_ready = per_sm >= 1;
+                // the pipelined form keeps ten owned-row vectors instead of four
+                P.pcg_smem_pipe = smem + 6 * (size_t)maxrows * sizeof(double);
+                const char* pe = std::getenv("GFNFF_PCG");
+                // default: pipelined for L2-resident matrices (latency-bound); the tiled product
+                // of large ones measured faster in the classic form
+                P.pcg_pipe = pe ? std::strcmp(pe, "classic") != 0 : !P.pcg_lower;
+                P.pcg_pipe = P.pcg_pipe && P.pcg_smem_pipe <= 220 * 1024;
+                if (P.pcg_pipe) {
+                    CK(cudaFuncSetAttribute((const void*)k_pcg_pipe, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)P.pcg_smem_pipe));
+                    int ps = 0;
+                    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ps, (const void*)k_pcg_pipe, kPcgThreads,
+                                                                     P.pcg_smem_pipe));
+                    P.pcg_pipe = ps >= 1;
+                }
             }
         }
     }
@@ -988,9 +1023,12 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
             if (env && !std::strcmp(env, "library")) cand = {Impl::SOLVE_LIBRARY};
             else if (env && !std::strcmp(env, "tiled")) cand = {Impl::SOLVE_TILED};
             else if (env && !std::strcmp(env, "pcg") && P.pcg_ready) cand = {Impl::SOLVE_PCG};
+            else if (env && !std::strcmp(env, "batched") && P.batch_ready && !P.resp_on) cand = {Impl::SOLVE_BATCH};
             else {
                 cand = {Impl::SOLVE_LIBRARY, Impl::SOLVE_TILED};
                 if (P.pcg_ready) cand.push_back(Impl::SOLVE_PCG);
+                // the batched kernel keeps no factor for the charge-response solve
+                if (P.batch_ready && !P.resp_on) cand.push_back(Impl::SOLVE_BATCH);
             }
             if (cand.size() == 1) {
                 P.solver = cand[0];
@@ -1052,7 +1090,12 @@ const char* Engine::solver_name() const
 {
     if (p_->nmol != 1) return "batched";
     if (p_->use_lu) return "lu";
-    return p_->solver == Impl::SOLVE_PCG ? "pcg" : (p_->solver == Impl::SOLVE_TILED ? "tiled" : "library");
+    switch (p_->solver) {
+    case Impl::SOLVE_PCG: return "pcg";
+    case Impl::SOLVE_TILED: return "tiled";
+    case Impl::SOLVE_BATCH: return "batched";
+    default: return "library";
+    }
 }
 
 int Engine::eeq_iterations()
@@ -1170,6 +1213,7 @@ void Engine::launch_body()
         hb_rep_terms();
     }
     P.mark(1);
+    k_boxes<<<nblk(n, kTile), kTile, 0, s>>>(n, P.pos.p, P.boxlo.p, P.boxhi.p);
     (mixed ? k_cn<float> : k_cn<double>)<<<tgrid, kTile, 0, s>>>(V, P.nsplit);
     P.mark(2);
     k_d4_weights<<<nblk(n), kBlock, 0, s>>>(V);
@@ -1181,7 +1225,7 @@ void Engine::launch_body()
     }
     // EEQ
     P.mark(3);
-    if (P.nmol == 1) {
+    if (P.nmol == 1 && !(P.solver == Impl::SOLVE_BATCH && !P.use_lu)) {
         const int sv = P.use_lu ? -1 : P.solver;
         const bool full = sv == -1 || (sv == Impl::SOLVE_PCG && !P.pcg_lower);
         const bool aug = sv == Impl::SOLVE_TILED;

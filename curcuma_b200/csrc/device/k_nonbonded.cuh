@@ -46,6 +46,56 @@ __global__ void k_positions(int n, const int* __restrict__ perm, const double* _
 }
 
 // ------------------------------------------------------------------------------------
+// tile boxes: min/max corner of every tile of kTile consecutive atoms.  Atoms are in
+// Morton order within a molecule, so a tile is compact in space and the short-range
+// pair kernels (CN, CN chain rule) skip partner tiles whose box is farther than their
+// cutoff from the row tile's box.  The box distance is a lower bound of every pair
+// distance in floating point too (min/max are exact, rounding is monotonic), so the
+// skipped pairs are exactly pairs the cutoff test would reject.
+// ------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(kTile) k_boxes(int n, const double4* __restrict__ pos, double4* lo, double4* hi)
+{
+    __shared__ double red[6][kTile / 32];
+    const int i = blockIdx.x * kTile + threadIdx.x;
+    const double4 p = pos[i < n ? i : blockIdx.x * kTile];
+    double v[6] = {p.x, p.y, p.z, -p.x, -p.y, -p.z};   // minima of x and of -x
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        for (int o = 16; o > 0; o >>= 1) v[k] = fmin(v[k], __shfl_xor_sync(0xffffffffu, v[k], o));
+        if (lane == 0) red[k][w] = v[k];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double r[6];
+        for (int k = 0; k < 6; ++k) {
+            r[k] = red[k][0];
+            for (int q = 1; q < kTile / 32; ++q) r[k] = fmin(r[k], red[k][q]);
+        }
+        lo[blockIdx.x] = make_double4(r[0], r[1], r[2], 0.0);
+        hi[blockIdx.x] = make_double4(-r[3], -r[4], -r[5], 0.0);
+    }
+}
+
+// true when every atom of the partner range [t0, t0 + cnt) is at least sqrt(cut2) from
+// every atom of the row tile starting at i0 (a multiple of kTile)
+__device__ __forceinline__ bool tiles_far(const View& V, int i0, int t0, int cnt, double cut2)
+{
+    const int a = i0 / kTile, b0 = t0 / kTile, b1 = (t0 + cnt - 1) / kTile;
+    double4 jl = V.boxlo[b0], jh = V.boxhi[b0];
+    if (b1 != b0) {
+        const double4 l2 = V.boxlo[b1], h2 = V.boxhi[b1];
+        jl = make_double4(fmin(jl.x, l2.x), fmin(jl.y, l2.y), fmin(jl.z, l2.z), 0.0);
+        jh = make_double4(fmax(jh.x, h2.x), fmax(jh.y, h2.y), fmax(jh.z, h2.z), 0.0);
+    }
+    const double4 il = V.boxlo[a], ih = V.boxhi[a];
+    const double dx = fmax(0.0, fmax(jl.x - ih.x, il.x - jh.x));
+    const double dy = fmax(0.0, fmax(jl.y - ih.y, il.y - jh.y));
+    const double dz = fmax(0.0, fmax(jl.z - ih.z, il.z - jh.z));
+    return dx * dx + dy * dy + dz * dz >= cut2;
+}
+
+// ------------------------------------------------------------------------------------
 // coordination numbers: erf counting over partners closer than 6 bohr
 // (cn_calculator.cpp:367-428); the log-squash is applied in k_d4_weights
 // ------------------------------------------------------------------------------------
@@ -63,6 +113,7 @@ __global__ void __launch_bounds__(kTile) k_cn(View V, int nsplit)
     const double kn = -7.5;
     double s = 0.0;
     for (int t0 = jb; t0 < je; t0 += kTile) {
+        if (tiles_far(V, i0, t0, min(kTile, je - t0), 36.0)) continue;   // uniform in the block
         __syncthreads();
         const int jl = t0 + threadIdx.x;
         if (jl < je) {
@@ -592,6 +643,7 @@ __global__ void __launch_bounds__(kTile) k_cn_chain(View V, int nsplit)
     const double kn = -7.5, sqrtpi = 1.77245385091;
     double gx = 0.0, gy = 0.0, gz = 0.0;
     for (int t0 = jb; t0 < je; t0 += kTile) {
+        if (tiles_far(V, i0, t0, min(kTile, je - t0), 36.0)) continue;   // uniform in the block
         __syncthreads();
         const int jl = t0 + threadIdx.x;
         if (jl < je) {

@@ -29,13 +29,14 @@ struct PCGArgs {
     const double* b;
     double* x;            // solution
     double* z;            // preconditioned residual (shared between grid blocks)
+    double* z2;           // k_pcg_pipe: second shared n-vector (published vectors alternate)
     const int2* blocks;   // preconditioner blocks {first row, size}
     const long long* boff;
     int maxrows;          // most rows owned by one grid block
     int maxinv;           // most inverse entries held by one grid block
     const int4* part;     // per grid block: rows [x, y), preconditioner blocks [z, w)
     const int* rblk;      // preconditioner block of every row
-    double* partial;      // gridDim.x * 4
+    double* partial;      // gridDim.x * 8
     unsigned int* bar;    // arrival count at [0], generation at [kBarGen]
     int* info;
     int* iters;
@@ -379,25 +380,14 @@ __device__ void invert_warp(const PCGArgs& A, int bk, double* I, double* colc)
     }
 }
 
-__global__ void __launch_bounds__(kPcgThreads) k_pcg(PCGArgs A)
+// inverses of the grid block's preconditioner blocks (Gauss-Jordan, SPD, no pivoting:
+// up to kPcgSmall rows by one thread, up to kPcgWarpMax by one warp, larger ones by the
+// whole block with G as scratch) and the per-row records of apply_precond
+__device__ void pcg_setup(const PCGArgs& A, int4 pt, long long boff0, double* G, double* Bs, int4* meta)
 {
-    extern __shared__ double sm[];
-    constexpr int GL = kPcgMaxBlock + 1;
-    const int4 pt = A.part[blockIdx.x];
-    const int row0 = pt.x, row1 = pt.y, nrow = row1 - row0;
-    const long long boff0 = pt.z < pt.w ? A.boff[pt.z] : 0;
-    double* p = sm;                              // n: search direction, replicated
-    double* G = p + ((A.n + 1) & ~1);            // kPcgMaxBlock x GL scratch (even offsets
-                                                 // keep the int4 records 16-byte aligned)
-    double* xs = G + kPcgMaxBlock * GL;          // owned rows: x, r, z, M p
-    double* rs = xs + A.maxrows;
-    double* zs = rs + A.maxrows;
-    double* Ap = zs + A.maxrows;
-    double* Bs = Ap + A.maxrows;                 // inverses of the owned blocks
-    int4* meta = reinterpret_cast<int4*>(Bs + A.maxinv);   // per owned row, see apply_precond
-    __shared__ unsigned int gen;
     __shared__ double piv;
-    if (threadIdx.x == 0) gen = *(volatile unsigned int*)(A.bar + kBarGen);
+    constexpr int GL = kPcgMaxBlock + 1;
+    const int row0 = pt.x, nrow = pt.y - pt.x;
     // ---- inverse of every owned preconditioner block (Gauss-Jordan on [M_bb | I]; SPD,
     // no pivoting); small blocks one per thread, larger ones by the whole grid block
     for (int bk = pt.z + threadIdx.x; bk < pt.w; bk += blockDim.x)
@@ -451,6 +441,28 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(PCGArgs A)
         const int2 bl = A.blocks[bk];
         meta[k] = make_int4(bl.x - row0, bl.y, (int)(A.boff[bk] - boff0) + (rr - bl.x) * bl.y, 0);
     }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kPcgThreads) k_pcg(PCGArgs A)
+{
+    extern __shared__ double sm[];
+    constexpr int GL = kPcgMaxBlock + 1;
+    const int4 pt = A.part[blockIdx.x];
+    const int row0 = pt.x, row1 = pt.y, nrow = row1 - row0;
+    const long long boff0 = pt.z < pt.w ? A.boff[pt.z] : 0;
+    double* p = sm;                              // n: search direction, replicated
+    double* G = p + ((A.n + 1) & ~1);            // kPcgMaxBlock x GL scratch (even offsets
+                                                 // keep the int4 records 16-byte aligned)
+    double* xs = G + kPcgMaxBlock * GL;          // owned rows: x, r, z, M p
+    double* rs = xs + A.maxrows;
+    double* zs = rs + A.maxrows;
+    double* Ap = zs + A.maxrows;
+    double* Bs = Ap + A.maxrows;                 // inverses of the owned blocks
+    int4* meta = reinterpret_cast<int4*>(Bs + A.maxinv);   // per owned row, see apply_precond
+    __shared__ unsigned int gen;
+    if (threadIdx.x == 0) gen = *(volatile unsigned int*)(A.bar + kBarGen);
+    pcg_setup(A, pt, boff0, G, Bs, meta);
     // ---- x = x0 (the previous solution, or 0), r = b - M x0, z = P^-1 r.  x0 is complete
     // in global memory since the previous launch, so no grid barrier is needed here.
     const bool warm = A.warm != nullptr && *A.warm != 0;
@@ -548,6 +560,213 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(PCGArgs A)
         const double beta = rzn / rz;
         rz = rzn;
         update_p(p, A.z, A.n, beta);
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < nrow; k += blockDim.x) A.x[row0 + k] = xs[k];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        *A.info = !ok ? 2 : (conv ? 0 : 3);
+        *A.iters = it;
+        if (A.warm) *A.warm = (ok && conv) ? 1 : 0;
+    }
+}
+
+}  // namespace
+
+namespace {
+
+// block partials (sum a, sum b, max c) into out[0..2]
+__device__ void block_sum3(double a, double b, double c, double* out)
+{
+    __shared__ double ra[32], rb[32], rc[32];
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_xor_sync(0xffffffffu, a, o);
+        b += __shfl_xor_sync(0xffffffffu, b, o);
+        c = fmax(c, __shfl_xor_sync(0xffffffffu, c, o));
+    }
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    __syncthreads();
+    if (lane == 0) { ra[w] = a; rb[w] = b; rc[w] = c; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double x = 0.0, y = 0.0, z = 0.0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) { x += ra[k]; y += rb[k]; z = fmax(z, rc[k]); }
+        __stcg(out, x);
+        __stcg(out + 1, y);
+        __stcg(out + 2, z);
+    }
+}
+
+// grid totals of block_sum3's partials (slot offset `set` in each block's 8 doubles),
+// identical in every block (fixed reduction order)
+__device__ void grid_totals3(const double* partial, int set, double& a, double& b, double& c)
+{
+    __shared__ double wa[32], wb[32], wc[32];
+    __syncthreads();
+    double x = 0.0, y = 0.0, z = 0.0;
+    for (int k = threadIdx.x; k < (int)gridDim.x; k += blockDim.x) {
+        x += __ldcg(partial + 8 * k + set);
+        y += __ldcg(partial + 8 * k + set + 1);
+        z = fmax(z, __ldcg(partial + 8 * k + set + 2));
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        x += __shfl_xor_sync(0xffffffffu, x, o);
+        y += __shfl_xor_sync(0xffffffffu, y, o);
+        z = fmax(z, __shfl_xor_sync(0xffffffffu, z, o));
+    }
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) { wa[w] = x; wb[w] = y; wc[w] = z; }
+    __syncthreads();
+    x = y = z = 0.0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) { x += wa[k]; y += wb[k]; z = fmax(z, wc[k]); }
+    a = x;
+    b = y;
+    c = z;
+}
+
+// Pipelined block-Jacobi preconditioned CG (P. Ghysels, W. Vanroose, Parallel Computing
+// 40 (2014) 224-238, the preconditioned pipelined CG): the iterates of k_pcg in exact
+// arithmetic, rearranged so that both inner products of an iteration (r.u, w.u) are
+// reduced together with the publication of m = P^-1 w, whose product n = M m is then
+// formed locally.  One grid barrier per iteration (k_pcg needs two; the tiled product
+// of large systems adds its own).  Published vectors and block partials alternate
+// between two buffers with the barrier count: set k is written before barrier k and
+// read right after it; the same buffer is written again (set k + 2) only after barrier
+// k + 1, which no block passes before it has finished reading set k.  The result is
+// accepted on the true residual b - M x; otherwise the recurrence restarts from it.
+__global__ void __launch_bounds__(kPcgThreads) k_pcg_pipe(PCGArgs A)
+{
+    extern __shared__ double sm[];
+    constexpr int GL = kPcgMaxBlock + 1;
+    const int4 pt = A.part[blockIdx.x];
+    const int row0 = pt.x, row1 = pt.y, nrow = row1 - row0;
+    const long long boff0 = pt.z < pt.w ? A.boff[pt.z] : 0;
+    const int R = A.maxrows;
+    double* v = sm;                              // n: operand of the next product, replicated
+    double* G = v + ((A.n + 1) & ~1);            // kPcgMaxBlock x GL scratch
+    double* xs = G + kPcgMaxBlock * GL;          // owned rows of x r u w z q s p m n
+    double* rs = xs + R;
+    double* us = rs + R;
+    double* ws = us + R;
+    double* zs = ws + R;
+    double* qs = zs + R;
+    double* ss = qs + R;
+    double* ps = ss + R;
+    double* ms = ps + R;
+    double* ns = ms + R;
+    double* Bs = ns + R;                         // inverses of the owned blocks
+    int4* meta = reinterpret_cast<int4*>(Bs + A.maxinv);
+    __shared__ unsigned int gen;
+    if (threadIdx.x == 0) gen = *(volatile unsigned int*)(A.bar + kBarGen);
+    pcg_setup(A, pt, boff0, G, Bs, meta);
+    bool ok = true;
+    int phase = 0;   // barrier count: selects the published vector and partial set
+    // out = (M v) for the owned rows, v replicated in shared memory
+    auto product = [&](double* out) {
+        if (A.lower) {
+            matvec_tiles(A, v, G);
+            ok = grid_sync(A.bar, gen) && ok;
+            ++phase;
+            take_tiles_result(A, row0, nrow, out);
+        } else {
+            matvec_rows(A, v, row0, row1, out);
+            __syncthreads();
+        }
+    };
+    // publish the owned rows of src, barrier, replicate the whole vector into v
+    auto publish = [&](const double* src, double pa, double pb, double pc, double& ta, double& tb, double& tc) {
+        double* pub = (phase & 1) ? A.z2 : A.z;
+        for (int k = threadIdx.x; k < nrow; k += blockDim.x) __stcg(pub + row0 + k, src[k]);
+        block_sum3(pa, pb, pc, A.partial + 8 * blockIdx.x + 4 * (phase & 1));
+        ok = grid_sync(A.bar, gen) && ok;
+        grid_totals3(A.partial, 4 * (phase & 1), ta, tb, tc);
+        update_p(v, pub, A.n, 0.0);
+        ++phase;
+        __syncthreads();
+    };
+    // ---- start: x0 (previous solution or 0), r = b - M x0, u = P^-1 r, w = M u
+    const bool warm = A.warm != nullptr && *A.warm != 0;
+    if (warm) {
+        update_p(v, A.x, A.n, 0.0);
+        __syncthreads();
+        product(ns);
+    }
+    double bmax_t = 0.0;
+    for (int k = threadIdx.x; k < nrow; k += blockDim.x) {
+        const double bv = A.b[row0 + k];
+        xs[k] = warm ? v[row0 + k] : 0.0;
+        rs[k] = warm ? bv - ns[k] : bv;
+        zs[k] = qs[k] = ss[k] = ps[k] = 0.0;
+        bmax_t = fmax(bmax_t, fabs(bv));
+    }
+    __syncthreads();
+    apply_precond(nrow, meta, Bs, rs, us);
+    double bmax = 0.0, t1, t2;
+    publish(us, 0.0, 0.0, bmax_t, t1, t2, bmax);
+    product(ws);
+    int it = 0;
+    bool conv = ok && bmax == 0.0, first = true;
+    double gam_prev = 1.0, alpha_prev = 1.0;
+    while (ok && !conv && it < A.max_iter) {
+        double g_t = 0.0, d_t = 0.0, rm_t = 0.0;
+        for (int k = threadIdx.x; k < nrow; k += blockDim.x) {
+            g_t += rs[k] * us[k];
+            d_t += ws[k] * us[k];
+            rm_t = fmax(rm_t, fabs(rs[k]));
+        }
+        __syncthreads();
+        apply_precond(nrow, meta, Bs, ws, ms);
+        double gam, del, rmax;
+        publish(ms, g_t, d_t, rm_t, gam, del, rmax);
+        if (!ok) break;
+        if (rmax <= A.tol * bmax) {
+            // accept only on the true residual r = b - M x; otherwise restart from it
+            double u1, u2;
+            publish(xs, 0.0, 0.0, 0.0, u1, u2, u1);
+            if (!ok) break;
+            product(ns);
+            double rt = 0.0;
+            for (int k = threadIdx.x; k < nrow; k += blockDim.x) {
+                rs[k] = A.b[row0 + k] - ns[k];
+                rt = fmax(rt, fabs(rs[k]));
+            }
+            __syncthreads();
+            apply_precond(nrow, meta, Bs, rs, us);
+            double rtrue;
+            publish(us, 0.0, 0.0, rt, u1, u2, rtrue);
+            if (!ok) break;
+            if (rtrue <= A.tol * bmax) {
+                conv = true;
+                break;
+            }
+            product(ws);
+            for (int k = threadIdx.x; k < nrow; k += blockDim.x) zs[k] = qs[k] = ss[k] = ps[k] = 0.0;
+            __syncthreads();
+            first = true;
+            continue;
+        }
+        ++it;
+        product(ns);
+        double beta, alpha;
+        if (first) {
+            beta = 0.0;
+            alpha = gam / del;
+        } else {
+            beta = gam / gam_prev;
+            alpha = gam / (del - beta * gam / alpha_prev);
+        }
+        first = false;
+        gam_prev = gam;
+        alpha_prev = alpha;
+        for (int k = threadIdx.x; k < nrow; k += blockDim.x) {
+            const double z = ns[k] + beta * zs[k], q = ms[k] + beta * qs[k];
+            const double sv = ws[k] + beta * ss[k], pv = us[k] + beta * ps[k];
+            zs[k] = z; qs[k] = q; ss[k] = sv; ps[k] = pv;
+            xs[k] += alpha * pv;
+            rs[k] -= alpha * sv;
+            us[k] -= alpha * q;
+            ws[k] -= alpha * z;
+        }
+        __syncthreads();
     }
     __syncthreads();
     for (int k = threadIdx.x; k < nrow; k += blockDim.x) A.x[row0 + k] = xs[k];
