@@ -244,7 +244,7 @@ struct View {
     int exact;                // drop the D4 dC6/dCN term
     double* cfar;             // n: potential of the Coulomb pairs beyond 100 bohr, or null
     const double* u;          // n: EEQ charge response, or null
-    // axis-aligned boxes of the tiles of 128 consecutive atoms (current geometry)
+    // axis-aligned boxes of the runs of 32 consecutive atoms (current geometry)
     const double4* boxlo;
     const double4* boxhi;
 };

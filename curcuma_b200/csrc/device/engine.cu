@@ -176,7 +176,7 @@ struct Engine::Impl {
     // Coulomb + D4 pairs: each pair once over a tile-pair list (default), or both
     // directions by rows (GFNFF_PAIRS=rows)
     DBuf<int2> symtiles;
-    DBuf<double4> boxlo, boxhi;   // per tile of kTile atoms
+    DBuf<double4> boxlo, boxhi;   // per run of kBoxAtoms atoms
     int nsym = 0;
     bool pairs_sym = true;
     // molecule structure and atom order
@@ -287,7 +287,7 @@ struct Engine::Impl {
         A.lower = pcg_lower ? pcg_cols : 0; A.yA = pyA.p; A.tiles = ptiles.p; A.ntiles = pcg_ntiles;
         void* args[] = {&A};
         if (pcg_pipe)
-            CK(cudaLaunchCooperativeKernel((const void*)k_pcg_pipe, dim3(pcg_grid), dim3(kPcgThreads), args,
+            CK(cudaLaunchCooperativeKernel((const void*)k_pcg_pipe, dim3(pcg_grid), dim3(kPcgPipeThreads), args,
                                            pcg_smem_pipe, stream));
         else
             CK(cudaLaunchCooperativeKernel((const void*)k_pcg, dim3(pcg_grid), dim3(kPcgThreads), args, pcg_smem,
@@ -503,7 +503,6 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
     for (int m = 0; m < nm; ++m) max_range = std::max(max_range, mols[m]->n);
     P.nsplit = pair_splits(n, max_range);
     {   // tile pairs (i tile <= j tile, both within the tile's molecules) of k_pairs_sym
-        const int nt0 = (n + kTile - 1) / kTile;
         std::vector<int2> tl;
         const int nt = (n + kST - 1) / kST;
         for (int I = 0; I < nt; ++I) {
@@ -511,8 +510,8 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
             for (int J = I; J * kST < hi; ++J) tl.push_back(make_int2(i0, J * kST));
         }
         P.symtiles.upload(tl);
-        P.boxlo.alloc(nt0);
-        P.boxhi.alloc(nt0);
+        P.boxlo.alloc((n + kBoxAtoms - 1) / kBoxAtoms);
+        P.boxhi.alloc((n + kBoxAtoms - 1) / kBoxAtoms);
         P.nsym = (int)tl.size();
         const char* pe = std::getenv("GFNFF_PAIRS");
         P.pairs_sym = !(pe && !std::strcmp(pe, "rows"));
@@ -990,7 +989,7 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
                     CK(cudaFuncSetAttribute((const void*)k_pcg_pipe, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             (int)P.pcg_smem_pipe));
                     int ps = 0;
-                    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ps, (const void*)k_pcg_pipe, kPcgThreads,
+                    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ps, (const void*)k_pcg_pipe, kPcgPipeThreads,
                                                                      P.pcg_smem_pipe));
                     P.pcg_pipe = ps >= 1;
                 }
@@ -1207,17 +1206,29 @@ void Engine::launch_body()
     if (P.natm) k_atm<<<nblk(P.natm), kBlock, 0, s2>>>(V, TripSoA{P.natm, P.at_i.p, P.at_j.p, P.at_k.p, P.at_c9.p, P.at_r0ij.p, P.at_r0ik.p, P.at_r0jk.p, P.at_sc.p});
     if (P.nbatm) k_batm<<<nblk(P.nbatm), kBlock, 0, s2>>>(V, TripSoA{P.nbatm, P.ba_i.p, P.ba_j.p, P.ba_k.p, P.ba_c9.p, nullptr, nullptr, nullptr, nullptr});
     };
-    if (fork) {
+    // Batches: the side terms start at once (the batched EEQ kernel fills every SM anyway).
+    // Single molecules: they fork right after the EEQ right-hand side and are issued after
+    // the solver's launch, so that the latency-bound cooperative PCG takes its SM slots first
+    // and the side kernels fill what it leaves (k_pcg uses half of an SM's registers).
+    const bool early = fork && P.nmol > 1;
+    if (early) {
         CK(cudaEventRecord(P.ev_fork0, s));
         CK(cudaStreamWaitEvent(s2, P.ev_fork0, 0));
         hb_rep_terms();
     }
+    auto side_after = [&]() {
+        if (!fork || early) return;
+        CK(cudaStreamWaitEvent(s2, P.ev_fork1, 0));
+        hb_rep_terms();
+        bonded_terms();
+        CK(cudaEventRecord(P.ev_join, s2));
+    };
     P.mark(1);
     k_boxes<<<nblk(n, kTile), kTile, 0, s>>>(n, P.pos.p, P.boxlo.p, P.boxhi.p);
     (mixed ? k_cn<float> : k_cn<double>)<<<tgrid, kTile, 0, s>>>(V, P.nsplit);
     P.mark(2);
     k_d4_weights<<<nblk(n), kBlock, 0, s>>>(V);
-    if (fork) {
+    if (early) {
         CK(cudaEventRecord(P.ev_fork1, s));
         CK(cudaStreamWaitEvent(s2, P.ev_fork1, 0));
         bonded_terms();
@@ -1239,6 +1250,7 @@ void Engine::launch_body()
             k_eeq_rhs<<<nblk(P.nred), kBlock, 0, s>>>(V, P.red2atom.p, P.anchor.p, P.qlist.p, P.nq, P.q0.p, P.bvec.p,
                                                       aug ? P.M.p + P.nred : nullptr, P.lda);
         P.mark(5);
+        if (fork) CK(cudaEventRecord(P.ev_fork1, s));
         if (P.nred > 0) {
             if (sv == Impl::SOLVE_TILED) {
                 P.chol_launch();
@@ -1252,13 +1264,16 @@ void Engine::launch_body()
                 CS(cusolverDnDgetrs(P.sol, CUBLAS_OP_N, P.nred, 1, P.M.p, P.lda, P.ipiv.p, P.bvec.p, P.nred, P.info2.p));
             }
         }
+        side_after();
     } else {
         P.mark(4);
         P.mark(5);
         CK(cudaMemsetAsync(P.bnext.p, 0, sizeof(int), s));
+        if (fork && !early) CK(cudaEventRecord(P.ev_fork1, s));   // single molecule, batched solver
         EEQBatch B{P.roff.p, P.moff.p, P.border.p, P.bitems.p, P.nbitems, P.bnext.p, P.batch_smem_max, P.red2atom.p,
                    P.anchor.p, P.qlist.p, P.nq, P.q0.p, P.M.p, P.bvec.p, P.info.p};
         k_eeq_batch<<<P.batch_grid, 512, P.batch_smem, s>>>(V, B);
+        side_after();
     }
     const double* ysol = P.bvec.p;
     if (P.nmol == 1 && !P.use_lu && P.solver == Impl::SOLVE_TILED) ysol = P.ysol.p;

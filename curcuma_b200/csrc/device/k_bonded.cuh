@@ -2,8 +2,9 @@
 // FP64 atomics, term energies summed per molecule.  Included by engine.cu (one translation unit).
 #pragma once
 
-// resident blocks per SM requested for the HB kernel: 4 caps it at 128 registers (a few
-// spills), which measured 1.5x faster than the uncapped 190 registers at 2 blocks per SM
+// resident blocks per SM requested for the FP64 HB kernel: 4 caps it at 128 registers (a
+// few spills), which measured 1.5x faster than the uncapped 190 registers at 2 blocks per
+// SM.  The FP32 form needs 94 registers without spills and asks for 5 blocks.
 #ifndef GFNFF_HB_MINBLOCKS
 #define GFNFF_HB_MINBLOCKS 4
 #endif
@@ -369,7 +370,8 @@ __device__ __forceinline__ R hb_len(V3<R> v, R& inv)
 // R = float, because the FP32 rounding of per-element-pair constants is the same for
 // every strong bond and would add up over thousands of them.
 template <class R>
-__global__ void __launch_bounds__(kBlock, GFNFF_HB_MINBLOCKS) k_hbonds(View V, HBSoA S, int t0, int t1)
+__global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 5 : GFNFF_HB_MINBLOCKS) k_hbonds(View V, HBSoA S, int t0,
+                                                                                        int t1)
 {
     const int t = t0 + blockIdx.x * blockDim.x + threadIdx.x;
     R etot = R(0.0);

@@ -46,53 +46,58 @@ __global__ void k_positions(int n, const int* __restrict__ perm, const double* _
 }
 
 // ------------------------------------------------------------------------------------
-// tile boxes: min/max corner of every tile of kTile consecutive atoms.  Atoms are in
-// Morton order within a molecule, so a tile is compact in space and the short-range
-// pair kernels (CN, CN chain rule) skip partner tiles whose box is farther than their
-// cutoff from the row tile's box.  The box distance is a lower bound of every pair
-// distance in floating point too (min/max are exact, rounding is monotonic), so the
-// skipped pairs are exactly pairs the cutoff test would reject.
+// atom boxes: min/max corner of every run of 32 consecutive atoms (a warp's atoms in the
+// pair kernels).  Atoms are in Morton order within a molecule, so a run is compact in
+// space and the short-range pair kernels (CN, CN chain rule) skip partner tiles, and a warp
+// skips partner runs, whose box is farther than the cutoff from its own.  The box distance
+// is a lower bound of every pair distance in floating point too (min/max are exact,
+// rounding is monotonic), so the skipped pairs are exactly pairs the cutoff test rejects.
 // ------------------------------------------------------------------------------------
+constexpr int kBoxAtoms = 32;
 __global__ void __launch_bounds__(kTile) k_boxes(int n, const double4* __restrict__ pos, double4* lo, double4* hi)
 {
-    __shared__ double red[6][kTile / 32];
     const int i = blockIdx.x * kTile + threadIdx.x;
-    const double4 p = pos[i < n ? i : blockIdx.x * kTile];
+    const int b = i / kBoxAtoms;
+    if (b * kBoxAtoms >= n) return;   // whole warp beyond the atoms
+    const double4 p = pos[i < n ? i : b * kBoxAtoms];
     double v[6] = {p.x, p.y, p.z, -p.x, -p.y, -p.z};   // minima of x and of -x
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
-    for (int k = 0; k < 6; ++k) {
+    for (int k = 0; k < 6; ++k)
         for (int o = 16; o > 0; o >>= 1) v[k] = fmin(v[k], __shfl_xor_sync(0xffffffffu, v[k], o));
-        if (lane == 0) red[k][w] = v[k];
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double r[6];
-        for (int k = 0; k < 6; ++k) {
-            r[k] = red[k][0];
-            for (int q = 1; q < kTile / 32; ++q) r[k] = fmin(r[k], red[k][q]);
-        }
-        lo[blockIdx.x] = make_double4(r[0], r[1], r[2], 0.0);
-        hi[blockIdx.x] = make_double4(-r[3], -r[4], -r[5], 0.0);
+    if ((threadIdx.x & 31) == 0) {
+        lo[b] = make_double4(v[0], v[1], v[2], 0.0);
+        hi[b] = make_double4(-v[3], -v[4], -v[5], 0.0);
     }
 }
 
-// true when every atom of the partner range [t0, t0 + cnt) is at least sqrt(cut2) from
-// every atom of the row tile starting at i0 (a multiple of kTile)
-__device__ __forceinline__ bool tiles_far(const View& V, int i0, int t0, int cnt, double cut2)
+// box of the atoms [a, b) (b > a), as the union of the 32-atom boxes covering it
+__device__ __forceinline__ void range_box(const View& V, int a, int b, double4& l, double4& h)
 {
-    const int a = i0 / kTile, b0 = t0 / kTile, b1 = (t0 + cnt - 1) / kTile;
-    double4 jl = V.boxlo[b0], jh = V.boxhi[b0];
-    if (b1 != b0) {
-        const double4 l2 = V.boxlo[b1], h2 = V.boxhi[b1];
-        jl = make_double4(fmin(jl.x, l2.x), fmin(jl.y, l2.y), fmin(jl.z, l2.z), 0.0);
-        jh = make_double4(fmax(jh.x, h2.x), fmax(jh.y, h2.y), fmax(jh.z, h2.z), 0.0);
+    l = V.boxlo[a / kBoxAtoms];
+    h = V.boxhi[a / kBoxAtoms];
+    for (int k = a / kBoxAtoms + 1; k <= (b - 1) / kBoxAtoms; ++k) {
+        const double4 l2 = V.boxlo[k], h2 = V.boxhi[k];
+        l = make_double4(fmin(l.x, l2.x), fmin(l.y, l2.y), fmin(l.z, l2.z), 0.0);
+        h = make_double4(fmax(h.x, h2.x), fmax(h.y, h2.y), fmax(h.z, h2.z), 0.0);
     }
-    const double4 il = V.boxlo[a], ih = V.boxhi[a];
+}
+
+__device__ __forceinline__ bool boxes_far(double4 il, double4 ih, double4 jl, double4 jh, double cut2)
+{
     const double dx = fmax(0.0, fmax(jl.x - ih.x, il.x - jh.x));
     const double dy = fmax(0.0, fmax(jl.y - ih.y, il.y - jh.y));
     const double dz = fmax(0.0, fmax(jl.z - ih.z, il.z - jh.z));
     return dx * dx + dy * dy + dz * dz >= cut2;
+}
+
+// true when every atom of [j0, j0 + cnt) is at least sqrt(cut2) from every atom of
+// [i0, i0 + ni)
+__device__ __forceinline__ bool ranges_far(const View& V, int i0, int ni, int j0, int cnt, double cut2)
+{
+    double4 il, ih, jl, jh;
+    range_box(V, i0, i0 + ni, il, ih);
+    range_box(V, j0, j0 + cnt, jl, jh);
+    return boxes_far(il, ih, jl, jh, cut2);
 }
 
 // ------------------------------------------------------------------------------------
@@ -112,8 +117,11 @@ __global__ void __launch_bounds__(kTile) k_cn(View V, int nsplit)
     const int2 rg = act ? V.jr[i] : make_int2(0, 0);
     const double kn = -7.5;
     double s = 0.0;
+    const int ni = min(kTile, V.n - i0);
+    const int w0 = i0 + (threadIdx.x & ~31), nw = max(0, min(32, V.n - w0));   // this warp's atoms
     for (int t0 = jb; t0 < je; t0 += kTile) {
-        if (tiles_far(V, i0, t0, min(kTile, je - t0), 36.0)) continue;   // uniform in the block
+        const int cnt = min(kTile, je - t0);
+        if (ranges_far(V, i0, ni, t0, cnt, 36.0)) continue;   // uniform in the block
         __syncthreads();
         const int jl = t0 + threadIdx.x;
         if (jl < je) {
@@ -122,9 +130,12 @@ __global__ void __launch_bounds__(kTile) k_cn(View V, int nsplit)
             sr[threadIdx.x] = V.rcov_cn[jl];
         }
         __syncthreads();
-        const int cnt = min(kTile, je - t0);
-        if (act) {
-            for (int jj = 0; jj < cnt; ++jj) {
+        if (nw == 0) continue;
+        for (int js = 0; js < cnt; js += 32) {
+            const int jn = min(32, cnt - js);
+            if (ranges_far(V, w0, nw, t0 + js, jn, 36.0)) continue;   // uniform in the warp
+            if (!act) continue;
+            for (int jj = js; jj < js + jn; ++jj) {
                 const double dx = pi.x - sx[jj], dy = pi.y - sy[jj], dz = pi.z - sz[jj];
                 const double d2 = dx * dx + dy * dy + dz * dz;
                 const int j = t0 + jj;
@@ -642,8 +653,11 @@ __global__ void __launch_bounds__(kTile) k_cn_chain(View V, int nsplit)
     const int2 rg = act ? V.jr[i] : make_int2(0, 0);
     const double kn = -7.5, sqrtpi = 1.77245385091;
     double gx = 0.0, gy = 0.0, gz = 0.0;
+    const int ni = min(kTile, V.n - i0);
+    const int w0 = i0 + (threadIdx.x & ~31), nw = max(0, min(32, V.n - w0));   // this warp's atoms
     for (int t0 = jb; t0 < je; t0 += kTile) {
-        if (tiles_far(V, i0, t0, min(kTile, je - t0), 36.0)) continue;   // uniform in the block
+        const int cnt = min(kTile, je - t0);
+        if (ranges_far(V, i0, ni, t0, cnt, 36.0)) continue;   // uniform in the block
         __syncthreads();
         const int jl = t0 + threadIdx.x;
         if (jl < je) {
@@ -653,9 +667,11 @@ __global__ void __launch_bounds__(kTile) k_cn_chain(View V, int nsplit)
             su[threadIdx.x] = V.v[jl];
         }
         __syncthreads();
-        const int cnt = min(kTile, je - t0);
         if (!act) continue;
-        for (int jj = 0; jj < cnt; ++jj) {
+        for (int js = 0; js < cnt; js += 32) {
+        const int jn = min(32, cnt - js);
+        if (ranges_far(V, w0, nw, t0 + js, jn, 36.0)) continue;   // uniform in the warp
+        for (int jj = js; jj < js + jn; ++jj) {
             const double dx = sx[jj] - pi.x, dy = sy[jj] - pi.y, dz = sz[jj] - pi.z;
             const double d2 = dx * dx + dy * dy + dz * dz;
             const int j = t0 + jj;
@@ -666,6 +682,7 @@ __global__ void __launch_bounds__(kTile) k_cn_chain(View V, int nsplit)
             const R de = R(kn / sqrtpi) * exp(R(-kn * kn) * dr * dr) / rs;
             const double f = -(double)(de / r) * (ui + su[jj]);
             gx += f * dx; gy += f * dy; gz += f * dz;
+        }
         }
     }
     if (act) {

@@ -20,7 +20,9 @@
 
 namespace {
 
-constexpr int kPcgThreads = 512;
+constexpr int kPcgThreads = 512;       // k_pcg: the whole SM (the tiled product wants the warps)
+constexpr int kPcgPipeThreads = 256;   // k_pcg_pipe: half of an SM's registers, so that the
+                                       // charge-independent term kernels run beside it
 constexpr int kPcgMaxBlock = 64;   // largest preconditioner block
 
 struct PCGArgs {
@@ -395,7 +397,7 @@ __device__ void pcg_setup(const PCGArgs& A, int4 pt, long long boff0, double* G,
     {
         __shared__ double colc[kPcgThreads / 32][32];
         const int warp = threadIdx.x >> 5;
-        for (int bk = pt.z + warp; bk < pt.w; bk += kPcgThreads / 32) {
+        for (int bk = pt.z + warp; bk < pt.w; bk += (int)(blockDim.x >> 5)) {
             const int s = A.blocks[bk].y;
             if (s > kPcgSmall && s <= kPcgWarpMax) invert_warp(A, bk, Bs + (A.boff[bk] - boff0), colc[warp]);
         }
@@ -633,7 +635,7 @@ __device__ void grid_totals3(const double* partial, int set, double& a, double& 
 // read right after it; the same buffer is written again (set k + 2) only after barrier
 // k + 1, which no block passes before it has finished reading set k.  The result is
 // accepted on the true residual b - M x; otherwise the recurrence restarts from it.
-__global__ void __launch_bounds__(kPcgThreads) k_pcg_pipe(PCGArgs A)
+__global__ void __launch_bounds__(kPcgPipeThreads, 2) k_pcg_pipe(PCGArgs A)
 {
     extern __shared__ double sm[];
     constexpr int GL = kPcgMaxBlock + 1;
