@@ -171,14 +171,18 @@ struct Engine::Impl {
     // chain and join before the CN chain rule.  GFNFF_STREAMS=1 keeps one stream.
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork0 = nullptr, ev_fork1 = nullptr, ev_join = nullptr;
+    bool side_early = false;   // GFNFF_SIDE_EARLY=1: fork at the start of the evaluation
     cusolverDnHandle_t sol = nullptr;
     int n = 0, nfrag = 0, K = 0, nred = 0, nmol = 0, nsplit = 1;
     // Coulomb + D4 pairs: each pair once over a tile-pair list (default), or both
     // directions by rows (GFNFF_PAIRS=rows)
     DBuf<int2> symtiles;
     DBuf<double4> boxlo, boxhi;   // per run of kBoxAtoms atoms
+    bool box_cull = false;        // CN kernels skip far tiles (single molecules >= 8192 atoms)
     int nsym = 0;
     bool pairs_sym = true;
+    bool pairs_occ = false;   // 10 blocks per SM (96 registers) instead of the unbounded 116
+    int pair_tile = 64;       // tile edge of k_pairs_sym
     // molecule structure and atom order
     DBuf<int> mol, perm;
     DBuf<int2> jr;
@@ -333,8 +337,8 @@ struct Engine::Impl {
         V.exact = opt.exact_gradient ? 1 : 0;
         V.cfar = resp_on ? cfar.p : nullptr;
         V.u = resp_on ? ures.p : nullptr;
-        V.boxlo = boxlo.p;
-        V.boxhi = boxhi.p;
+        V.boxlo = box_cull ? boxlo.p : nullptr;
+        V.boxhi = box_cull ? boxhi.p : nullptr;
         return V;
     }
     // caller index (molecule m, local atom a) -> internal index
@@ -349,6 +353,8 @@ Engine::Engine(const EngineOptions& opt) : p_(new Impl)
     CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
     // the EEQ chain is the critical path: its stream gets the higher priority
     CK(cudaStreamCreateWithPriority(&p_->stream, cudaStreamNonBlocking, hi));
+    const char* se = std::getenv("GFNFF_SIDE_EARLY");
+    p_->side_early = se && !std::strcmp(se, "1");
     const char* st = std::getenv("GFNFF_STREAMS");
     if (!(st && !std::strcmp(st, "1"))) {
         CK(cudaStreamCreateWithPriority(&p_->side, cudaStreamNonBlocking, lo));
@@ -504,17 +510,21 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
     P.nsplit = pair_splits(n, max_range);
     {   // tile pairs (i tile <= j tile, both within the tile's molecules) of k_pairs_sym
         std::vector<int2> tl;
-        const int nt = (n + kST - 1) / kST;
+        P.pair_tile = nm > 1 ? 32 : kST;
+        const int T = P.pair_tile, nt = (n + T - 1) / T;
         for (int I = 0; I < nt; ++I) {
-            const int i0 = I * kST, hi = hjr[std::min(n, i0 + kST) - 1].y;
-            for (int J = I; J * kST < hi; ++J) tl.push_back(make_int2(i0, J * kST));
+            const int i0 = I * T, hi = hjr[std::min(n, i0 + T) - 1].y;
+            for (int J = I; J * T < hi; ++J) tl.push_back(make_int2(i0, J * T));
         }
         P.symtiles.upload(tl);
         P.boxlo.alloc((n + kBoxAtoms - 1) / kBoxAtoms);
         P.boxhi.alloc((n + kBoxAtoms - 1) / kBoxAtoms);
+        P.box_cull = nm == 1 && n >= 8192;
         P.nsym = (int)tl.size();
         const char* pe = std::getenv("GFNFF_PAIRS");
         P.pairs_sym = !(pe && !std::strcmp(pe, "rows"));
+        const char* po = std::getenv("GFNFF_PAIRS_OCC");
+        P.pairs_occ = po && !std::strcmp(po, "1");
     }
     // ---- global element table (union of the molecules' D4 element slots) ----
     std::vector<int> gZ;
@@ -1206,11 +1216,13 @@ void Engine::launch_body()
     if (P.natm) k_atm<<<nblk(P.natm), kBlock, 0, s2>>>(V, TripSoA{P.natm, P.at_i.p, P.at_j.p, P.at_k.p, P.at_c9.p, P.at_r0ij.p, P.at_r0ik.p, P.at_r0jk.p, P.at_sc.p});
     if (P.nbatm) k_batm<<<nblk(P.nbatm), kBlock, 0, s2>>>(V, TripSoA{P.nbatm, P.ba_i.p, P.ba_j.p, P.ba_k.p, P.ba_c9.p, nullptr, nullptr, nullptr, nullptr});
     };
-    // Batches: the side terms start at once (the batched EEQ kernel fills every SM anyway).
-    // Single molecules: they fork right after the EEQ right-hand side and are issued after
-    // the solver's launch, so that the latency-bound cooperative PCG takes its SM slots first
-    // and the side kernels fill what it leaves (k_pcg uses half of an SM's registers).
-    const bool early = fork && P.nmol > 1;
+    // The side terms fork right before the EEQ solve and are issued after the solver's
+    // launch: the latency-bound cooperative PCG takes its SM slots first and the side
+    // kernels fill what it leaves (k_pcg_pipe uses half of an SM's registers); the batched
+    // EEQ kernel's blocks leave their SMs one by one when the work queue runs dry, while the
+    // largest molecules still factor, and the side kernels take those SMs.
+    // (GFNFF_SIDE_EARLY=1: fork at the start of the evaluation instead.)
+    const bool early = fork && P.side_early;
     if (early) {
         CK(cudaEventRecord(P.ev_fork0, s));
         CK(cudaStreamWaitEvent(s2, P.ev_fork0, 0));
@@ -1224,7 +1236,7 @@ void Engine::launch_body()
         CK(cudaEventRecord(P.ev_join, s2));
     };
     P.mark(1);
-    k_boxes<<<nblk(n, kTile), kTile, 0, s>>>(n, P.pos.p, P.boxlo.p, P.boxhi.p);
+    if (P.box_cull) k_boxes<<<nblk(n, kTile), kTile, 0, s>>>(n, P.pos.p, P.boxlo.p, P.boxhi.p);
     (mixed ? k_cn<float> : k_cn<double>)<<<tgrid, kTile, 0, s>>>(V, P.nsplit);
     P.mark(2);
     k_d4_weights<<<nblk(n), kBlock, 0, s>>>(V);
@@ -1250,7 +1262,7 @@ void Engine::launch_body()
             k_eeq_rhs<<<nblk(P.nred), kBlock, 0, s>>>(V, P.red2atom.p, P.anchor.p, P.qlist.p, P.nq, P.q0.p, P.bvec.p,
                                                       aug ? P.M.p + P.nred : nullptr, P.lda);
         P.mark(5);
-        if (fork) CK(cudaEventRecord(P.ev_fork1, s));
+        if (fork && !early) CK(cudaEventRecord(P.ev_fork1, s));
         if (P.nred > 0) {
             if (sv == Impl::SOLVE_TILED) {
                 P.chol_launch();
@@ -1285,7 +1297,9 @@ void Engine::launch_body()
         P.mark(7);
         hb_rep_terms();
     }
-    if (P.pairs_sym) k_pairs_sym<double><<<P.nsym, kST, 0, s>>>(V, P.symtiles.p);
+    if (P.pairs_sym && P.pair_tile == 32) k_pairs_sym<double, 16, 32><<<P.nsym, 32, 0, s>>>(V, P.symtiles.p);
+    else if (P.pairs_sym && P.pairs_occ) k_pairs_sym<double, 10, kST><<<P.nsym, kST, 0, s>>>(V, P.symtiles.p);
+    else if (P.pairs_sym) k_pairs_sym<double, 8, kST><<<P.nsym, kST, 0, s>>>(V, P.symtiles.p);
     else k_pairs<double><<<tgrid, kTile, 0, s>>>(V, P.nsplit);
     if (P.resp_on) {
         // u = B M^-1 B^T w with the factor (or the iteration) of this step's EEQ matrix

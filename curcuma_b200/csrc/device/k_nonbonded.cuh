@@ -46,12 +46,13 @@ __global__ void k_positions(int n, const int* __restrict__ perm, const double* _
 }
 
 // ------------------------------------------------------------------------------------
-// atom boxes: min/max corner of every run of 32 consecutive atoms (a warp's atoms in the
-// pair kernels).  Atoms are in Morton order within a molecule, so a run is compact in
-// space and the short-range pair kernels (CN, CN chain rule) skip partner tiles, and a warp
-// skips partner runs, whose box is farther than the cutoff from its own.  The box distance
-// is a lower bound of every pair distance in floating point too (min/max are exact,
-// rounding is monotonic), so the skipped pairs are exactly pairs the cutoff test rejects.
+// atom boxes: min/max corner of every run of 32 consecutive atoms.  Atoms are in Morton
+// order within a molecule, so a run is fairly compact in space and the short-range pair
+// kernels (CN, CN chain rule) skip partner tiles, and a warp partner runs of 32 atoms, whose
+// box is farther than the cutoff from its own (single molecules of 8192 atoms or more;
+// below that the tests cost more than they save, measured).  The box distance is a lower bound of every pair distance
+// in floating point too (min/max are exact, rounding is monotonic), so the skipped pairs
+// are exactly pairs the cutoff test rejects.
 // ------------------------------------------------------------------------------------
 constexpr int kBoxAtoms = 32;
 __global__ void __launch_bounds__(kTile) k_boxes(int n, const double4* __restrict__ pos, double4* lo, double4* hi)
@@ -121,7 +122,7 @@ __global__ void __launch_bounds__(kTile) k_cn(View V, int nsplit)
     const int w0 = i0 + (threadIdx.x & ~31), nw = max(0, min(32, V.n - w0));   // this warp's atoms
     for (int t0 = jb; t0 < je; t0 += kTile) {
         const int cnt = min(kTile, je - t0);
-        if (ranges_far(V, i0, ni, t0, cnt, 36.0)) continue;   // uniform in the block
+        if (V.boxlo && ranges_far(V, i0, ni, t0, cnt, 36.0)) continue;   // uniform in the block
         __syncthreads();
         const int jl = t0 + threadIdx.x;
         if (jl < je) {
@@ -130,11 +131,10 @@ __global__ void __launch_bounds__(kTile) k_cn(View V, int nsplit)
             sr[threadIdx.x] = V.rcov_cn[jl];
         }
         __syncthreads();
-        if (nw == 0) continue;
+        if (!act) continue;
         for (int js = 0; js < cnt; js += 32) {
             const int jn = min(32, cnt - js);
-            if (ranges_far(V, w0, nw, t0 + js, jn, 36.0)) continue;   // uniform in the warp
-            if (!act) continue;
+            if (V.boxlo && ranges_far(V, w0, nw, t0 + js, jn, 36.0)) continue;   // uniform in the warp
             for (int jj = js; jj < js + jn; ++jj) {
                 const double dx = pi.x - sx[jj], dy = pi.y - sy[jj], dz = pi.z - sz[jj];
                 const double d2 = dx * dx + dy * dy + dz * dz;
@@ -382,8 +382,9 @@ __global__ void __launch_bounds__(kTile) k_pairs(View V, int nsplit)
 
 // ------------------------------------------------------------------------------------
 // The same Coulomb + D4 pair terms with every pair evaluated once (Newton's third law).
-// Blocks take 64 x 64 tiles (i tile <= j tile, listed at set-up; only j > i within a
-// diagonal tile).  Row i keeps its sums in registers as in k_pairs; the j side of every
+// Blocks take T x T tiles (i tile <= j tile, listed at set-up; only j > i within a
+// diagonal tile; T = 64 for single molecules, 32 for batches of small molecules, whose
+// tiles would otherwise straddle molecules).  Row i keeps its sums in registers as in k_pairs; the j side of every
 // pair (gradient, dE/dCN_j from j's half contraction against i's current weights, and the
 // far-pair potential of the exact-gradient mode) is summed over the warp's 32 rows with
 // shuffles and kept per warp in shared memory, then added once per tile.
@@ -392,9 +393,9 @@ constexpr int kST = 64;
 
 // one D4 pair in arithmetic type R with both CN derivatives: energy e, dE/dr / r in dedr,
 // dE/dCN_i in dci, dE/dCN_j in dcj (wi: current weights of i in registers)
-template <class R>
+template <class R, int T>
 __device__ __forceinline__ void d4_pair_sym(double d2, const double* g0, const double* dgi, const double* dgj,
-                                            const double (*sw0)[kST], const double (*sw)[kST], int jj, int nrj,
+                                            const double (*sw0)[T], const double (*sw)[T], int jj, int nrj,
                                             int nri, const double (&wi)[7], double r4r2_d, double zz_d, bool want_dc,
                                             double& e, double& dedr, double& dci, double& dcj)
 {
@@ -422,14 +423,14 @@ __device__ __forceinline__ void d4_pair_sym(double d2, const double* g0, const d
     dcj = -(double)(dc6j * sum * zz);
 }
 
-template <class R>
-__global__ void __launch_bounds__(kST) k_pairs_sym(View V, const int2* __restrict__ tiles)
+template <class R, int MINB, int T>
+__global__ void __launch_bounds__(T, MINB) k_pairs_sym(View V, const int2* __restrict__ tiles)
 {
-    __shared__ double sx[kST], sy[kST], sz[kST], s0x[kST], s0y[kST], s0z[kST];
-    __shared__ double sq[kST], sa[kST], sze[kST], ssz[kST];
-    __shared__ double sw0[7][kST], sw[7][kST];
-    __shared__ int ssl[kST], snr[kST];
-    __shared__ double jacc[kST / 32][5][kST];
+    __shared__ double sx[T], sy[T], sz[T], s0x[T], s0y[T], s0z[T];
+    __shared__ double sq[T], sa[T], sze[T], ssz[T];
+    __shared__ double sw0[7][T], sw[7][T];
+    __shared__ int ssl[T], snr[T];
+    __shared__ double jacc[T / 32][5][T];
     const int2 tp = tiles[blockIdx.x];
     const int i0 = tp.x, j0 = tp.y, i = i0 + threadIdx.x;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -464,7 +465,7 @@ __global__ void __launch_bounds__(kST) k_pairs_sym(View V, const int2* __restric
     __syncthreads();
     const double tsp = 2.0 / 1.772453850905516;
     double ec = 0.0, ed = 0.0, gx = 0.0, gy = 0.0, gz = 0.0, dcn = 0.0, cfar = 0.0;
-    const int cnt = min(kST, V.n - j0);
+    const int cnt = min(T, V.n - j0);
     for (int jj = 0; jj < cnt; ++jj) {
         const int j = j0 + jj;
         double fx = 0.0, fy = 0.0, fz = 0.0, dcj = 0.0, cfj = 0.0;
@@ -505,10 +506,10 @@ __global__ void __launch_bounds__(kST) k_pairs_sym(View V, const int2* __restric
                 double e, dedr, dci;
                 // mixed form: pairs closer than 15 bohr (the strong ones) stay FP64
                 if (sizeof(R) == sizeof(double) || d2 < 225.0)
-                    d4_pair_sym<double>(d2, g0i + sj * 7, dgi + sj * 7, dgj, sw0, sw, jj, nrj, nri, wi, r4r2, zz,
+                    d4_pair_sym<double, T>(d2, g0i + sj * 7, dgi + sj * 7, dgj, sw0, sw, jj, nrj, nri, wi, r4r2, zz,
                                         want_dc, e, dedr, dci, dcj);
                 else
-                    d4_pair_sym<R>(d2, g0i + sj * 7, dgi + sj * 7, dgj, sw0, sw, jj, nrj, nri, wi, r4r2, zz,
+                    d4_pair_sym<R, T>(d2, g0i + sj * 7, dgi + sj * 7, dgj, sw0, sw, jj, nrj, nri, wi, r4r2, zz,
                                    want_dc, e, dedr, dci, dcj);
                 ed += e;
                 f += dedr;
@@ -541,7 +542,7 @@ __global__ void __launch_bounds__(kST) k_pairs_sym(View V, const int2* __restric
         for (int k = 0; k < 5; ++k) {
             a[k] = 0.0;
 #pragma unroll
-            for (int w = 0; w < kST / 32; ++w) a[k] += jacc[w][k][threadIdx.x];
+            for (int w = 0; w < T / 32; ++w) a[k] += jacc[w][k][threadIdx.x];
         }
         if (a[0] != 0.0) atomicAdd(V.grad + 3 * j, a[0]);
         if (a[1] != 0.0) atomicAdd(V.grad + 3 * j + 1, a[1]);
@@ -657,7 +658,7 @@ __global__ void __launch_bounds__(kTile) k_cn_chain(View V, int nsplit)
     const int w0 = i0 + (threadIdx.x & ~31), nw = max(0, min(32, V.n - w0));   // this warp's atoms
     for (int t0 = jb; t0 < je; t0 += kTile) {
         const int cnt = min(kTile, je - t0);
-        if (ranges_far(V, i0, ni, t0, cnt, 36.0)) continue;   // uniform in the block
+        if (V.boxlo && ranges_far(V, i0, ni, t0, cnt, 36.0)) continue;   // uniform in the block
         __syncthreads();
         const int jl = t0 + threadIdx.x;
         if (jl < je) {
@@ -670,7 +671,7 @@ __global__ void __launch_bounds__(kTile) k_cn_chain(View V, int nsplit)
         if (!act) continue;
         for (int js = 0; js < cnt; js += 32) {
         const int jn = min(32, cnt - js);
-        if (ranges_far(V, w0, nw, t0 + js, jn, 36.0)) continue;   // uniform in the warp
+        if (V.boxlo && ranges_far(V, w0, nw, t0 + js, jn, 36.0)) continue;   // uniform in the warp
         for (int jj = js; jj < js + jn; ++jj) {
             const double dx = sx[jj] - pi.x, dy = sy[jj] - pi.y, dz = sz[jj] - pi.z;
             const double d2 = dx * dx + dy * dy + dz * dz;
