@@ -272,6 +272,12 @@ struct Engine::Impl {
     bool pcg_warm = false;
     // matrices beyond L2 keep only their lower triangle; the PCG multiplies by tiles
     bool pcg_lower = false;
+    // mixed form, lower-triangle PCG, GFNFF_PCG_F32=1: M stored in FP32 (half the bytes per
+    // product; the solution is exact for the rounded matrix, whose charges enter the energy
+    // only at second order, the EEQ energy being stationary in them).  Measured slower than
+    // the FP64 form on the 20k cluster (9.2 vs 5.2 ms), so it is off by default.
+    bool pcg_f32 = false;
+    DBuf<float> Mf;
     // pipelined CG (one grid barrier per iteration; GFNFF_PCG=classic|pipelined forces one)
     bool pcg_pipe = true;
     size_t pcg_smem_pipe = 0;
@@ -289,6 +295,7 @@ struct Engine::Impl {
         A.bar = pbar.p; A.info = inf; A.iters = piters.p; A.max_iter = pcg_max_iter; A.tol = 1e-12;
         A.warm = pcg_warm ? pwarm.p + slot : nullptr;
         A.lower = pcg_lower ? pcg_cols : 0; A.yA = pyA.p; A.tiles = ptiles.p; A.ntiles = pcg_ntiles;
+        A.Mf = pcg_f32 ? Mf.p : nullptr;
         void* args[] = {&A};
         if (pcg_pipe)
             CK(cudaLaunchCooperativeKernel((const void*)k_pcg_pipe, dim3(pcg_grid), dim3(kPcgPipeThreads), args,
@@ -967,6 +974,9 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
                 {
                     const char* e = std::getenv("GFNFF_PCG_SYM");
                     P.pcg_lower = e ? std::strcmp(e, "0") != 0 : P.nred >= 4096;
+                    const char* ef = std::getenv("GFNFF_PCG_F32");
+                    P.pcg_f32 = P.pcg_lower && P.opt.precision == 1 && ef && !std::strcmp(ef, "1");
+                    if (P.pcg_f32) P.Mf.alloc((size_t)P.lda * P.nred);
                     const char* ec = std::getenv("GFNFF_PCG_COLS");
                     P.pcg_cols = (ec && !std::strcmp(ec, "8")) ? 2 : 1;
                     std::vector<int2> tl;
@@ -1254,8 +1264,11 @@ void Engine::launch_body()
         const bool aug = sv == Impl::SOLVE_TILED;
         if (P.nred > 0) {
             const long long nt = (P.nred + kMT - 1) / kMT;
-            k_eeq_M_tiles<<<(unsigned)(nt * (nt + 1) / 2), 256, 0, s>>>(V, P.red2atom.p, P.anchor.p, P.M.p, P.lda,
-                                                                      full ? 1 : 0);
+            const unsigned nb = (unsigned)(nt * (nt + 1) / 2);
+            if (sv == Impl::SOLVE_PCG && P.pcg_f32)
+                k_eeq_M_tiles<float><<<nb, 256, 0, s>>>(V, P.red2atom.p, P.anchor.p, P.Mf.p, P.lda, 0);
+            else
+                k_eeq_M_tiles<double><<<nb, 256, 0, s>>>(V, P.red2atom.p, P.anchor.p, P.M.p, P.lda, full ? 1 : 0);
         }
         P.mark(4);
         if (P.nred > 0)

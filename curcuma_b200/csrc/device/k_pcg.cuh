@@ -44,6 +44,7 @@ struct PCGArgs {
     int* iters;
     int* warm;            // when non-null and *warm != 0, x holds the previous solution of the
                           // same system and is the initial guess; set to 1 on convergence
+    const float* Mf;      // lower form in the mixed precision form: M stored in FP32 (M unused)
     int lower;            // 1 or 2: only the lower triangle of M is stored; M p by tiles
                           // (matvec_tiles, streaming 4 or 8 columns per warp at once)
     double* yA;           // lower: n-vector the tiles add M p into (zero between uses)
@@ -228,7 +229,8 @@ __device__ double matvec_rows(const PCGArgs& A, const double* v, int row0, int r
 // element (r, c) of M, from the lower triangle when only that is stored
 __device__ __forceinline__ double mget(const PCGArgs& A, int r, int c)
 {
-    return (A.lower && r < c) ? A.M[(size_t)r * A.lda + c] : A.M[(size_t)c * A.lda + r];
+    const size_t e = (A.lower && r < c) ? (size_t)r * A.lda + c : (size_t)c * A.lda + r;
+    return A.Mf ? (double)A.Mf[e] : A.M[e];
 }
 
 // Symmetric M p from the lower triangle, for matrices too large for L2: the tiles
@@ -240,8 +242,8 @@ __device__ __forceinline__ double mget(const PCGArgs& A, int r, int c)
 // A.yA.  Diagonal tiles use r >= c for u and r > c for v.  Returns the thread's part of
 // p^T M p.  The caller reads y after a grid barrier and zeroes what it read.
 constexpr int kPcgT = 128;
-template <int kPcgCols>   // columns a warp streams at once (4 * kPcgCols loads per lane in flight)
-__device__ double matvec_tiles_c(const PCGArgs& A, const double* p, double* red)
+template <int kPcgCols, class TM>   // columns a warp streams at once; matrix storage type
+__device__ double matvec_tiles_c(const PCGArgs& A, const TM* Mt, const double* p, double* red)
 {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     double pap = 0.0;
@@ -258,16 +260,17 @@ __device__ double matvec_tiles_c(const PCGArgs& A, const double* p, double* red)
             pr[i] = r < ni ? p[I0 + r] : 0.0;
         }
         for (int cb = warp * kPcgCols; cb < nj; cb += nw * kPcgCols) {
-            double m[kPcgCols][4], v[kPcgCols], pc[kPcgCols];
+            TM m[kPcgCols][4];   // kept in the storage type (FP32: half the registers)
+            double v[kPcgCols], pc[kPcgCols];
 #pragma unroll
             for (int q = 0; q < kPcgCols; ++q) {
                 const int c = cb + q;
                 pc[q] = c < nj ? p[J0 + c] : 0.0;
-                const double* col = A.M + (size_t)(J0 + (c < nj ? c : 0)) * A.lda + I0;
+                const TM* col = Mt + (size_t)(J0 + (c < nj ? c : 0)) * A.lda + I0;
 #pragma unroll
                 for (int i = 0; i < 4; ++i) {
                     const int r = lane + 32 * i;
-                    m[q][i] = (c < nj && r < ni && (!diag || r >= c)) ? __ldcs(col + r) : 0.0;
+                    m[q][i] = (c < nj && r < ni && (!diag || r >= c)) ? __ldcs(col + r) : TM(0);
                 }
             }
 #pragma unroll
@@ -277,8 +280,9 @@ __device__ double matvec_tiles_c(const PCGArgs& A, const double* p, double* red)
 #pragma unroll
                 for (int i = 0; i < 4; ++i) {
                     const int r = lane + 32 * i;
-                    u[i] += m[q][i] * pc[q];
-                    if (!diag || r > c) v[q] += m[q][i] * pr[i];
+                    const double mv = (double)m[q][i];
+                    u[i] += mv * pc[q];
+                    if (!diag || r > c) v[q] += mv * pr[i];
                 }
             }
 #pragma unroll
@@ -313,7 +317,8 @@ __device__ double matvec_tiles_c(const PCGArgs& A, const double* p, double* red)
 
 __device__ double matvec_tiles(const PCGArgs& A, const double* p, double* red)
 {
-    return A.lower == 2 ? matvec_tiles_c<8>(A, p, red) : matvec_tiles_c<4>(A, p, red);
+    if (A.Mf) return matvec_tiles_c<8>(A, A.Mf, p, red);   // 4-byte elements: twice the columns in flight
+    return A.lower == 2 ? matvec_tiles_c<8>(A, A.M, p, red) : matvec_tiles_c<4>(A, A.M, p, red);
 }
 
 // Ap for the owned rows after matvec_tiles and a grid barrier: read y (L2) and zero it

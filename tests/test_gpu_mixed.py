@@ -49,3 +49,17 @@ def test_mixed_topology_matches_fp64():
     assert a.setMolecule(Z, X) and b.setMolecule(Z, X)
     for kind, width in [(0, 2), (1, 3), (4, 2), (6, 4), (8, 1), (9, 1)]:
         assert np.array_equal(a.topology(kind, width), b.topology(kind, width)), kind
+
+
+@pytest.mark.parametrize("system", ["water400", "peptide"])
+def test_mixed_fp32_pcg_matrix(system, monkeypatch):
+    """The mixed form's optional FP32-stored lower-triangle PCG matrix (GFNFF_PCG_F32=1,
+    forced here on smaller systems): energy and gradient stay within the mixed bar against
+    the oracle."""
+    monkeypatch.setenv("GFNFF_EEQ_SOLVER", "pcg")
+    monkeypatch.setenv("GFNFF_PCG_SYM", "1")
+    monkeypatch.setenv("GFNFF_PCG_F32", "1")
+    Z, X = {"water400": lambda: workloads.water_cluster(400, 31),
+            "peptide": lambda: workloads.solvated_peptide(8, 60, 12)}[system]()
+    gpu, de, dg = _mixed_vs_oracle(Z, X)
+    assert gpu.eeqSolver() == "pcg"
