@@ -281,6 +281,15 @@ struct Engine::Impl {
     // pipelined CG (one grid barrier per iteration; GFNFF_PCG=classic|pipelined forces one)
     bool pcg_pipe = true;
     size_t pcg_smem_pipe = 0;
+    // shared-memory resident PCG (k_pcg_res, GFNFF_PCG_RES=1): the lower triangle of M lives
+    // in the SMs' shared memory for the whole solve, built there from the atoms.  Measured
+    // slower on 1000 waters (0.27 ms against 0.23 ms for build kernel + streamed PCG: the
+    // in-kernel build runs at one 256-thread block per SM, and the atomics-based product
+    // needs a second barrier per iteration), so it is off by default.
+    bool pcg_res = false;
+    size_t pcg_smem_res = 0;
+    int pcg_res_ntiles = 0, pcg_res_ntl = 0, pcg_res_gscratch = 0;
+    DBuf<int2> prtiles;
     DBuf<double> pz2;
     int pcg_cols = 1;   // 1: 4 columns per warp step, 2: 8 (GFNFF_PCG_COLS=8)
     DBuf<double> pyA;
@@ -297,7 +306,12 @@ struct Engine::Impl {
         A.lower = pcg_lower ? pcg_cols : 0; A.yA = pyA.p; A.tiles = ptiles.p; A.ntiles = pcg_ntiles;
         A.Mf = pcg_f32 ? Mf.p : nullptr;
         void* args[] = {&A};
-        if (pcg_pipe)
+        if (pcg_res) {
+            PCGRes R{view(), red2atom.p, anchor.p, prtiles.p, pcg_res_ntiles, pcg_res_ntl, pcg_res_gscratch};
+            void* rargs[] = {&A, &R};
+            CK(cudaLaunchCooperativeKernel((const void*)k_pcg_res, dim3(pcg_grid), dim3(kPcgPipeThreads), rargs,
+                                           pcg_smem_res, stream));
+        } else if (pcg_pipe)
             CK(cudaLaunchCooperativeKernel((const void*)k_pcg_pipe, dim3(pcg_grid), dim3(kPcgPipeThreads), args,
                                            pcg_smem_pipe, stream));
         else
@@ -1005,6 +1019,33 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
                 // of large ones measured faster in the classic form
                 P.pcg_pipe = pe ? std::strcmp(pe, "classic") != 0 : !P.pcg_lower;
                 P.pcg_pipe = P.pcg_pipe && P.pcg_smem_pipe <= 220 * 1024;
+                {
+                    const char* er = std::getenv("GFNFF_PCG_RES");
+                    const int nt64 = (P.nred + 63) / 64;
+                    std::vector<int2> rt;
+                    for (int i0 = 0; i0 < nt64; ++i0)
+                        for (int j0 = 0; j0 <= i0; ++j0) rt.push_back(make_int2(64 * i0, 64 * j0));
+                    int bigblk = 0;
+                    for (auto& b : blocks) bigblk = std::max(bigblk, b.y);
+                    P.pcg_res_ntiles = (int)rt.size();
+                    P.pcg_res_ntl = (P.pcg_res_ntiles + G - 1) / G;
+                    P.pcg_res_gscratch = bigblk > kPcgWarpMax ? 1 : 0;
+                    P.pcg_smem_res = ((size_t)((P.nred + 1) & ~1) + (size_t)P.pcg_res_ntl * 64 * 65 +
+                                      (P.pcg_res_gscratch ? (size_t)kPcgMaxBlock * (kPcgMaxBlock + 1) : 0) +
+                                      10 * (size_t)maxrows + maxinv) * sizeof(double) +
+                                     (size_t)maxrows * sizeof(int4);
+                    P.pcg_res = er && !std::strcmp(er, "1") && P.pcg_pipe && !P.pcg_lower &&
+                                P.pcg_res_ntl <= 5 && P.pcg_smem_res <= 200 * 1024;
+                    if (P.pcg_res) {
+                        P.prtiles.upload(rt);
+                        CK(cudaFuncSetAttribute((const void*)k_pcg_res, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                (int)P.pcg_smem_res));
+                        int rs = 0;
+                        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rs, (const void*)k_pcg_res, kPcgPipeThreads,
+                                                                         P.pcg_smem_res));
+                        P.pcg_res = rs >= 1;
+                    }
+                }
                 if (P.pcg_pipe) {
                     CK(cudaFuncSetAttribute((const void*)k_pcg_pipe, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             (int)P.pcg_smem_pipe));
@@ -1265,7 +1306,9 @@ void Engine::launch_body()
         if (P.nred > 0) {
             const long long nt = (P.nred + kMT - 1) / kMT;
             const unsigned nb = (unsigned)(nt * (nt + 1) / 2);
-            if (sv == Impl::SOLVE_PCG && P.pcg_f32)
+            if (sv == Impl::SOLVE_PCG && P.pcg_res)
+                ;   // the resident PCG builds its tiles itself
+            else if (sv == Impl::SOLVE_PCG && P.pcg_f32)
                 k_eeq_M_tiles<float><<<nb, 256, 0, s>>>(V, P.red2atom.p, P.anchor.p, P.Mf.p, P.lda, 0);
             else
                 k_eeq_M_tiles<double><<<nb, 256, 0, s>>>(V, P.red2atom.p, P.anchor.p, P.M.p, P.lda, full ? 1 : 0);

@@ -331,17 +331,24 @@ __device__ void take_tiles_result(const PCGArgs& A, int row0, int nrow, double* 
     __syncthreads();
 }
 
+// element accessor of the stored matrix (full, lower, or FP32 lower)
+struct MStored {
+    const PCGArgs* A;
+    __device__ __forceinline__ double operator()(int r, int c) const { return mget(*A, r, c); }
+};
+
 // inverse of a preconditioner block of at most kPcgSmall rows by one thread
 // (Gauss-Jordan in registers-sized local storage)
 constexpr int kPcgSmall = 4;
-__device__ void invert_small(const PCGArgs& A, int bk, double* I)
+template <class Get>
+__device__ void invert_small(const PCGArgs& A, int bk, double* I, Get get)
 {
     const int2 bl = A.blocks[bk];
     const int s = bl.y;
     double g[kPcgSmall][kPcgSmall], inv[kPcgSmall][kPcgSmall];
     for (int i = 0; i < s; ++i)
         for (int j = 0; j < s; ++j) {
-            g[i][j] = mget(A, bl.x + i, bl.x + j);
+            g[i][j] = get(bl.x + i, bl.x + j);
             inv[i][j] = i == j ? 1.0 : 0.0;
         }
     for (int c = 0; c < s; ++c) {
@@ -362,13 +369,14 @@ __device__ void invert_small(const PCGArgs& A, int bk, double* I)
 // doubles per warp), __syncwarp only.  M is stored in full and symmetric, so row i of
 // the block is read from column i of M (coalesced).
 constexpr int kPcgWarpMax = 32;
-__device__ void invert_warp(const PCGArgs& A, int bk, double* I, double* colc)
+template <class Get>
+__device__ void invert_warp(const PCGArgs& A, int bk, double* I, double* colc, Get get)
 {
     const int lane = threadIdx.x & 31;
     const int2 bl = A.blocks[bk];
     const int s = bl.y;
     if (lane < s)
-        for (int i = 0; i < s; ++i) I[i * s + lane] = mget(A, bl.x + lane, bl.x + i);
+        for (int i = 0; i < s; ++i) I[i * s + lane] = get(bl.x + lane, bl.x + i);
     __syncwarp();
     for (int c = 0; c < s; ++c) {
         colc[lane] = lane < s ? I[lane * s + c] : 0.0;
@@ -390,7 +398,8 @@ __device__ void invert_warp(const PCGArgs& A, int bk, double* I, double* colc)
 // inverses of the grid block's preconditioner blocks (Gauss-Jordan, SPD, no pivoting:
 // up to kPcgSmall rows by one thread, up to kPcgWarpMax by one warp, larger ones by the
 // whole block with G as scratch) and the per-row records of apply_precond
-__device__ void pcg_setup(const PCGArgs& A, int4 pt, long long boff0, double* G, double* Bs, int4* meta)
+template <class Get>
+__device__ void pcg_setup(const PCGArgs& A, int4 pt, long long boff0, double* G, double* Bs, int4* meta, Get get)
 {
     __shared__ double piv;
     constexpr int GL = kPcgMaxBlock + 1;
@@ -398,13 +407,13 @@ __device__ void pcg_setup(const PCGArgs& A, int4 pt, long long boff0, double* G,
     // ---- inverse of every owned preconditioner block (Gauss-Jordan on [M_bb | I]; SPD,
     // no pivoting); small blocks one per thread, larger ones by the whole grid block
     for (int bk = pt.z + threadIdx.x; bk < pt.w; bk += blockDim.x)
-        if (A.blocks[bk].y <= kPcgSmall) invert_small(A, bk, Bs + (A.boff[bk] - boff0));
+        if (A.blocks[bk].y <= kPcgSmall) invert_small(A, bk, Bs + (A.boff[bk] - boff0), get);
     {
         __shared__ double colc[kPcgThreads / 32][32];
         const int warp = threadIdx.x >> 5;
         for (int bk = pt.z + warp; bk < pt.w; bk += (int)(blockDim.x >> 5)) {
             const int s = A.blocks[bk].y;
-            if (s > kPcgSmall && s <= kPcgWarpMax) invert_warp(A, bk, Bs + (A.boff[bk] - boff0), colc[warp]);
+            if (s > kPcgSmall && s <= kPcgWarpMax) invert_warp(A, bk, Bs + (A.boff[bk] - boff0), colc[warp], get);
         }
     }
     for (int bk = pt.z; bk < pt.w; ++bk) {
@@ -415,7 +424,7 @@ __device__ void pcg_setup(const PCGArgs& A, int4 pt, long long boff0, double* G,
         __syncthreads();
         for (int e = threadIdx.x; e < s * s; e += blockDim.x) {
             const int i = e / s, j = e % s;
-            G[i * GL + j] = mget(A, bl.x + i, bl.x + j);
+            G[i * GL + j] = get(bl.x + i, bl.x + j);
             I[e] = i == j ? 1.0 : 0.0;
         }
         __syncthreads();
@@ -469,7 +478,7 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(PCGArgs A)
     int4* meta = reinterpret_cast<int4*>(Bs + A.maxinv);   // per owned row, see apply_precond
     __shared__ unsigned int gen;
     if (threadIdx.x == 0) gen = *(volatile unsigned int*)(A.bar + kBarGen);
-    pcg_setup(A, pt, boff0, G, Bs, meta);
+    pcg_setup(A, pt, boff0, G, Bs, meta, MStored{&A});
     // ---- x = x0 (the previous solution, or 0), r = b - M x0, z = P^-1 r.  x0 is complete
     // in global memory since the previous launch, so no grid barrier is needed here.
     const bool warm = A.warm != nullptr && *A.warm != 0;
@@ -664,7 +673,7 @@ __global__ void __launch_bounds__(kPcgPipeThreads, 2) k_pcg_pipe(PCGArgs A)
     int4* meta = reinterpret_cast<int4*>(Bs + A.maxinv);
     __shared__ unsigned int gen;
     if (threadIdx.x == 0) gen = *(volatile unsigned int*)(A.bar + kBarGen);
-    pcg_setup(A, pt, boff0, G, Bs, meta);
+    pcg_setup(A, pt, boff0, G, Bs, meta, MStored{&A});
     bool ok = true;
     int phase = 0;   // barrier count: selects the published vector and partial set
     // out = (M v) for the owned rows, v replicated in shared memory
@@ -727,6 +736,267 @@ __global__ void __launch_bounds__(kPcgPipeThreads, 2) k_pcg_pipe(PCGArgs A)
         if (!ok) break;
         if (rmax <= A.tol * bmax) {
             // accept only on the true residual r = b - M x; otherwise restart from it
+            double u1, u2;
+            publish(xs, 0.0, 0.0, 0.0, u1, u2, u1);
+            if (!ok) break;
+            product(ns);
+            double rt = 0.0;
+            for (int k = threadIdx.x; k < nrow; k += blockDim.x) {
+                rs[k] = A.b[row0 + k] - ns[k];
+                rt = fmax(rt, fabs(rs[k]));
+            }
+            __syncthreads();
+            apply_precond(nrow, meta, Bs, rs, us);
+            double rtrue;
+            publish(us, 0.0, 0.0, rt, u1, u2, rtrue);
+            if (!ok) break;
+            if (rtrue <= A.tol * bmax) {
+                conv = true;
+                break;
+            }
+            product(ws);
+            for (int k = threadIdx.x; k < nrow; k += blockDim.x) zs[k] = qs[k] = ss[k] = ps[k] = 0.0;
+            __syncthreads();
+            first = true;
+            continue;
+        }
+        ++it;
+        product(ns);
+        double beta, alpha;
+        if (first) {
+            beta = 0.0;
+            alpha = gam / del;
+        } else {
+            beta = gam / gam_prev;
+            alpha = gam / (del - beta * gam / alpha_prev);
+        }
+        first = false;
+        gam_prev = gam;
+        alpha_prev = alpha;
+        for (int k = threadIdx.x; k < nrow; k += blockDim.x) {
+            const double z = ns[k] + beta * zs[k], q = ms[k] + beta * qs[k];
+            const double sv = ws[k] + beta * ss[k], pv = us[k] + beta * ps[k];
+            zs[k] = z; qs[k] = q; ss[k] = sv; ps[k] = pv;
+            xs[k] += alpha * pv;
+            rs[k] -= alpha * sv;
+            us[k] -= alpha * q;
+            ws[k] -= alpha * z;
+        }
+        __syncthreads();
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < nrow; k += blockDim.x) A.x[row0 + k] = xs[k];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        *A.info = !ok ? 2 : (conv ? 0 : 3);
+        *A.iters = it;
+        if (A.warm) *A.warm = (ok && conv) ? 1 : 0;
+    }
+}
+
+}  // namespace
+
+namespace {
+
+// ------------------------------------------------------------------------------------
+// Shared-memory resident PCG for reduced systems whose lower triangle fits the SMs'
+// shared memory (up to ~2400 unknowns on 148 SMs).  Each block builds its 64x64 lower
+// tiles of M straight from the atoms at launch (no HBM matrix, no separate build kernel)
+// and keeps them for every product of the solve; a product adds each tile's row part and
+// transposed part into an L2 vector with FP64 atomics (one barrier), as matvec_tiles does
+// from HBM.  The iteration is the pipelined CG of k_pcg_pipe; the preconditioner blocks
+// are formed from the atoms too.
+// ------------------------------------------------------------------------------------
+struct PCGRes {
+    View V;
+    const int* red2atom;
+    const int* anchor;
+    const int2* tiles;   // 64 x 64 lower tiles {I0, J0}, dealt round-robin to the blocks
+    int ntiles;
+    int ntl;             // tiles per block (the most any block holds)
+    int gscratch;        // 1: preconditioner blocks beyond kPcgWarpMax need the G scratch
+};
+constexpr int kResT = 64, kResLd = kResT + 1;
+
+// element (r, c) of the reduced matrix from the atoms (same operations as k_eeq_M_tiles)
+struct MAtoms {
+    const PCGRes* R;
+    __device__ __forceinline__ double operator()(int r, int c) const
+    {
+        const View& V = R->V;
+        const int k = R->red2atom[r], ak = R->anchor[k], l = R->red2atom[c], al = R->anchor[l];
+        return eeq_a(V, k, l) - eeq_a(V, k, al) - eeq_a(V, ak, l) + eeq_a(V, ak, al);
+    }
+};
+
+// builds tile (I0, J0) into T (column-major, leading dimension kResLd); the tile's row
+// and column atoms (and anchors) are staged in shared memory first
+__device__ void res_build_tile(const PCGRes& R, int n, int I0, int J0, double* T)
+{
+    __shared__ double bx[4][kResT], by[4][kResT], bz[4][kResT], ba[4][kResT], bd[4][kResT];
+    __shared__ int bid[4][kResT];
+    const View& V = R.V;
+    __syncthreads();
+    for (int e = threadIdx.x; e < 4 * kResT; e += blockDim.x) {
+        const int w = e / kResT, t = e % kResT;
+        const int idx = (w < 2 ? I0 : J0) + t;
+        int a = -1;
+        if (idx < n) {
+            const int k = R.red2atom[idx];
+            a = (w & 1) ? R.anchor[k] : k;
+        }
+        bid[w][t] = a;
+        if (a >= 0) {
+            const double4 p = V.pos[a];
+            bx[w][t] = p.x; by[w][t] = p.y; bz[w][t] = p.z;
+            ba[w][t] = V.alpeeq[a];
+            bd[w][t] = V.adiag[a];
+        }
+    }
+    __syncthreads();
+    auto el = [&](int wa, int ia, int wb, int ib) {
+        if (bid[wa][ia] == bid[wb][ib]) return bd[wa][ia];
+        const double dx = bx[wa][ia] - bx[wb][ib], dy = by[wa][ia] - by[wb][ib], dz = bz[wa][ia] - bz[wb][ib];
+        const double d2 = dx * dx + dy * dy + dz * dz;
+        const double s = ba[wa][ia] + ba[wb][ib];
+        if (d2 >= 36.0 * s) return rsqrt(d2);
+        const double r = sqrt(d2);
+        return erf(r / sqrt(s)) / r;
+    };
+    const bool diag = I0 == J0;
+    for (int e = threadIdx.x; e < kResT * kResT; e += blockDim.x) {
+        const int c = e / kResT, r = e % kResT;
+        double v = 0.0;
+        if (I0 + r < n && J0 + c < n && (!diag || r >= c))
+            v = el(0, r, 2, c) - el(0, r, 3, c) - el(1, r, 2, c) + el(1, r, 3, c);
+        T[c * kResLd + r] = v;
+    }
+}
+
+// y += M v over the block's resident tiles: two tile groups of 128 threads, in each the
+// first 64 threads form the row sums u_r, the next 64 the column sums w_c
+__device__ void res_product(const PCGArgs& A, const PCGRes& R, const double* tl, int ntl, const double* v)
+{
+    const int g = threadIdx.x >> 7, t = threadIdx.x & 127, ng = blockDim.x >> 7;
+    for (int k = g; k < ntl; k += ng) {
+        const int2 tp = R.tiles[blockIdx.x + k * gridDim.x];
+        const int I0 = tp.x, J0 = tp.y;
+        const bool diag = I0 == J0;
+        const int ni = min(kResT, A.n - I0), nj = min(kResT, A.n - J0);
+        const double* T = tl + (size_t)k * kResT * kResLd;
+        if (t < kResT) {
+            const int r = t;
+            if (r < ni) {
+                double u0 = 0.0, u1 = 0.0;
+                const int cmax = diag ? r + 1 : nj;
+                int c = 0;
+                for (; c + 1 < cmax; c += 2) {
+                    u0 += T[c * kResLd + r] * v[J0 + c];
+                    u1 += T[(c + 1) * kResLd + r] * v[J0 + c + 1];
+                }
+                if (c < cmax) u0 += T[c * kResLd + r] * v[J0 + c];
+                atomicAdd(A.yA + I0 + r, u0 + u1);
+            }
+        } else {
+            const int c = t - kResT;
+            if (c < nj) {
+                double w0 = 0.0, w1 = 0.0;
+                int r = diag ? c + 1 : 0;
+                for (; r + 1 < ni; r += 2) {
+                    w0 += T[c * kResLd + r] * v[I0 + r];
+                    w1 += T[c * kResLd + r + 1] * v[I0 + r + 1];
+                }
+                if (r < ni) w0 += T[c * kResLd + r] * v[I0 + r];
+                if (w0 + w1 != 0.0) atomicAdd(A.yA + J0 + c, w0 + w1);
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kPcgPipeThreads, 1) k_pcg_res(PCGArgs A, PCGRes R)
+{
+    extern __shared__ double sm[];
+    constexpr int GL = kPcgMaxBlock + 1;
+    const int4 pt = A.part[blockIdx.x];
+    const int row0 = pt.x, row1 = pt.y, nrow = row1 - row0;
+    const long long boff0 = pt.z < pt.w ? A.boff[pt.z] : 0;
+    const int RR = A.maxrows;
+    double* v = sm;                                      // n: operand, replicated
+    double* tl = v + ((A.n + 1) & ~1);                   // R.ntl resident tiles
+    double* G = tl + (size_t)R.ntl * kResT * kResLd;     // scratch for large preconditioner blocks
+    double* xs = G + (R.gscratch ? kPcgMaxBlock * GL : 0);
+    double* rs = xs + RR;
+    double* us = rs + RR;
+    double* ws = us + RR;
+    double* zs = ws + RR;
+    double* qs = zs + RR;
+    double* ss = qs + RR;
+    double* ps = ss + RR;
+    double* ms = ps + RR;
+    double* ns = ms + RR;
+    double* Bs = ns + RR;
+    int4* meta = reinterpret_cast<int4*>(Bs + A.maxinv);
+    __shared__ unsigned int gen;
+    if (threadIdx.x == 0) gen = *(volatile unsigned int*)(A.bar + kBarGen);
+    int ntl = 0;
+    for (int t = blockIdx.x; t < R.ntiles; t += gridDim.x, ++ntl) {
+        const int2 tp = R.tiles[t];
+        res_build_tile(R, A.n, tp.x, tp.y, tl + (size_t)ntl * kResT * kResLd);
+    }
+    pcg_setup(A, pt, boff0, G, Bs, meta, MAtoms{&R});
+    bool ok = true;
+    int phase = 0;
+    auto product = [&](double* out) {
+        res_product(A, R, tl, ntl, v);
+        ok = grid_sync(A.bar, gen) && ok;
+        ++phase;
+        take_tiles_result(A, row0, nrow, out);
+    };
+    auto publish = [&](const double* src, double pa, double pb, double pc, double& ta, double& tb, double& tc) {
+        double* pub = (phase & 1) ? A.z2 : A.z;
+        for (int k = threadIdx.x; k < nrow; k += blockDim.x) __stcg(pub + row0 + k, src[k]);
+        block_sum3(pa, pb, pc, A.partial + 8 * blockIdx.x + 4 * (phase & 1));
+        ok = grid_sync(A.bar, gen) && ok;
+        grid_totals3(A.partial, 4 * (phase & 1), ta, tb, tc);
+        update_p(v, pub, A.n, 0.0);
+        ++phase;
+        __syncthreads();
+    };
+    // ---- start: x0 (previous solution or 0), r = b - M x0, u = P^-1 r, w = M u
+    const bool warm = A.warm != nullptr && *A.warm != 0;
+    if (warm) {
+        update_p(v, A.x, A.n, 0.0);
+        __syncthreads();
+        product(ns);
+    }
+    double bmax_t = 0.0;
+    for (int k = threadIdx.x; k < nrow; k += blockDim.x) {
+        const double bv = A.b[row0 + k];
+        xs[k] = warm ? v[row0 + k] : 0.0;
+        rs[k] = warm ? bv - ns[k] : bv;
+        zs[k] = qs[k] = ss[k] = ps[k] = 0.0;
+        bmax_t = fmax(bmax_t, fabs(bv));
+    }
+    __syncthreads();
+    apply_precond(nrow, meta, Bs, rs, us);
+    double bmax = 0.0, t1, t2;
+    publish(us, 0.0, 0.0, bmax_t, t1, t2, bmax);
+    product(ws);
+    int it = 0;
+    bool conv = ok && bmax == 0.0, first = true;
+    double gam_prev = 1.0, alpha_prev = 1.0;
+    while (ok && !conv && it < A.max_iter) {
+        double g_t = 0.0, d_t = 0.0, rm_t = 0.0;
+        for (int k = threadIdx.x; k < nrow; k += blockDim.x) {
+            g_t += rs[k] * us[k];
+            d_t += ws[k] * us[k];
+            rm_t = fmax(rm_t, fabs(rs[k]));
+        }
+        __syncthreads();
+        apply_precond(nrow, meta, Bs, ws, ms);
+        double gam, del, rmax;
+        publish(ms, g_t, d_t, rm_t, gam, del, rmax);
+        if (!ok) break;
+        if (rmax <= A.tol * bmax) {
             double u1, u2;
             publish(xs, 0.0, 0.0, 0.0, u1, u2, u1);
             if (!ok) break;

@@ -133,19 +133,22 @@ def test_error_paths():
     assert gpu.calculateEnergy(True) != 0.0 and not gpu.hasError()
 
 
-@pytest.mark.parametrize("solver", ["tiled", "library", "pcg", "pcg-lower", "pcg-classic", "batched"])
+@pytest.mark.parametrize("solver", ["tiled", "library", "pcg", "pcg-lower", "pcg-classic", "pcg-resident",
+                                    "batched"])
 @pytest.mark.parametrize("system", ["water64", "water200", "alkane", "peptide"])
 def test_eeq_solvers(solver, system, monkeypatch):
     """Every EEQ solver of the reduced system against the oracle; the 64-water cluster
     has 128 reduced unknowns, so the tiled Cholesky's right-hand-side row forms a tile of
     its own, and the alkane (one fragment) exercises the PCG with 64-row blocks.
     pcg-lower forces the PCG form of large systems (lower triangle only, M p by tiles),
-    pcg-classic the two-barrier CG iteration instead of the pipelined one;
+    pcg-classic the two-barrier CG iteration instead of the pipelined one, pcg-resident the
+    pipelined iteration over shared-memory resident tiles built from the atoms;
     batched is the per-molecule shared-memory solver, offered for molecules of at most
     320 atoms."""
     monkeypatch.setenv("GFNFF_PCG_SYM", "1" if solver == "pcg-lower" else "0")
     monkeypatch.setenv("GFNFF_PCG", "classic" if solver == "pcg-classic" else "pipelined")
-    solver = "pcg" if solver in ("pcg-lower", "pcg-classic") else solver
+    monkeypatch.setenv("GFNFF_PCG_RES", "1" if solver == "pcg-resident" else "0")
+    solver = "pcg" if solver in ("pcg-lower", "pcg-classic", "pcg-resident") else solver
     monkeypatch.setenv("GFNFF_EEQ_SOLVER", solver)
     Z, X = {"water64": lambda: workloads.water_cluster(64, 9),
             "water200": lambda: workloads.water_cluster(200, 10),
