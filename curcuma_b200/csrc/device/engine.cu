@@ -45,6 +45,9 @@ namespace gfnff {
 #include "k_eeq.cuh"
 #include "k_chol.cuh"
 #include "k_pcg.cuh"
+}  // namespace gfnff
+#include "../setup/linalg.h"
+namespace gfnff {
 
 namespace {
 
@@ -187,6 +190,7 @@ struct Engine::Impl {
     DBuf<int> mol, perm;
     DBuf<int2> jr;
     std::vector<int> h_perm, h_iperm, h_aoff;
+    std::vector<int> h_anchor, h_r2a;   // EEQ null-space maps (host copies)
     DBuf<double> e0;
     // model
     DBuf<double4> pos, pos0, hbref;
@@ -270,6 +274,13 @@ struct Engine::Impl {
     // response solve; probes (pcg_warm false) start from zero so that their timing is fair
     DBuf<int> pwarm;
     bool pcg_warm = false;
+    // Molecules with fragments of more than 32 unknowns (chains): the block-Jacobi inverses
+    // come from the set-up geometry, computed once on the host (blocks up to 128 unknowns,
+    // applied from global memory), instead of being recomputed in every launch from the
+    // current matrix.  The preconditioner is then slightly stale, which costs iterations
+    // only; the solve stays exact (GFNFF_PCG_PRE=0: off).
+    bool pcg_pre = false;
+    DBuf<double> pbinv;
     // matrices beyond L2 keep only their lower triangle; the PCG multiplies by tiles
     bool pcg_lower = false;
     // mixed form, lower-triangle PCG, GFNFF_PCG_F32=1: M stored in FP32 (half the bytes per
@@ -305,6 +316,7 @@ struct Engine::Impl {
         A.warm = pcg_warm ? pwarm.p + slot : nullptr;
         A.lower = pcg_lower ? pcg_cols : 0; A.yA = pyA.p; A.tiles = ptiles.p; A.ntiles = pcg_ntiles;
         A.Mf = pcg_f32 ? Mf.p : nullptr;
+        A.binv_pre = pcg_pre ? pbinv.p : nullptr;
         void* args[] = {&A};
         if (pcg_res) {
             PCGRes R{view(), red2atom.p, anchor.p, prtiles.p, pcg_res_ntiles, pcg_res_ntl, pcg_res_gscratch};
@@ -647,6 +659,8 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
         P.msize = ms;
         P.nq = (int)ql.size();
         P.anchor.upload(anchor); P.atom2red.upload(a2r); P.red2atom.upload(r2a);
+        P.h_anchor = anchor;
+        P.h_r2a = r2a;
         P.frag_off.upload(off); P.frag_atoms.upload(fa); P.q0.upload(q0); P.qlist.upload(ql);
         P.roff.upload(roff); P.moff.upload(moff);
         // batches, and single molecules small enough for the batched kernel's staging
@@ -922,6 +936,17 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
         // clusters this leaves the iteration count unchanged, so it is off by default.
         P.pcg_ready = false;
         std::vector<int2> blocks;
+        int blkmax = kPcgMaxBlock;
+        {
+            const Model& Mf0 = *mols[0];
+            std::vector<int> fsz(std::max(1, Mf0.nfrag), 0);
+            for (int a = 0; a < Mf0.n; ++a) ++fsz[Mf0.frag[a]];
+            int big = 0;
+            for (int c : fsz) big = std::max(big, c - 1);
+            const char* ep = std::getenv("GFNFF_PCG_PRE");
+            P.pcg_pre = big > kPcgWarpMax && !(ep && !std::strcmp(ep, "0"));
+            if (P.pcg_pre) blkmax = 128;
+        }
         {
             int group = 0;
             if (const char* e = std::getenv("GFNFF_PCG_BLOCK")) group = std::max(0, std::min(kPcgWarpMax, std::atoi(e)));
@@ -939,8 +964,13 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
                 const int nr = j - i - 1;   // the fragment's anchor is its first atom
                 if (nr > group) {
                     flush();
-                    for (int c = 0; c < nr; c += kPcgMaxBlock)
-                        blocks.push_back(make_int2(r + c, std::min(kPcgMaxBlock, nr - c)));
+                    // equal chunks of at most blkmax
+                    const int nch = (nr + blkmax - 1) / blkmax, base = nr / nch, extra = nr % nch;
+                    for (int c = 0, off = 0; c < nch; ++c) {
+                        const int sz = base + (c < extra ? 1 : 0);
+                        blocks.push_back(make_int2(r + off, sz));
+                        off += sz;
+                    }
                 } else if (nr > 0) {
                     if (cur + nr > group) flush();
                     if (cur == 0) cur0 = r;
@@ -952,13 +982,69 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
             flush();
             if (r != P.nred) blocks.clear();   // fragments not contiguous: no PCG
         }
+        if (!blocks.empty() && P.pcg_pre) {
+            // set-up-geometry inverses of every block (host Cholesky), row-major like the
+            // device-computed ones
+            auto A_el = [&](int a, int b) {
+                if (a == b) return adg[a];
+                const double dx = p0[a].x - p0[b].x, dy = p0[a].y - p0[b].y, dz = p0[a].z - p0[b].z;
+                const double d2 = dx * dx + dy * dy + dz * dz, sa = alp[a] + alp[b];
+                if (d2 >= 36.0 * sa) return 1.0 / std::sqrt(d2);
+                const double rr = std::sqrt(d2);
+                return std::erf(rr / std::sqrt(sa)) / rr;
+            };
+            std::vector<double> inv;
+            for (auto& b : blocks) {
+                const int sz = b.y;
+                std::vector<double> Mb((size_t)sz * sz), Ib((size_t)sz * sz, 0.0);
+                for (int i = 0; i < sz; ++i)
+                    for (int j = 0; j < sz; ++j) {
+                        const int k = P.h_r2a[b.x + i], ak = P.h_anchor[k];
+                        const int l = P.h_r2a[b.x + j], al = P.h_anchor[l];
+                        Mb[(size_t)i * sz + j] = A_el(k, l) - A_el(k, al) - A_el(ak, l) + A_el(ak, al);
+                    }
+                for (int i = 0; i < sz; ++i) Ib[(size_t)i * sz + i] = 1.0;
+                if (!linalg::cholesky(Mb.data(), sz)) {
+                    P.pcg_pre = false;   // not positive definite: inverses per launch instead
+                    break;
+                }
+                linalg::cholesky_solve(Mb.data(), sz, Ib.data(), sz);
+                inv.insert(inv.end(), Ib.begin(), Ib.end());
+            }
+            if (P.pcg_pre) P.pbinv.upload(inv);
+            else blocks.clear();   // rebuilt below with device-sized blocks
+        }
+        if (blocks.empty() && !P.pcg_pre && blkmax != kPcgMaxBlock) {
+            // the set-up inverses failed: fall back to per-fragment blocks of <= 64
+            std::vector<int> fr(n);
+            const Model& M0 = *mols[0];
+            for (int a = 0; a < n; ++a) fr[P.ix(0, a)] = M0.frag[a];
+            int r = 0, i = 0;
+            while (i < n) {
+                int j = i;
+                while (j < n && fr[j] == fr[i]) ++j;
+                const int nr = j - i - 1;
+                for (int c = 0; c < nr; c += kPcgMaxBlock)
+                    blocks.push_back(make_int2(r + c, std::min(kPcgMaxBlock, nr - c)));
+                r += nr;
+                i = j;
+            }
+            if (r != P.nred) blocks.clear();
+        }
         if (!blocks.empty()) {
             // rows per grid block: whole preconditioner blocks, about nred / nsm rows each
             std::vector<int4> part;
             std::vector<long long> boff;
             long long bo = 0;
             for (auto& b : blocks) { boff.push_back(bo); bo += (long long)b.y * b.y; }
-            const int G = std::max(1, std::min(nsm, (int)blocks.size()));
+            // the lower-triangle form from 4096 unknowns (the matrix leaves L2), and for chains
+            // with set-up block inverses from 1024: its tiled product balances work by tiles, so
+            // every SM takes part even where large preconditioner blocks, owned whole, would
+            // load a few blocks with most rows (Gly50 + 1500 waters: 1.45 -> 0.69 ms)
+            const char* esym = std::getenv("GFNFF_PCG_SYM");
+            const bool lower = esym ? std::strcmp(esym, "0") != 0
+                                    : (P.nred >= 4096 || (P.pcg_pre && P.nred >= 1024));
+            const int G = lower ? nsm : std::max(1, std::min(nsm, (int)blocks.size()));
             size_t bk = 0;
             int maxrows = 1;
             long long maxinv = 1;
@@ -972,6 +1058,7 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
                 maxinv = std::max(maxinv, (bk < blocks.size() ? boff[bk] : bo) - (b0 < (int)blocks.size() ? boff[b0] : bo));
             }
             // p (n), Gauss-Jordan scratch, x/r/z/Mp of the owned rows, owned block inverses
+            if (P.pcg_pre) maxinv = 0;      // inverses applied from global memory
             maxinv = (maxinv + 1) & ~1ll;   // keeps the int4 row records behind it 16-byte aligned
             const size_t smem =
                 ((size_t)((P.nred + 1) & ~1) + kPcgMaxBlock * (kPcgMaxBlock + 1) + 4 * (size_t)maxrows + maxinv) *
@@ -986,8 +1073,7 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
                 P.pcg_maxrows = maxrows;
                 P.pcg_maxinv = (int)maxinv;
                 {
-                    const char* e = std::getenv("GFNFF_PCG_SYM");
-                    P.pcg_lower = e ? std::strcmp(e, "0") != 0 : P.nred >= 4096;
+                    P.pcg_lower = lower;
                     const char* ef = std::getenv("GFNFF_PCG_F32");
                     P.pcg_f32 = P.pcg_lower && P.opt.precision == 1 && ef && !std::strcmp(ef, "1");
                     if (P.pcg_f32) P.Mf.alloc((size_t)P.lda * P.nred);

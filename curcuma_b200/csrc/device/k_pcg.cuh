@@ -45,6 +45,7 @@ struct PCGArgs {
     int* warm;            // when non-null and *warm != 0, x holds the previous solution of the
                           // same system and is the initial guess; set to 1 on convergence
     const float* Mf;      // lower form in the mixed precision form: M stored in FP32 (M unused)
+    const double* binv_pre;   // block inverses computed at set-up (global memory, boff layout), or null
     int lower;            // 1 or 2: only the lower triangle of M is stored; M p by tiles
                           // (matvec_tiles, streaming 4 or 8 columns per warp at once)
     double* yA;           // lower: n-vector the tiles add M p into (zero between uses)
@@ -404,6 +405,15 @@ __device__ void pcg_setup(const PCGArgs& A, int4 pt, long long boff0, double* G,
     __shared__ double piv;
     constexpr int GL = kPcgMaxBlock + 1;
     const int row0 = pt.x, nrow = pt.y - pt.x;
+    if (A.binv_pre) {   // inverses from set-up: only the row records
+        for (int k = threadIdx.x; k < nrow; k += blockDim.x) {
+            const int rr = row0 + k, bk = A.rblk[rr];
+            const int2 bl = A.blocks[bk];
+            meta[k] = make_int4(bl.x - row0, bl.y, (int)(A.boff[bk] - boff0) + (rr - bl.x) * bl.y, 0);
+        }
+        __syncthreads();
+        return;
+    }
     // ---- inverse of every owned preconditioner block (Gauss-Jordan on [M_bb | I]; SPD,
     // no pivoting); small blocks one per thread, larger ones by the whole grid block
     for (int bk = pt.z + threadIdx.x; bk < pt.w; bk += blockDim.x)
@@ -479,6 +489,7 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(PCGArgs A)
     __shared__ unsigned int gen;
     if (threadIdx.x == 0) gen = *(volatile unsigned int*)(A.bar + kBarGen);
     pcg_setup(A, pt, boff0, G, Bs, meta, MStored{&A});
+    const double* Bp = A.binv_pre ? A.binv_pre + boff0 : Bs;
     // ---- x = x0 (the previous solution, or 0), r = b - M x0, z = P^-1 r.  x0 is complete
     // in global memory since the previous launch, so no grid barrier is needed here.
     const bool warm = A.warm != nullptr && *A.warm != 0;
@@ -503,7 +514,7 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(PCGArgs A)
         bmax_t = fmax(bmax_t, fabs(bv));
     }
     __syncthreads();
-    double rz_t = apply_precond(nrow, meta, Bs, rs, zs);
+    double rz_t = apply_precond(nrow, meta, Bp, rs, zs);
     for (int k = threadIdx.x; k < nrow; k += blockDim.x) __stcg(A.z + row0 + k, zs[k]);
     block_sum_max(rz_t, bmax_t, A.partial + 4 * blockIdx.x);
     ok = grid_sync(A.bar, gen) && ok;
@@ -530,7 +541,7 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(PCGArgs A)
             rmax_t = fmax(rmax_t, fabs(rs[k]));
         }
         __syncthreads();
-        rz_t = apply_precond(nrow, meta, Bs, rs, zs);
+        rz_t = apply_precond(nrow, meta, Bp, rs, zs);
         for (int k = threadIdx.x; k < nrow; k += blockDim.x) __stcg(A.z + row0 + k, zs[k]);
         block_sum_max(rz_t, rmax_t, A.partial + 4 * blockIdx.x + 2);
         ok = grid_sync(A.bar, gen);
@@ -559,7 +570,7 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(PCGArgs A)
                 rmax_t = fmax(rmax_t, fabs(rs[k]));
             }
             __syncthreads();
-            rz_t = apply_precond(nrow, meta, Bs, rs, zs);
+            rz_t = apply_precond(nrow, meta, Bp, rs, zs);
             for (int k = threadIdx.x; k < nrow; k += blockDim.x) __stcg(A.z + row0 + k, zs[k]);
             block_sum_max(rz_t, rmax_t, A.partial + 4 * blockIdx.x + 2);
             ok = grid_sync(A.bar, gen);
@@ -674,6 +685,7 @@ __global__ void __launch_bounds__(kPcgPipeThreads, 2) k_pcg_pipe(PCGArgs A)
     __shared__ unsigned int gen;
     if (threadIdx.x == 0) gen = *(volatile unsigned int*)(A.bar + kBarGen);
     pcg_setup(A, pt, boff0, G, Bs, meta, MStored{&A});
+    const double* Bp = A.binv_pre ? A.binv_pre + boff0 : Bs;
     bool ok = true;
     int phase = 0;   // barrier count: selects the published vector and partial set
     // out = (M v) for the owned rows, v replicated in shared memory
@@ -715,7 +727,7 @@ __global__ void __launch_bounds__(kPcgPipeThreads, 2) k_pcg_pipe(PCGArgs A)
         bmax_t = fmax(bmax_t, fabs(bv));
     }
     __syncthreads();
-    apply_precond(nrow, meta, Bs, rs, us);
+    apply_precond(nrow, meta, Bp, rs, us);
     double bmax = 0.0, t1, t2;
     publish(us, 0.0, 0.0, bmax_t, t1, t2, bmax);
     product(ws);
@@ -730,7 +742,7 @@ __global__ void __launch_bounds__(kPcgPipeThreads, 2) k_pcg_pipe(PCGArgs A)
             rm_t = fmax(rm_t, fabs(rs[k]));
         }
         __syncthreads();
-        apply_precond(nrow, meta, Bs, ws, ms);
+        apply_precond(nrow, meta, Bp, ws, ms);
         double gam, del, rmax;
         publish(ms, g_t, d_t, rm_t, gam, del, rmax);
         if (!ok) break;
@@ -746,7 +758,7 @@ __global__ void __launch_bounds__(kPcgPipeThreads, 2) k_pcg_pipe(PCGArgs A)
                 rt = fmax(rt, fabs(rs[k]));
             }
             __syncthreads();
-            apply_precond(nrow, meta, Bs, rs, us);
+            apply_precond(nrow, meta, Bp, rs, us);
             double rtrue;
             publish(us, 0.0, 0.0, rt, u1, u2, rtrue);
             if (!ok) break;
@@ -943,6 +955,7 @@ __global__ void __launch_bounds__(kPcgPipeThreads, 1) k_pcg_res(PCGArgs A, PCGRe
         res_build_tile(R, A.n, tp.x, tp.y, tl + (size_t)ntl * kResT * kResLd);
     }
     pcg_setup(A, pt, boff0, G, Bs, meta, MAtoms{&R});
+    const double* Bp = A.binv_pre ? A.binv_pre + boff0 : Bs;
     bool ok = true;
     int phase = 0;
     auto product = [&](double* out) {
@@ -977,7 +990,7 @@ __global__ void __launch_bounds__(kPcgPipeThreads, 1) k_pcg_res(PCGArgs A, PCGRe
         bmax_t = fmax(bmax_t, fabs(bv));
     }
     __syncthreads();
-    apply_precond(nrow, meta, Bs, rs, us);
+    apply_precond(nrow, meta, Bp, rs, us);
     double bmax = 0.0, t1, t2;
     publish(us, 0.0, 0.0, bmax_t, t1, t2, bmax);
     product(ws);
@@ -992,7 +1005,7 @@ __global__ void __launch_bounds__(kPcgPipeThreads, 1) k_pcg_res(PCGArgs A, PCGRe
             rm_t = fmax(rm_t, fabs(rs[k]));
         }
         __syncthreads();
-        apply_precond(nrow, meta, Bs, ws, ms);
+        apply_precond(nrow, meta, Bp, ws, ms);
         double gam, del, rmax;
         publish(ms, g_t, d_t, rm_t, gam, del, rmax);
         if (!ok) break;
@@ -1007,7 +1020,7 @@ __global__ void __launch_bounds__(kPcgPipeThreads, 1) k_pcg_res(PCGArgs A, PCGRe
                 rt = fmax(rt, fabs(rs[k]));
             }
             __syncthreads();
-            apply_precond(nrow, meta, Bs, rs, us);
+            apply_precond(nrow, meta, Bp, rs, us);
             double rtrue;
             publish(us, 0.0, 0.0, rt, u1, u2, rtrue);
             if (!ok) break;
