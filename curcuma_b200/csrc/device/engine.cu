@@ -945,7 +945,10 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
             for (int c : fsz) big = std::max(big, c - 1);
             const char* ep = std::getenv("GFNFF_PCG_PRE");
             P.pcg_pre = big > kPcgWarpMax && !(ep && !std::strcmp(ep, "0"));
-            if (P.pcg_pre) blkmax = 128;
+            if (P.pcg_pre) {
+                blkmax = 128;
+                if (const char* eb = std::getenv("GFNFF_PCG_PREBLK")) blkmax = std::max(2, std::min(512, std::atoi(eb)));
+            }
         }
         {
             int group = 0;

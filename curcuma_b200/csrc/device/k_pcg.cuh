@@ -189,7 +189,8 @@ __device__ double apply_precond(int nrow, const int4* meta, const double* binv, 
 // pairs (lda is even) with eight independent pairs in flight per lane, so that one
 // row of L2-resident M costs a few L2 round trips rather than one per 32 elements.
 // Returns the thread's part of sum_r v_r (M v)_r.
-__device__ double matvec_rows(const PCGArgs& A, const double* v, int row0, int row1, double* out)
+template <int U>   // double2 loads in flight per lane
+__device__ double matvec_rows_u(const PCGArgs& A, const double* v, int row0, int row1, double* out)
 {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     const int n2 = A.n >> 1;
@@ -202,14 +203,14 @@ __device__ double matvec_rows(const PCGArgs& A, const double* v, int row0, int r
 #pragma unroll
         for (int u = 0; u < 8; ++u) s[u] = 0.0;
         int c = lane;
-        for (; c + 7 * 32 < n2; c += 8 * 32) {
-            double2 m[8];
+        for (; c + (U - 1) * 32 < n2; c += U * 32) {
+            double2 m[U];
 #pragma unroll
-            for (int u = 0; u < 8; ++u) m[u] = c2[c + 32 * u];
+            for (int u = 0; u < U; ++u) m[u] = c2[c + 32 * u];
 #pragma unroll
-            for (int u = 0; u < 8; ++u) {
+            for (int u = 0; u < U; ++u) {
                 const double2 w = v2[c + 32 * u];
-                s[u] += m[u].x * w.x + m[u].y * w.y;
+                s[u & 7] += m[u].x * w.x + m[u].y * w.y;
             }
         }
         for (; c < n2; c += 32) {
@@ -225,6 +226,13 @@ __device__ double matvec_rows(const PCGArgs& A, const double* v, int row0, int r
         }
     }
     return vmv;
+}
+
+// eight loads in flight per lane measured faster than sixteen (1000 waters: 0.188 vs 0.194 ms
+// per solve)
+__device__ double matvec_rows(const PCGArgs& A, const double* v, int row0, int row1, double* out)
+{
+    return matvec_rows_u<8>(A, v, row0, row1, out);
 }
 
 // element (r, c) of M, from the lower triangle when only that is stored
