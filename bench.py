@@ -193,6 +193,16 @@ def roofline(phase_avg, info, fp64_peak, hbm_peak, hbm_src):
             "peak_source": "measured (fma microbenchmark)" if bound == "fp64" else hbm_src}
 
 
+def cpu_model():
+    try:
+        for l in open("/proc/cpuinfo"):
+            if l.startswith("model name"):
+                return l.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def cpu_oracle_rate(Z, X, steps, warmup):
     from tests.oracle_api import Oracle
     o = Oracle(Z, X)
@@ -217,7 +227,7 @@ def run_reference(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
             "config": {"workload": f"config {args.config}: {desc}", "natoms": int(len(Z))},
-            "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+            "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "port", "cpu": cpu_model(),
                              "sample": f"{args.steps} full E+grad evaluations of the workload"},
             "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "note": "CPU restatement of curcuma's gfnff path (oracle/), all host threads; the "
@@ -460,6 +470,7 @@ def run_ours(args):
         info["eeq_flops"] = sum((len(z) - 1) ** 3 / 3.0 + 2.0 * (len(z) - 1) ** 2 for z, _ in mols)
     hbm_peak, hbm_src = measured_peaks()
     fp64_peak = gpu._lib.gfnff_fma_peak_tflops(local, 1)
+    fp32_peak = gpu._lib.gfnff_fma_peak_tflops(local, 0)
     roof = roofline(main["phase_avg"], info, fp64_peak, hbm_peak, hbm_src)
     steps = args.steps
     line = {"metric": METRIC, "value": main["value"], "unit": UNIT, "n_gpus": world, "steps": steps,
@@ -480,7 +491,9 @@ def run_ours(args):
                       for p, r in res.items()},
             "mixed_vs_fp64": res["mixed"]["value"] / res["fp64"]["value"],
             "mixed_error_vs_fp64": err,
-            "pairs": {"coulomb": nc, "dispersion": nd}, "terms": counts, "clocks": main["clocks"]}
+            "pairs": {"coulomb": nc, "dispersion": nd}, "terms": counts, "clocks": main["clocks"],
+            "peaks": {"fp64_fma_tflops": fp64_peak, "fp32_fma_tflops": fp32_peak, "hbm_gbs": hbm_peak,
+                      "source": "FMA: library microbenchmark (csrc/device/peaks.cu); HBM: " + hbm_src}}
     if mols:
         line["per_molecule_loop_fp64"] = loop
         line["batch_vs_loop"] = main["value"] / loop["value"]
@@ -502,6 +515,7 @@ def run_ours(args):
     if world == 1 and not args.no_cpu_baseline:
         rate, dt = cpu_oracle_rate(Z, X, 2 if n >= 2000 else 5, 1)
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                                "cpu": cpu_model(),
                                 "sample": f"{2 if n >= 2000 else 5} full E+grad evaluations of the same workload "
                                           f"({dt:.1f} s)"}
     print(json.dumps(line), flush=True)
