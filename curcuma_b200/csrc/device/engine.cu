@@ -152,6 +152,58 @@ int hb_near_count(const Model& m)
     return c;
 }
 
+// Hydrogen-bond data for the device: one int4 {A, H, B, case} per term (set-up distance
+// order) and per-atom tables, because every other term parameter is a function of one of
+// the three atoms (ff_workspace_gfnff.cpp:938-1409 reads them per term; here the terms of
+// one acceptor share them): charge scalings qs(q_H), qs(-q_A/B), basicity, acidity, vdW
+// radius, lone-pair parameter and the N-with-one-neighbour flag of an acceptor, its carbonyl
+// parent (case 3), and the bond graph (the neighbours of an acceptor and of its parent).
+struct HBHost {
+    std::vector<int4> rec;
+    std::vector<double> qh, qa, bas, aci, rvdw, zlp;
+    std::vector<int> pc, nfl;
+    std::vector<std::vector<int>> nbr;
+    int mismatch = 0;
+    explicit HBHost(int n) : qh(n, 0.0), qa(n, 0.0), bas(n, 0.0), aci(n, 0.0), rvdw(n, 0.0), zlp(n, 1.0),
+                             pc(n, -1), nfl(n, 0), nbr(n) {}
+    void set(double& slot, bool& seen, double v)
+    {
+        if (seen && slot != v) ++mismatch;
+        slot = v;
+        seen = true;
+    }
+    template <class Map>
+    void add(const Model& M, Map X)
+    {
+        auto qs = [](double q) { const double e = std::exp(15.0 * q); return e / (e + 1.0); };
+        std::vector<char> sh(M.n, 0), sa(M.n, 0), sb(M.n, 0), sc(M.n, 0);
+        for (int a = 0; a < M.n; ++a) {
+            const int i = X(a);
+            rvdw[i] = M.rvdw[a];
+            for (int x : M.adj[a]) nbr[i].push_back(X(x));
+            const int z = M.Z[a];
+            zlp[i] = (z >= 1 && z <= 86) ? gfnff_tables::repz[z - 1] : 1.0;
+            nfl[i] = (z == 7 && M.adj[a].size() == 1) ? 1 : 0;
+        }
+        for (int ti : hb_order(M)) {
+            const HBTerm& t = M.hbonds[ti];
+            const int A = X(t.a), H = X(t.h), B = X(t.b);
+            rec.push_back(make_int4(A, H, B, t.case_type));
+            bool s1 = sh[t.h], s2 = sa[t.a], s3 = sa[t.b], s4 = sb[t.a], s5 = sb[t.b], s6 = sc[t.a], s7 = sc[t.b];
+            set(qh[H], s1, qs(t.q_h));
+            set(qa[A], s2, qs(-t.q_a));
+            set(qa[B], s3, qs(-t.q_b));
+            set(bas[A], s4, t.bas_a);
+            set(bas[B], s5, t.bas_b);
+            set(aci[A], s6, t.aci_a);
+            set(aci[B], s7, t.aci_b);
+            sh[t.h] = 1; sa[t.a] = sa[t.b] = 1; sb[t.a] = sb[t.b] = 1; sc[t.a] = sc[t.b] = 1;
+            if (t.case_type == 3 && t.parent_c >= 0) pc[B] = X(t.parent_c);
+            if (t.case_type >= 2 && t.nb_b != M.adj[t.b]) ++mismatch;
+        }
+    }
+};
+
 // blocks of a tiled pair kernel: enough partner slices to give every SM a few blocks
 int pair_splits(int n, int max_range)
 {
@@ -223,8 +275,22 @@ struct Engine::Impl {
     DBuf<double> at_c9, at_r0ij, at_r0ik, at_r0jk, at_sc;
     DBuf<int> ba_i, ba_j, ba_k;
     DBuf<double> ba_c9;
-    DBuf<int> h_a, h_h, h_b, h_c, h_pc, h_nbo, h_nb, h_nco, h_nc, h_nfl;
-    DBuf<double> h_ba, h_bb, h_aa, h_ab, h_QH, h_QA, h_QB, h_rv, h_zlp;
+    DBuf<int4> h_rec;
+    DBuf<double> h_qh, h_qa, h_bas, h_aci, h_rvdw, h_zlp;
+    DBuf<int> h_pc, h_nfl, h_adjo, h_adj;
+    void upload_hb(const HBHost& T)
+    {
+        if (T.mismatch) throw std::runtime_error("HB set-up: per-term parameters differ for one atom");
+        std::vector<int> off{0}, adj;
+        for (auto& l : T.nbr) {
+            adj.insert(adj.end(), l.begin(), l.end());
+            off.push_back((int)adj.size());
+        }
+        h_rec.upload(T.rec); h_qh.upload(T.qh); h_qa.upload(T.qa); h_bas.upload(T.bas); h_aci.upload(T.aci);
+        h_rvdw.upload(T.rvdw); h_zlp.upload(T.zlp); h_pc.upload(T.pc); h_nfl.upload(T.nfl);
+        h_adjo.upload(off); h_adj.upload(adj);
+        nhb = (int)T.rec.size();
+    }
     DBuf<int> x_a, x_x, x_b;
     DBuf<double> x_pre, x_rv;
     DBuf<int> r_off, r_j;
@@ -462,31 +528,10 @@ void Engine::upload_hbxb(const Model& m)
         P.b_cki.upload(cki); P.b_ckj.upload(ckj); P.b_sh.upload(sh); P.b_ff.upload(ff);
     }
     {
-        std::vector<int> a, h, b, c, pc, nbo{0}, nb, nco{0}, nc, nfl;
-        std::vector<double> ba, bb, aa, ab, QH, QA, QB, rv, zlp;
-        auto qs = [](double q, double st, double sf) { const double e = std::exp(st * q); return e / (e + sf); };
-        for (int ti : hb_order(m)) {
-            const HBTerm& t = m.hbonds[ti];
-            a.push_back(X(t.a)); h.push_back(X(t.h)); b.push_back(X(t.b)); c.push_back(t.case_type);
-            pc.push_back(t.parent_c >= 0 ? X(t.parent_c) : -1);
-            for (int x : t.nb_b) nb.push_back(X(x));
-            nbo.push_back((int)nb.size());
-            if (t.case_type == 3) for (int x : t.nb_c) nc.push_back(X(x));
-            nco.push_back((int)nc.size());
-            ba.push_back(t.bas_a); bb.push_back(t.bas_b); aa.push_back(t.aci_a); ab.push_back(t.aci_b);
-            QH.push_back(qs(t.q_h, 15.0, 1.0)); QA.push_back(qs(-t.q_a, 15.0, 1.0)); QB.push_back(qs(-t.q_b, 15.0, 1.0));
-            rv.push_back(m.rvdw[t.a] + m.rvdw[t.b]);
-            const int zb = m.Z[t.b];
-            zlp.push_back((zb >= 1 && zb <= 86) ? gfnff_tables::repz[zb - 1] : 1.0);
-            nfl.push_back((zb == 7 && t.nb_b.size() == 1) ? 1 : 0);
-        }
-        P.nhb = (int)m.hbonds.size();
+        HBHost T(P.n);
+        T.add(m, X);
+        P.upload_hb(T);
         P.nhb_near = hb_near_count(m);
-        P.h_a.upload(a); P.h_h.upload(h); P.h_b.upload(b); P.h_c.upload(c); P.h_pc.upload(pc);
-        P.h_nbo.upload(nbo); P.h_nb.upload(nb); P.h_nco.upload(nco); P.h_nc.upload(nc);
-        P.h_ba.upload(ba); P.h_bb.upload(bb); P.h_aa.upload(aa); P.h_ab.upload(ab);
-        P.h_QH.upload(QH); P.h_QA.upload(QA); P.h_QB.upload(QB); P.h_rv.upload(rv); P.h_zlp.upload(zlp);
-        P.h_nfl.upload(nfl);
     }
     {
         std::vector<int> a, x, b;
@@ -825,8 +870,7 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
     } else {   // bonds, HB and XB of every molecule (HB/XB lists stay those of the setup)
         std::vector<int> bi, bj, bh, off{0}, hb;
         std::vector<double> fc, al, r0i, r0j, cki, ckj, sh, ff;
-        std::vector<int> a, h, b, c, pc, nbo{0}, nbv, nco{0}, ncv, nfl;
-        std::vector<double> ba, bb, aa, abv, QH, QA, QB, rv, zlp;
+        HBHost hbt(n);
         std::vector<int> xa, xx, xb;
         std::vector<double> xpre, xrv;
         auto qs = [](double q, double st, double sf) { const double e = std::exp(st * q); return e / (e + sf); };
@@ -844,21 +888,7 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
                 if (H >= 0) for (int x : byH[H]) hb.push_back(X(x));
                 off.push_back((int)hb.size());
             }
-            for (int ti : hb_order(M)) {
-                const HBTerm& t = M.hbonds[ti];
-                a.push_back(X(t.a)); h.push_back(X(t.h)); b.push_back(X(t.b)); c.push_back(t.case_type);
-                pc.push_back(t.parent_c >= 0 ? X(t.parent_c) : -1);
-                for (int x : t.nb_b) nbv.push_back(X(x));
-                nbo.push_back((int)nbv.size());
-                if (t.case_type == 3) for (int x : t.nb_c) ncv.push_back(X(x));
-                nco.push_back((int)ncv.size());
-                ba.push_back(t.bas_a); bb.push_back(t.bas_b); aa.push_back(t.aci_a); abv.push_back(t.aci_b);
-                QH.push_back(qs(t.q_h, 15.0, 1.0)); QA.push_back(qs(-t.q_a, 15.0, 1.0)); QB.push_back(qs(-t.q_b, 15.0, 1.0));
-                rv.push_back(M.rvdw[t.a] + M.rvdw[t.b]);
-                const int zb = M.Z[t.b];
-                zlp.push_back((zb >= 1 && zb <= 86) ? gfnff_tables::repz[zb - 1] : 1.0);
-                nfl.push_back((zb == 7 && t.nb_b.size() == 1) ? 1 : 0);
-            }
+            hbt.add(M, X);
             for (auto& t : M.xbonds) {
                 xa.push_back(X(t.a)); xx.push_back(X(t.x)); xb.push_back(X(t.b));
                 xpre.push_back(-qs(-t.q_b, 15.0, 0.03) * t.aci_x * qs(t.q_x, 15.0, 0.03));
@@ -869,13 +899,8 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
         P.b_i.upload(bi); P.b_j.upload(bj); P.b_h.upload(bh); P.b_off.upload(off); P.b_hb.upload(hb);
         P.b_fc.upload(fc); P.b_al.upload(al); P.b_r0i.upload(r0i); P.b_r0j.upload(r0j);
         P.b_cki.upload(cki); P.b_ckj.upload(ckj); P.b_sh.upload(sh); P.b_ff.upload(ff);
-        P.nhb = (int)a.size();
+        P.upload_hb(hbt);
         P.nhb_near = P.nhb;   // batches: every HB term in FP64
-        P.h_a.upload(a); P.h_h.upload(h); P.h_b.upload(b); P.h_c.upload(c); P.h_pc.upload(pc);
-        P.h_nbo.upload(nbo); P.h_nb.upload(nbv); P.h_nco.upload(nco); P.h_nc.upload(ncv);
-        P.h_ba.upload(ba); P.h_bb.upload(bb); P.h_aa.upload(aa); P.h_ab.upload(abv);
-        P.h_QH.upload(QH); P.h_QA.upload(QA); P.h_QB.upload(QB); P.h_rv.upload(rv); P.h_zlp.upload(zlp);
-        P.h_nfl.upload(nfl);
         P.nxb = (int)xa.size();
         P.x_a.upload(xa); P.x_x.upload(xx); P.x_b.upload(xb); P.x_pre.upload(xpre); P.x_rv.upload(xrv);
     }
@@ -1332,8 +1357,8 @@ void Engine::launch_body()
     cudaStream_t s2 = fork ? P.side : s;
     auto hb_rep_terms = [&]() {
     if (P.nhb) {
-        HBSoA H{P.nhb, P.h_a.p, P.h_h.p, P.h_b.p, P.h_c.p, P.h_pc.p, P.h_nbo.p, P.h_nb.p, P.h_nco.p, P.h_nc.p,
-                P.h_ba.p, P.h_bb.p, P.h_aa.p, P.h_ab.p, P.h_QH.p, P.h_QA.p, P.h_QB.p, P.h_rv.p, P.h_zlp.p, P.h_nfl.p};
+        HBSoA H{P.nhb, P.h_rec.p, P.h_qh.p, P.h_qa.p, P.h_bas.p, P.h_aci.p, P.h_rvdw.p, P.h_zlp.p,
+                P.h_pc.p, P.h_nfl.p, P.h_adjo.p, P.h_adj.p};
         const int split = mixed ? P.nhb_near : P.nhb;
         if (split > 0) k_hbonds<double><<<nblk(split), kBlock, 0, s2>>>(V, H, 0, split);
         if (P.nhb > split) k_hbonds<float><<<nblk(P.nhb - split), kBlock, 0, s2>>>(V, H, split, P.nhb);

@@ -334,9 +334,10 @@ __global__ void k_batm(View V, TripSoA A)
 
 struct HBSoA {
     int n;
-    const int *a, *h, *b, *cas, *pc, *nbb_off, *nbb, *nbc_off, *nbc;
-    const double *bas_a, *bas_b, *aci_a, *aci_b, *QH, *QA, *QB, *rv, *zlp;
-    const int* nflag;   // acceptor is N with a single neighbour: neighbour cutoff 2.0
+    const int4* rec;                                     // per term {A, H, B, case}
+    const double *qh, *qa, *bas, *aci, *rvdw, *zlp;      // per atom
+    const int *pc, *nflag, *adj_off, *adj;               // per atom: carbonyl parent, N with one
+                                                         // neighbour (cutoff 2.0), bond graph CSR
 };
 
 // Arithmetic of the HB kernel.  FP64 keeps IEEE operations but divides by reciprocals
@@ -375,22 +376,24 @@ __global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 5 : GFNFF_HB_MINBLOCK
 {
     const int t = t0 + blockIdx.x * blockDim.x + threadIdx.x;
     R etot = R(0.0);
+    const int4 rec = t < t1 ? S.rec[t] : make_int4(-1, 0, 0, 0);
     if (t < t1) {
         using P3 = V3<R>;
-        const double4 org = V.pos[S.h[t]];   // H as the local origin
+        const double4 org = V.pos[rec.y];   // H as the local origin
         const R HB_BACUT = R(49.0), HB_SCUT = R(22.0), HB_ALP = R(6.0), HB_NBCUT = R(11.20);
         const R TORS_HB = R(0.94), BEND_HB = R(0.20), HBLPCUT = R(56.0);
-        const int A = S.a[t], H = S.h[t], Bq = S.b[t], cs = S.cas[t];
+        const int A = rec.x, H = rec.y, Bq = rec.z, cs = rec.w;
         P3 pA = ldr<R>(V.pos, A, org), pH = ldr<R>(V.pos, H, org), pB = ldr<R>(V.pos, Bq, org);
         R irAH, irHB, irAB;
         const R rAH = hb_len(pH - pA, irAH), rHB = hb_len(pB - pH, irHB), rAB = hb_len(pB - pA, irAB);
         if (rAB <= R(50.0)) {
             const R rAH4 = rAH * rAH * rAH * rAH, rHB4 = rHB * rHB * rHB * rHB;
             const R den = hb_rcp(rAH4 + rHB4);
-            const R QH = S.QH[t], QA = S.QA[t], QB = S.QB[t];
-            const R bas = (QA * S.bas_a[t] * rAH4 + QB * S.bas_b[t] * rHB4) * den;
-            const R aci = (S.aci_b[t] * rAH4 + S.aci_a[t] * rHB4) * den;
-            const R rv = S.rv[t];
+            const R QH = S.qh[H], QA = S.qa[A], QB = S.qa[Bq];
+            const double bas_a = S.bas[A], bas_b = S.bas[Bq], aci_a = S.aci[A], aci_b = S.aci[Bq];
+            const R bas = (QA * R(bas_a) * rAH4 + QB * R(bas_b) * rHB4) * den;
+            const R aci = (R(aci_b) * rAH4 + R(aci_a) * rHB4) * den;
+            const R rv = R(S.rvdw[A] + S.rvdw[Bq]);
             const R irv = hb_rcp(rv);
             const R rab2 = rAB * rAB, irab2 = irAB * irAB;
             // HB_ALP = 6: integer powers
@@ -405,12 +408,12 @@ __global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 5 : GFNFF_HB_MINBLOCK
                 const R ex = bacut * ((rAH + rHB) * irAB - R(1.0));
                 doutl = ex > R(15.0) ? R(0.0) : R(2.0) * hb_rcp(R(1.0) + hb_exp(ex));
             }
-            const int nb0 = S.nbb_off[t], nb1 = S.nbb_off[t + 1];
-            const R nbc = (S.nflag[t] ? R(2.0) : HB_NBCUT) * irv;
+            const int nb0 = S.adj_off[Bq], nb1 = S.adj_off[Bq + 1];
+            const R nbc = (S.nflag[Bq] ? R(2.0) : HB_NBCUT) * irv;
             R onb = R(1.0);
             if (cs >= 2)
                 for (int p = nb0; p < nb1; ++p) {
-                    P3 pn = ldr<R>(V.pos, S.nbb[p], org);
+                    P3 pn = ldr<R>(V.pos, S.adj[p], org);
                     R ia, ib;
                     const R ra = hb_len(pn - pA, ia), rb = hb_len(pn - pB, ib);
                     const R ex = nbc * ((ra + rb) * irAB - R(1.0));
@@ -422,9 +425,9 @@ __global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 5 : GFNFF_HB_MINBLOCK
             int nlp = 0;
             P3 lpv = P3{0, 0, 0}, lpp = pB;
             if (cs == 4) {
-                lpd = R(0.50) - R(0.018) * S.zlp[t];
+                lpd = R(0.50) - R(0.018) * S.zlp[Bq];
                 nlp = nb1 - nb0;
-                for (int p = nb0; p < nb1; ++p) lpv = lpv + (ldr<R>(V.pos, S.nbb[p], org) - pB);
+                for (int p = nb0; p < nb1; ++p) lpv = lpv + (ldr<R>(V.pos, S.adj[p], org) - pB);
                 const R vn = nrm(lpv);
                 if (vn > R(1e-10) && nlp > 0) {
                     lpp = pB + (-lpd) * (hb_rcp(vn) * lpv);
@@ -439,7 +442,7 @@ __global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 5 : GFNFF_HB_MINBLOCK
             const R qhoutl = QH * doutl * onb * olp;
             R eangl = R(1.0), etors = R(1.0);
             P3 ga3[3] = {P3{0, 0, 0}, P3{0, 0, 0}, P3{0, 0, 0}};
-            const int Ci = S.pc[t];
+            const int Ci = cs == 3 ? S.pc[Bq] : -1;
             const bool c3 = (cs == 3 && Ci != -1);
             if (c3) {
                 const R c0 = R(120.0) * R(kPi) / R(180.0);
@@ -460,8 +463,8 @@ __global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 5 : GFNFF_HB_MINBLOCK
                 ga3[0] = deda + dedc;
                 ga3[1] = -R(1.0) * deda;
                 ga3[2] = -R(1.0) * dedc;
-                for (int p = S.nbc_off[t]; p < S.nbc_off[t + 1]; ++p) {
-                    const int D = S.nbc[p];
+                for (int p = S.adj_off[Ci]; p < S.adj_off[Ci + 1]; ++p) {
+                    const int D = S.adj[p];
                     if (D == Bq) continue;
                     P3 g[4];
                     const R phi = dihedral(ldr<R>(V.pos, D, org), pB, va, pH, g);
@@ -473,7 +476,7 @@ __global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 5 : GFNFF_HB_MINBLOCK
             R gs = R(1.0);
             if (cs == 2 || cs == 4) gs = R(0.268);
             else if (cs == 3) gs = R(0.350);
-            const R cst = S.aci_a[t] * S.bas_b[t] * QA * QB * gs;
+            const R cst = R(aci_a) * R(bas_b) * QA * QB * gs;
             const R E = cs >= 2 ? -rdamp * qhoutl * cst * eangl * etors : -bas * aci * rdamp * qhoutl;
             etot = E;
 
@@ -512,7 +515,7 @@ __global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 5 : GFNFF_HB_MINBLOCK
                     gb = gb + dgbo;
                     gh = gh - dgao - dgbo;
                     for (int p = nb0; p < nb1; ++p) {
-                        const int nb = S.nbb[p];
+                        const int nb = S.adj[p];
                         P3 pn = ldr<R>(V.pos, nb, org);
                         P3 dranb = pA - pn, drbnb = pB - pn;
                         R ia, ib;
@@ -563,7 +566,7 @@ __global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 5 : GFNFF_HB_MINBLOCK
                             P3 gnb = P3{out[0], out[1], out[2]};
                             gb = gb + gnb;
                             P3 share = (R(1.0) / (R)nlp) * gnb;
-                            for (int p = nb0; p < nb1; ++p) agrad(V.grad, S.nbb[p], -R(1.0) * share);
+                            for (int p = nb0; p < nb1; ++p) agrad(V.grad, S.adj[p], -R(1.0) * share);
                         }
                     }
                     if (c3) {
@@ -573,8 +576,8 @@ __global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 5 : GFNFF_HB_MINBLOCK
                         agrad(V.grad, Ci, bterm * ga3[1]);
                         agrad(V.grad, H, bterm * ga3[2]);
                         P3 va = ldr<R>(V.pos, Ci, org);
-                        for (int p = S.nbc_off[t]; p < S.nbc_off[t + 1]; ++p) {
-                            const int D = S.nbc[p];
+                        for (int p = S.adj_off[Ci]; p < S.adj_off[Ci + 1]; ++p) {
+                            const int D = S.adj[p];
                             if (D == Bq) continue;
                             P3 g[4];
                             const R phi = dihedral(ldr<R>(V.pos, D, org), pB, va, pH, g);
@@ -591,7 +594,7 @@ __global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 5 : GFNFF_HB_MINBLOCK
                         }
                     }
                 } else {
-                    const R caa = QA * S.bas_a[t], cbb = QB * S.bas_b[t];
+                    const R caa = QA * R(bas_a), cbb = QB * R(bas_b);
                     const R rterm = -aci * rdamp * qhoutl, dterm = -aci * bas * qhoutl;
                     const R sterm = -rdamp * bas * qhoutl, aterm = -aci * bas * rdamp * QH;
                     const R tmp = den * den * R(4.0);
@@ -601,10 +604,10 @@ __global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 5 : GFNFF_HB_MINBLOCK
                     gi = (cbb - caa) * dd24b * rterm;
                     gb = gi * drbh;
                     gh = -R(1.0) * ga - gb;
-                    gi = (S.aci_b[t] - S.aci_a[t]) * dd24a;
+                    gi = R(aci_b - aci_a) * dd24a;
                     P3 dga = (gi * sterm) * drah;
                     ga = ga + dga;
-                    gi = (S.aci_a[t] - S.aci_b[t]) * dd24b;
+                    gi = R(aci_a - aci_b) * dd24b;
                     P3 dgb = (gi * sterm) * drbh;
                     gb = gb + dgb;
                     gh = gh - dga - dgb;
@@ -628,7 +631,7 @@ __global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 5 : GFNFF_HB_MINBLOCK
             }
         }
     }
-    eadd(V, (double)etot, t < t1 ? V.mol[S.a[t]] : -1, T_HB);
+    eadd(V, (double)etot, t < t1 ? V.mol[rec.x] : -1, T_HB);
 }
 
 
