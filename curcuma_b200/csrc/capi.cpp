@@ -192,6 +192,9 @@ gfnff_status gfnff_energy_and_gradient_batch(gfnff_handle* h, const double* xyz,
             throw std::runtime_error("H2D copy failed");
         h->eng->enqueue(h->eng->d_xyz_scratch(), false);
         h->eng->fetch_batch(h->pin_terms.data(), h->pin_grad, st.data());
+        // the CN neighbour list no longer covers this geometry: rebuild it around it (this
+        // evaluation used the all-pairs CN kernels)
+        if (h->eng->cn_list_stale()) h->eng->refresh_cn_list();
     } catch (const std::exception& e) {
         return fail(h, GFNFF_CUDA_ERROR, e.what());
     }
@@ -248,6 +251,9 @@ gfnff_status gfnff_energy_and_gradient(gfnff_handle* h, const double* xyz, doubl
             h->eng->enqueue(h->eng->d_xyz_scratch(), false);
             h->eng->fetch(h->pin_out, h->pin_grad, h->pin_status, nullptr);
         }
+        // the CN neighbour list no longer covers this geometry: rebuild it around it (this
+        // evaluation used the all-pairs CN kernels)
+        if (h->eng->cn_list_stale()) h->eng->refresh_cn_list();
     } catch (const std::exception& e) {
         return fail(h, GFNFF_CUDA_ERROR, e.what());
     }
@@ -407,6 +413,7 @@ gfnff_status gfnff_md_nve(gfnff_handle* h, int nsteps, double dt_fs, double* xyz
                 ekin[done + t] = ek[t];
             }
             done += chunk;
+            if (worst == 0 && h->eng->cn_list_stale(true)) h->eng->refresh_cn_list();
             if (h->nmol == 0 && h->opt.hbond && worst == 0) {
                 double msd = 0.0;
                 h->eng->fetch(nullptr, nullptr, nullptr, &msd);

@@ -233,6 +233,60 @@ struct Engine::Impl {
     // directions by rows (GFNFF_PAIRS=rows)
     DBuf<int2> symtiles;
     DBuf<double4> boxlo, boxhi;   // per run of kBoxAtoms atoms
+    // CN neighbour list (k_cn_nl, k_cn_chain_nl): pairs within 6 + kCnSkin bohr of the
+    // reference geometry cnl_ref, CSR by atom; cnl_bad = 1 once an atom moved more than
+    // kCnSkin / 2 from it (GFNFF_CN_LIST=0: all-pairs kernels only)
+    static constexpr double kCnSkin = 1.0;
+    bool cnl_on = false;
+    int* cnl_bad_host = nullptr;   // pinned; refreshed by fetch()
+    DBuf<int> cnl_off, cnl_j, cnl_bad;
+    DBuf<double4> cnl_ref;
+    void build_cn_list(const std::vector<double4>& p, const std::vector<int2>& jr)
+    {
+        const int nn = (int)p.size();
+        const double rc = 6.0 + kCnSkin, rc2 = rc * rc;
+        std::vector<std::vector<int>> rows(nn);
+        for (int a0 = 0; a0 < nn;) {   // per molecule (contiguous atom range)
+            const int a1 = jr[a0].y;
+            double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+            for (int i = a0; i < a1; ++i) {
+                const double c[3] = {p[i].x, p[i].y, p[i].z};
+                for (int d = 0; d < 3; ++d) { lo[d] = std::min(lo[d], c[d]); hi[d] = std::max(hi[d], c[d]); }
+            }
+            int dim[3];
+            for (int d = 0; d < 3; ++d) dim[d] = std::max(1, std::min(256, (int)((hi[d] - lo[d]) / rc) + 1));
+            auto cell = [&](const double4& q, int d) {
+                const double c = d == 0 ? q.x : (d == 1 ? q.y : q.z);
+                return std::min(dim[d] - 1, std::max(0, (int)((c - lo[d]) / rc)));
+            };
+            std::vector<std::vector<int>> grid((size_t)dim[0] * dim[1] * dim[2]);
+            for (int i = a0; i < a1; ++i)
+                grid[((size_t)cell(p[i], 2) * dim[1] + cell(p[i], 1)) * dim[0] + cell(p[i], 0)].push_back(i);
+            for (int i = a0; i < a1; ++i) {
+                const int cx = cell(p[i], 0), cy = cell(p[i], 1), cz = cell(p[i], 2);
+                for (int z = std::max(0, cz - 1); z <= std::min(dim[2] - 1, cz + 1); ++z)
+                    for (int y = std::max(0, cy - 1); y <= std::min(dim[1] - 1, cy + 1); ++y)
+                        for (int x = std::max(0, cx - 1); x <= std::min(dim[0] - 1, cx + 1); ++x)
+                            for (int j : grid[((size_t)z * dim[1] + y) * dim[0] + x]) {
+                                if (j == i) continue;
+                                const double dx = p[i].x - p[j].x, dy = p[i].y - p[j].y, dz = p[i].z - p[j].z;
+                                if (dx * dx + dy * dy + dz * dz < rc2) rows[i].push_back(j);
+                            }
+                std::sort(rows[i].begin(), rows[i].end());
+            }
+            a0 = a1;
+        }
+        std::vector<int> off{0}, js;
+        for (auto& r : rows) {
+            js.insert(js.end(), r.begin(), r.end());
+            off.push_back((int)js.size());
+        }
+        cnl_off.upload(off);
+        cnl_j.upload(js);
+        cnl_ref.upload(p);
+        const int zero = 0;
+        cnl_bad.upload(std::vector<int>{zero});
+    }
     bool box_cull = false;        // CN kernels skip far tiles (single molecules >= 8192 atoms)
     int nsym = 0;
     bool pairs_sym = true;
@@ -495,6 +549,7 @@ Engine::~Engine()
     for (auto& e : p_->ev)
         if (e) cudaEventDestroy(e);
     if (p_->sol) cusolverDnDestroy(p_->sol);
+    if (p_->cnl_bad_host) cudaFreeHost(p_->cnl_bad_host);
     for (cudaEvent_t e : {p_->ev_fork0, p_->ev_fork1, p_->ev_join})
         if (e) cudaEventDestroy(e);
     if (p_->side) cudaStreamDestroy(p_->side);
@@ -660,6 +715,15 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
         }
     }
     P.pos0.upload(p0); P.hbref.upload(p0); P.pos.alloc(n);
+    {
+        const char* ecl = std::getenv("GFNFF_CN_LIST");
+        P.cnl_on = !(ecl && !std::strcmp(ecl, "0"));
+        if (P.cnl_on) {
+            if (!P.cnl_bad_host) CK(cudaMallocHost(&P.cnl_bad_host, sizeof(int)));
+            *P.cnl_bad_host = 0;
+            P.build_cn_list(p0, hjr);
+        }
+    }
     P.rcov_cn.upload(rcn); P.rcov43.upload(r43); P.rcov_d3.upload(rd3);
     P.chi_base.upload(chi); P.cnf.upload(cnf); P.gam.upload(gam); P.alpeeq.upload(alp); P.adiag.upload(adg);
     P.qa.upload(qa); P.slot.upload(slot); P.nref.upload(nref); P.refcn.upload(rcn7); P.w0.upload(w07);
@@ -1330,7 +1394,8 @@ void Engine::launch_positions(const double* d_xyz, bool bohr)
     P.mark(0);
     CK(cudaMemsetAsync(P.msd.p, 0, sizeof(double), P.stream));
     k_positions<<<nblk(P.n), kBlock, 0, P.stream>>>(P.n, P.perm.p, d_xyz, bohr ? 1.0 : kAngToBohr, P.pos.p,
-                                                   P.hbref.p, P.msd.p);
+                                                   P.hbref.p, P.msd.p, P.cnl_on ? P.cnl_ref.p : nullptr,
+                                                   0.25 * Impl::kCnSkin * Impl::kCnSkin, P.cnl_bad.p);
 }
 
 // everything after the positions, reading and writing engine buffers only, so that it
@@ -1402,7 +1467,13 @@ void Engine::launch_body()
     };
     P.mark(1);
     if (P.box_cull) k_boxes<<<nblk(n, kTile), kTile, 0, s>>>(n, P.pos.p, P.boxlo.p, P.boxhi.p);
-    (mixed ? k_cn<float> : k_cn<double>)<<<tgrid, kTile, 0, s>>>(V, P.nsplit);
+    if (P.cnl_on) {
+        (mixed ? k_cn_nl<float> : k_cn_nl<double>)<<<nblk((long)n * 32), kBlock, 0, s>>>(V, P.cnl_off.p, P.cnl_j.p,
+                                                                                         P.cnl_bad.p);
+        (mixed ? k_cn<float> : k_cn<double>)<<<tgrid, kTile, 0, s>>>(V, P.nsplit, P.cnl_bad.p);
+    } else {
+        (mixed ? k_cn<float> : k_cn<double>)<<<tgrid, kTile, 0, s>>>(V, P.nsplit, nullptr);
+    }
     P.mark(2);
     k_d4_weights<<<nblk(n), kBlock, 0, s>>>(V);
     if (early) {
@@ -1490,7 +1561,12 @@ void Engine::launch_body()
     if (fork) CK(cudaStreamWaitEvent(s, P.ev_join, 0));
     P.mark(10);
     k_post<<<nblk(n), kBlock, 0, s>>>(V);
-    k_cn_chain<double><<<tgrid, kTile, 0, s>>>(V, P.nsplit);
+    if (P.cnl_on) {
+        k_cn_chain_nl<<<nblk((long)n * 32), kBlock, 0, s>>>(V, P.cnl_off.p, P.cnl_j.p, P.cnl_bad.p);
+        k_cn_chain<double><<<tgrid, kTile, 0, s>>>(V, P.nsplit, P.cnl_bad.p);
+    } else {
+        k_cn_chain<double><<<tgrid, kTile, 0, s>>>(V, P.nsplit, nullptr);
+    }
     P.mark(11);
     k_outputs<<<nblk(n), kBlock, 0, s>>>(V, P.gout.p, P.qout.p, P.cnout.p, P.bad.p);
     k_finish<<<nblk(P.nmol), kBlock, 0, s>>>(V, (P.nred > 0 || P.nmol > 1) ? P.info.p : nullptr, P.bad.p, P.e0.p,
@@ -1516,6 +1592,7 @@ void Engine::fetch(double* terms, double* grad, int* status, double* hb_msd)
     if (grad) CK(cudaMemcpyAsync(grad, P.gout.p, 3 * (size_t)P.n * sizeof(double), cudaMemcpyDeviceToHost, P.stream));
     if (status) CK(cudaMemcpyAsync(status, P.status.p, sizeof(int), cudaMemcpyDeviceToHost, P.stream));
     if (hb_msd) CK(cudaMemcpyAsync(hb_msd, P.msd.p, sizeof(double), cudaMemcpyDeviceToHost, P.stream));
+    if (P.cnl_on) CK(cudaMemcpyAsync(P.cnl_bad_host, P.cnl_bad.p, sizeof(int), cudaMemcpyDeviceToHost, P.stream));
     CK(cudaStreamSynchronize(P.stream));
 }
 
@@ -1525,6 +1602,7 @@ void Engine::fetch_batch(double* terms16, double* grad, int* status)
     if (terms16) CK(cudaMemcpyAsync(terms16, P.E.p, 16 * (size_t)P.nmol * sizeof(double), cudaMemcpyDeviceToHost, P.stream));
     if (grad) CK(cudaMemcpyAsync(grad, P.gout.p, 3 * (size_t)P.n * sizeof(double), cudaMemcpyDeviceToHost, P.stream));
     if (status) CK(cudaMemcpyAsync(status, P.status.p, (size_t)P.nmol * sizeof(int), cudaMemcpyDeviceToHost, P.stream));
+    if (P.cnl_on) CK(cudaMemcpyAsync(P.cnl_bad_host, P.cnl_bad.p, sizeof(int), cudaMemcpyDeviceToHost, P.stream));
     CK(cudaStreamSynchronize(P.stream));
 }
 
@@ -1556,6 +1634,30 @@ std::vector<int> Engine::device_dispersion_pairs()
     v.reserve(2 * c);
     for (auto& p : h) { v.push_back(p.x); v.push_back(p.y); }
     return v;
+}
+
+bool Engine::cn_list_stale(bool read_now)
+{
+    Impl& P = *p_;
+    if (!P.cnl_on) return false;
+    if (read_now) {
+        CK(cudaStreamSynchronize(P.stream));
+        CK(cudaMemcpy(P.cnl_bad_host, P.cnl_bad.p, sizeof(int), cudaMemcpyDeviceToHost));
+    }
+    return *P.cnl_bad_host != 0;
+}
+
+void Engine::refresh_cn_list()
+{
+    Impl& P = *p_;
+    if (!P.cnl_on) return;
+    CK(cudaStreamSynchronize(P.stream));
+    std::vector<double4> p(P.n);
+    CK(cudaMemcpy(p.data(), P.pos.p, (size_t)P.n * sizeof(double4), cudaMemcpyDeviceToHost));
+    std::vector<int2> jr(P.n);
+    CK(cudaMemcpy(jr.data(), P.jr.p, (size_t)P.n * sizeof(int2), cudaMemcpyDeviceToHost));
+    P.drop_graphs();   // the list buffers are reallocated
+    P.build_cn_list(p, jr);
 }
 
 void Engine::set_hb_reference(const double* xyz_bohr)

@@ -59,6 +59,12 @@ public:
     std::vector<int> device_dispersion_pairs();
     // sets the HB reference geometry (bohr, host, caller order) for the refresh test
     void set_hb_reference(const double* xyz_bohr);
+    // the CN neighbour list no longer covers the geometry of the last evaluation (its
+    // evaluations fell back to the all-pairs CN kernels); refresh_cn_list rebuilds it
+    // around that geometry
+    // (read_now: read the device flag; otherwise the value fetched with the last results)
+    bool cn_list_stale(bool read_now = false);
+    void refresh_cn_list();
     // switches the EEQ solve to pivoted LU (after a NOT_SPD status); false if already
     bool switch_to_lu();
     // switches an iterative EEQ solve to the direct one (after REFINE_NOT_CONVERGED)

@@ -30,8 +30,11 @@ __device__ __forceinline__ void tile_range(const View& V, int i0, int nsplit, in
 // geometry in (caller order -> internal order) and the HB refresh metric
 // (gfnff_method.cpp:2228-2259)
 // ------------------------------------------------------------------------------------
+// (nl_ref, nl_bad): reference geometry of the CN neighbour list; an atom more than
+// sqrt(nl_lim2) away from it marks the list stale (kept until the host rebuilds it)
 __global__ void k_positions(int n, const int* __restrict__ perm, const double* __restrict__ xyz, double scale,
-                            double4* pos, const double4* __restrict__ ref, double* msd)
+                            double4* pos, const double4* __restrict__ ref, double* msd,
+                            const double4* __restrict__ nl_ref, double nl_lim2, int* nl_bad)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double s = 0.0;
@@ -41,6 +44,11 @@ __global__ void k_positions(int n, const int* __restrict__ perm, const double* _
         pos[i] = make_double4(x, y, z, 0.0);
         const double4 r = ref[i];
         s = (x - r.x) * (x - r.x) + (y - r.y) * (y - r.y) + (z - r.z) * (z - r.z);
+        if (nl_ref) {
+            const double4 q = nl_ref[i];
+            const double d2 = (x - q.x) * (x - q.x) + (y - q.y) * (y - q.y) + (z - q.z) * (z - q.z);
+            if (d2 > nl_lim2) atomicOr(nl_bad, 1);
+        }
     }
     block_add(s, msd);
 }
@@ -106,8 +114,9 @@ __device__ __forceinline__ bool ranges_far(const View& V, int i0, int ni, int j0
 // (cn_calculator.cpp:367-428); the log-squash is applied in k_d4_weights
 // ------------------------------------------------------------------------------------
 template <class R>
-__global__ void __launch_bounds__(kTile) k_cn(View V, int nsplit)
+__global__ void __launch_bounds__(kTile) k_cn(View V, int nsplit, const int* nl_bad)
 {
+    if (nl_bad && *nl_bad == 0) return;   // the neighbour-list kernel does the work
     __shared__ double sx[kTile], sy[kTile], sz[kTile], sr[kTile];
     const int i0 = blockIdx.x * kTile, i = i0 + threadIdx.x;
     int jb, je;
@@ -641,8 +650,9 @@ __global__ void k_post(View V)
 // CN chain rule: grad_i += sum_j dS_ij/dr (u_i + u_j) (x_i - x_j)/r over the 6 bohr
 // neighbours (gfnff_method.cpp:5837-6260, forcefieldthread.h:80-109)
 template <class R>
-__global__ void __launch_bounds__(kTile) k_cn_chain(View V, int nsplit)
+__global__ void __launch_bounds__(kTile) k_cn_chain(View V, int nsplit, const int* nl_bad)
 {
+    if (nl_bad && *nl_bad == 0) return;   // the neighbour-list kernel does the work
     __shared__ double sx[kTile], sy[kTile], sz[kTile], sr[kTile], su[kTile];
     const int i0 = blockIdx.x * kTile, i = i0 + threadIdx.x;
     int jb, je;
@@ -737,6 +747,75 @@ __global__ void k_disp_count(int n, const double4* pos0, const int2* jr, unsigne
     if (d2_exact(pos0[i], pos0[j]) <= 3600.0) {
         const unsigned long long s = atomicAdd(cnt, 1ull);
         if (out && s < cap) out[s] = make_int2(i, j);
+    }
+}
+
+
+// ------------------------------------------------------------------------------------
+// CN and CN chain rule over a Verlet neighbour list (pairs within 6 + 1 bohr at the list's
+// reference geometry, same molecule; CSR by atom, both directions): a warp per atom, lanes
+// over its partners.  Valid while no atom moved more than half the 1-bohr skin (checked in
+// k_positions every evaluation); a stale list hands the work back to the all-pairs kernels
+// above in the same launch sequence, and the host rebuilds it.  Same arithmetic per pair as
+// k_cn / k_cn_chain; only the summation order of an atom's partners differs.
+// ------------------------------------------------------------------------------------
+template <class R>
+__global__ void __launch_bounds__(kBlock) k_cn_nl(View V, const int* __restrict__ off, const int* __restrict__ nbr,
+                                                 const int* nl_bad)
+{
+    if (*nl_bad) return;
+    const int i = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (i >= V.n) return;
+    const double4 pi = V.pos[i];
+    const double ri = V.rcov_cn[i];
+    const double kn = -7.5;
+    double s = 0.0;
+    for (int p = off[i] + lane; p < off[i + 1]; p += 32) {
+        const int j = nbr[p];
+        const double4 pj = V.pos[j];
+        const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+        const double d2 = dx * dx + dy * dy + dz * dz;
+        if (!(d2 < 36.0)) continue;
+        const R r = sqrt((R)d2);
+        const R rc = (R)(ri + V.rcov_cn[j]);
+        s += (double)(R(0.5) * (R(1) + erf(R(kn) * ((r - rc) / rc))));
+    }
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0 && s != 0.0) atomicAdd(V.cnraw + i, s);
+}
+
+__global__ void __launch_bounds__(kBlock) k_cn_chain_nl(View V, const int* __restrict__ off,
+                                                       const int* __restrict__ nbr, const int* nl_bad)
+{
+    if (*nl_bad) return;
+    const int i = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (i >= V.n) return;
+    const double4 pi = V.pos[i];
+    const double ri = V.rcov_cn[i], ui = V.v[i];
+    const double kn = -7.5, sqrtpi = 1.77245385091;
+    double gx = 0.0, gy = 0.0, gz = 0.0;
+    for (int p = off[i] + lane; p < off[i + 1]; p += 32) {
+        const int j = nbr[p];
+        const double4 pj = V.pos[j];
+        const double dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
+        const double d2 = dx * dx + dy * dy + dz * dz;
+        if (!(d2 < 36.0)) continue;
+        const double r = sqrt(d2);
+        const double rs = ri + V.rcov_cn[j];
+        const double dr = (r - rs) / rs;
+        const double de = (kn / sqrtpi) * exp(-kn * kn * dr * dr) / rs;
+        const double f = -(de / r) * (ui + V.v[j]);
+        gx += f * dx; gy += f * dy; gz += f * dz;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        gx += __shfl_down_sync(0xffffffffu, gx, o);
+        gy += __shfl_down_sync(0xffffffffu, gy, o);
+        gz += __shfl_down_sync(0xffffffffu, gz, o);
+    }
+    if (lane == 0) {
+        if (gx != 0.0) atomicAdd(V.grad + 3 * i, gx);
+        if (gy != 0.0) atomicAdd(V.grad + 3 * i + 1, gy);
+        if (gz != 0.0) atomicAdd(V.grad + 3 * i + 2, gz);
     }
 }
 

@@ -212,3 +212,24 @@ def test_pcg_warm_start(system, monkeypatch):
                 assert np.abs(g.getGradient() - G).max() < G_TOL
                 assert np.abs(g.getCharges() - q).max() < 1e-9
     assert sum(iters["1"][1:]) < sum(iters["0"][1:]), iters
+
+
+def test_cn_neighbour_list_refresh():
+    """CN and its chain rule run over a neighbour list with a 1-bohr skin.  Geometries that
+    move atoms more than half the skin make the list stale: that evaluation falls back to the
+    all-pairs kernels and the host rebuilds the list around it.  Every geometry of the
+    sequence matches the oracle either way."""
+    Z, X = workloads.water_cluster(64, 9)
+    rng = np.random.default_rng(3)
+    geoms = [X + rng.normal(scale=s, size=X.shape) for s in (0.02, 0.15, 0.15, 0.02)]
+    o = Oracle(Z, X)
+    g = GFNFF()
+    assert g.setMolecule(Z, X)
+    for Xk in geoms:
+        g.updateGeometry(Xk)
+        e = g.calculateEnergy(True)
+        assert not g.hasError(), g.getErrorMessage()
+        T, G, q, cn = o.engrad(Xk)
+        assert abs(e - T["total"]) < E_TOL
+        assert np.abs(g.getGradient() - G).max() < G_TOL
+        assert np.abs(g.getCoordinationNumbers() - cn).max() < 1e-12
