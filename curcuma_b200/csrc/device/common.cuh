@@ -43,7 +43,11 @@ struct DBuf {
     void upload(const std::vector<T>& v)
     {
         alloc(v.size());
-        if (!v.empty()) CK(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+        if (v.empty()) return;
+        CK(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+        // a copy from pageable memory may return before its DMA has landed, and the engine's
+        // streams do not wait for the legacy stream: wait here
+        CK(cudaStreamSynchronize(cudaStreamLegacy));
     }
     void free()
     {

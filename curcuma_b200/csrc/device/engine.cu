@@ -1612,7 +1612,7 @@ std::vector<int> Engine::device_dispersion_pairs()
     if (P.n > 65535) throw std::runtime_error("device_dispersion_pairs: at most 65535 atoms");
     DBuf<unsigned long long> cnt;
     cnt.alloc(1);
-    CK(cudaMemset(cnt.p, 0, sizeof(unsigned long long)));
+    CK(cudaMemsetAsync(cnt.p, 0, sizeof(unsigned long long), P.stream));
     dim3 g(nblk(P.n), P.n);
     k_disp_count<<<g, kBlock, 0, P.stream>>>(P.n, P.pos0.p, P.jr.p, cnt.p, nullptr, 0);
     unsigned long long c = 0;
@@ -1620,7 +1620,7 @@ std::vector<int> Engine::device_dispersion_pairs()
     CK(cudaStreamSynchronize(P.stream));
     DBuf<int2> out;
     out.alloc(c);
-    CK(cudaMemset(cnt.p, 0, sizeof(unsigned long long)));
+    CK(cudaMemsetAsync(cnt.p, 0, sizeof(unsigned long long), P.stream));
     k_disp_count<<<g, kBlock, 0, P.stream>>>(P.n, P.pos0.p, P.jr.p, cnt.p, out.p, c);
     std::vector<int2> h(c);
     if (c) CK(cudaMemcpyAsync(h.data(), out.p, c * sizeof(int2), cudaMemcpyDeviceToHost, P.stream));

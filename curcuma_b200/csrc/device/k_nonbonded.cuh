@@ -243,10 +243,11 @@ __global__ void __launch_bounds__(kBlock) k_repulsion(View V, const int* off, co
             gy += __shfl_down_sync(0xffffffffu, gy, o);
             gz += __shfl_down_sync(0xffffffffu, gz, o);
         }
+        // atomics: the kernel runs beside others that add to the same gradient entries
         if (lane == 0) {
-            V.grad[3 * i] += gx;
-            V.grad[3 * i + 1] += gy;
-            V.grad[3 * i + 2] += gz;
+            if (gx != 0.0) atomicAdd(V.grad + 3 * i, gx);
+            if (gy != 0.0) atomicAdd(V.grad + 3 * i + 1, gy);
+            if (gz != 0.0) atomicAdd(V.grad + 3 * i + 2, gz);
         }
     }
     const int m = i < V.n ? V.mol[i] : -1;
@@ -405,8 +406,9 @@ constexpr int kST = 64;
 template <class R, int T>
 __device__ __forceinline__ void d4_pair_sym(double d2, const double* g0, const double* dgi, const double* dgj,
                                             const double (*sw0)[T], const double (*sw)[T], int jj, int nrj,
-                                            int nri, const double (&wi)[7], double r4r2_d, double zz_d, bool want_dc,
-                                            double& e, double& dedr, double& dci, double& dcj)
+                                            int nri, const double (&wi)[7], double r4r2_d, double sr4r2_d,
+                                            double zz_d, bool want_dc, double& e, double& dedr, double& dci,
+                                            double& dcj)
 {
     R c6 = R(0), dc6i = R(0), dc6j = R(0);
     for (int b = 0; b < nrj; ++b) c6 += (R)__ldg(g0 + b) * (R)sw0[b][jj];
@@ -418,12 +420,14 @@ __device__ __forceinline__ void d4_pair_sym(double d2, const double* g0, const d
     }
     const R q2 = (R)d2;
     const R r4r2 = (R)r4r2_d;
-    const R t = R(0.58) * sqrt(r4r2) + R(4.80);
+    const R t = R(0.58) * (R)sr4r2_d + R(4.80);   // sr4r2_d = sqrt(r4r2) from per-atom roots
     const R r0sq = t * t;
     const R zz = (R)zz_d;
     const R r6 = q2 * q2 * q2, r06 = r0sq * r0sq * r0sq;
-    const R t6 = R(1) / (r6 + r06);
-    const R t8 = R(1) / (r6 * q2 + r06 * r0sq);
+    // 1/a and 1/b from one division: a*b stays below 1e24 for r <= 50 bohr
+    const R a6 = r6 + r06, a8 = r6 * q2 + r06 * r0sq;
+    const R inv = R(1) / (a6 * a8);
+    const R t6 = a8 * inv, t8 = a6 * inv;
     const R sum = t6 + R(2) * r4r2 * t8;
     e = -(double)(c6 * sum * zz);
     const R d6 = R(-6) * q2 * q2 * t6 * t6, d8 = R(-8) * r6 * t8 * t8;
@@ -436,7 +440,7 @@ template <class R, int MINB, int T>
 __global__ void __launch_bounds__(T, MINB) k_pairs_sym(View V, const int2* __restrict__ tiles)
 {
     __shared__ double sx[T], sy[T], sz[T], s0x[T], s0y[T], s0z[T];
-    __shared__ double sq[T], sa[T], sze[T], ssz[T];
+    __shared__ double sq[T], sa[T], sze[T], ssz[T], srz[T];
     __shared__ double sw0[7][T], sw[7][T];
     __shared__ int ssl[T], snr[T];
     __shared__ double jacc[T / 32][5][T];
@@ -463,6 +467,7 @@ __global__ void __launch_bounds__(T, MINB) k_pairs_sym(View V, const int2* __res
             sx[u] = p.x; sy[u] = p.y; sz[u] = p.z;
             s0x[u] = p0.x; s0y[u] = p0.y; s0z[u] = p0.z;
             sq[u] = V.q[jl]; sa[u] = V.alpeeq[jl]; sze[u] = V.zeta[jl]; ssz[u] = V.szr[jl];
+            srz[u] = sqrt(ssz[u]);
             ssl[u] = V.slot[jl]; snr[u] = V.nref[jl];
 #pragma unroll
             for (int b = 0; b < 7; ++b) {
@@ -473,6 +478,7 @@ __global__ void __launch_bounds__(T, MINB) k_pairs_sym(View V, const int2* __res
     }
     __syncthreads();
     const double tsp = 2.0 / 1.772453850905516;
+    const double s3i = sqrt(3.0 * szi);   // sqrt(r4r2) of a pair = s3i * sqrt(szr_j)
     double ec = 0.0, ed = 0.0, gx = 0.0, gy = 0.0, gz = 0.0, dcn = 0.0, cfar = 0.0;
     const int cnt = min(T, V.n - j0);
     for (int jj = 0; jj < cnt; ++jj) {
@@ -511,15 +517,15 @@ __global__ void __launch_bounds__(T, MINB) k_pairs_sym(View V, const int2* __res
             if (d2 <= 2500.0 && d2_exact(p0i, make_double4(s0x[jj], s0y[jj], s0z[jj], 0.0)) <= 3600.0) {
                 const int sj = ssl[jj], nrj = snr[jj];
                 const double* dgj = V.hdg + ((size_t)j * V.K + si) * 7;
-                const double r4r2 = 3.0 * szi * ssz[jj], zz = zi * sze[jj];
+                const double r4r2 = 3.0 * szi * ssz[jj], sr4r2 = s3i * srz[jj], zz = zi * sze[jj];
                 double e, dedr, dci;
                 // mixed form: pairs closer than 15 bohr (the strong ones) stay FP64
                 if (sizeof(R) == sizeof(double) || d2 < 225.0)
-                    d4_pair_sym<double, T>(d2, g0i + sj * 7, dgi + sj * 7, dgj, sw0, sw, jj, nrj, nri, wi, r4r2, zz,
-                                        want_dc, e, dedr, dci, dcj);
+                    d4_pair_sym<double, T>(d2, g0i + sj * 7, dgi + sj * 7, dgj, sw0, sw, jj, nrj, nri, wi, r4r2,
+                                           sr4r2, zz, want_dc, e, dedr, dci, dcj);
                 else
-                    d4_pair_sym<R, T>(d2, g0i + sj * 7, dgi + sj * 7, dgj, sw0, sw, jj, nrj, nri, wi, r4r2, zz,
-                                   want_dc, e, dedr, dci, dcj);
+                    d4_pair_sym<R, T>(d2, g0i + sj * 7, dgi + sj * 7, dgj, sw0, sw, jj, nrj, nri, wi, r4r2, sr4r2,
+                                      zz, want_dc, e, dedr, dci, dcj);
                 ed += e;
                 f += dedr;
                 dcn += dci;

@@ -129,8 +129,8 @@ __device__ void grid_totals(const double* partial, int slot, double& sum, double
     __syncthreads();
     double a = 0.0, b = 0.0;
     for (int k = threadIdx.x; k < (int)gridDim.x; k += blockDim.x) {
-        a += __ldcg(partial + 4 * k + slot);
-        b = fmax(b, __ldcg(partial + 4 * k + slot + 1));
+        a += __ldcg(partial + 8 * k + slot);
+        b = fmax(b, __ldcg(partial + 8 * k + slot + 1));
     }
     for (int o = 16; o > 0; o >>= 1) {
         a += __shfl_xor_sync(0xffffffffu, a, o);
@@ -524,10 +524,12 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(PCGArgs A)
     __syncthreads();
     double rz_t = apply_precond(nrow, meta, Bp, rs, zs);
     for (int k = threadIdx.x; k < nrow; k += blockDim.x) __stcg(A.z + row0 + k, zs[k]);
-    block_sum_max(rz_t, bmax_t, A.partial + 4 * blockIdx.x);
+    // the start totals have a slot of their own: a fast block writes its first p.Mp
+    // partial into slot 0 before a slow one has read these after the barrier
+    block_sum_max(rz_t, bmax_t, A.partial + 8 * blockIdx.x + 4);
     ok = grid_sync(A.bar, gen) && ok;
     double rz = 0.0, bmax = 0.0;
-    if (ok) grid_totals(A.partial, 0, rz, bmax);
+    if (ok) grid_totals(A.partial, 4, rz, bmax);
     update_p(p, A.z, A.n, 0.0);
     int it = 0;
     bool conv = ok && bmax == 0.0;
@@ -535,7 +537,7 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(PCGArgs A)
         ++it;
         __syncthreads();
         const double pap_t = A.lower ? matvec_tiles(A, p, G) : matvec_rows(A, p, row0, row1, Ap);
-        block_sum_max(pap_t, 0.0, A.partial + 4 * blockIdx.x);
+        block_sum_max(pap_t, 0.0, A.partial + 8 * blockIdx.x);
         ok = grid_sync(A.bar, gen);
         if (!ok) break;
         if (A.lower) take_tiles_result(A, row0, nrow, Ap);
@@ -551,7 +553,7 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(PCGArgs A)
         __syncthreads();
         rz_t = apply_precond(nrow, meta, Bp, rs, zs);
         for (int k = threadIdx.x; k < nrow; k += blockDim.x) __stcg(A.z + row0 + k, zs[k]);
-        block_sum_max(rz_t, rmax_t, A.partial + 4 * blockIdx.x + 2);
+        block_sum_max(rz_t, rmax_t, A.partial + 8 * blockIdx.x + 2);
         ok = grid_sync(A.bar, gen);
         if (!ok) break;
         double rzn, rmax;
@@ -580,7 +582,7 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(PCGArgs A)
             __syncthreads();
             rz_t = apply_precond(nrow, meta, Bp, rs, zs);
             for (int k = threadIdx.x; k < nrow; k += blockDim.x) __stcg(A.z + row0 + k, zs[k]);
-            block_sum_max(rz_t, rmax_t, A.partial + 4 * blockIdx.x + 2);
+            block_sum_max(rz_t, rmax_t, A.partial + 8 * blockIdx.x + 2);
             ok = grid_sync(A.bar, gen);
             if (!ok) break;
             grid_totals(A.partial, 2, rzn, rmax);

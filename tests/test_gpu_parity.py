@@ -233,3 +233,25 @@ def test_cn_neighbour_list_refresh():
         assert abs(e - T["total"]) < E_TOL
         assert np.abs(g.getGradient() - G).max() < G_TOL
         assert np.abs(g.getCoordinationNumbers() - cn).max() < 1e-12
+
+
+@pytest.mark.parametrize("pcg_form", ["classic", "pipelined"])
+def test_side_stream_gradients_repeat(pcg_form, monkeypatch):
+    """The charge-independent terms run on a second stream beside the pair kernels, and both
+    add into the same gradient entries.  Every one of many evaluations at one geometry must
+    reproduce the oracle's gradient: an update lost between the streams shows up as a few
+    atoms off by 1e-5..1e-2 Eh/bohr in some evaluations.  The classic PCG fills every SM, so
+    the side kernels run after it, at the same time as the pair kernels."""
+    monkeypatch.setenv("GFNFF_EEQ_SOLVER", "pcg")
+    monkeypatch.setenv("GFNFF_PCG", pcg_form)
+    Z, X = workloads.water_cluster(200, 10)
+    T, G, _, _ = Oracle(Z, X).engrad(X)
+    g = GFNFF()
+    assert g.setMolecule(Z, X)
+    worst = 0.0
+    for _ in range(25):
+        e = g.calculateEnergy(True)
+        assert not g.hasError(), g.getErrorMessage()
+        assert abs(e - T["total"]) < E_TOL
+        worst = max(worst, np.abs(g.getGradient() - G).max())
+    assert worst < G_TOL, worst
