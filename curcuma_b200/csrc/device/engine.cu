@@ -27,6 +27,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <type_traits>
 #include <map>
 #include <numeric>
 #include <stdexcept>
@@ -226,6 +227,10 @@ struct Engine::Impl {
     // chain and join before the CN chain rule.  GFNFF_STREAMS=1 keeps one stream.
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork0 = nullptr, ev_fork1 = nullptr, ev_join = nullptr;
+    // D4 pairs, when split from the Coulomb pairs, on a stream of their own beside the side
+    // terms (GFNFF_D4_STREAM=0: before them on the side stream)
+    cudaStream_t side_d4 = nullptr;
+    cudaEvent_t ev_join_d4 = nullptr;
     bool side_early = false;   // GFNFF_SIDE_EARLY=1: fork at the start of the evaluation
     cusolverDnHandle_t sol = nullptr;
     int n = 0, nfrag = 0, K = 0, nred = 0, nmol = 0, nsplit = 1;
@@ -292,6 +297,9 @@ struct Engine::Impl {
     bool pairs_sym = true;
     bool pairs_occ = false;   // 10 blocks per SM (96 registers) instead of the unbounded 116
     int pair_tile = 64;       // tile edge of k_pairs_sym
+    // D4 pairs (charge-independent) on the side stream beside the EEQ solve, Coulomb pairs
+    // after it on the main stream (GFNFF_PAIRS_SPLIT=0: both in one pass after the solve)
+    int pairs_split = 1;   // 0 off, 1 unless the solver fills every SM, 2 always
     // molecule structure and atom order
     DBuf<int> mol, perm;
     DBuf<int2> jr;
@@ -514,6 +522,11 @@ Engine::Engine(const EngineOptions& opt) : p_(new Impl)
         CK(cudaEventCreateWithFlags(&p_->ev_fork0, cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&p_->ev_fork1, cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&p_->ev_join, cudaEventDisableTiming));
+        const char* ds = std::getenv("GFNFF_D4_STREAM");
+        if (!(ds && !std::strcmp(ds, "0"))) {
+            CK(cudaStreamCreateWithPriority(&p_->side_d4, cudaStreamNonBlocking, lo));
+            CK(cudaEventCreateWithFlags(&p_->ev_join_d4, cudaEventDisableTiming));
+        }
     }
     CS(cusolverDnCreate(&p_->sol));
     CS(cusolverDnSetStream(p_->sol, p_->stream));
@@ -550,9 +563,10 @@ Engine::~Engine()
         if (e) cudaEventDestroy(e);
     if (p_->sol) cusolverDnDestroy(p_->sol);
     if (p_->cnl_bad_host) cudaFreeHost(p_->cnl_bad_host);
-    for (cudaEvent_t e : {p_->ev_fork0, p_->ev_fork1, p_->ev_join})
+    for (cudaEvent_t e : {p_->ev_fork0, p_->ev_fork1, p_->ev_join, p_->ev_join_d4})
         if (e) cudaEventDestroy(e);
     if (p_->side) cudaStreamDestroy(p_->side);
+    if (p_->side_d4) cudaStreamDestroy(p_->side_d4);
     if (p_->stream) cudaStreamDestroy(p_->stream);
 }
 
@@ -658,6 +672,8 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
         P.pairs_sym = !(pe && !std::strcmp(pe, "rows"));
         const char* po = std::getenv("GFNFF_PAIRS_OCC");
         P.pairs_occ = po && !std::strcmp(po, "1");
+        const char* ps = std::getenv("GFNFF_PAIRS_SPLIT");
+        P.pairs_split = !ps ? 1 : (!std::strcmp(ps, "0") ? 0 : (!std::strcmp(ps, "1") ? 2 : 1));
     }
     // ---- global element table (union of the molecules' D4 element slots) ----
     std::vector<int> gZ;
@@ -1452,6 +1468,28 @@ void Engine::launch_body()
     // EEQ kernel's blocks leave their SMs one by one when the work queue runs dry, while the
     // largest molecules still factor, and the side kernels take those SMs.
     // (GFNFF_SIDE_EARLY=1: fork at the start of the evaluation instead.)
+    // Coulomb + D4 pairs by tile pairs (each pair once); PART selects the terms
+    auto pairs_sym = [&](auto part, cudaStream_t st) {
+        constexpr int PT = decltype(part)::value;
+        if (P.pair_tile == 32) k_pairs_sym<double, 16, 32, PT><<<P.nsym, 32, 0, st>>>(V, P.symtiles.p);
+        else if (P.pairs_occ) k_pairs_sym<double, 10, kST, PT><<<P.nsym, kST, 0, st>>>(V, P.symtiles.p);
+        else k_pairs_sym<double, 8, kST, PT><<<P.nsym, kST, 0, st>>>(V, P.symtiles.p);
+    };
+    // split unless the solver is the classic PCG, whose cooperative grid fills every SM:
+    // then nothing runs beside it, and the split pass costs more than it hides
+    const bool full_sm_solver = P.nmol == 1 && !P.use_lu && P.solver == Impl::SOLVE_PCG && !P.pcg_pipe;
+    const bool split = fork && P.pairs_sym && P.pairs_split > 0 && (P.pairs_split == 2 || !full_sm_solver);
+    // own stream for batches and direct solvers (512 conformers: 0.98 -> 0.93 ms); beside
+    // the pipelined PCG it slows the solver's barriers, so there it queues on the side stream
+    // (1000 waters: 0.469 ms there, 0.524 ms on its own stream)
+    const bool pcg_single = P.nmol == 1 && !P.use_lu && P.solver == Impl::SOLVE_PCG;
+    cudaStream_t sd = split && P.side_d4 && !pcg_single ? P.side_d4 : s2;
+    auto d4_pairs = [&]() {   // after ev_fork1 (the CN weights exist)
+        if (!split) return;
+        if (sd != s2) CK(cudaStreamWaitEvent(sd, P.ev_fork1, 0));
+        pairs_sym(std::integral_constant<int, kPairD4>{}, sd);
+        if (sd != s2) CK(cudaEventRecord(P.ev_join_d4, sd));
+    };
     const bool early = fork && P.side_early;
     if (early) {
         CK(cudaEventRecord(P.ev_fork0, s));
@@ -1461,6 +1499,7 @@ void Engine::launch_body()
     auto side_after = [&]() {
         if (!fork || early) return;
         CK(cudaStreamWaitEvent(s2, P.ev_fork1, 0));
+        d4_pairs();
         hb_rep_terms();
         bonded_terms();
         CK(cudaEventRecord(P.ev_join, s2));
@@ -1479,6 +1518,7 @@ void Engine::launch_body()
     if (early) {
         CK(cudaEventRecord(P.ev_fork1, s));
         CK(cudaStreamWaitEvent(s2, P.ev_fork1, 0));
+        d4_pairs();
         bonded_terms();
         CK(cudaEventRecord(P.ev_join, s2));
     }
@@ -1538,9 +1578,8 @@ void Engine::launch_body()
         P.mark(7);
         hb_rep_terms();
     }
-    if (P.pairs_sym && P.pair_tile == 32) k_pairs_sym<double, 16, 32><<<P.nsym, 32, 0, s>>>(V, P.symtiles.p);
-    else if (P.pairs_sym && P.pairs_occ) k_pairs_sym<double, 10, kST><<<P.nsym, kST, 0, s>>>(V, P.symtiles.p);
-    else if (P.pairs_sym) k_pairs_sym<double, 8, kST><<<P.nsym, kST, 0, s>>>(V, P.symtiles.p);
+    if (split) pairs_sym(std::integral_constant<int, kPairCoul>{}, s);
+    else if (P.pairs_sym) pairs_sym(std::integral_constant<int, kPairBoth>{}, s);
     else k_pairs<double><<<tgrid, kTile, 0, s>>>(V, P.nsplit);
     if (P.resp_on) {
         // u = B M^-1 B^T w with the factor (or the iteration) of this step's EEQ matrix
@@ -1559,6 +1598,7 @@ void Engine::launch_body()
         k_resp_pairs<<<tgrid, kTile, 0, s>>>(V, P.nsplit);
     }
     if (fork) CK(cudaStreamWaitEvent(s, P.ev_join, 0));
+    if (split && sd != s2) CK(cudaStreamWaitEvent(s, P.ev_join_d4, 0));
     P.mark(10);
     k_post<<<nblk(n), kBlock, 0, s>>>(V);
     if (P.cnl_on) {

@@ -436,49 +436,69 @@ __device__ __forceinline__ void d4_pair_sym(double d2, const double* g0, const d
     dcj = -(double)(dc6j * sum * zz);
 }
 
-template <class R, int MINB, int T>
+// PART selects the terms: kPairCoul (needs this step's charges), kPairD4 (needs only the
+// CN weights, so it can run beside the EEQ solve), or both in one pass
+constexpr int kPairCoul = 1, kPairD4 = 2, kPairBoth = 3;
+template <class R, int MINB, int T, int PART>
 __global__ void __launch_bounds__(T, MINB) k_pairs_sym(View V, const int2* __restrict__ tiles)
 {
-    __shared__ double sx[T], sy[T], sz[T], s0x[T], s0y[T], s0z[T];
-    __shared__ double sq[T], sa[T], sze[T], ssz[T], srz[T];
-    __shared__ double sw0[7][T], sw[7][T];
-    __shared__ int ssl[T], snr[T];
-    __shared__ double jacc[T / 32][5][T];
+    constexpr bool COUL = (PART & kPairCoul) != 0, D4 = (PART & kPairD4) != 0;
+    constexpr int NA = 5;   // j-side sums: fx, fy, fz, dE/dCN_j (D4), far potential (Coulomb)
+    __shared__ double sx[T], sy[T], sz[T];
+    __shared__ double sq[COUL ? T : 1], sa[COUL ? T : 1];
+    __shared__ double s0x[D4 ? T : 1], s0y[D4 ? T : 1], s0z[D4 ? T : 1];
+    __shared__ double sze[D4 ? T : 1], ssz[D4 ? T : 1], srz[D4 ? T : 1];
+    __shared__ double sw0[D4 ? 7 : 1][T], sw[D4 ? 7 : 1][T];
+    __shared__ int ssl[D4 ? T : 1], snr[D4 ? T : 1];
+    __shared__ double jacc[T / 32][NA][T];
     const int2 tp = tiles[blockIdx.x];
     const int i0 = tp.x, j0 = tp.y, i = i0 + threadIdx.x;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const bool act = i < V.n;
     const int ic = act ? i : i0;
-    const double4 pi = V.pos[ic], p0i = V.pos0[ic];
-    const double ai = V.alpeeq[ic], qi = V.q[ic], zi = V.zeta[ic], szi = V.szr[ic];
+    const double4 pi = V.pos[ic];
     const int2 rg = act ? V.jr[i] : make_int2(0, 0);
-    const int si = V.slot[ic], nri = V.nref[ic];
+    double ai = 0.0, qi = 0.0;
+    if constexpr (COUL) { ai = V.alpeeq[ic]; qi = V.q[ic]; }
+    double4 p0i = make_double4(0.0, 0.0, 0.0, 0.0);
+    double zi = 0.0, szi = 0.0, s3i = 0.0;
+    int si = 0, nri = 0;
     double wi[7];
+    const double* g0i = nullptr;
+    const double* dgi = nullptr;
+    if constexpr (D4) {
+        p0i = V.pos0[ic];
+        zi = V.zeta[ic]; szi = V.szr[ic];
+        s3i = sqrt(3.0 * szi);   // sqrt(r4r2) of a pair = s3i * sqrt(szr_j)
+        si = V.slot[ic]; nri = V.nref[ic];
 #pragma unroll
-    for (int a = 0; a < 7; ++a) wi[a] = V.w[(size_t)ic * 7 + a];
-    const double* g0i = V.g0 + (size_t)ic * V.K * 7;
-    const double* dgi = V.hdg + (size_t)ic * V.K * 7;
-    const bool want_dc = !V.exact, want_far = V.cfar != nullptr;
+        for (int a = 0; a < 7; ++a) wi[a] = V.w[(size_t)ic * 7 + a];
+        g0i = V.g0 + (size_t)ic * V.K * 7;
+        dgi = V.hdg + (size_t)ic * V.K * 7;
+    }
+    const bool want_dc = !V.exact, want_far = COUL && V.cfar != nullptr;
     {
         const int jl = j0 + threadIdx.x;
         if (jl < V.n) {
             const int u = threadIdx.x;
-            const double4 p = V.pos[jl], p0 = V.pos0[jl];
+            const double4 p = V.pos[jl];
             sx[u] = p.x; sy[u] = p.y; sz[u] = p.z;
-            s0x[u] = p0.x; s0y[u] = p0.y; s0z[u] = p0.z;
-            sq[u] = V.q[jl]; sa[u] = V.alpeeq[jl]; sze[u] = V.zeta[jl]; ssz[u] = V.szr[jl];
-            srz[u] = sqrt(ssz[u]);
-            ssl[u] = V.slot[jl]; snr[u] = V.nref[jl];
+            if constexpr (COUL) { sq[u] = V.q[jl]; sa[u] = V.alpeeq[jl]; }
+            if constexpr (D4) {
+                const double4 p0 = V.pos0[jl];
+                s0x[u] = p0.x; s0y[u] = p0.y; s0z[u] = p0.z;
+                sze[u] = V.zeta[jl]; ssz[u] = V.szr[jl]; srz[u] = sqrt(ssz[u]);
+                ssl[u] = V.slot[jl]; snr[u] = V.nref[jl];
 #pragma unroll
-            for (int b = 0; b < 7; ++b) {
-                sw0[b][u] = V.w0[(size_t)jl * 7 + b];
-                sw[b][u] = V.w[(size_t)jl * 7 + b];
+                for (int b = 0; b < 7; ++b) {
+                    sw0[b][u] = V.w0[(size_t)jl * 7 + b];
+                    sw[b][u] = V.w[(size_t)jl * 7 + b];
+                }
             }
         }
     }
     __syncthreads();
     const double tsp = 2.0 / 1.772453850905516;
-    const double s3i = sqrt(3.0 * szi);   // sqrt(r4r2) of a pair = s3i * sqrt(szr_j)
     double ec = 0.0, ed = 0.0, gx = 0.0, gy = 0.0, gz = 0.0, dcn = 0.0, cfar = 0.0;
     const int cnt = min(T, V.n - j0);
     for (int jj = 0; jj < cnt; ++jj) {
@@ -491,55 +511,62 @@ __global__ void __launch_bounds__(T, MINB) k_pairs_sym(View V, const int2* __res
             d2 = dx * dx + dy * dy + dz * dz;
             valid = d2 >= 1e-20;
         }
+        bool hit = false;   // this lane has a j-side contribution
         if (valid) {
             double f = 0.0;   // dE/dr / r
-            if (d2 <= 10000.0) {
-                const double s = ai + sa[jj];
-                const double qq = qi * sq[jj];
-                if (d2 >= 36.0 * s) {
-                    const double ir = rsqrt(d2);
-                    const double e = qq * ir;
-                    ec += e;
-                    f -= e * ir * ir;
-                } else {
-                    const double r = sqrt(d2);
-                    const double g = 1.0 / sqrt(s);
-                    const double gr = g * r;
-                    const double ef = erf(gr);
-                    ec += qq * ef / r;
-                    f += qq * ((g * exp(-gr * gr) * tsp) / r - ef / d2) / r;
+            if constexpr (COUL) {
+                hit = true;
+                if (d2 <= 10000.0) {
+                    const double s = ai + sa[jj];
+                    const double qq = qi * sq[jj];
+                    if (d2 >= 36.0 * s) {
+                        const double ir = rsqrt(d2);
+                        const double e = qq * ir;
+                        ec += e;
+                        f -= e * ir * ir;
+                    } else {
+                        const double r = sqrt(d2);
+                        const double g = 1.0 / sqrt(s);
+                        const double gr = g * r;
+                        const double ef = erf(gr);
+                        ec += qq * ef / r;
+                        f += qq * ((g * exp(-gr * gr) * tsp) / r - ef / d2) / r;
+                    }
+                } else if (want_far) {
+                    const double ir = rsqrt(d2);   // cut pair: its EEQ element is 1/r
+                    cfar += sq[jj] * ir;
+                    cfj = qi * ir;
                 }
-            } else if (want_far) {
-                const double ir = rsqrt(d2);   // cut pair: its EEQ element is 1/r
-                cfar += sq[jj] * ir;
-                cfj = qi * ir;
             }
-            if (d2 <= 2500.0 && d2_exact(p0i, make_double4(s0x[jj], s0y[jj], s0z[jj], 0.0)) <= 3600.0) {
-                const int sj = ssl[jj], nrj = snr[jj];
-                const double* dgj = V.hdg + ((size_t)j * V.K + si) * 7;
-                const double r4r2 = 3.0 * szi * ssz[jj], sr4r2 = s3i * srz[jj], zz = zi * sze[jj];
-                double e, dedr, dci;
-                // mixed form: pairs closer than 15 bohr (the strong ones) stay FP64
-                if (sizeof(R) == sizeof(double) || d2 < 225.0)
-                    d4_pair_sym<double, T>(d2, g0i + sj * 7, dgi + sj * 7, dgj, sw0, sw, jj, nrj, nri, wi, r4r2,
-                                           sr4r2, zz, want_dc, e, dedr, dci, dcj);
-                else
-                    d4_pair_sym<R, T>(d2, g0i + sj * 7, dgi + sj * 7, dgj, sw0, sw, jj, nrj, nri, wi, r4r2, sr4r2,
-                                      zz, want_dc, e, dedr, dci, dcj);
-                ed += e;
-                f += dedr;
-                dcn += dci;
+            if constexpr (D4) {
+                if (d2 <= 2500.0 && d2_exact(p0i, make_double4(s0x[jj], s0y[jj], s0z[jj], 0.0)) <= 3600.0) {
+                    hit = true;
+                    const int sj = ssl[jj], nrj = snr[jj];
+                    const double* dgj = V.hdg + ((size_t)j * V.K + si) * 7;
+                    const double r4r2 = 3.0 * szi * ssz[jj], sr4r2 = s3i * srz[jj], zz = zi * sze[jj];
+                    double e, dedr, dci;
+                    // mixed form: pairs closer than 15 bohr (the strong ones) stay FP64
+                    if (sizeof(R) == sizeof(double) || d2 < 225.0)
+                        d4_pair_sym<double, T>(d2, g0i + sj * 7, dgi + sj * 7, dgj, sw0, sw, jj, nrj, nri, wi, r4r2,
+                                               sr4r2, zz, want_dc, e, dedr, dci, dcj);
+                    else
+                        d4_pair_sym<R, T>(d2, g0i + sj * 7, dgi + sj * 7, dgj, sw0, sw, jj, nrj, nri, wi, r4r2,
+                                          sr4r2, zz, want_dc, e, dedr, dci, dcj);
+                    ed += e;
+                    f += dedr;
+                    dcn += dci;
+                }
             }
             gx += f * dx; gy += f * dy; gz += f * dz;
             fx = -f * dx; fy = -f * dy; fz = -f * dz;
         }
-        if (__any_sync(0xffffffffu, valid)) {
+        if (__any_sync(0xffffffffu, hit)) {
             for (int o = 16; o > 0; o >>= 1) {
                 fx += __shfl_xor_sync(0xffffffffu, fx, o);
                 fy += __shfl_xor_sync(0xffffffffu, fy, o);
                 fz += __shfl_xor_sync(0xffffffffu, fz, o);
             }
-            if (want_dc)
+            if (D4 && want_dc)
                 for (int o = 16; o > 0; o >>= 1) dcj += __shfl_xor_sync(0xffffffffu, dcj, o);
             if (want_far)
                 for (int o = 16; o > 0; o >>= 1) cfj += __shfl_xor_sync(0xffffffffu, cfj, o);
@@ -552,9 +579,9 @@ __global__ void __launch_bounds__(T, MINB) k_pairs_sym(View V, const int2* __res
     __syncthreads();
     if (threadIdx.x < cnt) {
         const int j = j0 + threadIdx.x;
-        double a[5];
+        double a[NA];
 #pragma unroll
-        for (int k = 0; k < 5; ++k) {
+        for (int k = 0; k < NA; ++k) {
             a[k] = 0.0;
 #pragma unroll
             for (int w = 0; w < T / 32; ++w) a[k] += jacc[w][k][threadIdx.x];
@@ -573,8 +600,8 @@ __global__ void __launch_bounds__(T, MINB) k_pairs_sym(View V, const int2* __res
         if (cfar != 0.0) atomicAdd(V.cfar + i, cfar);
     }
     const int m = act ? V.mol[i] : -1;
-    eadd(V, ec, m, T_COUL);
-    eadd(V, ed, m, T_DISP);
+    if constexpr (COUL) eadd(V, ec, m, T_COUL);
+    if constexpr (D4) eadd(V, ed, m, T_DISP);
 }
 
 // ------------------------------------------------------------------------------------
