@@ -1571,7 +1571,8 @@ void Engine::launch_body()
     const double* ysol = P.bvec.p;
     if (P.nmol == 1 && !P.use_lu && P.solver == Impl::SOLVE_TILED) ysol = P.ysol.p;
     if (P.nmol == 1 && !P.use_lu && P.solver == Impl::SOLVE_PCG) ysol = P.px.p;
-    k_eeq_expand<<<nblk(n), kBlock, 0, s>>>(V, P.q0.p, P.atom2red.p, P.frag_off.p, P.frag_atoms.p, ysol, P.q.p);
+    k_eeq_expand<<<nblk((long)P.nfrag * 32), kBlock, 0, s>>>(P.nfrag, P.q0.p, P.atom2red.p, P.frag_off.p,
+                                                              P.frag_atoms.p, ysol, P.q.p);
     P.mark(6);
     if (!fork) {
         bonded_terms();
@@ -1594,7 +1595,8 @@ void Engine::launch_body()
         } else {   // the Cholesky factor (cuSOLVER or the tiled kernel) is in M
             CS(cusolverDnDpotrs(P.sol, CUBLAS_FILL_MODE_LOWER, P.nred, 1, P.M.p, P.lda, P.bres.p, P.nred, P.info2.p));
         }
-        k_eeq_expand<<<nblk(n), kBlock, 0, s>>>(V, nullptr, P.atom2red.p, P.frag_off.p, P.frag_atoms.p, y, P.ures.p);
+        k_eeq_expand<<<nblk((long)P.nfrag * 32), kBlock, 0, s>>>(P.nfrag, nullptr, P.atom2red.p, P.frag_off.p,
+                                                                  P.frag_atoms.p, y, P.ures.p);
         k_resp_pairs<<<tgrid, kTile, 0, s>>>(V, P.nsplit);
     }
     if (fork) CK(cudaStreamWaitEvent(s, P.ev_join, 0));

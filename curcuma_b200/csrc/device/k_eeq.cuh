@@ -140,24 +140,25 @@ __global__ void k_chol_info(const int* err, int* info)
 }
 
 // out = q0 + B y (q0 null: B y)
-__global__ void k_eeq_expand(View V, const double* q0, const int* atom2red, const int* frag_off,
+__global__ void k_eeq_expand(int nfrag, const double* q0, const int* atom2red, const int* frag_off,
                              const int* frag_atoms, const double* y, double* out)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= V.n) return;
-    const double base = q0 ? q0[i] : 0.0;
-    const int rr = atom2red[i];
-    if (rr >= 0) {
-        out[i] = base + y[rr];
-    } else {
+    // one warp per fragment; frag_atoms[frag_off[f]] is the fragment's anchor (its first atom)
+    const int f = (int)(((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    if (f >= nfrag) return;   // whole warps
+    const int p0 = frag_off[f], p1 = frag_off[f + 1];
+    double s = 0.0;
+    for (int p = p0 + 1 + lane; p < p1; p += 32) {
+        const int a = frag_atoms[p];
+        const double v = y[atom2red[a]];
+        out[a] = (q0 ? q0[a] : 0.0) + v;
+        s += v;
+    }
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) {
         // anchor: minus the sum of its fragment's reduced variables
-        const int f = -rr - 1;
-        double s = 0.0;
-        for (int p = frag_off[f]; p < frag_off[f + 1]; ++p) {
-            const int ra = atom2red[frag_atoms[p]];
-            if (ra >= 0) s += y[ra];
-        }
-        out[i] = base - s;
+        const int a = frag_atoms[p0];
+        out[a] = (q0 ? q0[a] : 0.0) - s;
     }
 }
 
