@@ -287,6 +287,7 @@ def measure(args, precision, Z, X, torch, dist, world, local, mols=None):
     if world > 1:
         dist.barrier()
     step_ms = [a.elapsed_time(b) for a, b in events]
+    kpe = gpu.kernelsPerEvaluation()   # of the graph the timed steps replayed
     # phase split: the same steps again with CUDA events between the phases (direct
     # launches), for the roofline of the dominant kernel
     phases = np.zeros(len(_lib.PHASES))
@@ -332,7 +333,8 @@ def measure(args, precision, Z, X, torch, dist, world, local, mols=None):
             "phase_avg": {k: v / steps for k, v in zip(_lib.PHASES, phases)}, "status": worst,
             "e2e": {"value": world * nmol * steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 3 * n * 8,
                     "d2h_bytes_per_step": (3 * n + 16 * nmol) * 8 + 4 * nmol},
-            "clocks": clk, "setup_s": setup_s, "solver": gpu.eeqSolver(), "iters": gpu.eeqIterations()}
+            "clocks": clk, "setup_s": setup_s, "solver": gpu.eeqSolver(), "iters": gpu.eeqIterations(),
+            "kernels_per_eval": kpe}
 
 
 def per_molecule_loop(mols, local):
@@ -441,12 +443,9 @@ def run_ours(args):
         counts = {k: len(gpu.topology(kind, w)) for k, kind, w in
                   [("bonds", 0, 2), ("angles", 1, 3), ("torsions", 2, 4), ("inversions", 3, 4), ("hbonds", 6, 4),
                    ("xbonds", 7, 3), ("atm", 12, 3), ("batm", 13, 3)]}
-    # kernels of this library per step: positions, cn, d4w, eeq matrix, rhs, solve (+info),
-    # expand, repulsion, pairs, post, chain, outputs, finish, and one per non-empty term list
-    fixed = 13 + (1 if main["solver"] in ("pcg", "tiled") else 0)
-    launches = fixed + (8 if mols else
-                        sum(1 for k in ("bonds", "angles", "torsions", "inversions", "hbonds", "xbonds", "atm", "batm")
-                            if counts[k] > 0))
+    # kernels of this library per step, counted by the library in the captured step graph
+    # (kernel nodes whose code is in libgfnff_b200.so, cuSOLVER's not included) + positions
+    launches = main["kernels_per_eval"]
     if rank != 0:
         if world > 1:
             dist.destroy_process_group()
@@ -483,7 +482,8 @@ def run_ours(args):
                        "eeq_iterations_last_step": main["iters"],
                        "l2": "flushed before every timed step (256 MiB write)",
                        "parallelism": f"replicas x{world}", "setup_s": round(main["setup_s"], 3)},
-            "e2e": main["e2e"], "gpu_launches": launches * steps, "roofline": roof,
+            "e2e": main["e2e"], "gpu_launches": launches * steps if launches > 0 else None,
+            "kernels_per_step": launches, "roofline": roof,
             "phase_ms": {k: round(v, 4) for k, v in main["phase_avg"].items()},
             "step_ms_median": statistics.median(main["step_ms"]), "status": main["status"],
             "forms": {p: {"value": r["value"], "e2e": r["e2e"]["value"], "eeq_solver": r["solver"],

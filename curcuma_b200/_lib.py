@@ -21,7 +21,7 @@ EXPORTED = ["gfnff_default_options", "gfnff_create", "gfnff_setup", "gfnff_energ
             "gfnff_coordination_numbers", "gfnff_get_topology", "gfnff_sizes", "gfnff_last_error",
             "gfnff_destroy", "gfnff_set_phase_timing", "gfnff_phase_times", "gfnff_fma_peak_tflops",
             "gfnff_eeq_charges_noalloc", "gfnff_eeq_solver", "gfnff_eeq_iterations", "gfnff_setup_batch",
-            "gfnff_energy_and_gradient_batch", "gfnff_md_nve"]
+            "gfnff_energy_and_gradient_batch", "gfnff_md_nve", "gfnff_kernels_per_evaluation"]
 PHASES = ["positions", "cn", "d4_weights", "eeq_matrix", "eeq_rhs", "eeq_solve", "bonded",
           "hbonds", "repulsion", "pairs", "post_chain", "finish"]
 
@@ -67,6 +67,7 @@ def load():
     lib.gfnff_eeq_solver.argtypes = [c_v]
     lib.gfnff_eeq_solver.restype = ctypes.c_char_p
     lib.gfnff_eeq_iterations.argtypes = [c_v]
+    lib.gfnff_kernels_per_evaluation.argtypes = [c_v]
     lib.gfnff_setup_batch.argtypes = [c_v, c_i, P(c_i), P(c_i), P(c_d), P(c_i)]
     lib.gfnff_energy_and_gradient_batch.argtypes = [c_v, P(c_d), P(c_d), P(c_d), P(c_i)]
     lib.gfnff_md_nve.argtypes = [c_v, c_i, c_d, P(c_d), P(c_d), P(c_d), P(c_d), P(c_d)]

@@ -441,6 +441,12 @@ const char* gfnff_eeq_solver(gfnff_handle* h)
     return h->eng->solver_name();
 }
 
+int gfnff_kernels_per_evaluation(gfnff_handle* h)
+{
+    if (!h || !h->ready) return -1;
+    return h->eng->kernels_per_evaluation();
+}
+
 int gfnff_eeq_iterations(gfnff_handle* h)
 {
     if (!h || !h->ready) return -1;

@@ -27,6 +27,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <dlfcn.h>
 #include <type_traits>
 #include <map>
 #include <numeric>
@@ -466,6 +467,7 @@ struct Engine::Impl {
     // launches, and a capture that fails falls back to them for good.
     cudaGraphExec_t graph = nullptr;
     bool graphs_ok = true;
+    int graph_kernels = -1;   // kernel nodes of this library in the captured step graph
     DBuf<double> etot;   // molecule totals of the last evaluation
     // exact-gradient mode: EEQ charge response of the Coulomb pairs cut at 100 bohr
     bool resp_on = false;
@@ -1366,6 +1368,41 @@ int Engine::eeq_iterations()
 // unit) combination and replayed while the model and the solver choice stay the same;
 // phase timing (events between phases) and GFNFF_GRAPHS=0 use direct launches, and a
 // capture that fails falls back to them for good.
+// kernel nodes of a captured graph whose host stub lies in this shared object (library
+// kernels, e.g. cuSOLVER's, are not counted)
+static void own_marker() {}
+static int own_kernel_nodes(cudaGraph_t g)
+{
+    Dl_info self{};
+    if (!dladdr((void*)&own_marker, &self) || !self.dli_fname) return -1;
+    size_t nn = 0;
+    if (cudaGraphGetNodes(g, nullptr, &nn) != cudaSuccess) return -1;
+    std::vector<cudaGraphNode_t> nodes(nn);
+    if (nn && cudaGraphGetNodes(g, nodes.data(), &nn) != cudaSuccess) return -1;
+    int k = 0;
+    for (cudaGraphNode_t nd : nodes) {
+        cudaGraphNodeType t;
+        if (cudaGraphNodeGetType(nd, &t) != cudaSuccess || t != cudaGraphNodeTypeKernel) continue;
+        cudaKernelNodeParams kp{};
+        // nodes of kernels from another runtime instance (cuSOLVER links its own) are not
+        // known to this one: the query fails for them, and its error must not stay pending
+        if (cudaGraphKernelNodeGetParams(nd, &kp) != cudaSuccess) {
+            cudaGetLastError();
+            continue;
+        }
+        Dl_info di{};
+        if (dladdr(kp.func, &di) && di.dli_fname && !std::strcmp(di.dli_fname, self.dli_fname)) ++k;
+    }
+    cudaGetLastError();
+    return k;
+}
+
+int Engine::kernels_per_evaluation() const
+{
+    // the positions kernel is launched before the replayed graph
+    return p_->graph && p_->graph_kernels >= 0 ? p_->graph_kernels + 1 : -1;
+}
+
 void Engine::enqueue(const double* d_xyz, bool bohr, double* d_energies)
 {
     Impl& P = *p_;
@@ -1384,6 +1421,7 @@ void Engine::enqueue(const double* d_xyz, bool bohr, double* d_energies)
                 }
                 const cudaError_t e = cudaStreamEndCapture(P.stream, &graph);
                 ok = ok && e == cudaSuccess && graph;
+                if (ok) P.graph_kernels = own_kernel_nodes(graph);
                 if (ok) ok = cudaGraphInstantiate(&P.graph, graph, 0) == cudaSuccess;
                 if (graph) cudaGraphDestroy(graph);
             }

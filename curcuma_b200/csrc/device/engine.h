@@ -73,6 +73,9 @@ public:
     const char* solver_name() const;
     // iterations of the last iterative EEQ solve (0 for direct solvers)
     int eeq_iterations();
+    // kernels of this library per evaluation while the step replays as a graph (-1 before
+    // the first capture or with direct launches)
+    int kernels_per_evaluation() const;
     // per-phase CUDA-event timing of enqueue(); phase_ms returns the milliseconds of the
     // last evaluation per phase (order of kPhaseNames) after the stream has finished
     void set_timing(bool on);

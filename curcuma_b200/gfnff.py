@@ -191,6 +191,10 @@ class GFNFF:
         """Iterations of the last iterative EEQ solve (0 for direct solvers)."""
         return int(self._lib.gfnff_eeq_iterations(self._h))
 
+    def kernelsPerEvaluation(self):
+        """Kernels of this library per evaluation of the replayed step graph (-1: none yet)."""
+        return int(self._lib.gfnff_kernels_per_evaluation(self._h))
+
     def sizes(self):
         n, f = ctypes.c_int(), ctypes.c_int()
         self._check(self._lib.gfnff_sizes(self._h, ctypes.byref(n), ctypes.byref(f)))

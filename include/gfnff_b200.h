@@ -174,6 +174,12 @@ const char* gfnff_eeq_solver(gfnff_handle* h);
  * reference. */
 int gfnff_eeq_iterations(gfnff_handle* h);
 
+/* Kernels of this library launched per evaluation while the step replays as a CUDA graph
+ * (the kernel nodes of the captured graph whose code is in this library, plus the
+ * positions kernel launched before it); -1 before the first evaluation or with direct
+ * launches.  Diagnostic without a counterpart in the reference. */
+int gfnff_kernels_per_evaluation(gfnff_handle* h);
+
 /* Last error message of the handle (static storage when h is NULL). */
 const char* gfnff_last_error(gfnff_handle* h);
 

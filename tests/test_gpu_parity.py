@@ -255,3 +255,25 @@ def test_side_stream_gradients_repeat(pcg_form, monkeypatch):
         assert abs(e - T["total"]) < E_TOL
         worst = max(worst, np.abs(g.getGradient() - G).max())
     assert worst < G_TOL, worst
+
+
+def test_kernels_per_evaluation(monkeypatch):
+    """The library counts its own kernels in the captured step graph (cuSOLVER's are not
+    counted); direct launches report -1."""
+    Z, X = workloads.water_cluster(64, 9)
+    counts = {}
+    for solver in ("pcg", "library"):
+        monkeypatch.setenv("GFNFF_EEQ_SOLVER", solver)
+        g = GFNFF()
+        assert g.setMolecule(Z, X)
+        g.calculateEnergy(True)
+        k1 = g.kernelsPerEvaluation()
+        g.calculateEnergy(True)
+        assert g.kernelsPerEvaluation() == k1
+        counts[solver] = k1
+    assert 12 <= counts["library"] < counts["pcg"] <= 40, counts
+    monkeypatch.setenv("GFNFF_GRAPHS", "0")
+    g = GFNFF()
+    assert g.setMolecule(Z, X)
+    g.calculateEnergy(True)
+    assert g.kernelsPerEvaluation() == -1
