@@ -53,7 +53,10 @@ def parse():
     return ap.parse_args()
 
 
-def workload(cfg):
+def workload(cfg, rank=0):
+    """The structure(s) of a config.  Under torchrun the conformer batch is a molecule shard
+    per rank: every rank evaluates a batch of its own (seed 1004 + 1000 rank), so per-GPU work
+    stays fixed as ranks are added (no collective on the data path)."""
     from curcuma_b200 import workloads as W
     if cfg == 1:
         return "n-C64H130 all-trans, 0.05 A noise (seed 1001)", *W.alkane(64, 1001)
@@ -64,11 +67,20 @@ def workload(cfg):
     if cfg == 5:
         return "6000 H2O + 40 C20H42 (seed 1005)", *W.large_cluster(6000, 40, 20, 1005)
     if cfg == 4:
-        mols = W.conformer_batch(512, 1004)
+        seed = 1004 + 1000 * rank
+        mols = W.conformer_batch(512, seed)
         Z = np.concatenate([z for z, _ in mols])
         X = np.concatenate([x for _, x in mols])
-        return "512 saturated C/N/O chains, 20-300 atoms log-uniform (seed 1004)", Z, X, mols
+        return f"512 saturated C/N/O chains, 20-300 atoms log-uniform (seed {seed})", Z, X, mols
     raise SystemExit(f"unknown config {cfg}")
+
+
+def max_over_ranks(x, dist, device):
+    """The largest value over all ranks (times are reported for the slowest rank)."""
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
 
 
 def perturbed(X, k, sigma=0.01, seed=7):
@@ -304,9 +316,7 @@ def measure(args, precision, Z, X, torch, dist, world, local, mols=None):
     torch.cuda.synchronize()
     total_ms = float(sum(step_ms))
     if world > 1:
-        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+        total_ms = max_over_ranks(total_ms, dist, "cuda")
     lib.gfnff_set_phase_timing(h, 0)
     # end to end through the host C ABI: host coordinates in, energy + gradient out
     hostX = [perturbed(X, 5000 + k) for k in range(steps)]
@@ -326,9 +336,7 @@ def measure(args, precision, Z, X, torch, dist, world, local, mols=None):
     e2e_s = time.perf_counter() - t
     clk = clocks.stop()
     if world > 1:
-        tt = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_s = float(tt.item())
+        e2e_s = max_over_ranks(e2e_s, dist, "cuda")
     return {"gpu": gpu, "value": world * nmol * steps / (total_ms * 1e-3), "total_ms": total_ms, "step_ms": step_ms,
             "phase_avg": {k: v / steps for k, v in zip(_lib.PHASES, phases)}, "status": worst,
             "e2e": {"value": world * nmol * steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 3 * n * 8,
@@ -417,7 +425,7 @@ def run_ours(args):
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
-    wl = workload(args.config)
+    wl = workload(args.config, rank)
     desc, Z, X = wl[:3]
     mols = wl[3] if len(wl) > 3 else None
     n = len(Z)
@@ -481,7 +489,8 @@ def run_ours(args):
                        "precision": args.precision, "eeq_solver": main["solver"],
                        "eeq_iterations_last_step": main["iters"],
                        "l2": "flushed before every timed step (256 MiB write)",
-                       "parallelism": f"replicas x{world}", "setup_s": round(main["setup_s"], 3)},
+                       "parallelism": (f"molecule shards x{world} (a batch per rank)" if mols else
+                                       f"replicas x{world}"), "setup_s": round(main["setup_s"], 3)},
             "e2e": main["e2e"], "gpu_launches": launches * steps if launches > 0 else None,
             "kernels_per_step": launches, "roofline": roof,
             "phase_ms": {k: round(v, 4) for k, v in main["phase_avg"].items()},

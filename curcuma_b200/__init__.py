@@ -5,5 +5,6 @@ parameters) once per molecule, then energy + gradient per geometry on the GPU th
 C ABI declared in ``include/gfnff_b200.h``.
 """
 from .gfnff import FP64, MIXED, GFNFF, atomic_masses, maxwell_boltzmann  # noqa: F401
+from .sharding import shard_by_cost  # noqa: F401
 
-__all__ = ["GFNFF", "FP64", "MIXED", "atomic_masses", "maxwell_boltzmann"]
+__all__ = ["GFNFF", "FP64", "MIXED", "atomic_masses", "maxwell_boltzmann", "shard_by_cost"]
