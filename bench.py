@@ -215,16 +215,20 @@ def cpu_model():
     return "unknown"
 
 
-def cpu_oracle_rate(Z, X, steps, warmup):
+def cpu_oracle_rate(Z, X, steps, warmup, min_seconds=0.0, max_steps=64):
+    """Evaluations/s of the CPU oracle: at least `steps` evaluations, more (up to max_steps)
+    until min_seconds have passed.  Returns (rate, seconds, evaluations)."""
     from tests.oracle_api import Oracle
     o = Oracle(Z, X)
     for k in range(warmup):
         o.engrad(perturbed(X, 1000 + k))
     t = time.perf_counter()
-    for k in range(steps):
+    k = 0
+    while k < steps or (time.perf_counter() - t < min_seconds and k < max_steps):
         o.engrad(perturbed(X, 2000 + k))
+        k += 1
     dt = time.perf_counter() - t
-    return steps / dt, dt
+    return k / dt, dt, k
 
 
 def run_reference(args):
@@ -233,7 +237,7 @@ def run_reference(args):
         return
     desc, Z, X = workload(args.config)
     threads = os.cpu_count()
-    rate, dt = cpu_oracle_rate(Z, X, args.steps, args.warmup)
+    rate, dt, _ = cpu_oracle_rate(Z, X, args.steps, args.warmup)
     line = {"metric": METRIC, "value": rate, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -522,11 +526,10 @@ def run_ours(args):
         line["fd_check"] = {"exact_fp64": fd_check(exact["fp64"], X),
                             "reference_fp64": fd_check(res["fp64"]["gpu"], X)}
     if world == 1 and not args.no_cpu_baseline:
-        rate, dt = cpu_oracle_rate(Z, X, 2 if n >= 2000 else 5, 1)
+        rate, dt, k = cpu_oracle_rate(Z, X, 2, 1, min_seconds=10.0)
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
                                 "cpu": cpu_model(),
-                                "sample": f"{2 if n >= 2000 else 5} full E+grad evaluations of the same workload "
-                                          f"({dt:.1f} s)"}
+                                "sample": f"{k} full E+grad evaluations of the same workload ({dt:.1f} s)"}
     print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()

@@ -58,7 +58,7 @@ def build_library(force: bool = False) -> Path:
     for src in CPP_SOURCES:
         obj = BUILD / (src.stem + ".o")
         if force or _stale(obj, [src] + hdr):
-            _run([CXX, "-O2", "-std=c++17", "-fPIC", "-fopenmp", f"-I{CUDA / 'include'}", "-c", src, "-o", obj])
+            _run([CXX, "-O3", "-std=c++17", "-fPIC", "-fopenmp", f"-I{CUDA / 'include'}", "-c", src, "-o", obj])
         objs.append(obj)
     if force or _stale(LIB, objs):
         _run([CXX, "-shared", "-o", LIB, *objs, f"-L{CUDA / 'lib64'}", "-lcudart", "-lcusolver", "-lgomp",

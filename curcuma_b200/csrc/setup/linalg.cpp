@@ -52,23 +52,57 @@ bool cholesky(double* A, int n)
     return true;
 }
 
+namespace {
+
+// forward and backward substitution for columns [c0, c0 + W) of B (row-major, nrhs columns):
+// rows of B are updated as contiguous segments, L is read by rows
+template <int W>
+void solve_columns(const double* L, int n, double* B, int nrhs, int c0, int w)
+{
+    double acc[W];
+    for (int i = 0; i < n; ++i) {   // L y = b
+        const double* li = L + (size_t)i * n;
+        for (int c = 0; c < W; ++c) acc[c] = 0.0;
+        for (int p = 0; p < i; ++p) {
+            const double l = li[p];
+            const double* bp = B + (size_t)p * nrhs + c0;
+            if (w == W) {
+                for (int c = 0; c < W; ++c) acc[c] += l * bp[c];
+            } else {
+                for (int c = 0; c < w; ++c) acc[c] += l * bp[c];
+            }
+        }
+        double* bi = B + (size_t)i * nrhs + c0;
+        for (int c = 0; c < w; ++c) bi[c] = (bi[c] - acc[c]) / li[i];
+    }
+    for (int i = n - 1; i >= 0; --i) {   // L^T x = y, row i final once the rows below are done
+        const double* li = L + (size_t)i * n;
+        double* bi = B + (size_t)i * nrhs + c0;
+        for (int c = 0; c < w; ++c) bi[c] /= li[i];
+        for (int p = 0; p < i; ++p) {
+            const double l = li[p];
+            if (l == 0.0) continue;
+            double* bp = B + (size_t)p * nrhs + c0;
+            if (w == W) {
+                for (int c = 0; c < W; ++c) bp[c] -= l * bi[c];
+            } else {
+                for (int c = 0; c < w; ++c) bp[c] -= l * bi[c];
+            }
+        }
+    }
+}
+
+}  // namespace
+
 void cholesky_solve(const double* L, int n, double* B, int nrhs)
 {
-#pragma omp parallel for schedule(static) if (nrhs > 4)
-    for (int c = 0; c < nrhs; ++c) {
-        // forward: L y = b
-        for (int i = 0; i < n; ++i) {
-            double s = B[(size_t)i * nrhs + c];
-            const double* ri = L + (size_t)i * n;
-            for (int p = 0; p < i; ++p) s -= ri[p] * B[(size_t)p * nrhs + c];
-            B[(size_t)i * nrhs + c] = s / ri[i];
-        }
-        // backward: L^T x = y
-        for (int i = n - 1; i >= 0; --i) {
-            double s = B[(size_t)i * nrhs + c];
-            for (int p = i + 1; p < n; ++p) s -= L[(size_t)p * n + i] * B[(size_t)p * nrhs + c];
-            B[(size_t)i * nrhs + c] = s / L[(size_t)i * n + i];
-        }
+    // blocks of 16 right-hand sides per thread (the EEQ solve has one per fragment)
+    constexpr int W = 16;
+    const int nb = (nrhs + W - 1) / W;
+#pragma omp parallel for schedule(dynamic, 1) if (nb > 1)
+    for (int k = 0; k < nb; ++k) {
+        const int c0 = k * W;
+        solve_columns<W>(L, n, B, nrhs, c0, std::min(W, nrhs - c0));
     }
 }
 
