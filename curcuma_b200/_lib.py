@@ -21,7 +21,8 @@ EXPORTED = ["gfnff_default_options", "gfnff_create", "gfnff_setup", "gfnff_energ
             "gfnff_coordination_numbers", "gfnff_get_topology", "gfnff_sizes", "gfnff_last_error",
             "gfnff_destroy", "gfnff_set_phase_timing", "gfnff_phase_times", "gfnff_fma_peak_tflops",
             "gfnff_eeq_charges_noalloc", "gfnff_eeq_solver", "gfnff_eeq_iterations", "gfnff_setup_batch",
-            "gfnff_energy_and_gradient_batch", "gfnff_md_nve", "gfnff_kernels_per_evaluation"]
+            "gfnff_energy_and_gradient_batch", "gfnff_md_nve", "gfnff_kernels_per_evaluation",
+            "gfnff_save_parameters", "gfnff_setup_from_parameters", "gfnff_write_parameters"]
 PHASES = ["positions", "cn", "d4_weights", "eeq_matrix", "eeq_rhs", "eeq_solve", "bonded",
           "hbonds", "repulsion", "pairs", "post_chain", "finish"]
 
@@ -68,6 +69,9 @@ def load():
     lib.gfnff_eeq_solver.restype = ctypes.c_char_p
     lib.gfnff_eeq_iterations.argtypes = [c_v]
     lib.gfnff_kernels_per_evaluation.argtypes = [c_v]
+    lib.gfnff_save_parameters.argtypes = [c_v, ctypes.c_char_p]
+    lib.gfnff_setup_from_parameters.argtypes = [c_v, ctypes.c_char_p, c_i, P(c_i)]
+    lib.gfnff_write_parameters.argtypes = [c_i, P(c_i), P(c_d), c_i, c_i, ctypes.c_char_p]
     lib.gfnff_setup_batch.argtypes = [c_v, c_i, P(c_i), P(c_i), P(c_d), P(c_i)]
     lib.gfnff_energy_and_gradient_batch.argtypes = [c_v, P(c_d), P(c_d), P(c_d), P(c_i)]
     lib.gfnff_md_nve.argtypes = [c_v, c_i, c_d, P(c_d), P(c_d), P(c_d), P(c_d), P(c_d)]

@@ -87,6 +87,8 @@ gfnff_status gfnff_create(const gfnff_options* opts, gfnff_handle** out)
     return GFNFF_OK;
 }
 
+static gfnff_status finish_setup(gfnff_handle* h, int n);
+
 gfnff_status gfnff_setup(gfnff_handle* h, int n, const int* Z, const double* xyz, int charge)
 {
     if (!h) return fail(nullptr, GFNFF_INVALID_ARG, "handle is NULL");
@@ -99,6 +101,12 @@ gfnff_status gfnff_setup(gfnff_handle* h, int n, const int* Z, const double* xyz
     } catch (const std::exception& e) {
         return fail(h, GFNFF_SETUP_FAILED, e.what());
     }
+    return finish_setup(h, n);
+}
+
+// upload of h->model and the per-handle host staging (gfnff_setup, gfnff_setup_from_parameters)
+static gfnff_status finish_setup(gfnff_handle* h, int n)
+{
     try {
         h->eng->upload(h->model);
         if (h->pin_xyz) cudaFreeHost(h->pin_xyz);
@@ -118,6 +126,48 @@ gfnff_status gfnff_setup(gfnff_handle* h, int n, const int* Z, const double* xyz
     h->natoms = n;
     h->batch.clear();
     h->ready = true;
+    return GFNFF_OK;
+}
+
+gfnff_status gfnff_save_parameters(gfnff_handle* h, const char* path)
+{
+    if (!h) return fail(nullptr, GFNFF_INVALID_ARG, "handle is NULL");
+    if (!path) return fail(h, GFNFF_INVALID_ARG, "NULL path");
+    if (!h->ready || h->nmol) return fail(h, GFNFF_NOT_READY, "gfnff_setup has not been called");
+    try {
+        save_parameters(h->model, path);
+    } catch (const std::exception& e) {
+        return fail(h, GFNFF_INVALID_ARG, e.what());
+    }
+    return GFNFF_OK;
+}
+
+gfnff_status gfnff_setup_from_parameters(gfnff_handle* h, const char* path, int natoms, const int* Z)
+{
+    if (!h) return fail(nullptr, GFNFF_INVALID_ARG, "handle is NULL");
+    if (!path || natoms <= 0 || !Z) return fail(h, GFNFF_INVALID_ARG, "invalid path or molecule");
+    h->ready = false;
+    try {
+        Model m = load_parameters(path);
+        if (m.n != natoms || !std::equal(m.Z.begin(), m.Z.end(), Z))
+            return fail(h, GFNFF_SETUP_FAILED, "parameter file is for another structure");
+        h->model = std::move(m);
+    } catch (const std::exception& e) {
+        return fail(h, GFNFF_SETUP_FAILED, e.what());
+    }
+    return finish_setup(h, h->model.n);
+}
+
+gfnff_status gfnff_write_parameters(int n, const int* Z, const double* xyz, int charge, int hbond, const char* path)
+{
+    if (n <= 0 || !Z || !xyz || !path) return fail(nullptr, GFNFF_INVALID_ARG, "invalid molecule or path");
+    try {
+        SetupOptions so;
+        so.hbond = hbond != 0;
+        save_parameters(build_model(n, Z, xyz, charge, so), path);
+    } catch (const std::exception& e) {
+        return fail(nullptr, GFNFF_SETUP_FAILED, e.what());
+    }
     return GFNFF_OK;
 }
 

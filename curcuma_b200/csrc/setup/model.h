@@ -114,6 +114,12 @@ Model build_model(int n, const int* Z, const double* xyz_ang, int charge,
 // (gfnff_method.cpp:1597-1690); also rebuilds the bond <-> HB cross reference.
 void redetect_hbxb(Model& m, const double* xyz_bohr);
 
+// Parameter file (the whole set-up result, binary, this library's own format): written by
+// save_parameters, read back by load_parameters, which throws std::runtime_error on a
+// missing, truncated or foreign file.
+void save_parameters(const Model& m, const char* path);
+Model load_parameters(const char* path);
+
 // D4 helpers shared by setup, oracle and device upload.
 void d4_weights(const Model& m, int atom, double cn, double* w, double* dw);
 

@@ -78,6 +78,34 @@ class GFNFF:
         self._err = ""
         return True
 
+    def saveParameters(self, path) -> bool:
+        """Writes the set-up result of this molecule to a parameter file."""
+        st = self._lib.gfnff_save_parameters(self._h, str(path).encode())
+        if st != _lib.GFNFF_OK:
+            self._err = self._lib.gfnff_last_error(self._h).decode()
+            return False
+        return True
+
+    def setMoleculeFromParameters(self, path, Z, xyz_angstrom) -> bool:
+        """setMolecule with the set-up read from a parameter file made for this structure
+        (saveParameters or write_parameters); xyz_angstrom is the geometry evaluated until
+        updateGeometry is called."""
+        Z = np.ascontiguousarray(Z, dtype=np.int32)
+        X = np.ascontiguousarray(xyz_angstrom, dtype=np.float64).reshape(-1, 3)
+        if len(Z) != len(X):
+            raise ValueError("Z and geometry sizes differ")
+        st = self._lib.gfnff_setup_from_parameters(self._h, str(path).encode(), len(Z),
+                                                   Z.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
+        if st != _lib.GFNFF_OK:
+            self._err = self._lib.gfnff_last_error(self._h).decode()
+            return False
+        self._n = len(Z)
+        self._xyz = X.copy()
+        self._grad = np.zeros((self._n, 3))
+        self._masses = atomic_masses(Z)
+        self._err = ""
+        return True
+
     def updateGeometry(self, xyz_angstrom) -> bool:
         X = np.ascontiguousarray(xyz_angstrom, dtype=np.float64).reshape(-1, 3)
         if X.shape[0] != self._n:
@@ -218,3 +246,18 @@ class GFNFF:
             self.close()
         except Exception:
             pass
+
+
+def write_parameters(Z, xyz_angstrom, path, charge: int = 0, hbond: bool = True) -> None:
+    """Runs the GFN-FF set-up on the host and writes its parameter file (no GPU needed);
+    GFNFF.setMoleculeFromParameters reads it."""
+    lib = _lib.load()
+    Z = np.ascontiguousarray(Z, dtype=np.int32)
+    X = np.ascontiguousarray(xyz_angstrom, dtype=np.float64).reshape(-1, 3)
+    if len(Z) != len(X):
+        raise ValueError("Z and geometry sizes differ")
+    st = lib.gfnff_write_parameters(len(Z), Z.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                    X.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), int(charge),
+                                    1 if hbond else 0, str(path).encode())
+    if st != _lib.GFNFF_OK:
+        raise RuntimeError(lib.gfnff_last_error(None).decode())

@@ -69,6 +69,21 @@ gfnff_status gfnff_create(const gfnff_options* opts, gfnff_handle** out);
 gfnff_status gfnff_setup(gfnff_handle* h, int natoms, const int* Z, const double* xyz_angstrom,
                          int total_charge);
 
+/* Parameter file: the complete set-up result (topology, parameters, term lists) of the
+ * handle's molecule, so that a later run on the same structure skips the set-up.  Plays the
+ * role of curcuma's parameter caching (`<input>.param.json`, PARAMETER_CACHING.md) and
+ * topology export/import (ff_methods/gfnff_method.cpp:2515-2811); the format is this
+ * library's own binary image, read only by a build with the same record layouts.
+ * gfnff_save_parameters writes the model of a single-molecule handle after gfnff_setup
+ * (with the HB/XB lists of the last detection); gfnff_setup_from_parameters replaces
+ * gfnff_setup with a file (the file's set-up options apply) and refuses a file made for
+ * another structure (natoms and Z must match); gfnff_write_parameters runs the set-up on
+ * the host and writes the file without a handle or a GPU. */
+gfnff_status gfnff_save_parameters(gfnff_handle* h, const char* path);
+gfnff_status gfnff_setup_from_parameters(gfnff_handle* h, const char* path, int natoms, const int* Z);
+gfnff_status gfnff_write_parameters(int natoms, const int* Z, const double* xyz_angstrom, int total_charge,
+                                    int hbond, const char* path);
+
 /* Replaces updateGeometry + calculateEnergy(true) + copyGradientTo
  * (gfnff_method.cpp:1692-2226, computational_method.h:121-123).  energy and grad are
  * host pointers; grad may be NULL for energy only (the gradient is still computed);

@@ -865,6 +865,19 @@ oracle_handle* oracle_create(int n, const int* Z, const double* xyz_ang, int cha
     }
 }
 
+// the model read from a parameter file (the product's set-up cache) instead of a fresh set-up
+oracle_handle* oracle_create_from_parameters(const char* path)
+{
+    try {
+        auto* h = new oracle_handle;
+        h->m = load_parameters(path);
+        return h;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return nullptr;
+    }
+}
+
 void oracle_destroy(oracle_handle* h) { delete h; }
 const char* oracle_last_error(void) { return g_err.c_str(); }
 

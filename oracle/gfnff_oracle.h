@@ -19,6 +19,8 @@ typedef struct oracle_handle oracle_handle;
 // Runs the host setup (shared with the product) for n atoms, xyz in Angstrom.
 // Returns NULL on failure; oracle_last_error() tells why.
 oracle_handle* oracle_create(int n, const int* Z, const double* xyz_ang, int charge);
+// The model of a parameter file written by the library (gfnff_write_parameters); NULL on failure.
+oracle_handle* oracle_create_from_parameters(const char* path);
 void oracle_destroy(oracle_handle* h);
 const char* oracle_last_error(void);
 

@@ -28,6 +28,8 @@ def lib():
         c_v, c_i = ctypes.c_void_p, ctypes.c_int
         L.oracle_create.restype = c_v
         L.oracle_create.argtypes = [c_i, c_v, c_v, c_i]
+        L.oracle_create_from_parameters.restype = c_v
+        L.oracle_create_from_parameters.argtypes = [ctypes.c_char_p]
         L.oracle_destroy.argtypes = [c_v]
         L.oracle_last_error.restype = ctypes.c_char_p
         L.oracle_engrad.argtypes = [c_v, c_v, c_v, c_v, c_v, c_v, c_i]
@@ -49,6 +51,17 @@ class Oracle:
         self.h = lib().oracle_create(self.n, self.Z.ctypes.data, X.ctypes.data, int(charge))
         if not self.h:
             raise RuntimeError(lib().oracle_last_error().decode())
+
+    @classmethod
+    def from_parameters(cls, path, Z):
+        """The oracle over the model stored in a parameter file (for round-trip checks)."""
+        self = cls.__new__(cls)
+        self.Z = np.ascontiguousarray(Z, dtype=np.int32)
+        self.n = len(self.Z)
+        self.h = lib().oracle_create_from_parameters(str(path).encode())
+        if not self.h:
+            raise RuntimeError(lib().oracle_last_error().decode())
+        return self
 
     def engrad(self, xyz, nthreads=0):
         X = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)

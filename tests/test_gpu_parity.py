@@ -277,3 +277,27 @@ def test_kernels_per_evaluation(monkeypatch):
     assert g.setMolecule(Z, X)
     g.calculateEnergy(True)
     assert g.kernelsPerEvaluation() == -1
+
+
+def test_setup_from_parameter_file(tmp_path, monkeypatch):
+    """A handle set up from a parameter file evaluates like one set up from the structure (the
+    same model; only the order of the FP64 atomic sums differs between any two runs), and
+    refuses a file made for another structure."""
+    monkeypatch.setenv("GFNFF_EEQ_SOLVER", "library")   # no timing-dependent solver choice
+    Z, X = workloads.water_cluster(64, 9)
+    a = GFNFF()
+    assert a.setMolecule(Z, X)
+    path = tmp_path / "water64.param.bin"
+    assert a.saveParameters(path), a.getErrorMessage()
+    b = GFNFF()
+    assert b.setMoleculeFromParameters(path, Z, X), b.getErrorMessage()
+    Xk = X + np.random.default_rng(2).normal(scale=0.01, size=X.shape)
+    for g in (a, b):
+        g.updateGeometry(Xk)
+    ea, eb = a.calculateEnergy(True), b.calculateEnergy(True)
+    assert abs(ea - eb) < 1e-11 and np.abs(a.getGradient() - b.getGradient()).max() < 1e-12
+    c = GFNFF()
+    Zo = Z.copy()
+    Zo[0] = 7
+    assert not c.setMoleculeFromParameters(path, Zo, X)
+    assert "another structure" in c.getErrorMessage()
