@@ -40,13 +40,21 @@ class GFNFF:
     def __init__(self, precision: int = FP64, device: int = 0, hbond: bool = True,
                  hb_rmsd_bohr: float = 0.3, exact_gradient: bool = False):
         self._lib = _lib.load()
+        self._params = {"precision": "mixed" if precision == MIXED else "fp64", "gpu_device": device,
+                        "hbond": bool(hbond), "hb_rmsd_bohr": hb_rmsd_bohr,
+                        "exact_gradient": bool(exact_gradient), "threads": 1}
+        self._h = None
+        self._create()
+
+    def _create(self):
+        p = self._params
         opts = _lib.Options()
         self._lib.gfnff_default_options(ctypes.byref(opts))
-        opts.precision = precision
-        opts.device = device
-        opts.hbond = 1 if hbond else 0
-        opts.hb_rmsd_bohr = hb_rmsd_bohr
-        opts.gradient = 1 if exact_gradient else 0
+        opts.precision = MIXED if p["precision"] == "mixed" else FP64
+        opts.device = int(p["gpu_device"])
+        opts.hbond = 1 if p["hbond"] else 0
+        opts.hb_rmsd_bohr = float(p["hb_rmsd_bohr"])
+        opts.gradient = 1 if p["exact_gradient"] else 0
         h = ctypes.c_void_p()
         st = self._lib.gfnff_create(ctypes.byref(opts), ctypes.byref(h))
         if st != _lib.GFNFF_OK:
@@ -201,6 +209,83 @@ class GFNFF:
 
     def getErrorMessage(self) -> str:
         return self._err
+
+    def getCN(self) -> np.ndarray:
+        """Coordination numbers of the last evaluation (GFNFFComputationalMethod::getCN)."""
+        return self.getCoordinationNumbers()
+
+    def copyGradientTo(self, target) -> None:
+        """Gradient (Eh/bohr) into a preallocated N x 3 array (computational_method.h:121-123)."""
+        target[...] = self._grad
+
+    def hasGradient(self) -> bool:
+        return True
+
+    def NumGrad(self, dx: float = 1e-5) -> np.ndarray:
+        """Central-difference gradient of calculateEnergy in Eh/bohr, dx in Angstrom; restores
+        the current geometry and its results (one more evaluation) afterwards.
+        ComputationalMethod::NumGrad has this signature; its GFN-FF implementation keeps the
+        base version, which returns an empty matrix."""
+        X0 = self._xyz.copy()
+        G = np.zeros((self._n, 3))
+        for a in range(self._n):
+            for d in range(3):
+                for sgn in (1.0, -1.0):
+                    X = X0.copy()
+                    X[a, d] += sgn * dx
+                    self.updateGeometry(X)
+                    G[a, d] += sgn * self.calculateEnergy(False)
+        self.updateGeometry(X0)
+        self.calculateEnergy(True)
+        return G / (2.0 * dx) * 0.529177210903   # per Angstrom -> per bohr
+
+    def getBondOrders(self) -> np.ndarray:
+        """curcuma's GFN-FF keeps a zero vector of N(N-1)/2 bond orders
+        (ff_methods/gfnff_method.cpp:783); the same here."""
+        return np.zeros(self._n * (self._n - 1) // 2)
+
+    def getDipole(self) -> np.ndarray:
+        """(0, 0, 0), as GFNFFComputationalMethod::getDipole returns."""
+        return np.zeros(3)
+
+    def getMethodName(self) -> str:
+        return "gfnff"
+
+    def isThreadSafe(self) -> bool:
+        return False
+
+    def setThreadCount(self, threads: int) -> None:
+        """Recorded in the parameters; the per-geometry work runs on the GPU, the host set-up
+        uses OpenMP (OMP_NUM_THREADS)."""
+        self._params["threads"] = threads if threads > 0 else 1
+
+    def setParameters(self, params: dict) -> None:
+        """precision ("fp64"/"mixed"), gpu_device, hbond, hb_rmsd_bohr, exact_gradient, threads.
+        A new handle is made with them: call setMolecule again afterwards."""
+        unknown = set(params) - set(self._params)
+        if unknown:
+            raise KeyError(f"unknown parameters: {sorted(unknown)}")
+        new = dict(self._params, **params)
+        if new["precision"] not in ("fp64", "mixed"):
+            raise ValueError("precision must be 'fp64' or 'mixed'")
+        if {k: v for k, v in new.items() if k != "threads"} != \
+                {k: v for k, v in self._params.items() if k != "threads"}:
+            self.close()
+            self._params = new
+            self._create()
+        self._params = new
+
+    def getParameters(self) -> dict:
+        return dict(self._params)
+
+    def clearError(self) -> None:
+        self._err = ""
+
+    def getHBCount(self) -> int:
+        return len(self.topology(6, 4)) if self._n else 0
+
+    def getXBCount(self) -> int:
+        return len(self.topology(7, 3)) if self._n else 0
 
     # -- extras ----------------------------------------------------------------------
     def topology(self, kind: int, width: int) -> np.ndarray:

@@ -301,3 +301,36 @@ def test_setup_from_parameter_file(tmp_path, monkeypatch):
     Zo[0] = 7
     assert not c.setMoleculeFromParameters(path, Zo, X)
     assert "another structure" in c.getErrorMessage()
+
+
+def test_computational_method_interface():
+    """The rest of curcuma's ComputationalMethod interface on the Python mirror."""
+    g = golden("H2O")
+    Z, X = np.array(g["Z"]), np.array(g["xyz_angstrom"], dtype=float)
+    m = GFNFF(exact_gradient=True)
+    assert m.setMolecule(Z, X)
+    e = m.calculateEnergy(True)
+    assert m.getMethodName() == "gfnff" and m.hasGradient() and not m.isThreadSafe()
+    buf = np.empty((len(Z), 3))
+    m.copyGradientTo(buf)
+    assert np.array_equal(buf, m.getGradient())
+    assert np.array_equal(m.getCN(), m.getCoordinationNumbers())
+    assert m.getBondOrders().shape == (3,) and not m.getBondOrders().any()
+    assert not m.getDipole().any()
+    assert m.getHBCount() >= 0 and m.getXBCount() == 0
+    # exact mode: the analytic gradient is the derivative of the energy
+    G = m.getGradient()
+    assert np.abs(m.NumGrad(1e-4) - G).max() < 1e-6
+    assert np.abs(m.getGradient() - G).max() < 1e-12     # results of the restored geometry
+    assert m.calculateEnergy(True) == pytest.approx(e, abs=1e-12)
+    m.setThreadCount(4)
+    assert m.getParameters()["threads"] == 4
+    m.setParameters({"precision": "mixed", "exact_gradient": False})
+    assert m.getParameters()["precision"] == "mixed"
+    assert m.setMolecule(Z, X)
+    assert abs(m.calculateEnergy(True) - e) < 1e-6
+    assert not m.updateGeometry(X[:2]) and m.hasError()
+    m.clearError()
+    assert not m.hasError()
+    with pytest.raises(KeyError):
+        m.setParameters({"no_such_key": 1})
