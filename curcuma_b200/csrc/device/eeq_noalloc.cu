@@ -57,12 +57,39 @@ Scratch carve(double* base, int n)
     return s;
 }
 
+// Failure codes in meta[1]: every kernel after k_na_check returns early when it is set,
+// and k_na_expand turns it into the status (d_q is then left as the caller had it).
+constexpr int kFailNotSpd = 1;
+constexpr int kFailBadFragment = 2;
+
+// Validation pass: reads only d_frag and writes only the fragment counts (indexed by
+// ids already checked to lie in [0, nfrag)) and meta.  Flags an id outside [0, nfrag)
+// and a fragment id that no atom carries (its target charge would be lost).  One block.
+__global__ void k_na_check(int n, int nfrag, const int* frag, Scratch s)
+{
+    int* count = s.a2r;   // nfrag <= n ints, rewritten by k_na_prepare afterwards
+    for (int f = threadIdx.x; f < nfrag; f += blockDim.x) count[f] = 0;
+    if (threadIdx.x == 0) s.meta[1] = 0;
+    __syncthreads();
+    bool bad = false;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const int f = frag[i];
+        if (f < 0 || f >= nfrag) bad = true;
+        else atomicAdd(&count[f], 1);
+    }
+    __syncthreads();
+    for (int f = threadIdx.x; f < nfrag; f += blockDim.x)
+        if (count[f] == 0) bad = true;
+    if (bad) atomicOr(&s.meta[1], kFailBadFragment);
+}
+
 // fragment anchors (first atom), uniform q0 = qfrag/n_f, reduced index maps; one thread
-// (n <= kMaxAtoms).  Everything it reads later is written here first.
+// (n <= kMaxAtoms).  Everything it reads later is written here first.  Runs only after
+// k_na_check accepted every fragment id (a bad id would index outside the scratch).
 __global__ void k_na_prepare(int n, int nfrag, const double* xyz, const int* frag, const double* qfrag,
                              Scratch s)
 {
-    if (blockIdx.x != 0) return;
+    if (blockIdx.x != 0 || s.meta[1] != 0) return;
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
         s.pos[4 * i] = xyz[3 * i];
         s.pos[4 * i + 1] = xyz[3 * i + 1];
@@ -73,9 +100,7 @@ __global__ void k_na_prepare(int n, int nfrag, const double* xyz, const int* fra
     int* first = s.r2a + n;          // nfrag <= n ints of temporary space
     for (int f = 0; f < nfrag; ++f) first[f] = -1;
     for (int i = 0; i < n; ++i) if (first[frag[i]] < 0) first[frag[i]] = i;
-    // counts in a2r temporarily
-    for (int f = 0; f < nfrag; ++f) s.a2r[f] = 0;
-    for (int i = 0; i < n; ++i) s.a2r[frag[i]] += 1;
+    // a2r still holds the per-fragment atom counts of k_na_check (every count >= 1)
     for (int i = 0; i < n; ++i) s.q0[i] = qfrag[frag[i]] / (double)s.a2r[frag[i]];
     for (int i = 0; i < n; ++i) s.anchor[i] = first[frag[i]];
     int nred = 0;
@@ -84,14 +109,13 @@ __global__ void k_na_prepare(int n, int nfrag, const double* xyz, const int* fra
         else { s.a2r[i] = nred; s.r2a[nred++] = i; }
     }
     s.meta[0] = nred;
-    s.meta[1] = 0;
 }
 
 __global__ void k_na_matrix(int n, const double* alpha, const double* gam, Scratch s)
 {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = blockIdx.y;
-    if (j >= n) return;
+    if (j >= n || s.meta[1] != 0) return;
     double v;
     if (i == j) {
         v = gam[i] + 0.797884560802866 / sqrt(alpha[i]);
@@ -110,7 +134,7 @@ __global__ void k_na_residual(int n, const double* chi, const double* cnf, const
 {
     const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
-    if (i >= n) return;
+    if (i >= n || s.meta[1] != 0) return;
     double acc = 0.0;
     for (int j = lane; j < n; j += 32) acc += s.A[(size_t)i * n + j] * s.q0[j];
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
@@ -119,6 +143,7 @@ __global__ void k_na_residual(int n, const double* chi, const double* cnf, const
 
 __global__ void k_na_reduce(int n, Scratch s)
 {
+    if (s.meta[1] != 0) return;
     const int nred = s.meta[0];
     const int lc = blockIdx.x * blockDim.x + threadIdx.x;
     const int kc = blockIdx.y;
@@ -133,6 +158,7 @@ __global__ void k_na_reduce(int n, Scratch s)
 // Cholesky of M (row-major, lower triangle) and the two triangular solves, one block
 __global__ void __launch_bounds__(kThreads) k_na_cholesky_solve(Scratch s)
 {
+    if (s.meta[1] != 0) return;   // uniform over the block
     const int m = s.meta[0];
     __shared__ double inv;
     __shared__ int bad;
@@ -161,7 +187,7 @@ __global__ void __launch_bounds__(kThreads) k_na_cholesky_solve(Scratch s)
         __syncthreads();
     }
     if (bad) {
-        if (tid == 0) s.meta[1] = 1;
+        if (tid == 0) s.meta[1] = kFailNotSpd;
         return;
     }
     // L y = b (column sweep), then L^T x = y
@@ -182,11 +208,15 @@ __global__ void __launch_bounds__(kThreads) k_na_cholesky_solve(Scratch s)
     }
 }
 
+// q = q0 + B y; the status of the call.  On a failure (bad fragment id, no Cholesky
+// factor) only the status is written and d_q keeps the caller's contents.
 __global__ void k_na_expand(int n, const int* frag, Scratch s, double* q, int* status)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i == 0) *status = s.meta[1] ? GFNFF_NOT_SPD : GFNFF_OK;
-    if (i >= n) return;
+    const int fail = s.meta[1];
+    if (i == 0)
+        *status = (fail & kFailBadFragment) ? GFNFF_INVALID_ARG : (fail ? GFNFF_NOT_SPD : GFNFF_OK);
+    if (i >= n || fail != 0) return;
     const int rr = s.a2r[i];
     if (rr >= 0) {
         q[i] = s.q0[i] + s.b[rr];
@@ -221,14 +251,19 @@ extern "C" gfnff_status gfnff_eeq_charges_noalloc(int natoms, int nfrag, const d
         }
         base = g_addr[dev];
     }
+    // an error left pending by earlier, unrelated work stays the caller's to read: report
+    // it without launching (and without clearing it)
+    if (cudaPeekAtLastError() != cudaSuccess) return GFNFF_CUDA_ERROR;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const int n = natoms;
     Scratch sc = carve(base, n);
+    k_na_check<<<1, kThreads, 0, s>>>(n, nfrag, d_frag, sc);
     k_na_prepare<<<1, 256, 0, s>>>(n, nfrag, d_xyz_bohr, d_frag, d_qfrag, sc);
     k_na_matrix<<<dim3((n + 127) / 128, n), 128, 0, s>>>(n, d_alpha, d_gam, sc);
     k_na_residual<<<(n * 32 + 127) / 128, 128, 0, s>>>(n, d_chi, d_cnf, d_cn, sc);
     k_na_reduce<<<dim3((n + 127) / 128, n), 128, 0, s>>>(n, sc);
     k_na_cholesky_solve<<<1, kThreads, 0, s>>>(sc);
     k_na_expand<<<(n + 127) / 128, 128, 0, s>>>(n, d_frag, sc, d_q, d_status);
+    // nothing was pending before the launches, so an error now is one of them
     return cudaGetLastError() == cudaSuccess ? GFNFF_OK : GFNFF_CUDA_ERROR;
 }

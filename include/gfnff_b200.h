@@ -163,14 +163,20 @@ double gfnff_fma_peak_tflops(int device, int fp64);
  * start-up).  No counterpart in the reference.  Every buffer is a device pointer owned
  * by the caller: d_xyz_bohr (N*3), per-atom d_alpha (alpha^2 as in the EEQ matrix),
  * d_gam (hardness incl. corrections), d_chi (-chi + corrections), d_cnf, d_cn, d_frag
- * (0-based fragment ids), d_qfrag (nfrag target charges); outputs d_q (N) and d_status
- * (1 int, gfnff_status of the device solve: GFNFF_NOT_SPD when the reduced EEQ matrix
- * has no Cholesky factor).  Work is enqueued on `stream` (a cudaStream_t, NULL = legacy
- * default) without host synchronisation.  All intermediate storage is one file-scope
- * device array sized for GFNFF_NOALLOC_MAX_ATOMS atoms (about 17 MB, held by every GPU
- * that loads the library until exit); larger systems return GFNFF_INVALID_ARG.  The first
- * call on a device looks the array up (cudaGetSymbolAddress) and should come before any
- * stream capture.  All calls share the array: calls that overlap on the GPU race. */
+ * (0-based fragment ids, each in [0, nfrag) and each id used by at least one atom),
+ * d_qfrag (nfrag target charges); outputs d_q (N) and d_status (1 int, gfnff_status of
+ * the device solve: GFNFF_INVALID_ARG when a fragment id is out of range or unused,
+ * GFNFF_NOT_SPD when the reduced EEQ matrix has no Cholesky factor; on either failure
+ * d_q is not written).  The fragment ids are checked on the device, in a pass that reads
+ * them before anything is indexed by them.  Work is enqueued on `stream` (a
+ * cudaStream_t, NULL = legacy default) without host synchronisation.  All intermediate
+ * storage is one file-scope device array sized for GFNFF_NOALLOC_MAX_ATOMS atoms (about
+ * 17 MB, held by every GPU that loads the library until exit); larger systems return
+ * GFNFF_INVALID_ARG.  The first call on a device looks the array up
+ * (cudaGetSymbolAddress) and should come before any stream capture.  All calls share the
+ * array: calls that overlap on the GPU race.  A CUDA error already pending when the call
+ * starts is returned as GFNFF_CUDA_ERROR without launching anything and is left pending
+ * for the caller; an error of this call's own launches is returned and cleared. */
 #define GFNFF_NOALLOC_MAX_ATOMS 1024
 gfnff_status gfnff_eeq_charges_noalloc(int natoms, int nfrag, const double* d_xyz_bohr, const double* d_alpha,
                                        const double* d_gam, const double* d_chi, const double* d_cnf,

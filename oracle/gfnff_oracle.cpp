@@ -952,6 +952,9 @@ int oracle_atom_data(oracle_handle* h, int which, double* out)
         case 3: src = &m.gam; break;
         case 4: src = &m.chi_base; break;
         case 5: src = &m.cnf; break;
+        case 6:   // target charge of the atom's fragment
+            for (int i = 0; i < m.n; ++i) out[i] = m.qfrag[m.frag[i]];
+            return 0;
         default: return 1;
     }
     std::copy(src->begin(), src->end(), out);

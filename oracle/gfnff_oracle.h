@@ -41,7 +41,7 @@ int oracle_redetect_hbxb(oracle_handle* h, const double* xyz_ang);
 // Returns the record count; copies up to cap ints (count*width) into out when non-NULL.
 long oracle_list(oracle_handle* h, int kind, int* out, long cap);
 // Per-atom setup data: which = 0 qa (Phase-1 charges), 1 setup CN, 2 alpeeq, 3 gam,
-// 4 chi_base, 5 cnf.  Returns 0 on success.
+// 4 chi_base, 5 cnf, 6 target charge of the atom's fragment.  Returns 0 on success.
 int oracle_atom_data(oracle_handle* h, int which, double* out);
 // Number of fragments
 int oracle_nfrag(oracle_handle* h);
