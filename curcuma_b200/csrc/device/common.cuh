@@ -29,6 +29,9 @@ enum {
 
 constexpr int kBlock = 128;
 constexpr double kPi = 3.14159265358979323846;
+// mixed form: the EEQ solution is refined until the FP64 residual ||b - M y||_inf of the
+// reduced system is at most this (Hartree per charge unit)
+constexpr double kRefineTol = 1e-10;
 
 template <class T>
 struct DBuf {

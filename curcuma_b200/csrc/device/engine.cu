@@ -45,6 +45,7 @@ namespace gfnff {
 #include "k_bonded.cuh"
 #include "k_nonbonded.cuh"
 #include "k_eeq.cuh"
+#include "k_eeq_tc.cuh"
 #include "k_chol.cuh"
 #include "k_pcg.cuh"
 }  // namespace gfnff
@@ -323,6 +324,14 @@ struct Engine::Impl {
     int nbitems = 0;
     int batch_smem_max = 0, batch_grid = 1;
     size_t batch_smem = 0;
+    // mixed form: molecules with kWarpMaxRed < nr <= kTcMaxRed are factored on the tensor
+    // cores (FP32, 3xTF32 updates) and refined in FP64 against their FP64 lower tiles M64
+    bool batch_tc = false;
+    DBuf<double> M64;
+    DBuf<long long> m64off;
+    DBuf<int> refine;      // largest number of refinement corrections of the last launch
+    DBuf<int4> tc_tiles;   // {molecule, R, C} of every FP64 tile (k_eeq_tc_tiles)
+    int n_tc_tiles = 0;
     // bonded lists
     DBuf<int> b_i, b_j, b_h, b_off, b_hb;
     DBuf<double> b_fc, b_al, b_r0i, b_r0j, b_cki, b_ckj, b_sh, b_ff;
@@ -803,12 +812,18 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
                              [&](int x, int y) { return roff[x + 1] - roff[x] > roff[y + 1] - roff[y]; });
             P.border.upload(ord);
             P.bnext.alloc(1);
+            // mixed form: the tensor-core path (k_eeq_tc.cuh) for every molecule of at most
+            // kTcMaxRed unknowns (GFNFF_BATCH_TC=0: the FP64 paths)
+            const char* etc = std::getenv("GFNFF_BATCH_TC");
+            P.batch_tc = P.opt.precision == 1 && !(etc && !std::strcmp(etc, "0"));
             // work items: large molecules one per block, small ones in packs of kWarpMols
-            // (one warp each)
+            // (one warp each, FP64); in the mixed form every molecule is a block item (one
+            // small molecule on a block's tensor-core path measured far below a warp item of
+            // eight, whose column-by-column FP64 updates are latency-bound)
             std::vector<int4> items;
             for (int k = 0; k < nm;) {
                 const int nr = roff[ord[k] + 1] - roff[ord[k]];
-                if (nr > kWarpMaxRed || mols[ord[k]]->n > kWarpAtoms) {
+                if (P.batch_tc || nr > kWarpMaxRed || mols[ord[k]]->n > kWarpAtoms) {
                     items.push_back(make_int4(k, 1, 0, 0));
                     ++k;
                 } else {
@@ -843,6 +858,41 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
                             (big > smax ? (size_t)budget : (size_t)fit * (fit + 3) / 2 + 2 * (size_t)(fit + 1) + 2)) *
                            8;
             P.batch_smem = std::max<size_t>(P.batch_smem, (size_t)kWarpMols * kWarpRegion * 8);
+            // mixed form: FP64 lower tiles of the molecules of the tensor-core path
+            if (P.batch_tc) {
+                // molecules with at most kTcMaxRed unknowns: their FP64 tiles (built at full
+                // occupancy by k_eeq_tc_tiles)
+                std::vector<long long> o64(nm, 0);
+                std::vector<int4> tl;
+                long long tot = 0;
+                for (int m = 0; m < nm; ++m) {
+                    const int nr = roff[m + 1] - roff[m];
+                    o64[m] = tot;
+                    if (nr < 1 || nr > kTcMaxRed) continue;
+                    const int T = (nr + 31) / 32;
+                    for (int R = 0; R < T; ++R)
+                        for (int C = 0; C <= R; ++C) tl.push_back(make_int4(m, R, C, 0));
+                    tot += (long long)T * (T + 1) / 2 * 1024;
+                }
+                P.m64off.upload(o64);
+                P.M64.alloc((size_t)std::max<long long>(1, tot));
+                P.tc_tiles.upload(tl);
+                P.n_tc_tiles = (int)tl.size();
+                // work items by estimated time, longest first (measured on the 512-conformer
+                // batch: a tensor-core molecule ~0.75 us per unknown, a warp item of eight
+                // small FP64 molecules ~2.5x a tensor-core molecule of its largest size, the
+                // FP64 block path ~2x): the long warp items no longer end the queue
+                auto cost = [&](const int4& it) {
+                    const int nr0 = roff[ord[it.x] + 1] - roff[ord[it.x]];   // largest of the item
+                    if (it.z) return 1.9 * nr0;
+                    return nr0 <= kTcMaxRed ? 0.75 * nr0 : 1.5 * nr0;
+                };
+                std::stable_sort(items.begin(), items.end(),
+                                 [&](const int4& a, const int4& b) { return cost(a) > cost(b); });
+                P.bitems.upload(items);
+                P.refine.alloc(1);
+                P.batch_smem = std::max<size_t>(P.batch_smem, (size_t)kTcSmemBytes);
+            }
             CK(cudaFuncSetAttribute((const void*)k_eeq_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)P.batch_smem));
             int per_sm = 0, nsm = 0;
@@ -1339,7 +1389,8 @@ bool Engine::switch_to_lu()
 
 bool Engine::switch_to_direct()
 {
-    if (p_->nmol != 1 || p_->solver != Impl::SOLVE_PCG) return false;
+    if (p_->nmol != 1) return false;
+    if (p_->solver != Impl::SOLVE_PCG && !(p_->solver == Impl::SOLVE_BATCH && p_->batch_tc)) return false;
     p_->drop_graphs();
     p_->solver = Impl::SOLVE_LIBRARY;
     return true;
@@ -1359,6 +1410,13 @@ const char* Engine::solver_name() const
 
 int Engine::eeq_iterations()
 {
+    const bool batched = p_->nmol != 1 || (!p_->use_lu && p_->solver == Impl::SOLVE_BATCH);
+    if (batched && p_->batch_tc) {   // refinement corrections of the tensor-core path
+        int it = 0;
+        CK(cudaStreamSynchronize(p_->stream));
+        CK(cudaMemcpy(&it, p_->refine.p, sizeof(int), cudaMemcpyDeviceToHost));
+        return it;
+    }
     if (p_->nmol != 1 || p_->use_lu || p_->solver != Impl::SOLVE_PCG) return 0;
     int it = 0;
     CK(cudaStreamSynchronize(p_->stream));
@@ -1605,7 +1663,12 @@ void Engine::launch_body()
         CK(cudaMemsetAsync(P.bnext.p, 0, sizeof(int), s));
         if (fork && !early) CK(cudaEventRecord(P.ev_fork1, s));   // single molecule, batched solver
         EEQBatch B{P.roff.p, P.moff.p, P.border.p, P.bitems.p, P.nbitems, P.bnext.p, P.batch_smem_max, P.red2atom.p,
-                   P.anchor.p, P.qlist.p, P.nq, P.q0.p, P.M.p, P.bvec.p, P.info.p};
+                   P.anchor.p, P.qlist.p, P.nq, P.q0.p, P.M.p, P.bvec.p, P.info.p,
+                   P.batch_tc ? 1 : 0, P.M64.p, P.m64off.p, kRefineTol, P.refine.p};
+        if (P.batch_tc) {
+            CK(cudaMemsetAsync(P.refine.p, 0, sizeof(int), s));
+            if (P.n_tc_tiles) k_eeq_tc_tiles<<<P.n_tc_tiles, 256, 0, s>>>(V, B, P.tc_tiles.p);
+        }
         k_eeq_batch<<<P.batch_grid, 512, P.batch_smem, s>>>(V, B);
         side_after();
     }

@@ -201,7 +201,17 @@ struct EEQBatch {
     double* M;              // global copies for the large molecules
     double* y;              // solution (reduced index space)
     int* info;
+    // mixed form: molecules with kWarpMaxRed < nr <= kTcMaxRed take the tensor-core
+    // factorisation with FP64 refinement (k_eeq_tc.cuh); 0 in the FP64 form
+    int tc;
+    double* M64;            // FP64 lower tiles of those molecules
+    const long long* m64off;
+    double tol;             // refinement target ||b - M y||_inf
+    int* refine;            // largest number of refinement corrections of the launch
 };
+
+__device__ void tc_solve(const View& V, const EEQBatch& P, int m, double* S);
+constexpr int kTcMaxRedFwd = 304;   // kTcMaxRed of k_eeq_tc.cuh
 
 // one molecule's atoms staged in shared memory: positions, alpha, EEQ diagonal, the
 // reduced index maps (local atom indices) and the rhs row.  For a molecule of one
@@ -619,7 +629,7 @@ __device__ void warp_solve(const View& V, const EEQBatch& P, int m, double* R)
 
 __global__ void __launch_bounds__(512) k_eeq_batch(View V, EEQBatch P)
 {
-    extern __shared__ double S[];
+    extern __shared__ __align__(16) double S[];
     __shared__ int4 item;
     for (;;) {
         __syncthreads();
@@ -640,6 +650,10 @@ __global__ void __launch_bounds__(512) k_eeq_batch(View V, EEQBatch P)
         double* y = P.y + r0;
         if (nr == 0) {
             if (threadIdx.x == 0) P.info[m] = 0;
+            continue;
+        }
+        if (P.tc && nr <= kTcMaxRedFwd) {
+            tc_solve(V, P, m, S);
             continue;
         }
         bool ok;
