@@ -963,4 +963,29 @@ int oracle_atom_data(oracle_handle* h, int which, double* out)
 
 int oracle_nfrag(oracle_handle* h) { return h ? h->m.nfrag : -1; }
 
+long oracle_term_params(oracle_handle* h, int kind, double* out, long cap)
+{
+    if (!h) return -1;
+    const Model& m = h->m;
+    std::vector<double> v;
+    if (kind == 0) {
+        for (const auto& b : m.bonds) v.insert(v.end(), {(double)b.i, (double)b.j, b.fc, b.alpha, b.r0_setup, b.rabshift, b.ff});
+    } else if (kind == 1) {
+        for (const auto& a : m.angles) v.insert(v.end(), {(double)a.i, (double)a.j, (double)a.k, a.fc, a.theta0});
+    } else if (kind == 2) {
+        for (int t = 0; t < (int)m.torsions.size(); ++t) {
+            const auto& q = m.torsions[t];
+            v.insert(v.end(), {(double)q.i, (double)q.j, (double)q.k, (double)q.l, q.V, q.n, q.phi0,
+                               t < m.n_primary_torsions ? 1.0 : 0.0});
+        }
+    } else if (kind == 3) {
+        for (const auto& q : m.inversions) v.insert(v.end(), {(double)q.i, (double)q.j, (double)q.k, (double)q.l, q.fc, q.omega0, (double)q.type});
+    } else {
+        return -1;
+    }
+    const int width = kind == 0 ? 7 : (kind == 1 ? 5 : (kind == 2 ? 8 : 7));
+    if (out) std::copy(v.begin(), v.begin() + std::min<long>(cap, (long)v.size()), out);
+    return (long)v.size() / width;
+}
+
 }  // extern "C"

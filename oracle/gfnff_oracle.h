@@ -45,6 +45,12 @@ long oracle_list(oracle_handle* h, int kind, int* out, long cap);
 int oracle_atom_data(oracle_handle* h, int which, double* out);
 // Number of fragments
 int oracle_nfrag(oracle_handle* h);
+// Per-term set-up parameters as doubles (indices as doubles), for comparisons with the
+// reference's fixture parameter lists: kind 0 bonds (i, j, fc, alpha, r0 at the set-up CN in
+// bohr, shift, ff), 1 angles (i, j, k, fc, theta0 rad; j the centre), 2 torsions (i, j, k, l, V, n, phi0,
+// primary flag), 3 inversions (i, j, k, l, fc, omega0, type).  Returns the record count;
+// copies up to cap doubles into out when non-NULL.
+long oracle_term_params(oracle_handle* h, int kind, double* out, long cap);
 
 #ifdef __cplusplus
 }

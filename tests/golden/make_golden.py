@@ -4,13 +4,17 @@
 Sources (curcuma test suite, read from a checkout given on the command line):
 * ``test_cases/reference_data/*.ref.json``: geometry (bohr), per-term energies, Phase-2
   charges, CN, hybridisation, gradient norm for 15 molecules (xtb GFN-FF values that
-  curcuma's test_gfnff_validation.cpp checks against, tolerances at :175-215).
+  curcuma's test_gfnff_validation.cpp checks against, tolerances at :175-215), and the
+  per-term parameter lists of the same files: bonds (atoms, r0 in Angstrom from the set-up
+  formula (ra + rb) ff + shift, kbond = the exponent, prefactor = the force constant),
+  angles (centre first, phi0 in degrees, fc), torsions (atoms, n, phi0, V).
 * ``test_cases/molecules/larger/{complex,caffeine}.xyz`` with the CLI golden totals of
   ``test_cases/cli/gfnff/01_complex_gfnff_singlepoint/run_test.sh:19-30`` and
   ``test_cases/cli/gfnff_gpu/01_gfnff_gpu_singlepoint/run_test.sh:17-18``.
 
 Output: one JSON per molecule in this directory with Z, xyz (Angstrom) and the
-reference values.  Usage: ``python make_golden.py /path/to/curcuma``.
+reference values.  Usage: ``python make_golden.py /path/to/curcuma`` (the checkout is a
+required argument).
 """
 import json
 import re
@@ -47,8 +51,15 @@ def main(root: str):
             "gradient_norm": d.get("gradients", {}).get("norm"),
             "cn": d.get("topology", {}).get("coordination_numbers", []),
             "hybridization": d.get("topology", {}).get("hybridizations", []),
+            "bonds": [[b["atoms"][0], b["atoms"][1], b["r0"], b["kbond"], b["prefactor"]] for b in d.get("bonds", [])],
+            "angles": [[a["atoms"][0], a["atoms"][1], a["atoms"][2], a["phi0"], a["fc"]] for a in d.get("angles", [])],
+            "torsions": [[*t["atoms"], t["n"], t["phi0"], t["V"]] for t in d.get("torsions", [])],
         }
-        (out / f"{rec['name']}.json").write_text(json.dumps(rec, indent=1))
+        text = json.dumps({k: v for k, v in rec.items() if k not in ("bonds", "angles", "torsions")}, indent=1)
+        # parameter lists one record per line
+        lists = ",\n".join(f' "{k}": [' + ",".join(json.dumps(r) for r in rec[k]) + "]"
+                            for k in ("bonds", "angles", "torsions"))
+        (out / f"{rec['name']}.json").write_text(text[:-2] + ",\n" + lists + "\n}")
     cli = [("complex", "test_cases/cli/gfnff/01_complex_gfnff_singlepoint/run_test.sh",
             "REFERENCE_TOTAL_ENERGY", 5e-6),
            ("caffeine", "test_cases/cli/gfnff_gpu/01_gfnff_gpu_singlepoint/run_test.sh", None, 2e-5)]
@@ -68,4 +79,6 @@ def main(root: str):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py /path/to/curcuma-checkout")
+    main(sys.argv[1])

@@ -39,6 +39,8 @@ def lib():
         L.oracle_list.restype = ctypes.c_long
         L.oracle_atom_data.argtypes = [c_v, c_i, c_v]
         L.oracle_nfrag.argtypes = [c_v]
+        L.oracle_term_params.argtypes = [c_v, c_i, c_v, ctypes.c_long]
+        L.oracle_term_params.restype = ctypes.c_long
         _lib = L
     return _lib
 
@@ -89,6 +91,14 @@ class Oracle:
         out = np.zeros(self.n)
         lib().oracle_atom_data(self.h, which, out.ctypes.data)
         return out
+
+    def term_params(self, kind):
+        """Set-up parameters per term (see oracle_term_params): a (count, width) array."""
+        width = {0: 7, 1: 5, 2: 8, 3: 7}[kind]
+        cnt = lib().oracle_term_params(self.h, kind, None, 0)
+        out = np.zeros(max(1, cnt * width))
+        lib().oracle_term_params(self.h, kind, out.ctypes.data, out.size)
+        return out[:cnt * width].reshape(cnt, width)
 
     @property
     def nfrag(self):

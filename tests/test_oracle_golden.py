@@ -67,3 +67,80 @@ def test_polymer_total():
     ref = sum(g["energy_components"].values())
     # reference total tolerance of the validation runner (1e-4 Eh)
     assert abs(T["total"] - ref) < 1e-4
+
+
+# ---- the shared set-up against the fixtures' per-term parameter lists ------------------
+# The reference fixtures (xtb GFN-FF values) list every bond, angle and primary torsion with
+# its parameters.  The set-up (shared by the product library and the oracle) must produce
+# the same lists and the same parameters; the tolerances are the printed precision of the
+# fixtures, except r0, which the fixture computes from xtb's own set-up CN (agreement 3e-5 A).
+BOHR_A = 0.529177210903
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_fixture_bond_list_and_parameters(name):
+    g = golden(name)
+    o = Oracle(g["Z"], g["xyz_angstrom"])
+    ours = {(int(min(r[0], r[1])), int(max(r[0], r[1]))): r for r in o.term_params(0)}
+    ref = {(min(b[0], b[1]), max(b[0], b[1])): b for b in g["bonds"]}
+    assert set(ours) == set(ref), f"{name}: bond lists differ"
+    for k, (_, _, r0, kbond, pref) in ref.items():
+        i, j, fc, alpha, r0_rt, shift, ff = ours[k]
+        assert abs(fc - pref) < 5e-8, (name, k, fc, pref)            # force constant
+        assert abs(alpha - kbond) < 1e-7, (name, k, alpha, kbond)    # exponent
+        # the fixture's r0 is the set-up formula (ra + rb) ff + shift; the per-step formula
+        # (ra + rb + shift) ff differs from it by shift (ff - 1)
+        assert abs((r0_rt - shift * (ff - 1.0)) * BOHR_A - r0) < 5e-5, (name, k)
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_fixture_angle_list_and_parameters(name):
+    g = golden(name)
+    o = Oracle(g["Z"], g["xyz_angstrom"])
+    ours = {(int(r[1]), int(min(r[0], r[2])), int(max(r[0], r[2]))): r for r in o.term_params(1)}
+    ref = {(a[0], min(a[1], a[2]), max(a[1], a[2])): a for a in g["angles"]}   # centre first
+    assert set(ours) == set(ref), f"{name}: angle lists differ"
+    for k, (_, _, _, phi0, fc) in ref.items():
+        assert abs(np.degrees(ours[k][4]) - phi0) < 1e-5, (name, k)
+        assert abs(ours[k][3] - fc) < 5e-8, (name, k)
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_fixture_torsion_list_and_parameters(name):
+    """The fixtures list the primary torsions; curcuma adds extra torsions
+    (ff_workspace_gfnff.cpp:388-487, calcExtraTorsions) on quadruples of the primary list,
+    which xtb's fixture does not print: triose 14, complex 4, polymer 601 extra terms."""
+    g = golden(name)
+    o = Oracle(g["Z"], g["xyz_angstrom"])
+    T = o.term_params(2)
+    prim = T[T[:, 7] == 1.0]
+    assert len(prim) == len(g["torsions"]), name
+
+    def key(i, j, k, l):   # a dihedral read in either direction
+        return (j, k, i, l) if j < k else (k, j, l, i)
+
+    ours = {}
+    for r in prim:
+        ours.setdefault(key(*map(int, r[:4])), []).append(r)
+    ref = {}
+    for t in g["torsions"]:
+        ref.setdefault(key(*t[:4]), []).append(t)
+    assert set(ours) == set(ref), f"{name}: torsion quadruples differ"
+    for k, terms in ref.items():
+        assert len(ours[k]) == len(terms)
+        for t in terms:
+            n, phi0, V = t[4], t[5], t[6]
+            match = [r for r in ours[k] if r[5] == n and abs(r[6] - phi0) < 1e-9 and abs(r[4] - V) < 5e-7]
+            assert match, (name, k, t)
+    # the extra torsions sit on quadruples of the primary list
+    for r in T[T[:, 7] == 0.0]:
+        assert key(*map(int, r[:4])) in ours
+
+
+@pytest.mark.parametrize("name", [n for n in golden_names() if golden(n)["cn"]])
+def test_fixture_coordination_numbers(name):
+    """Set-up CN against the fixture's CN (printed to 0.01; the reference test's bar is
+    |dCN| < 0.01, test_gfnff_validation.cpp:128-145)."""
+    g = golden(name)
+    o = Oracle(g["Z"], g["xyz_angstrom"])
+    assert np.abs(o.atom_data(1) - np.array(g["cn"])).max() < 0.01
