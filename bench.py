@@ -1,9 +1,12 @@
 #!/usr/bin/env python3
 """GFN-FF energy + gradient throughput on B200.
 
-Default workload: a seeded 1000-water cluster (3000 atoms, 1000 fragments, 1.0 g/cm^3),
-mixed form, with the FP64 form measured beside it.  One step = one energy + analytic
-gradient evaluation of a fresh geometry (MD-like perturbation of the cluster).
+Default workload: the 20,480-atom cluster (6000 H2O + 40 C20H42, 6040 fragments; the largest
+single-GPU configuration and one of the two the mixed-vs-FP64 target is quoted on), mixed
+form, with the FP64 form measured beside it; the 512-conformer batch (20-300 atoms, the
+other target configuration) is measured in the same run and reported under "configs".  One
+step = one energy + analytic gradient evaluation of a fresh geometry (MD-like perturbation of
+the structure; for the batch, of every molecule).
 
 * ``value``: evaluations/s with coordinates resident in HBM, through the device entry
   point ``gfnff_energy_and_gradient_device``; each step timed with CUDA events on the
@@ -12,13 +15,18 @@ gradient evaluation of a fresh geometry (MD-like perturbation of the cluster).
   (host coordinates in, energy + gradient + terms out, copies inside the timed region).
 * ``roofline``: the dominant phase of the step against its arithmetic (FP64 FMA, measured
   by the library's microbenchmark) or HBM (MEASURED_PEAKS.json) bound.
-* ``cpu_baseline``: the CPU oracle (a restatement of curcuma's CPU gfnff path, all host
-  threads) on the same structure; rank 0 at N=1 only.
+* ``error_vs_oracle``: both forms against the CPU oracle (FP64 restatement of curcuma's CPU
+  path) at the workload's own geometry, computed in the CPU-baseline leg.
+* ``cpu_baseline``: the CPU oracle on the same workload at all host threads and at one
+  thread (bounded samples: whole evaluations for the single structures, a time-bounded
+  number of molecules for the batch); rank 0 at N=1 only.
 
 ``--impl reference`` times that CPU restatement alone as the reference arm (the
 reference's own CPU code cannot be built here: Eigen and friends are fetched at configure
-time).  Multi-GPU: ``--gpus N`` under torchrun runs independent replicas (weak scaling, no
-collective on the data path); timings are reduced with MAX over ranks.
+time).  Multi-GPU: ``--gpus N`` under torchrun runs independent replicas of the single
+structures (weak scaling, no collective on the data path) and splits one conformer ensemble
+into cost-balanced molecule shards gathered on rank 0; timings are reduced with MAX over
+ranks.
 """
 import argparse
 import ctypes
@@ -44,7 +52,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", type=int, default=2)
+    ap.add_argument("--config", type=int, default=5)
+    ap.add_argument("--also", default="4",
+                    help="comma-separated further configs measured in the same run ('' = none)")
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", action="store_true",
@@ -53,11 +63,14 @@ def parse():
     return ap.parse_args()
 
 
-def workload(cfg, rank=0):
-    """The structure(s) of a config.  Under torchrun the conformer batch is a molecule shard
-    per rank: every rank evaluates a batch of its own (seed 1004 + 1000 rank), so per-GPU work
-    stays fixed as ranks are added (no collective on the data path)."""
+def workload(cfg, rank=0, world=1):
+    """The structure(s) of a config.  Under torchrun the single structures are replicas (every
+    rank evaluates the same structure) and the conformer batch is one ensemble (seed 1004)
+    split into cost-balanced molecule shards, one per rank (``shard_by_cost``); the fourth
+    entry of a batch is (molecules of this rank, their indices in the ensemble, the
+    ensemble)."""
     from curcuma_b200 import workloads as W
+    from curcuma_b200.sharding import shard_by_cost
     if cfg == 1:
         return "n-C64H130 all-trans, 0.05 A noise (seed 1001)", *W.alkane(64, 1001)
     if cfg == 2:
@@ -67,11 +80,13 @@ def workload(cfg, rank=0):
     if cfg == 5:
         return "6000 H2O + 40 C20H42 (seed 1005)", *W.large_cluster(6000, 40, 20, 1005)
     if cfg == 4:
-        seed = 1004 + 1000 * rank
-        mols = W.conformer_batch(512, seed)
+        ens = W.conformer_batch(512, 1004)
+        idx = shard_by_cost([len(z) for z, _ in ens], world)[rank]
+        mols = [ens[i] for i in idx]
         Z = np.concatenate([z for z, _ in mols])
         X = np.concatenate([x for _, x in mols])
-        return f"512 saturated C/N/O chains, 20-300 atoms log-uniform (seed {seed})", Z, X, mols
+        return ("512 saturated C/N/O chains, 20-300 atoms log-uniform (seed 1004)", Z, X,
+                (mols, idx, ens))
     raise SystemExit(f"unknown config {cfg}")
 
 
@@ -215,49 +230,99 @@ def cpu_model():
     return "unknown"
 
 
-def cpu_oracle_rate(Z, X, steps, warmup, min_seconds=0.0, max_steps=64):
-    """Evaluations/s of the CPU oracle: at least `steps` evaluations, more (up to max_steps)
-    until min_seconds have passed.  Returns (rate, seconds, evaluations)."""
+def oracle_results(Z, X, mols, nthreads=0):
+    """The CPU oracle at the workload's own geometry: (total energies per molecule,
+    gradient N x 3, seconds of the oracle evaluations)."""
     from tests.oracle_api import Oracle
+    parts = mols if mols else [(Z, X)]
+    E, G, secs = [], [], 0.0
+    for z, x in parts:
+        o = Oracle(z, x)
+        t = time.perf_counter()
+        T, g, q, cn = o.engrad(x, nthreads)
+        secs += time.perf_counter() - t
+        E.append(T["total"])
+        G.append(g)
+    return np.array(E), np.concatenate(G), secs
+
+
+def cpu_rate(Z, X, mols, nthreads, budget_s, max_evals=64):
+    """Evaluations/s of the CPU oracle on a bounded sample of the workload: whole evaluations
+    of the structure (at least one, more while the budget lasts), or molecules of the batch
+    in ensemble order until the budget is spent (oracle set-up not timed).  Returns
+    (rate, seconds, evaluations, description)."""
+    from tests.oracle_api import Oracle
+    if mols:
+        k, secs = 0, 0.0
+        while secs < budget_s and k < len(mols):
+            z, x = mols[k]
+            o = Oracle(z, x)
+            t = time.perf_counter()
+            o.engrad(perturbed(x, 2000 + k), nthreads)
+            secs += time.perf_counter() - t
+            k += 1
+        return k / secs, secs, k, f"{k} molecules of the ensemble, one E+grad each"
     o = Oracle(Z, X)
-    for k in range(warmup):
-        o.engrad(perturbed(X, 1000 + k))
     t = time.perf_counter()
     k = 0
-    while k < steps or (time.perf_counter() - t < min_seconds and k < max_steps):
-        o.engrad(perturbed(X, 2000 + k))
+    while k < 1 or (time.perf_counter() - t < budget_s and k < max_evals):
+        o.engrad(perturbed(X, 2000 + k), nthreads)
         k += 1
     dt = time.perf_counter() - t
-    return k / dt, dt, k
+    return k / dt, dt, k, f"{k} full E+grad evaluation(s) of the structure"
+
+
+def cpu_baseline(Z, X, mols, budget_s=20.0, t1_limit_s=60.0):
+    """T = all host threads and T = 1 (the latter only where one evaluation at one thread
+    fits t1_limit_s, estimated from the all-thread time)."""
+    threads = os.cpu_count()
+    rate, dt, k, what = cpu_rate(Z, X, mols, 0, budget_s)
+    out = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port", "cpu": cpu_model(),
+           "sample": f"{what} ({dt:.1f} s)", "what": "CPU restatement of curcuma's gfnff path (oracle/)"}
+    est1 = (dt / k) * threads
+    if mols or est1 <= t1_limit_s:
+        r1, d1, k1, w1 = cpu_rate(Z, X, mols, 1, budget_s)
+        out["t1"] = {"value": r1, "unit": UNIT, "cores": 1, "sample": f"{w1} ({d1:.1f} s)"}
+    else:
+        out["t1"] = {"value": None, "cores": 1,
+                     "skipped": f"one evaluation at one thread estimated at {est1:.0f} s"}
+    return out
 
 
 def run_reference(args):
+    """The reference arm: the CPU restatement of curcuma's path on all host threads, on the
+    default workload; a bounded sample (at least one whole evaluation, at most ~60 s of
+    evaluations, or molecules of the batch) stands for --steps K (echoed as given)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    desc, Z, X = workload(args.config)
+    wl = workload(args.config)
+    desc, Z, X = wl[:3]
+    mols = wl[3][0] if len(wl) > 3 else None
     threads = os.cpu_count()
-    rate, dt, _ = cpu_oracle_rate(Z, X, args.steps, args.warmup)
+    rate, dt, k, what = cpu_rate(Z, X, mols, 0, 60.0)
     line = {"metric": METRIC, "value": rate, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / rate,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
             "config": {"workload": f"config {args.config}: {desc}", "natoms": int(len(Z))},
             "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "port", "cpu": cpu_model(),
-                             "sample": f"{args.steps} full E+grad evaluations of the workload"},
+                             "sample": f"{what} ({dt:.1f} s); --steps/--warmup bound nothing here"},
             "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "note": "CPU restatement of curcuma's gfnff path (oracle/), all host threads; the "
                     "reference's own build needs network-fetched Eigen and is unavailable here"}
     print(json.dumps(line), flush=True)
 
 
-def measure(args, precision, Z, X, torch, dist, world, local, mols=None):
+def measure(args, precision, Z, X, torch, dist, world, local, mols=None, units=None):
     """Device-timed and end-to-end throughput of one precision form on the workload
-    (molecule evaluations per second; a batch handle evaluates all molecules per step)."""
+    (molecule evaluations per second; a batch handle evaluates all molecules per step).
+    units: molecule evaluations per step over all ranks (default: world x this rank's)."""
     from curcuma_b200 import GFNFF, _lib
 
     n = len(Z)
     nmol = len(mols) if mols else 1
+    units = units if units is not None else world * nmol
     gpu = GFNFF(precision=0 if precision == "fp64" else 1, device=local)
     t0 = time.perf_counter()
     ok = gpu.setMoleculeBatch(mols) if mols else gpu.setMolecule(Z, X)
@@ -341,9 +406,9 @@ def measure(args, precision, Z, X, torch, dist, world, local, mols=None):
     clk = clocks.stop()
     if world > 1:
         e2e_s = max_over_ranks(e2e_s, dist, "cuda")
-    return {"gpu": gpu, "value": world * nmol * steps / (total_ms * 1e-3), "total_ms": total_ms, "step_ms": step_ms,
+    return {"gpu": gpu, "value": units * steps / (total_ms * 1e-3), "total_ms": total_ms, "step_ms": step_ms,
             "phase_avg": {k: v / steps for k, v in zip(_lib.PHASES, phases)}, "status": worst,
-            "e2e": {"value": world * nmol * steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 3 * n * 8,
+            "e2e": {"value": units * steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 3 * n * 8,
                     "d2h_bytes_per_step": (3 * n + 16 * nmol) * 8 + 4 * nmol},
             "clocks": clk, "setup_s": setup_s, "solver": gpu.eeqSolver(), "iters": gpu.eeqIterations(),
             "kernels_per_eval": kpe}
@@ -417,6 +482,120 @@ def fd_check(gpu, X, n_atoms=64, h_bohr=1e-4):
             "rms_err_eh_per_bohr": float(np.sqrt(np.mean(np.square(err))))}
 
 
+def run_config(args, cfg, torch, dist, world, rank, local):
+    """Both precision forms on one config: device-timed and end-to-end throughput, phase split,
+    roofline of the dominant phase, both forms at the workload's own geometry (gathered in
+    ensemble order for a sharded batch), and at N=1 the CPU leg (the oracle's results for the
+    error of both forms, and the timed CPU baselines).  Returns rank 0's summary (None on the
+    other ranks); every rank takes the same collective steps."""
+    from curcuma_b200.sharding import gather_ensemble
+
+    wl = workload(cfg, rank, world)
+    desc, Z, X = wl[:3]
+    shard = wl[3] if len(wl) > 3 else None
+    mols = shard[0] if shard else None
+    n = len(Z)
+    units = len(shard[2]) if shard else world
+    forms = [args.precision] + [p for p in ("mixed", "fp64") if p != args.precision]
+    res = {p: measure(args, p, Z, X, torch, dist, world, local, mols, units=units) for p in forms}
+    main = res[args.precision]
+    gpu = main["gpu"]
+    natoms, nfrag = gpu.sizes()
+    # both forms at the workload's own geometry: energies per molecule and gradients
+    at_x = {}
+    for p in forms:
+        g = res[p]["gpu"]
+        g.updateGeometry(X)
+        e = np.atleast_1d(g.calculateEnergyBatch()[0] if mols else g.calculateEnergy(True))
+        if g.hasError():
+            raise SystemExit(g.getErrorMessage())
+        at_x[p] = (e, g.getGradient())
+    gathered = None
+    if shard and world > 1:
+        sizes = [len(z) for z, _ in shard[2]]
+        at_x = {p: gather_ensemble(shard[1], e, G, sizes, dist.all_gather_object, world) for p, (e, G) in at_x.items()}
+        gathered = {"molecules": len(sizes), "ranks": world, "energy_sum_eh": float(at_x[args.precision][0].sum())}
+    launches = main["kernels_per_eval"]
+    loop = per_molecule_loop(mols, local) if (mols and world == 1) else None
+    if rank != 0:
+        return None
+    if mols:
+        nc = nd = 0
+        for z, x in mols:
+            a_, b_ = pair_counts(z, x)
+            nc += a_
+            nd += b_
+        hbs = []
+        counts = {"molecules": len(mols)}
+    else:
+        nc, nd = pair_counts(Z, X)
+        hbs = gpu.topology(6, 4)
+        counts = {k: len(gpu.topology(kind, w)) for k, kind, w in
+                  [("bonds", 0, 2), ("angles", 1, 3), ("torsions", 2, 4), ("inversions", 3, 4), ("hbonds", 6, 4),
+                   ("xbonds", 7, 3), ("atm", 12, 3), ("batm", 13, 3)]}
+    sym = os.environ.get("GFNFF_PCG_SYM")
+    info = {"n": n, "nred": n - nfrag, "config": cfg, "coulomb_pairs": nc, "disp_pairs": nd,
+            "solver": main["solver"], "iters": main["iters"],
+            "pcg_lower": (sym != "0") if sym is not None else (n - nfrag) >= 4096,
+            "bytes_hbonds": len(hbs) * (19 * 8 + 3 * 48 + 2 * 48)}
+    if mols:   # block-diagonal EEQ: one reduced system per molecule (one fragment each)
+        info["eeq_flops"] = sum((len(z) - 1) ** 3 / 3.0 + 2.0 * (len(z) - 1) ** 2 for z, _ in mols)
+    hbm_peak, hbm_src = measured_peaks()
+    fp64_peak = gpu._lib.gfnff_fma_peak_tflops(local, 1)
+    roof = roofline(main["phase_avg"], info, fp64_peak, hbm_peak, hbm_src)
+    if roof["kernel"] == "eeq_solve" and main["solver"] == "pcg" and main["iters"] > 0:
+        # the solve as iteration latency (what bounds it while M stays in L2)
+        roof["us_per_iteration"] = 1e3 * roof["ms"] / (main["iters"] + 2)
+        roof["matrix_in_l2"] = not info["pcg_lower"]
+    summary = {
+        "workload": f"config {cfg}: {desc}", "natoms": natoms, "nfrag": nfrag,
+        "value": main["value"], "e2e": main["e2e"], "ms_per_step": main["total_ms"] / args.steps,
+        "step_ms_median": statistics.median(main["step_ms"]), "status": main["status"],
+        "setup_s": round(main["setup_s"], 3), "gpu_launches_per_step": launches, "roofline": roof,
+        "forms": {p: {"value": r["value"], "e2e": r["e2e"]["value"], "eeq_solver": r["solver"],
+                      "eeq_iterations_last_step": r["iters"],
+                      "phase_ms": {k: round(v, 4) for k, v in r["phase_avg"].items()}}
+                  for p, r in res.items()},
+        "mixed_vs_fp64": res["mixed"]["value"] / res["fp64"]["value"],
+        "mixed_vs_fp64_e2e": res["mixed"]["e2e"]["value"] / res["fp64"]["e2e"]["value"],
+        "pairs": {"coulomb": nc, "dispersion": nd}, "terms": counts, "clocks": main["clocks"],
+        "parallelism": (f"one ensemble in {world} cost-balanced molecule shards, gathered on the host" if mols
+                        else f"replicas x{world}"),
+        "scaling": "strong" if mols and world > 1 else "weak",
+    }
+    if gathered:
+        summary["gathered"] = gathered
+    if loop:
+        summary["per_molecule_loop_fp64"] = loop
+        summary["batch_vs_loop"] = main["value"] / loop["value"]
+    if cfg == 3:
+        from curcuma_b200 import GFNFF
+        exact = {}
+        for p in ("mixed", "fp64"):
+            g = GFNFF(precision=0 if p == "fp64" else 1, device=local, exact_gradient=True)
+            if not g.setMolecule(Z, X):
+                raise SystemExit(g.getErrorMessage())
+            exact[p] = g
+        summary["md"] = {p: md_run(g, Z, X) for p, g in exact.items()}
+        summary["md"]["gradient"] = "exact (derivative of the energy)"
+        summary["md"]["note"] = ("C3 spans 274 bohr: ~500 atom pairs cross the 100 bohr Coulomb cut of the "
+                                 "reference's energy every step, each a jump of up to ~2e-3 Eh, so E_total "
+                                 "random-walks independently of dt; systems without cut pairs conserve it")
+        summary["fd_check"] = {"exact_fp64": fd_check(exact["fp64"], X),
+                               "reference_fp64": fd_check(res["fp64"]["gpu"], X)}
+    if world == 1 and not args.no_cpu_baseline:
+        # CPU leg: the oracle at the workload's geometry gives the error of both forms, then
+        # the timed baselines
+        E_o, G_o, _ = oracle_results(Z, X, mols)
+        summary["error_vs_oracle"] = {
+            p: {"dE_eh": float(np.abs(e - E_o).max()), "max_dF_eh_per_bohr": float(np.abs(G - G_o).max())}
+            for p, (e, G) in at_x.items()}
+        summary["error_vs_oracle"]["geometry"] = "the workload's own geometry" + (
+            ", every molecule" if mols else "")
+        summary["cpu_baseline"] = cpu_baseline(Z, X, mols)
+    return summary
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -429,107 +608,41 @@ def run_ours(args):
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
-    wl = workload(args.config, rank)
-    desc, Z, X = wl[:3]
-    mols = wl[3] if len(wl) > 3 else None
-    n = len(Z)
-    # headline: the requested form; the other form is measured beside it
-    forms = [args.precision] + [p for p in ("mixed", "fp64") if p != args.precision]
-    res = {p: measure(args, p, Z, X, torch, dist, world, local, mols) for p in forms}
-    main = res[args.precision]
-    gpu = main["gpu"]
-    natoms, nfrag = gpu.sizes()
-    # accuracy of the mixed form against the FP64 form on one geometry
-    Xc = perturbed(X, 9999)
-    em, ef = [], []
-    for p in ("mixed", "fp64"):
-        g = res[p]["gpu"]
-        g.updateGeometry(Xc)
-        em.append(np.atleast_1d(g.calculateEnergyBatch()[0] if mols else g.calculateEnergy(True)))
-        ef.append(g.getGradient())
-    err = {"dE_eh": float(np.abs(em[0] - em[1]).max()), "max_dF_eh_per_bohr": float(np.abs(ef[0] - ef[1]).max())}
-    if mols:
-        counts = {"molecules": len(mols)}
-        loop = per_molecule_loop(mols, local)
-    else:
-        counts = {k: len(gpu.topology(kind, w)) for k, kind, w in
-                  [("bonds", 0, 2), ("angles", 1, 3), ("torsions", 2, 4), ("inversions", 3, 4), ("hbonds", 6, 4),
-                   ("xbonds", 7, 3), ("atm", 12, 3), ("batm", 13, 3)]}
-    # kernels of this library per step, counted by the library in the captured step graph
-    # (kernel nodes whose code is in libgfnff_b200.so, cuSOLVER's not included) + positions
-    launches = main["kernels_per_eval"]
+    cfgs = [args.config] + [int(c) for c in args.also.split(",") if c.strip() and int(c) != args.config]
+    summaries = {c: run_config(args, c, torch, dist, world, rank, local) for c in cfgs}
     if rank != 0:
         if world > 1:
             dist.destroy_process_group()
         return
-    if mols:
-        nc = nd = 0
-        for z, x in mols:
-            a_, b_ = pair_counts(z, x)
-            nc += a_
-            nd += b_
-        hbs = []
-    else:
-        nc, nd = pair_counts(Z, X)
-        hbs = gpu.topology(6, 4)
-    sym = os.environ.get("GFNFF_PCG_SYM")
-    info = {"n": n, "nred": n - nfrag, "config": args.config, "coulomb_pairs": nc, "disp_pairs": nd,
-            "solver": main["solver"], "iters": main["iters"],
-            "pcg_lower": (sym != "0") if sym is not None else (n - nfrag) >= 4096,
-            "bytes_hbonds": len(hbs) * (19 * 8 + 3 * 48 + 2 * 48)}
-    if mols:   # block-diagonal EEQ: one reduced system per molecule (one fragment each)
-        info["eeq_flops"] = sum((len(z) - 1) ** 3 / 3.0 + 2.0 * (len(z) - 1) ** 2 for z, _ in mols)
+    head = summaries[args.config]
     hbm_peak, hbm_src = measured_peaks()
-    fp64_peak = gpu._lib.gfnff_fma_peak_tflops(local, 1)
-    fp32_peak = gpu._lib.gfnff_fma_peak_tflops(local, 0)
-    roof = roofline(main["phase_avg"], info, fp64_peak, hbm_peak, hbm_src)
+    from curcuma_b200 import _lib
+    lib = _lib.load()
+    fp64_peak = lib.gfnff_fma_peak_tflops(local, 1)
+    fp32_peak = lib.gfnff_fma_peak_tflops(local, 0)
     steps = args.steps
-    line = {"metric": METRIC, "value": main["value"], "unit": UNIT, "n_gpus": world, "steps": steps,
-            "warmup": args.warmup, "ms_per_step": main["total_ms"] / steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None,
+    launches = head["gpu_launches_per_step"]
+    line = {"metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": steps,
+            "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True,
+            "scaling": head["scaling"], "vs_baseline": None,
             "dtype": "f64" if args.precision == "fp64" else "mixed(f32 short-range, f64 long-range/EEQ/sums)",
             "data": "synthetic",
-            "config": {"workload": f"config {args.config}: {desc}", "natoms": natoms, "nfrag": nfrag,
-                       "precision": args.precision, "eeq_solver": main["solver"],
-                       "eeq_iterations_last_step": main["iters"],
+            "config": {"workload": head["workload"], "natoms": head["natoms"], "nfrag": head["nfrag"],
+                       "precision": args.precision, "eeq_solver": head["forms"][args.precision]["eeq_solver"],
+                       "eeq_iterations_last_step": head["forms"][args.precision]["eeq_iterations_last_step"],
                        "l2": "flushed before every timed step (256 MiB write)",
-                       "parallelism": (f"molecule shards x{world} (a batch per rank)" if mols else
-                                       f"replicas x{world}"), "setup_s": round(main["setup_s"], 3)},
-            "e2e": main["e2e"], "gpu_launches": launches * steps if launches > 0 else None,
-            "kernels_per_step": launches, "roofline": roof,
-            "phase_ms": {k: round(v, 4) for k, v in main["phase_avg"].items()},
-            "step_ms_median": statistics.median(main["step_ms"]), "status": main["status"],
-            "forms": {p: {"value": r["value"], "e2e": r["e2e"]["value"], "eeq_solver": r["solver"],
-                          "phase_ms": {k: round(v, 4) for k, v in r["phase_avg"].items()}}
-                      for p, r in res.items()},
-            "mixed_vs_fp64": res["mixed"]["value"] / res["fp64"]["value"],
-            "mixed_error_vs_fp64": err,
-            "pairs": {"coulomb": nc, "dispersion": nd}, "terms": counts, "clocks": main["clocks"],
+                       "parallelism": head["parallelism"], "setup_s": head["setup_s"]},
+            "e2e": head["e2e"], "gpu_launches": launches * steps if launches and launches > 0 else None,
+            "kernels_per_step": launches, "roofline": head["roofline"],
+            "phase_ms": head["forms"][args.precision]["phase_ms"], "step_ms_median": head["step_ms_median"],
+            "status": head["status"], "forms": head["forms"], "mixed_vs_fp64": head["mixed_vs_fp64"],
+            "mixed_vs_fp64_e2e": head["mixed_vs_fp64_e2e"], "clocks": head["clocks"],
             "peaks": {"fp64_fma_tflops": fp64_peak, "fp32_fma_tflops": fp32_peak, "hbm_gbs": hbm_peak,
-                      "source": "FMA: library microbenchmark (csrc/device/peaks.cu); HBM: " + hbm_src}}
-    if mols:
-        line["per_molecule_loop_fp64"] = loop
-        line["batch_vs_loop"] = main["value"] / loop["value"]
-    if args.config == 3:
-        from curcuma_b200 import GFNFF
-        exact = {}
-        for p in ("mixed", "fp64"):
-            g = GFNFF(precision=0 if p == "fp64" else 1, device=local, exact_gradient=True)
-            if not g.setMolecule(Z, X):
-                raise SystemExit(g.getErrorMessage())
-            exact[p] = g
-        line["md"] = {p: md_run(g, Z, X) for p, g in exact.items()}
-        line["md"]["gradient"] = "exact (derivative of the energy)"
-        line["md"]["note"] = ("C3 spans 274 bohr: ~500 atom pairs cross the 100 bohr Coulomb cut of the "
-                              "reference's energy every step, each a jump of up to ~2e-3 Eh, so E_total "
-                              "random-walks independently of dt; systems without cut pairs conserve it")
-        line["fd_check"] = {"exact_fp64": fd_check(exact["fp64"], X),
-                            "reference_fp64": fd_check(res["fp64"]["gpu"], X)}
-    if world == 1 and not args.no_cpu_baseline:
-        rate, dt, k = cpu_oracle_rate(Z, X, 2, 1, min_seconds=10.0)
-        line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
-                                "cpu": cpu_model(),
-                                "sample": f"{k} full E+grad evaluations of the same workload ({dt:.1f} s)"}
+                      "source": "FMA: library microbenchmark (csrc/device/peaks.cu); HBM: " + hbm_src},
+            "configs": {str(c): v for c, v in summaries.items()}}
+    for k in ("error_vs_oracle", "cpu_baseline"):
+        if k in head:
+            line[k] = head[k]
     print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
@@ -545,7 +658,7 @@ def run_profile(args):
     torch.cuda.set_device(0)
     wl = workload(args.config)
     desc, Z, X = wl[:3]
-    mols = wl[3] if len(wl) > 3 else None
+    mols = wl[3][0] if len(wl) > 3 else None
     g = GFNFF(precision=0 if args.precision == "fp64" else 1, device=0)
     if not (g.setMoleculeBatch(mols) if mols else g.setMolecule(Z, X)):
         raise SystemExit(g.getErrorMessage())

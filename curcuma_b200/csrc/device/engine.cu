@@ -451,9 +451,11 @@ struct Engine::Impl {
         A.M = M.p; A.lda = lda; A.n = nred; A.b = rhs; A.x = x; A.z = pz.p; A.z2 = pz2.p;
         A.blocks = pblocks.p; A.boff = pboff.p; A.maxrows = pcg_maxrows; A.maxinv = pcg_maxinv; A.part = ppart.p; A.rblk = prblk.p; A.partial = ppartial.p;
         A.bar = pbar.p; A.info = inf; A.iters = piters.p; A.max_iter = pcg_max_iter;
-        // true residual <= tol max|b|: 1e-12 in the FP64 form; 1e-9 in the mixed form, whose bar
-        // (1e-6 Eh, 1e-5 Eh/bohr against FP64) the resulting charge error stays far below
-        A.tol = opt.precision == 1 ? 1e-9 : 1e-12;
+        // true residual (FP64) <= 1e-12 max|b| in the FP64 form; <= 1e-10 absolute in the mixed
+        // form (kRefineTol, the bar of its refined solves); not reached within max_iter:
+        // REFINE_NOT_CONVERGED, and the host entry point retries with the direct solver
+        A.tol = 1e-12;
+        A.tol_abs = opt.precision == 1 ? kRefineTol : 0.0;
         A.warm = pcg_warm ? pwarm.p + slot : nullptr;
         A.lower = pcg_lower ? pcg_cols : 0; A.yA = pyA.p; A.tiles = ptiles.p; A.ntiles = pcg_ntiles;
         A.Mf = pcg_f32 ? Mf.p : nullptr;

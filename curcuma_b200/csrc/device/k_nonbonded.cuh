@@ -109,6 +109,25 @@ __device__ __forceinline__ bool ranges_far(const View& V, int i0, int ni, int j0
     return boxes_far(il, ih, jl, jh, cut2);
 }
 
+// One counting term 0.5 (1 + erf(kn (r - rc) / rc)), kn = -7.5, of the GFN-FF CN
+// (cn_calculator.cpp:367-428); d2 = r^2, rc = the pair's covalent radius sum (bohr).  FP64:
+// as written.  FP32 (mixed form): the argument in FP64, then the identity 0.5 (1 + erf(z)) =
+// 0.5 erfc(-z) with only the small tail erfc(|z|) in FP32, subtracted from an exact 1 for
+// z >= 0 and accumulated in FP64: 1 + erf(z) in FP32 cancels to a few significant bits for
+// the distant pairs, whose rounding then adds up over ~100 partners per atom.
+template <class R>
+__device__ __forceinline__ double cn_count(double d2, double rc)
+{
+    const double r = sqrt(d2);
+    const double z = -7.5 * ((r - rc) / rc);
+    if constexpr (std::is_same<R, double>::value) {
+        return 0.5 * (1.0 + erf(z));
+    } else {
+        const double t = (double)erfcf((float)fabs(z));
+        return z >= 0.0 ? 1.0 - 0.5 * t : 0.5 * t;
+    }
+}
+
 // ------------------------------------------------------------------------------------
 // coordination numbers: erf counting over partners closer than 6 bohr
 // (cn_calculator.cpp:367-428); the log-squash is applied in k_d4_weights
@@ -125,7 +144,6 @@ __global__ void __launch_bounds__(kTile) k_cn(View V, int nsplit, const int* nl_
     const double4 pi = act ? V.pos[i] : make_double4(0.0, 0.0, 0.0, 0.0);
     const double ri = act ? V.rcov_cn[i] : 0.0;
     const int2 rg = act ? V.jr[i] : make_int2(0, 0);
-    const double kn = -7.5;
     double s = 0.0;
     const int ni = min(kTile, V.n - i0);
     const int w0 = i0 + (threadIdx.x & ~31), nw = max(0, min(32, V.n - w0));   // this warp's atoms
@@ -149,9 +167,7 @@ __global__ void __launch_bounds__(kTile) k_cn(View V, int nsplit, const int* nl_
                 const double d2 = dx * dx + dy * dy + dz * dz;
                 const int j = t0 + jj;
                 if (!(d2 < 36.0) || j == i || j < rg.x || j >= rg.y) continue;
-                const R r = sqrt((R)d2);
-                const R rc = (R)(ri + sr[jj]);
-                s += (double)(R(0.5) * (R(1) + erf(R(kn) * ((r - rc) / rc))));
+                s += cn_count<R>(d2, ri + sr[jj]);
             }
         }
     }
@@ -801,7 +817,6 @@ __global__ void __launch_bounds__(kBlock) k_cn_nl(View V, const int* __restrict_
     if (i >= V.n) return;
     const double4 pi = V.pos[i];
     const double ri = V.rcov_cn[i];
-    const double kn = -7.5;
     double s = 0.0;
     for (int p = off[i] + lane; p < off[i + 1]; p += 32) {
         const int j = nbr[p];
@@ -809,9 +824,7 @@ __global__ void __launch_bounds__(kBlock) k_cn_nl(View V, const int* __restrict_
         const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
         const double d2 = dx * dx + dy * dy + dz * dz;
         if (!(d2 < 36.0)) continue;
-        const R r = sqrt((R)d2);
-        const R rc = (R)(ri + V.rcov_cn[j]);
-        s += (double)(R(0.5) * (R(1) + erf(R(kn) * ((r - rc) / rc))));
+        s += cn_count<R>(d2, ri + V.rcov_cn[j]);
     }
     for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
     if (lane == 0 && s != 0.0) atomicAdd(V.cnraw + i, s);

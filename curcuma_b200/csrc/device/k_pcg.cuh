@@ -52,7 +52,9 @@ struct PCGArgs {
     const int2* tiles;    // lower: tiles {first row I0, first column J0}, I0 >= J0
     int ntiles;
     int max_iter;
-    double tol;           // converged when max|b - M x| <= tol * max|b|
+    double tol;           // converged when max|b - M x| <= tol * max|b| ...
+    double tol_abs;       // ... or, when > 0, when max|b - M x| <= tol_abs (the mixed form's
+                          // FP64 true-residual bar); the residual is always computed in FP64
 };
 
 // grid-wide barrier (all blocks co-resident); false when the wait gave up.  The block's
@@ -62,6 +64,11 @@ struct PCGArgs {
 // counter bar[0] and the generation bar[kBarGen] sit on different 128-byte lines, so the
 // polling reads do not queue behind the arrival atomics; the generation counter makes
 // the barrier reusable without a reset in between.
+__device__ __forceinline__ double pcg_threshold(const PCGArgs& A, double bmax)
+{
+    return A.tol_abs > 0.0 ? A.tol_abs : A.tol * bmax;
+}
+
 constexpr int kBarGen = 32;
 __device__ __forceinline__ unsigned int atom_add_release(unsigned int* p, unsigned int v)
 {
@@ -558,7 +565,7 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(PCGArgs A)
         if (!ok) break;
         double rzn, rmax;
         grid_totals(A.partial, 2, rzn, rmax);
-        if (rmax <= A.tol * bmax) {
+        if (rmax <= pcg_threshold(A, bmax)) {
             // accept only on the true residual r = b - M x; otherwise restart from it
             for (int k = threadIdx.x; k < nrow; k += blockDim.x) __stcg(A.x + row0 + k, xs[k]);
             ok = grid_sync(A.bar, gen);
@@ -586,7 +593,7 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(PCGArgs A)
             ok = grid_sync(A.bar, gen);
             if (!ok) break;
             grid_totals(A.partial, 2, rzn, rmax);
-            if (rmax <= A.tol * bmax) {
+            if (rmax <= pcg_threshold(A, bmax)) {
                 conv = true;
                 break;
             }
@@ -756,7 +763,7 @@ __global__ void __launch_bounds__(kPcgPipeThreads, 2) k_pcg_pipe(PCGArgs A)
         double gam, del, rmax;
         publish(ms, g_t, d_t, rm_t, gam, del, rmax);
         if (!ok) break;
-        if (rmax <= A.tol * bmax) {
+        if (rmax <= pcg_threshold(A, bmax)) {
             // accept only on the true residual r = b - M x; otherwise restart from it
             double u1, u2;
             publish(xs, 0.0, 0.0, 0.0, u1, u2, u1);
@@ -772,7 +779,7 @@ __global__ void __launch_bounds__(kPcgPipeThreads, 2) k_pcg_pipe(PCGArgs A)
             double rtrue;
             publish(us, 0.0, 0.0, rt, u1, u2, rtrue);
             if (!ok) break;
-            if (rtrue <= A.tol * bmax) {
+            if (rtrue <= pcg_threshold(A, bmax)) {
                 conv = true;
                 break;
             }
@@ -1019,7 +1026,7 @@ __global__ void __launch_bounds__(kPcgPipeThreads, 1) k_pcg_res(PCGArgs A, PCGRe
         double gam, del, rmax;
         publish(ms, g_t, d_t, rm_t, gam, del, rmax);
         if (!ok) break;
-        if (rmax <= A.tol * bmax) {
+        if (rmax <= pcg_threshold(A, bmax)) {
             double u1, u2;
             publish(xs, 0.0, 0.0, 0.0, u1, u2, u1);
             if (!ok) break;
@@ -1034,7 +1041,7 @@ __global__ void __launch_bounds__(kPcgPipeThreads, 1) k_pcg_res(PCGArgs A, PCGRe
             double rtrue;
             publish(us, 0.0, 0.0, rt, u1, u2, rtrue);
             if (!ok) break;
-            if (rtrue <= A.tol * bmax) {
+            if (rtrue <= pcg_threshold(A, bmax)) {
                 conv = true;
                 break;
             }

@@ -186,7 +186,8 @@ static int engrad(const Model& m, const double* xb, double* T, double* gout, dou
             }
         }
         for (int i = 0; i < n; ++i) x[i] = m.chi_base[i] + m.cnf[i] * std::sqrt(cn[i]);
-        if (!linalg::eeq_schur_solve(A.data(), n, x.data(), m.frag.data(), m.nfrag, m.qfrag.data(), q.data())) {
+        if (!linalg::eeq_schur_solve(A.data(), n, x.data(), m.frag.data(), m.nfrag, m.qfrag.data(), q.data(),
+                                     n >= 1024)) {
             g_err = "EEQ solve failed";
             return 3;
         }
