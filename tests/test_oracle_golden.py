@@ -144,3 +144,21 @@ def test_fixture_coordination_numbers(name):
     g = golden(name)
     o = Oracle(g["Z"], g["xyz_angstrom"])
     assert np.abs(o.atom_data(1) - np.array(g["cn"])).max() < 0.01
+
+
+@pytest.mark.parametrize("x_el", [17, 35, 53])
+def test_halogen_dimer_has_one_xbond(x_el):
+    """No fixture has a halogen bond: the oracle's XB term on CH3X...NH3 (one C-X...N triple,
+    a few mEh, growing from Cl to I as the XB strength parameters do)."""
+    from tests.halogen_dimers import dimer
+    Z, X = dimer(x_el)
+    o = Oracle(Z, X)
+    T, G, q, cn = o.engrad(X)
+    assert o.topology(7, 3).tolist() == [[0, 1, 5]]
+    assert -0.02 < T["xbond"] < -1e-3
+
+
+def test_halogen_bond_strength_order():
+    from tests.halogen_dimers import dimer
+    e = [Oracle(*dimer(x)).engrad(dimer(x)[1])[0]["xbond"] for x in (17, 35, 53)]
+    assert e[0] > e[1] > e[2]
