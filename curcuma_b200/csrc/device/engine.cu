@@ -427,6 +427,10 @@ struct Engine::Impl {
     // the FP64 form on the 20k cluster (9.2 vs 5.2 ms), so it is off by default.
     bool pcg_f32 = false;
     DBuf<float> Mf;
+    // mixed form, lower-triangle systems: k_pcg_ir (FP32-matrix CG inside FP64 refinement,
+    // both triangles of M built in one pass: FP64 for the residuals, FP32 for the products)
+    bool pcg_ir = false;
+    size_t pcg_smem_ir = 0;
     // pipelined CG (one grid barrier per iteration; GFNFF_PCG=classic|pipelined forces one)
     bool pcg_pipe = true;
     size_t pcg_smem_pipe = 0;
@@ -458,10 +462,18 @@ struct Engine::Impl {
         A.tol_abs = opt.precision == 1 ? kRefineTol : 0.0;
         A.warm = pcg_warm ? pwarm.p + slot : nullptr;
         A.lower = pcg_lower ? pcg_cols : 0; A.yA = pyA.p; A.tiles = ptiles.p; A.ntiles = pcg_ntiles;
-        A.Mf = pcg_f32 ? Mf.p : nullptr;
+        A.Mf = (pcg_f32 || pcg_ir) ? Mf.p : nullptr;
+        A.max_outer = 6;
+        {
+            const char* er = std::getenv("GFNFF_PCG_IR_REL");
+            A.inner_rel = er ? std::atof(er) : 1e-6;
+        }
         A.binv_pre = pcg_pre ? pbinv.p : nullptr;
         void* args[] = {&A};
-        if (pcg_res) {
+        if (pcg_ir) {
+            CK(cudaLaunchCooperativeKernel((const void*)k_pcg_ir, dim3(pcg_grid), dim3(kPcgThreads), args,
+                                           pcg_smem_ir, stream));
+        } else if (pcg_res) {
             PCGRes R{view(), red2atom.p, anchor.p, prtiles.p, pcg_res_ntiles, pcg_res_ntl, pcg_res_gscratch};
             void* rargs[] = {&A, &R};
             CK(cudaLaunchCooperativeKernel((const void*)k_pcg_res, dim3(pcg_grid), dim3(kPcgPipeThreads), rargs,
@@ -1241,7 +1253,11 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
                     P.pcg_lower = lower;
                     const char* ef = std::getenv("GFNFF_PCG_F32");
                     P.pcg_f32 = P.pcg_lower && P.opt.precision == 1 && ef && !std::strcmp(ef, "1");
-                    if (P.pcg_f32) P.Mf.alloc((size_t)P.lda * P.nred);
+                    // mixed form, lower-triangle systems: FP32-matrix CG inside FP64 refinement
+                    // (k_pcg_ir; GFNFF_PCG_IR=0: the FP64 classic PCG at the absolute bar)
+                    const char* eir = std::getenv("GFNFF_PCG_IR");
+                    P.pcg_ir = P.pcg_lower && P.opt.precision == 1 && !P.pcg_f32 && !(eir && !std::strcmp(eir, "0"));
+                    if (P.pcg_f32 || P.pcg_ir) P.Mf.alloc((size_t)P.lda * P.nred);
                     const char* ec = std::getenv("GFNFF_PCG_COLS");
                     P.pcg_cols = (ec && !std::strcmp(ec, "8")) ? 2 : 1;
                     std::vector<int2> tl;
@@ -1263,6 +1279,17 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
                 int per_sm = 0;
                 CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)k_pcg, kPcgThreads, smem));
                 P.pcg_ready = per_sm >= 1;
+                if (P.pcg_ir) {   // one more owned-row vector (the inner correction d), even-sized
+                    P.pcg_smem_ir = smem + (size_t)((maxrows + 1) & ~1) * sizeof(double);
+                    int ps = 0;
+                    if (P.pcg_smem_ir <= 220 * 1024) {
+                        CK(cudaFuncSetAttribute((const void*)k_pcg_ir, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                (int)P.pcg_smem_ir));
+                        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ps, (const void*)k_pcg_ir, kPcgThreads,
+                                                                         P.pcg_smem_ir));
+                    }
+                    P.pcg_ir = ps >= 1;
+                }
                 // the pipelined form keeps ten owned-row vectors instead of four
                 P.pcg_smem_pipe = smem + 6 * (size_t)maxrows * sizeof(double);
                 const char* pe = std::getenv("GFNFF_PCG");
@@ -1637,7 +1664,8 @@ void Engine::launch_body()
             else if (sv == Impl::SOLVE_PCG && P.pcg_f32)
                 k_eeq_M_tiles<float><<<nb, 256, 0, s>>>(V, P.red2atom.p, P.anchor.p, P.Mf.p, P.lda, 0);
             else
-                k_eeq_M_tiles<double><<<nb, 256, 0, s>>>(V, P.red2atom.p, P.anchor.p, P.M.p, P.lda, full ? 1 : 0);
+                k_eeq_M_tiles<double><<<nb, 256, 0, s>>>(V, P.red2atom.p, P.anchor.p, P.M.p, P.lda, full ? 1 : 0,
+                                                         sv == Impl::SOLVE_PCG && P.pcg_ir ? P.Mf.p : nullptr);
         }
         P.mark(4);
         if (P.nred > 0)

@@ -662,9 +662,16 @@ __global__ void k_xbonds(View V, XBSoA S)
             const double pre = S.pre[t];
             etot = R * pre;
             const double st = pow6(XB_SCUT * rv / (rXB * rXB));
-            const double dds = -2.0 * ALP * dsh * st / (rXB * (1.0 + st));
             const double lt = pow6((rXB * rXB) / LC);
-            const double ddl = -2.0 * ALP * rXB * dlg * lt / (LC * (1.0 + lt));
+            // damping derivatives d dsh/dr and d dlg/dr.  curcuma's analytic gradient
+            // (ff_workspace_gfnff.cpp:1465-1476) uses -2 a dsh s^a / (r (1 + s^a)) for the
+            // short-range factor, whose true derivative has the opposite sign, and an extra
+            // factor t = r^2/LC in the long-range one; the reference mode keeps those for
+            // parity, the exact mode (the derivative of the energy) uses the true ones
+            const double dds = V.exact ? 2.0 * ALP * dsh * dsh * st / rXB
+                                       : -2.0 * ALP * dsh * st / (rXB * (1.0 + st));
+            const double ddl = V.exact ? -2.0 * ALP * dlg * dlg * lt / rXB
+                                       : -2.0 * ALP * rXB * dlg * lt / (LC * (1.0 + lt));
             const double et = exp(ex), de = 1.0 + et;
             const double do_ax = -2.0 * et * XB_BACUT / (rAB * de * de);
             const double do_ab = 2.0 * et * XB_BACUT * (rAX + rXB) / (rAB * rAB * de * de);

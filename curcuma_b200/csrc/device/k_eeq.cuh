@@ -48,7 +48,8 @@ __global__ void k_eeq_M(View V, const int* __restrict__ red2atom, const int* __r
 constexpr int kMT = 32;
 template <class TM>   // storage type of M: double, or float for the FP32-stored PCG matrix
 __global__ void __launch_bounds__(256) k_eeq_M_tiles(View V, const int* __restrict__ red2atom,
-                                                    const int* __restrict__ anchor, TM* M, int lda, int full)
+                                                    const int* __restrict__ anchor, TM* M, int lda, int full,
+                                                    float* M32 = nullptr)   // optional FP32 copy (k_pcg_ir)
 {
     __shared__ double px[4][kMT], py[4][kMT], pz[4][kMT], pa[4][kMT];   // rows k, rows ak, cols l, cols al
     __shared__ int pid[4][kMT];
@@ -90,13 +91,19 @@ __global__ void __launch_bounds__(256) k_eeq_M_tiles(View V, const int* __restri
         double v = 0.0;
         if (r < n && c < n) v = el(0, tx, 2, cc) - el(0, tx, 3, cc) - el(1, tx, 2, cc) + el(1, tx, 3, cc);
         T[cc][tx] = v;
-        if (r < n && c < n && (full || r >= c)) M[(size_t)c * lda + r] = (TM)v;
+        if (r < n && c < n && (full || r >= c)) {
+            M[(size_t)c * lda + r] = (TM)v;
+            if (M32) M32[(size_t)c * lda + r] = (float)v;
+        }
     }
     if (!full || tr == tc) return;
     __syncthreads();
     for (int rr = ty; rr < kMT; rr += 8) {   // (c, r) entries: row c0 + tx of column r0 + rr
         const int r = r0 + rr, c = c0 + tx;
-        if (r < n && c < n) M[(size_t)r * lda + c] = (TM)T[tx][rr];
+        if (r < n && c < n) {
+            M[(size_t)r * lda + c] = (TM)T[tx][rr];
+            if (M32) M32[(size_t)r * lda + c] = (float)T[tx][rr];
+        }
     }
 }
 

@@ -55,6 +55,8 @@ struct PCGArgs {
     double tol;           // converged when max|b - M x| <= tol * max|b| ...
     double tol_abs;       // ... or, when > 0, when max|b - M x| <= tol_abs (the mixed form's
                           // FP64 true-residual bar); the residual is always computed in FP64
+    int max_outer;        // k_pcg_ir: FP64 residual corrections at most
+    double inner_rel;     // k_pcg_ir: inner solve to ||r_inner||_inf <= inner_rel ||r||_inf
 };
 
 // grid-wide barrier (all blocks co-resident); false when the wait gave up.  The block's
@@ -604,6 +606,206 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(PCGArgs A)
         const double beta = rzn / rz;
         rz = rzn;
         update_p(p, A.z, A.n, beta);
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < nrow; k += blockDim.x) A.x[row0 + k] = xs[k];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        *A.info = !ok ? 2 : (conv ? 0 : 3);
+        *A.iters = it;
+        if (A.warm) *A.warm = (ok && conv) ? 1 : 0;
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// Mixed form, large systems (the lower-triangle tiled form): block-Jacobi CG on the FP32 copy
+// of M inside FP64 iterative refinement.  Outer step: the true residual r = b - M x with the
+// FP64 lower triangle (A.M); stop when ||r||_inf <= tol_abs (info 0) or after max_outer
+// corrections (info 3, REFINE_NOT_CONVERGED).  Otherwise CG on the FP32 lower triangle
+// (A.Mf: half the bytes of every product, FP32 arithmetic inside a tile) solves M32 d = r
+// from d = 0, and x += d.  The inner solve stops at inner_rel ||r||_inf, but not below half
+// the bar: one correction cannot lower the true residual by more than the FP32 rounding of M
+// allows (~1e-6 relative), so the next outer step finishes from there.  Preconditioner blocks
+// as in k_pcg; the partial-sum slots follow k_pcg's rule (the outer totals have a slot of
+// their own).  iters: the inner iterations of all outer steps.
+// ------------------------------------------------------------------------------------
+__device__ double matvec_tiles64(const PCGArgs& A, const double* p, double* red)
+{
+    return A.lower == 2 ? matvec_tiles_c<8>(A, A.M, p, red) : matvec_tiles_c<4>(A, A.M, p, red);
+}
+
+// The inner products of k_pcg_ir: the FP32 lower triangle with FP32 arithmetic inside a tile
+// (elements, the direction's tile segments and the partial sums stay FP32: the inner solve
+// needs ~1e-6 relative accuracy, a 128-term FP32 sum gives ~1e-7), the tile's row and column
+// sums added to y as FP64 atomics, as in matvec_tiles_c.  No per-element FP64 conversion.
+__device__ double matvec_tiles_f32(const PCGArgs& A, const double* p, float* red)
+{
+    constexpr int kCols = 8;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    double pap = 0.0;
+    const float* Mt = A.Mf;
+    for (int t = blockIdx.x; t < A.ntiles; t += gridDim.x) {
+        const int2 tl = A.tiles[t];
+        const int I0 = tl.x, J0 = tl.y;
+        const bool diag = I0 == J0;
+        const int ni = min(kPcgT, A.n - I0), nj = min(kPcgT, A.n - J0);
+        float u[4], pr[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int r = lane + 32 * i;
+            u[i] = 0.f;
+            pr[i] = r < ni ? (float)p[I0 + r] : 0.f;
+        }
+        for (int cb = warp * kCols; cb < nj; cb += nw * kCols) {
+            float m[kCols][4], v[kCols], pc[kCols];
+#pragma unroll
+            for (int q = 0; q < kCols; ++q) {
+                const int c = cb + q;
+                pc[q] = c < nj ? (float)p[J0 + c] : 0.f;
+                const float* col = Mt + (size_t)(J0 + (c < nj ? c : 0)) * A.lda + I0;
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int r = lane + 32 * i;
+                    m[q][i] = (c < nj && r < ni && (!diag || r >= c)) ? __ldcs(col + r) : 0.f;
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < kCols; ++q) {
+                const int c = cb + q;
+                v[q] = 0.f;
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int r = lane + 32 * i;
+                    u[i] = fmaf(m[q][i], pc[q], u[i]);
+                    if (!diag || r > c) v[q] = fmaf(m[q][i], pr[i], v[q]);
+                }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+                for (int q = 0; q < kCols; ++q) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+            float vq = 0.f;
+#pragma unroll
+            for (int q = 0; q < kCols; ++q)
+                if (lane == q) vq = v[q];
+            if (lane < kCols) {
+                const int c = cb + lane;
+                if (c < nj && vq != 0.f) {
+                    atomicAdd(A.yA + J0 + c, (double)vq);
+                    pap += p[J0 + c] * (double)vq;
+                }
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i) red[warp * kPcgT + lane + 32 * i] = u[i];
+        __syncthreads();
+        for (int r = threadIdx.x; r < ni; r += blockDim.x) {
+            double s = 0.0;
+            for (int w = 0; w < nw; ++w) s += (double)red[w * kPcgT + r];
+            atomicAdd(A.yA + I0 + r, s);
+            pap += p[I0 + r] * s;
+        }
+        __syncthreads();
+    }
+    return pap;
+}
+
+__global__ void __launch_bounds__(kPcgThreads) k_pcg_ir(PCGArgs A)
+{
+    extern __shared__ double sm[];
+    constexpr int GL = kPcgMaxBlock + 1;
+    const int4 pt = A.part[blockIdx.x];
+    const int row0 = pt.x, row1 = pt.y, nrow = row1 - row0;
+    const long long boff0 = pt.z < pt.w ? A.boff[pt.z] : 0;
+    double* p = sm;                              // n, replicated: x (residuals) or the CG direction
+    double* G = p + ((A.n + 1) & ~1);            // kPcgMaxBlock x GL scratch
+    double* xs = G + kPcgMaxBlock * GL;          // owned rows: x, r, z, M p, d
+    double* rs = xs + A.maxrows;
+    double* zs = rs + A.maxrows;
+    double* Ap = zs + A.maxrows;
+    double* ds = Ap + A.maxrows;
+    double* Bs = ds + ((A.maxrows + 1) & ~1);    // inverses of the owned blocks (an even offset
+                                                 // keeps the int4 row records 16-byte aligned)
+    int4* meta = reinterpret_cast<int4*>(Bs + A.maxinv);
+    __shared__ unsigned int gen;
+    if (threadIdx.x == 0) gen = *(volatile unsigned int*)(A.bar + kBarGen);
+    pcg_setup(A, pt, boff0, G, Bs, meta, MStored{&A});
+    const double* Bp = A.binv_pre ? A.binv_pre + boff0 : Bs;
+    const bool warm = A.warm != nullptr && *A.warm != 0;   // uniform over the grid
+    bool ok = true, conv = false;
+    int it = 0;
+    for (int k = threadIdx.x; k < nrow; k += blockDim.x) xs[k] = warm ? __ldcg(A.x + row0 + k) : 0.0;
+    for (int outer = 0; ok; ++outer) {
+        // ---- FP64 true residual r = b - M x (x = 0 on a cold start: r = b); x is complete in
+        // global memory (the previous launch, or the barrier after the last correction)
+        const bool have_x = warm || outer > 0;
+        if (have_x) {
+            update_p(p, A.x, A.n, 0.0);
+            __syncthreads();
+            matvec_tiles64(A, p, G);
+            ok = grid_sync(A.bar, gen);
+            if (!ok) break;
+            take_tiles_result(A, row0, nrow, Ap);
+        }
+        double rmax_t = 0.0;
+        for (int k = threadIdx.x; k < nrow; k += blockDim.x) {
+            const double r = A.b[row0 + k] - (have_x ? Ap[k] : 0.0);
+            rs[k] = r;
+            ds[k] = 0.0;
+            rmax_t = fmax(rmax_t, fabs(r));
+        }
+        __syncthreads();
+        double rz_t = apply_precond(nrow, meta, Bp, rs, zs);
+        for (int k = threadIdx.x; k < nrow; k += blockDim.x) __stcg(A.z + row0 + k, zs[k]);
+        block_sum_max(rz_t, rmax_t, A.partial + 8 * blockIdx.x + 4);
+        ok = grid_sync(A.bar, gen);
+        if (!ok) break;
+        double rz = 0.0, rmax = 0.0;
+        grid_totals(A.partial, 4, rz, rmax);
+        if (rmax <= A.tol_abs) {
+            conv = true;
+            break;
+        }
+        if (outer >= A.max_outer || it >= A.max_iter) break;
+        const double stop = fmax(A.inner_rel * rmax, 0.5 * A.tol_abs);
+        update_p(p, A.z, A.n, 0.0);
+        // ---- inner CG on the FP32 matrix: M32 d = r from d = 0
+        while (it < A.max_iter) {
+            ++it;
+            __syncthreads();
+            const double pap_t = matvec_tiles_f32(A, p, reinterpret_cast<float*>(G));
+            block_sum_max(pap_t, 0.0, A.partial + 8 * blockIdx.x);
+            ok = grid_sync(A.bar, gen);
+            if (!ok) break;
+            take_tiles_result(A, row0, nrow, Ap);
+            double pap, unused;
+            grid_totals(A.partial, 0, pap, unused);
+            const double alpha = rz / pap;
+            double rin_t = 0.0;
+            for (int k = threadIdx.x; k < nrow; k += blockDim.x) {
+                ds[k] += alpha * p[row0 + k];
+                rs[k] -= alpha * Ap[k];
+                rin_t = fmax(rin_t, fabs(rs[k]));
+            }
+            __syncthreads();
+            rz_t = apply_precond(nrow, meta, Bp, rs, zs);
+            for (int k = threadIdx.x; k < nrow; k += blockDim.x) __stcg(A.z + row0 + k, zs[k]);
+            block_sum_max(rz_t, rin_t, A.partial + 8 * blockIdx.x + 2);
+            ok = grid_sync(A.bar, gen);
+            if (!ok) break;
+            double rzn, rin;
+            grid_totals(A.partial, 2, rzn, rin);
+            if (rin <= stop) break;
+            const double beta = rzn / rz;
+            rz = rzn;
+            update_p(p, A.z, A.n, beta);
+        }
+        if (!ok) break;
+        // ---- x += d, published for the next residual
+        for (int k = threadIdx.x; k < nrow; k += blockDim.x) {
+            xs[k] += ds[k];
+            __stcg(A.x + row0 + k, xs[k]);
+        }
+        ok = grid_sync(A.bar, gen);
     }
     __syncthreads();
     for (int k = threadIdx.x; k < nrow; k += blockDim.x) A.x[row0 + k] = xs[k];
