@@ -22,7 +22,8 @@ EXPORTED = ["gfnff_default_options", "gfnff_create", "gfnff_setup", "gfnff_energ
             "gfnff_destroy", "gfnff_set_phase_timing", "gfnff_phase_times", "gfnff_fma_peak_tflops",
             "gfnff_eeq_charges_noalloc", "gfnff_eeq_solver", "gfnff_eeq_iterations", "gfnff_setup_batch",
             "gfnff_energy_and_gradient_batch", "gfnff_md_nve", "gfnff_kernels_per_evaluation",
-            "gfnff_save_parameters", "gfnff_setup_from_parameters", "gfnff_write_parameters"]
+            "gfnff_save_parameters", "gfnff_setup_from_parameters", "gfnff_write_parameters",
+            "gfnff_pair_kernel"]
 PHASES = ["positions", "cn", "d4_weights", "eeq_matrix", "eeq_rhs", "eeq_solve", "bonded",
           "hbonds", "repulsion", "pairs", "post_chain", "finish"]
 
@@ -67,6 +68,8 @@ def load():
     lib.gfnff_eeq_charges_noalloc.argtypes = [c_i, c_i] + [c_v] * 11
     lib.gfnff_eeq_solver.argtypes = [c_v]
     lib.gfnff_eeq_solver.restype = ctypes.c_char_p
+    lib.gfnff_pair_kernel.argtypes = [c_v]
+    lib.gfnff_pair_kernel.restype = ctypes.c_char_p
     lib.gfnff_eeq_iterations.argtypes = [c_v]
     lib.gfnff_kernels_per_evaluation.argtypes = [c_v]
     lib.gfnff_save_parameters.argtypes = [c_v, ctypes.c_char_p]
@@ -77,7 +80,7 @@ def load():
     lib.gfnff_md_nve.argtypes = [c_v, c_i, c_d, P(c_d), P(c_d), P(c_d), P(c_d), P(c_d)]
     for name in EXPORTED:
         if name not in ("gfnff_default_options", "gfnff_stream", "gfnff_last_error", "gfnff_fma_peak_tflops",
-                        "gfnff_eeq_solver"):
+                        "gfnff_eeq_solver", "gfnff_pair_kernel"):
             getattr(lib, name).restype = c_i
     _lib = lib
     return lib

@@ -491,6 +491,12 @@ const char* gfnff_eeq_solver(gfnff_handle* h)
     return h->eng->solver_name();
 }
 
+const char* gfnff_pair_kernel(gfnff_handle* h)
+{
+    if (!h || !h->ready) return "";
+    return h->eng->pair_kernel_name();
+}
+
 int gfnff_kernels_per_evaluation(gfnff_handle* h)
 {
     if (!h || !h->ready) return -1;

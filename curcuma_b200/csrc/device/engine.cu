@@ -30,6 +30,7 @@
 #include <dlfcn.h>
 #include <type_traits>
 #include <map>
+#include <mutex>
 #include <numeric>
 #include <stdexcept>
 #include <string>
@@ -299,6 +300,13 @@ struct Engine::Impl {
     bool pairs_sym = true;
     bool pairs_occ = false;   // 10 blocks per SM (96 registers) instead of the unbounded 116
     int pair_tile = 64;       // tile edge of k_pairs_sym
+    // Coulomb + D4 pair kernel variant, chosen at set-up by timing (tune_pairs): tile edge
+    // (atoms per block side) and blocks per SM of k_pairs_sym, or both directions by rows
+    enum { PAIRS_SYM32 = 0, PAIRS_SYM64 = 1, PAIRS_SYM64_OCC = 2, PAIRS_ROWS = 3 };
+    int pair_variant = PAIRS_SYM64;
+    DBuf<int2> symtiles32;    // tile list of the 32-atom variant (symtiles: 64)
+    int nsym32 = 0;
+    float pair_ms[4] = {-1.f, -1.f, -1.f, -1.f};   // the tuner's timings (ms per launch)
     // D4 pairs (charge-independent) on the side stream beside the EEQ solve, Coulomb pairs
     // after it on the main stream (GFNFF_PAIRS_SPLIT=0: both in one pass after the solve)
     int pairs_split = 1;   // 0 off, 1 unless the solver fills every SM, 2 always
@@ -504,6 +512,17 @@ struct Engine::Impl {
         if (graph) cudaGraphExecDestroy(graph);
         graph = nullptr;
     }
+    // one launch of the chosen Coulomb + D4 pair kernel variant (PART: the terms)
+    template <int PART>
+    void launch_pairs_sym(int variant, const View& V, cudaStream_t st)
+    {
+        if (variant == PAIRS_SYM32)
+            k_pairs_sym<double, 16, 32, PART><<<nsym32, 32, 0, st>>>(V, symtiles32.p);
+        else if (variant == PAIRS_SYM64_OCC)
+            k_pairs_sym<double, 10, kST, PART><<<nsym, kST, 0, st>>>(V, symtiles.p);
+        else
+            k_pairs_sym<double, 8, kST, PART><<<nsym, kST, 0, st>>>(V, symtiles.p);
+    }
     cudaEvent_t ev[Engine::kNumPhases + 1] = {};
     void mark(int k)
     {
@@ -684,14 +703,21 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
     for (int m = 0; m < nm; ++m) max_range = std::max(max_range, mols[m]->n);
     P.nsplit = pair_splits(n, max_range);
     {   // tile pairs (i tile <= j tile, both within the tile's molecules) of k_pairs_sym
-        std::vector<int2> tl;
-        P.pair_tile = nm > 1 ? 32 : kST;
-        const int T = P.pair_tile, nt = (n + T - 1) / T;
-        for (int I = 0; I < nt; ++I) {
-            const int i0 = I * T, hi = hjr[std::min(n, i0 + T) - 1].y;
-            for (int J = I; J * T < hi; ++J) tl.push_back(make_int2(i0, J * T));
-        }
+        // both tile edges (the tuner picks one): tile pairs I <= J within the rows' molecules
+        auto tiles = [&](int T) {
+            std::vector<int2> tl;
+            const int nt = (n + T - 1) / T;
+            for (int I = 0; I < nt; ++I) {
+                const int i0 = I * T, hi = hjr[std::min(n, i0 + T) - 1].y;
+                for (int J = I; J * T < hi; ++J) tl.push_back(make_int2(i0, J * T));
+            }
+            return tl;
+        };
+        const std::vector<int2> tl = tiles(kST), tl32 = tiles(32);
         P.symtiles.upload(tl);
+        P.symtiles32.upload(tl32);
+        P.nsym32 = (int)tl32.size();
+        P.pair_tile = nm > 1 ? 32 : kST;
         P.boxlo.alloc((n + kBoxAtoms - 1) / kBoxAtoms);
         P.boxhi.alloc((n + kBoxAtoms - 1) / kBoxAtoms);
         P.box_cull = nm == 1 && n >= 8192;
@@ -700,6 +726,10 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
         P.pairs_sym = !(pe && !std::strcmp(pe, "rows"));
         const char* po = std::getenv("GFNFF_PAIRS_OCC");
         P.pairs_occ = po && !std::strcmp(po, "1");
+        // the variant before tuning (batches: 32-atom tiles, which straddle fewer molecules)
+        P.pair_variant = !P.pairs_sym ? Impl::PAIRS_ROWS
+                         : (P.pair_tile == 32 ? Impl::PAIRS_SYM32
+                                              : (P.pairs_occ ? Impl::PAIRS_SYM64_OCC : Impl::PAIRS_SYM64));
         const char* ps = std::getenv("GFNFF_PAIRS_SPLIT");
         P.pairs_split = !ps ? 1 : (!std::strcmp(ps, "0") ? 0 : (!std::strcmp(ps, "1") ? 2 : 1));
     }
@@ -1402,10 +1432,100 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
             }
         }
     }
+    tune_pairs(mols);
     P.graphs_ok = graphs_setting;
     // from here on PCG starts from the previous step's solution (GFNFF_PCG_WARM=0: from zero)
     const char* warm_env = std::getenv("GFNFF_PCG_WARM");
     P.pcg_warm = !(warm_env && !std::strcmp(warm_env, "0"));
+}
+
+// Tile-shape autotuner of the Coulomb + D4 pair kernel.  Candidates: k_pairs_sym with 32- or
+// 64-atom tiles (a block is one warp or two; the tile edge is the atom block width and the
+// partners a warp takes per step), the 64-atom tiles also at 10 blocks per SM (96 registers)
+// instead of 8, and both directions by rows (k_pairs).  After one evaluation at the set-up
+// geometry (valid charges and weights in the buffers), each candidate runs once untimed and
+// three times between CUDA events on the handle's stream (both terms, PART = both); the
+// fastest is kept.  The pick is cached per (device, batch or single molecule, size bucket
+// floor(log2 N)) for the process, so further handles of similar systems skip the timing.
+// GFNFF_PAIRS_TUNE=0, GFNFF_PAIRS=rows and GFNFF_PAIRS_OCC=1 keep the untuned choice;
+// GFNFF_PAIRS_VARIANT=sym32|sym64|sym64_occ10|rows forces one.
+void Engine::tune_pairs(const std::vector<const Model*>& mols)
+{
+    Impl& P = *p_;
+    const char* et = std::getenv("GFNFF_PAIRS_TUNE");
+    const char* pe = std::getenv("GFNFF_PAIRS");
+    const char* po = std::getenv("GFNFF_PAIRS_OCC");
+    if (const char* ev = std::getenv("GFNFF_PAIRS_VARIANT")) {   // forced: sym32|sym64|sym64_occ10|rows
+        const char* names[4] = {"sym32", "sym64", "sym64_occ10", "rows"};
+        for (int v = 0; v < 4; ++v)
+            if (!std::strcmp(ev, names[v])) {
+                P.pair_variant = v;
+                P.pairs_sym = v != Impl::PAIRS_ROWS;
+            }
+        return;
+    }
+    if ((et && !std::strcmp(et, "0")) || pe || po || P.n < 2) return;
+    static std::mutex mu;
+    static std::map<std::tuple<int, int, int>, int> cache;
+    int bucket = 0;
+    while ((2 << bucket) <= P.n) ++bucket;
+    const auto key = std::make_tuple(P.opt.device, P.nmol > 1 ? 1 : 0, bucket);
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        const auto it = cache.find(key);
+        if (it != cache.end()) {
+            P.pair_variant = it->second;
+            P.pairs_sym = P.pair_variant != Impl::PAIRS_ROWS;
+            return;
+        }
+    }
+    std::vector<double> h;
+    for (const Model* m : mols) h.insert(h.end(), m->xyz_setup.begin(), m->xyz_setup.end());
+    DBuf<double> x;
+    x.upload(h);
+    enqueue(x.p, true);
+    View V = P.view();
+    const dim3 tgrid(nblk(P.n, kTile), P.nsplit);
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    float best = 1e30f;
+    int pick = P.pair_variant;
+    for (int v = 0; v < 4; ++v) {
+        auto run = [&]() {
+            if (v == Impl::PAIRS_ROWS) k_pairs<double><<<tgrid, kTile, 0, P.stream>>>(V, P.nsplit);
+            else P.launch_pairs_sym<kPairBoth>(v, V, P.stream);
+        };
+        run();
+        CK(cudaEventRecord(e0, P.stream));
+        for (int r = 0; r < 3; ++r) run();
+        CK(cudaEventRecord(e1, P.stream));
+        CK(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        P.pair_ms[v] = ms / 3.f;
+        if (ms < best) {
+            best = ms;
+            pick = v;
+        }
+    }
+    CK(cudaGetLastError());
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    P.pair_variant = pick;
+    P.pairs_sym = pick != Impl::PAIRS_ROWS;
+    std::lock_guard<std::mutex> lock(mu);
+    cache[key] = pick;
+}
+
+const char* Engine::pair_kernel_name() const
+{
+    switch (p_->pair_variant) {
+    case Impl::PAIRS_SYM32: return "sym32";
+    case Impl::PAIRS_SYM64_OCC: return "sym64_occ10";
+    case Impl::PAIRS_ROWS: return "rows";
+    default: return "sym64";
+    }
 }
 
 bool Engine::switch_to_lu()
@@ -1599,9 +1719,7 @@ void Engine::launch_body()
     // Coulomb + D4 pairs by tile pairs (each pair once); PART selects the terms
     auto pairs_sym = [&](auto part, cudaStream_t st) {
         constexpr int PT = decltype(part)::value;
-        if (P.pair_tile == 32) k_pairs_sym<double, 16, 32, PT><<<P.nsym, 32, 0, st>>>(V, P.symtiles.p);
-        else if (P.pairs_occ) k_pairs_sym<double, 10, kST, PT><<<P.nsym, kST, 0, st>>>(V, P.symtiles.p);
-        else k_pairs_sym<double, 8, kST, PT><<<P.nsym, kST, 0, st>>>(V, P.symtiles.p);
+        P.template launch_pairs_sym<PT>(P.pair_variant, V, st);
     };
     // split unless the solver is the classic PCG, whose cooperative grid fills every SM:
     // then nothing runs beside it, and the split pass costs more than it hides

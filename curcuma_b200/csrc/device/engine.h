@@ -71,6 +71,9 @@ public:
     bool switch_to_direct();
     // EEQ solver in use: "library", "tiled", "pcg", "lu" or "batched"
     const char* solver_name() const;
+    // Coulomb + D4 pair kernel variant picked by the set-up autotuner: "sym32", "sym64",
+    // "sym64_occ10" or "rows"
+    const char* pair_kernel_name() const;
     // iterations of the last iterative EEQ solve (0 for direct solvers)
     int eeq_iterations();
     // kernels of this library per evaluation while the step replays as a graph (-1 before
@@ -86,6 +89,7 @@ public:
     static constexpr int kNumTerms = 14;
 
 private:
+    void tune_pairs(const std::vector<const Model*>& mols);
     void launch_positions(const double* d_xyz, bool bohr);
     void launch_body();
     struct Impl;

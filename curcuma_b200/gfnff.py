@@ -296,6 +296,10 @@ class GFNFF:
                                                  out.size, ctypes.byref(cnt)))
         return out[:cnt.value * width].reshape(cnt.value, width) if width > 1 else out[:cnt.value]
 
+    def pairKernel(self) -> str:
+        """Pair kernel variant picked by the set-up autotuner (diagnostic)."""
+        return self._lib.gfnff_pair_kernel(self._h).decode()
+
     def eeqSolver(self) -> str:
         """EEQ solver chosen at setup ("library", "tiled", "pcg", "lu", "batched")."""
         return self._lib.gfnff_eeq_solver(self._h).decode()

@@ -190,6 +190,13 @@ gfnff_status gfnff_eeq_charges_noalloc(int natoms, int nfrag, const double* d_xy
  * (eeq_solver.cpp:1448-2086); this query has no counterpart there. */
 const char* gfnff_eeq_solver(gfnff_handle* h);
 
+/* Variant of the Coulomb + D4 pair kernel that the set-up autotuner picked for the
+ * handle's system by timing: "sym32" / "sym64" (each pair once over 32- or 64-atom tiles),
+ * "sym64_occ10" (64-atom tiles at 10 blocks per SM) or "rows" (both directions by rows); ""
+ * before setup.  The pick is cached per device, batch or single molecule and size bucket.
+ * Diagnostic without a counterpart in the reference. */
+const char* gfnff_pair_kernel(gfnff_handle* h);
+
 /* Iterations of the last iterative EEQ solve (0 for the direct solvers, -1 before
  * setup); synchronises the handle's stream.  Diagnostic without a counterpart in the
  * reference. */
