@@ -387,7 +387,7 @@ struct Engine::Impl {
     // EEQ solver of a single-molecule engine (chosen at upload, see upload_batch)
     enum { SOLVE_LIBRARY = 0, SOLVE_TILED = 1, SOLVE_PCG = 2, SOLVE_BATCH = 3 };
     bool batch_ready = false;   // the batched kernel's structures exist (batches, small molecules)
-    int solver = SOLVE_LIBRARY;
+    int solver = SOLVE_TILED;
     // persistent tiled Cholesky (k_chol)
     DBuf<int4> ctasks;
     DBuf<int> cflags;      // next, err, cnt[nt*nt], fin[nt*nt], ydone[nt]
@@ -1378,13 +1378,15 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
         DBuf<double> x;
         std::vector<double> h(mols[0]->xyz_setup);
         x.upload(h);
-        P.solver = Impl::SOLVE_LIBRARY;
+        // the probe factors with the in-house tiled Cholesky (k_chol: NOT_SPD on a pivot <= 0)
+        P.solver = Impl::SOLVE_TILED;
         enqueue(x.p, true);
         int st = 0;
         fetch(nullptr, nullptr, &st, nullptr);
         if (st == GFNFF_NOT_SPD) P.use_lu = true;
-        // Solver: GFNFF_EEQ_SOLVER=library|tiled|pcg forces one; otherwise the fastest of
-        // the available ones over three evaluations at the setup geometry
+        // Solver: GFNFF_EEQ_SOLVER=library|tiled|pcg|batched forces one; otherwise the fastest
+        // of the in-house ones (tiled, pcg, batched) over three evaluations at the setup
+        // geometry.  cuSOLVER ("library") is an explicit opt-in only.
         if (!P.use_lu) {
             const char* env = std::getenv("GFNFF_EEQ_SOLVER");
             std::vector<int> cand;
@@ -1393,7 +1395,7 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
             else if (env && !std::strcmp(env, "pcg") && P.pcg_ready) cand = {Impl::SOLVE_PCG};
             else if (env && !std::strcmp(env, "batched") && P.batch_ready && !P.resp_on) cand = {Impl::SOLVE_BATCH};
             else {
-                cand = {Impl::SOLVE_LIBRARY, Impl::SOLVE_TILED};
+                cand = {Impl::SOLVE_TILED};
                 if (P.pcg_ready) cand.push_back(Impl::SOLVE_PCG);
                 // the batched kernel keeps no factor for the charge-response solve
                 if (P.batch_ready && !P.resp_on) cand.push_back(Impl::SOLVE_BATCH);
@@ -1405,7 +1407,7 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
                 CK(cudaEventCreate(&e0));
                 CK(cudaEventCreate(&e1));
                 float best = 1e30f;
-                int pick = Impl::SOLVE_LIBRARY;
+                int pick = Impl::SOLVE_TILED;
                 for (int c : cand) {
                     P.solver = c;
                     if (c == Impl::SOLVE_PCG) P.pcg_max_iter = 200;
@@ -1541,7 +1543,7 @@ bool Engine::switch_to_direct()
     if (p_->nmol != 1) return false;
     if (p_->solver != Impl::SOLVE_PCG && !(p_->solver == Impl::SOLVE_BATCH && p_->batch_tc)) return false;
     p_->drop_graphs();
-    p_->solver = Impl::SOLVE_LIBRARY;
+    p_->solver = Impl::SOLVE_TILED;   // the in-house FP64 Cholesky
     return true;
 }
 

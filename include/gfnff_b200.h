@@ -183,10 +183,13 @@ gfnff_status gfnff_eeq_charges_noalloc(int natoms, int nfrag, const double* d_xy
                                        const double* d_cn, const int* d_frag, const double* d_qfrag,
                                        double* d_q, int* d_status, void* stream);
 
-/* Name of the EEQ solver chosen for the handle's molecule at setup: "library" (cuSOLVER
- * Cholesky), "tiled" (persistent tiled Cholesky), "pcg" (block-Jacobi conjugate
- * gradients, true residual <= 1e-12 max|b|), "lu" (indefinite matrix) or "batched"; ""
- * before setup.  curcuma's EEQSolver also picks among several solvers
+/* Name of the EEQ solver chosen for the handle's molecule at setup: "tiled" (the in-house
+ * persistent tiled Cholesky), "pcg" (block-Jacobi conjugate gradients; FP64 true residual
+ * <= 1e-12 max|b| in the FP64 form, <= 1e-10 in the mixed form), "batched" (per-molecule
+ * shared-memory Cholesky; tensor-core factorisation with FP64 refinement in the mixed
+ * form), "lu" (indefinite matrix, cuSOLVER's pivoted LU) or "library" (cuSOLVER's Cholesky,
+ * only when GFNFF_EEQ_SOLVER=library asks for it); "" before setup.  The choice is made by
+ * timing the in-house solvers at setup.  curcuma's EEQSolver also picks among several solvers
  * (eeq_solver.cpp:1448-2086); this query has no counterpart there. */
 const char* gfnff_eeq_solver(gfnff_handle* h);
 
