@@ -441,43 +441,27 @@ gfnff_status gfnff_md_nve(gfnff_handle* h, int nsteps, double dt_fs, double* xyz
     if (!h->ready) return fail(h, GFNFF_NOT_READY, "gfnff_setup has not been called");
     if (nsteps < 0 || !(dt_fs > 0.0) || !xyz || !vel || !mass || !epot || !ekin)
         return fail(h, GFNFF_INVALID_ARG, "invalid MD arguments");
+    if (h->nmol) return fail(h, GFNFF_INVALID_ARG, "batch handle (MD runs on single-molecule handles)");
     const int n = h->natoms;
     for (int i = 0; i < n; ++i)
         if (!(mass[i] > 0.0)) return fail(h, GFNFF_INVALID_ARG, "non-positive mass");
     try {
-        // chunks of 100 steps; between chunks the HB/XB lists are re-detected when the
-        // RMSD-like measure sqrt(sum d^2)/N exceeds the threshold (single molecules)
-        int done = 0, worst = 0;
-        std::vector<double> ep, ek;
-        while (done < nsteps && worst == 0) {
-            const int chunk = std::min(100, nsteps - done);
-            ep.assign(chunk + 1, 0.0);
-            ek.assign(chunk + 1, 0.0);
-            md_nve(*h->eng, chunk, dt_fs, xyz, vel, mass, ep.data(), ek.data(), &worst);
-            if (done == 0) {
-                epot[0] = ep[0];
-                ekin[0] = ek[0];
-            }
-            for (int t = 1; t <= chunk; ++t) {
-                epot[done + t] = ep[t];
-                ekin[done + t] = ek[t];
-            }
-            done += chunk;
-            if (worst == 0 && h->eng->cn_list_stale(true)) h->eng->refresh_cn_list();
-            if (h->nmol == 0 && h->opt.hbond && worst == 0) {
-                double msd = 0.0;
-                h->eng->fetch(nullptr, nullptr, nullptr, &msd);
-                if (std::sqrt(msd) / (double)n > h->opt.hb_rmsd_bohr) {
-                    std::vector<double> xb(3 * (size_t)n);
-                    for (int k = 0; k < 3 * n; ++k) xb[k] = xyz[k] * kAngToBohr;
-                    redetect_hbxb(h->model, xb.data());
-                    h->eng->upload_hbxb(h->model);
-                    h->eng->set_hb_reference(xb.data());
-                    h->hb_ref = xb;
-                }
-            }
+        // the HB/XB lists follow the trajectory step by step, as curcuma's evaluation does
+        // before every energy (gfnff_method.cpp:1597-1613): the device loop finds the
+        // first step over the threshold and rolls back to it for the re-detection
+        MdRefresh R;
+        if (h->opt.hbond) {
+            R.hb_rmsd_bohr = h->opt.hb_rmsd_bohr;
+            h->eng->set_hb_reference(h->hb_ref.data());
+            R.redetect = [h](const double* xb) {
+                redetect_hbxb(h->model, xb);
+                h->eng->upload_hbxb(h->model);
+                h->eng->set_hb_reference(xb);
+                h->hb_ref.assign(xb, xb + 3 * (size_t)h->model.n);
+            };
         }
-        for (int t = done + 1; t <= nsteps; ++t) epot[t] = ekin[t] = 0.0;
+        int worst = 0;
+        md_nve(*h->eng, nsteps, dt_fs, xyz, vel, mass, epot, ekin, &worst, &R);
         if (worst != 0) return fail(h, (gfnff_status)worst, "MD stopped: evaluation failed");
     } catch (const std::exception& e) {
         return fail(h, GFNFF_CUDA_ERROR, e.what());

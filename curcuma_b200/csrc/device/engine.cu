@@ -49,6 +49,7 @@ namespace gfnff {
 #include "k_eeq_tc.cuh"
 #include "k_chol.cuh"
 #include "k_pcg.cuh"
+#include "k_lu.cuh"
 }  // namespace gfnff
 #include "../setup/linalg.h"
 namespace gfnff {
@@ -384,6 +385,10 @@ struct Engine::Impl {
     int lwork = 0;
     int lda = 2;           // leading dimension of M (>= nred + 1, even; row nred holds b for k_chol)
     bool use_lu = false;   // reduced EEQ matrix not positive definite: pivoted LU instead
+    // in-house pivoted LU (k_lu_factor): grid, pivot candidates, grid barrier
+    int lu_grid = 1;
+    DBuf<double> lupart;
+    DBuf<unsigned int> lubar;
     // EEQ solver of a single-molecule engine (chosen at upload, see upload_batch)
     enum { SOLVE_LIBRARY = 0, SOLVE_TILED = 1, SOLVE_PCG = 2, SOLVE_BATCH = 3 };
     bool batch_ready = false;   // the batched kernel's structures exist (batches, small molecules)
@@ -1119,6 +1124,15 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
         P.ipiv.alloc(P.nred);
         int nsm = 0;
         CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, P.opt.device));
+        // in-house pivoted LU (indefinite matrices): one co-resident block per SM
+        {
+            int per_sm = 0;
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)k_lu_factor, kLuThreads, 0));
+            P.lu_grid = std::max(1, std::min(nsm, nsm * per_sm));
+            P.lupart.alloc(2 * (size_t)P.lu_grid);
+            P.lubar.alloc(2 * kBarGen);
+            CK(cudaMemset(P.lubar.p, 0, 2 * kBarGen * sizeof(unsigned int)));
+        }
         // persistent tiled Cholesky: task list, flags, co-resident grid
         {
             auto tasks = chol_tasks(P.nred);
@@ -1801,9 +1815,12 @@ void Engine::launch_body()
             } else if (sv == Impl::SOLVE_LIBRARY) {
                 CS(cusolverDnDpotrf(P.sol, CUBLAS_FILL_MODE_LOWER, P.nred, P.M.p, P.lda, P.work.p, P.lwork, P.info.p));
                 CS(cusolverDnDpotrs(P.sol, CUBLAS_FILL_MODE_LOWER, P.nred, 1, P.M.p, P.lda, P.bvec.p, P.nred, P.info2.p));
-            } else {
-                CS(cusolverDnDgetrf(P.sol, P.nred, P.nred, P.M.p, P.lda, P.work.p, P.ipiv.p, P.info.p));
-                CS(cusolverDnDgetrs(P.sol, CUBLAS_OP_N, P.nred, 1, P.M.p, P.lda, P.ipiv.p, P.bvec.p, P.nred, P.info2.p));
+            } else {   // indefinite: in-house pivoted LU, b eliminated along, then U x = y
+                CK(cudaMemsetAsync(P.lubar.p, 0, sizeof(unsigned int), s));
+                LUArgs L{P.M.p, P.lda, P.nred, P.bvec.p, P.ipiv.p, P.info.p, P.lupart.p, P.lubar.p};
+                void* args[] = {&L};
+                CK(cudaLaunchCooperativeKernel((const void*)k_lu_factor, dim3(P.lu_grid), dim3(kLuThreads), args, 0, s));
+                k_lu_back<<<1, 1024, 0, s>>>(P.M.p, P.lda, P.nred, P.bvec.p, P.info.p);
             }
         }
         side_after();
@@ -1841,13 +1858,13 @@ void Engine::launch_body()
         k_resp_rhs<<<nblk(P.nred), kBlock, 0, s>>>(V, P.red2atom.p, P.anchor.p, P.bres.p);
         const double* y = P.bres.p;
         if (P.use_lu) {
-            CS(cusolverDnDgetrs(P.sol, CUBLAS_OP_N, P.nred, 1, P.M.p, P.lda, P.ipiv.p, P.bres.p, P.nred, P.info2.p));
+            k_lu_solve_rhs<<<1, 1024, 0, s>>>(P.M.p, P.lda, P.nred, P.ipiv.p, P.bres.p, P.info.p);
         } else if (P.solver == Impl::SOLVE_PCG) {
             P.pcg_launch(P.bres.p, P.xres.p, P.info3.p, 1);
             k_merge_info<<<1, 1, 0, s>>>(P.info.p, P.info3.p);
             y = P.xres.p;
-        } else {   // the Cholesky factor (cuSOLVER or the tiled kernel) is in M
-            CS(cusolverDnDpotrs(P.sol, CUBLAS_FILL_MODE_LOWER, P.nred, 1, P.M.p, P.lda, P.bres.p, P.nred, P.info2.p));
+        } else {   // the Cholesky factor (the tiled kernel, or cuSOLVER when asked for) is in M
+            k_chol_solve_rhs<<<1, 1024, 0, s>>>(P.M.p, P.lda, P.nred, P.bres.p, P.info.p);
         }
         k_eeq_expand<<<nblk((long)P.nfrag * 32), kBlock, 0, s>>>(P.nfrag, nullptr, P.atom2red.p, P.frag_off.p,
                                                                   P.frag_atoms.p, y, P.ures.p);

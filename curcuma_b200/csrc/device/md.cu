@@ -26,25 +26,53 @@ constexpr double kAngToBohrMd = 1.0 / 0.529177210903;
         if (e_ != cudaSuccess) throw std::runtime_error(std::string("CUDA (md): ") + cudaGetErrorString(e_)); \
     } while (0)
 
-// v += -dt/2 g / m ; x += dt v
+// Per-run device record: [0] first step whose evaluation should have used refreshed HB/XB
+// lists (-1: none), [1] first step whose evaluation failed (-1: none), [2] its status.
+struct MdFlags {
+    int* rec;
+    const double* msd;      // the engine's sum of squared displacements vs the HB reference
+    const int* eval_st;     // the engine's status of the last evaluation
+    double thr;             // HB/XB refresh threshold (bohr); <= 0 disables the record
+    int natoms;
+    double *xs, *vs;        // state before the recorded step's evaluation
+    __device__ bool refresh_due() const
+    {
+        return thr > 0.0 && rec[0] < 0 && sqrt(*msd) / (double)natoms > thr;
+    }
+};
+
+// v += -dt/2 g / m ; x += dt v.  Thread 0 first closes the record of the previous step
+// tprev (whose measure is still in msd; the next evaluation resets it).
 __global__ void k_kick_drift(int n3, double dt, const double* __restrict__ invm, const double* __restrict__ g,
-                             double* v, double* x)
+                             double* v, double* x, MdFlags F, int tprev)
 {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k == 0 && F.refresh_due()) F.rec[0] = tprev;
     if (k >= n3) return;
     const double vk = v[k] - 0.5 * dt * g[k] * invm[k / 3];
     v[k] = vk;
     x[k] += dt * vk;
 }
 
-// v += -dt/2 g / m and ekin += sum m v^2 / 2
+// after step t's evaluation: keep (x, v) if the step is due for a refresh, note a failed
+// evaluation, then v += -dt/2 g / m and ekin += sum m v^2 / 2
 __global__ void k_kick_ekin(int n3, double dt, const double* __restrict__ invm, const double* __restrict__ g,
-                            double* v, double* ekin)
+                            double* v, const double* __restrict__ x, double* ekin, MdFlags F, int t)
 {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool snap = F.refresh_due();   // rec[0] is written only by later kernels
+    if (k == 0 && *F.eval_st != 0 && F.rec[1] < 0) {
+        F.rec[1] = t;
+        F.rec[2] = *F.eval_st;
+    }
     double e = 0.0;
     if (k < n3) {
-        const double vk = v[k] - 0.5 * dt * g[k] * invm[k / 3];
+        const double v0 = v[k];
+        if (snap) {
+            F.xs[k] = x[k];
+            F.vs[k] = v0;
+        }
+        const double vk = v0 - 0.5 * dt * g[k] * invm[k / 3];
         v[k] = vk;
         e = 0.5 * vk * vk / invm[k / 3];
     }
@@ -58,6 +86,19 @@ __global__ void k_kick_ekin(int n3, double dt, const double* __restrict__ invm, 
         for (int o = 16; o > 0; o >>= 1) e += __shfl_down_sync(0xffffffffu, e, o);
         if (lane == 0 && e != 0.0) atomicAdd(ekin, e);
     }
+}
+
+// the record of the chunk's last step t
+__global__ void k_md_close(MdFlags F, int t)
+{
+    if (F.refresh_due()) F.rec[0] = t;
+}
+
+__global__ void k_md_reset(int* rec)
+{
+    rec[0] = -1;
+    rec[1] = -1;
+    rec[2] = 0;
 }
 
 template <class T>
@@ -75,46 +116,76 @@ struct Dev {
 }  // namespace
 
 int md_nve(Engine& eng, int nsteps, double dt_fs, double* xyz_ang, double* vel_ang_fs, const double* mass_amu,
-           double* epot, double* ekin, int* status)
+           double* epot, double* ekin, int* status, const MdRefresh* refresh)
 {
     const int n = eng.natoms(), n3 = 3 * n;
     cudaStream_t s = (cudaStream_t)eng.stream();
     const double dt = dt_fs * kFsToAtu;
     const double vconv = kAngToBohrMd / kFsToAtu;   // A/fs -> bohr/atu
+    const bool hb = refresh && refresh->hb_rmsd_bohr > 0.0 && refresh->redetect;
     std::vector<double> hx(n3), hv(n3), him(n);
     for (int k = 0; k < n3; ++k) {
         hx[k] = xyz_ang[k] * kAngToBohrMd;
         hv[k] = vel_ang_fs[k] * vconv;
     }
     for (int i = 0; i < n; ++i) him[i] = 1.0 / (mass_amu[i] * kAmuToMe);
-    Dev<double> x(n3), v(n3), invm(n), ep(nsteps + 1), ek(nsteps + 1);
+    Dev<double> x(n3), v(n3), invm(n), ep(nsteps + 1), ek(nsteps + 1), xs(hb ? n3 : 1), vs(hb ? n3 : 1);
+    Dev<int> rec(3);
     MDCK(cudaMemcpyAsync(x.p, hx.data(), n3 * sizeof(double), cudaMemcpyHostToDevice, s));
     MDCK(cudaMemcpyAsync(v.p, hv.data(), n3 * sizeof(double), cudaMemcpyHostToDevice, s));
     MDCK(cudaMemcpyAsync(invm.p, him.data(), n * sizeof(double), cudaMemcpyHostToDevice, s));
+    MDCK(cudaMemsetAsync(ep.p, 0, (nsteps + 1) * sizeof(double), s));
     MDCK(cudaMemsetAsync(ek.p, 0, (nsteps + 1) * sizeof(double), s));
+    const MdFlags F{rec.p, eng.d_hb_msd(), eng.d_status(), hb ? refresh->hb_rmsd_bohr : 0.0, n, xs.p, vs.p};
     const int B = 256, G = (n3 + B - 1) / B;
-    // step 0: forces at the start geometry and the initial kinetic energy
-    eng.enqueue(x.p, true, ep.p);
-    k_kick_ekin<<<G, B, 0, s>>>(n3, 0.0, invm.p, eng.d_grad(), v.p, ek.p);
-    int worst = 0;
-    for (int t = 1; t <= nsteps; ++t) {
-        k_kick_drift<<<G, B, 0, s>>>(n3, dt, invm.p, eng.d_grad(), v.p, x.p);
-        eng.enqueue(x.p, true, ep.p + t);
-        k_kick_ekin<<<G, B, 0, s>>>(n3, dt, invm.p, eng.d_grad(), v.p, ek.p + t);
-        if (t % 100 == 0 || t == nsteps) {   // status check without stalling every step
-            int h = 0;
-            MDCK(cudaMemcpyAsync(&h, eng.d_status(), sizeof(int), cudaMemcpyDeviceToHost, s));
-            MDCK(cudaStreamSynchronize(s));
-            worst = std::max(worst, h);
-            if (h != 0) break;
+    int h_rec[3];
+    int worst = 0, last_good = nsteps, resumed_at = -1;
+    int t = 0;
+    bool fresh = true;   // step t starts from a recorded state: no drift before its evaluation
+    k_md_reset<<<1, 1, 0, s>>>(rec.p);
+    while (t <= nsteps) {
+        // chunks of up to 100 evaluations; the host reads the record once per chunk
+        const int end = std::min(t + 99, nsteps);
+        for (int u = t; u <= end; ++u) {
+            if (!(u == t && fresh)) k_kick_drift<<<G, B, 0, s>>>(n3, dt, invm.p, eng.d_grad(), v.p, x.p, F, u - 1);
+            eng.enqueue(x.p, true, ep.p + u);
+            k_kick_ekin<<<G, B, 0, s>>>(n3, u == 0 ? 0.0 : dt, invm.p, eng.d_grad(), v.p, x.p, ek.p + u, F, u);
         }
+        k_md_close<<<1, 1, 0, s>>>(F, end);
+        MDCK(cudaGetLastError());
+        MDCK(cudaMemcpyAsync(h_rec, rec.p, sizeof(h_rec), cudaMemcpyDeviceToHost, s));
+        MDCK(cudaStreamSynchronize(s));
+        const int due = h_rec[0], failed = h_rec[1];
+        if (failed >= 0 && (due < 0 || failed < due)) {
+            worst = h_rec[2];
+            last_good = failed;
+            break;
+        }
+        if (due >= 0) {
+            // roll back to the state before step `due`, refresh the lists there, redo it
+            if (due == resumed_at) throw std::runtime_error("md: HB/XB refresh did not reset the reference geometry");
+            MDCK(cudaMemcpyAsync(x.p, xs.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, s));
+            MDCK(cudaMemcpyAsync(v.p, vs.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, s));
+            MDCK(cudaMemcpyAsync(hx.data(), xs.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, s));
+            MDCK(cudaMemsetAsync(ek.p + due, 0, (nsteps + 1 - due) * sizeof(double), s));
+            k_md_reset<<<1, 1, 0, s>>>(rec.p);
+            MDCK(cudaStreamSynchronize(s));
+            refresh->redetect(hx.data());
+            t = due;
+            fresh = true;
+            resumed_at = due;
+            continue;
+        }
+        if (end < nsteps && eng.cn_list_stale(true)) eng.refresh_cn_list();
+        t = end + 1;
+        fresh = false;
     }
-    MDCK(cudaGetLastError());
     MDCK(cudaMemcpyAsync(hx.data(), x.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, s));
     MDCK(cudaMemcpyAsync(hv.data(), v.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, s));
     MDCK(cudaMemcpyAsync(epot, ep.p, (nsteps + 1) * sizeof(double), cudaMemcpyDeviceToHost, s));
     MDCK(cudaMemcpyAsync(ekin, ek.p, (nsteps + 1) * sizeof(double), cudaMemcpyDeviceToHost, s));
     MDCK(cudaStreamSynchronize(s));
+    for (int u = last_good + 1; u <= nsteps; ++u) epot[u] = ekin[u] = 0.0;
     for (int k = 0; k < n3; ++k) {
         xyz_ang[k] = hx[k] / kAngToBohrMd;
         vel_ang_fs[k] = hv[k] / vconv;

@@ -75,6 +75,59 @@ def test_device_md_matches_host_driven_verlet():
     assert np.abs(dev.velocities() - v * BOHR * 41.341373335).max() < 1e-8
 
 
+def _approaching_waters():
+    """Two waters 8.6 A apart (O-O), out of each other's hydrogen-bond candidate range
+    (about 8.4 A), the second moving at 0.02 A/fs towards the first: the HB list gains the
+    dimer's four terms at the first refresh after the pair comes into range (step 64 at
+    the default threshold, 43 at 0.1 bohr in the oracle's run of the same loop)."""
+    w = workloads.water_geometry()
+    X = np.vstack([w, w * np.array([-1.0, 1.0, 1.0]) + np.array([8.6, 0.0, 0.0])])
+    Z = np.array([8, 1, 1, 8, 1, 1])
+    V = np.zeros((6, 3))
+    V[3:, 0] = -0.02
+    V += np.random.default_rng(3).normal(scale=2e-3, size=V.shape)
+    return Z, X, V
+
+
+@pytest.mark.parametrize("thr", [0.3, 0.1])
+def test_hb_lists_refresh_at_the_same_steps_as_the_host_loop(thr):
+    """The device loop re-detects the HB/XB lists at the first step whose
+    sqrt(sum d^2)/N exceeds the threshold (rolling back to that step), which is where the
+    single-point path, called once per step from the host, re-detects them too."""
+    Z, X, V0 = _approaching_waters()
+    m = atomic_masses(Z)
+    nsteps = 240
+    host = GFNFF(hb_rmsd_bohr=thr)
+    assert host.setMolecule(Z, X)
+    dt = 0.5 * 41.341373335
+    me = m * 1822.888486209
+    x = X / BOHR
+    v = V0 / (BOHR * 41.341373335)
+    ep_h = np.zeros(nsteps + 1)
+    counts = []
+    host.updateGeometry(x * BOHR)
+    ep_h[0] = host.calculateEnergy(True)
+    g = host.getGradient()
+    counts.append(host.getHBCount())
+    for t in range(1, nsteps + 1):
+        v -= 0.5 * dt * g / me[:, None]
+        x += dt * v
+        host.updateGeometry(x * BOHR)
+        ep_h[t] = host.calculateEnergy(True)
+        g = host.getGradient()
+        v -= 0.5 * dt * g / me[:, None]
+        counts.append(host.getHBCount())
+    changes = [t for t in range(1, len(counts)) if counts[t] != counts[t - 1]]
+    assert changes and changes[0] % 100 != 0, counts   # the list changes inside a chunk
+    dev = GFNFF(hb_rmsd_bohr=thr)
+    assert dev.setMolecule(Z, X)
+    ep, ek = dev.runMD(nsteps, 0.5, V0)
+    assert not dev.hasError(), dev.getErrorMessage()
+    assert dev.getHBCount() == counts[-1]
+    assert np.abs(ep - ep_h).max() < 1e-8, np.abs(ep - ep_h).argmax()
+    assert np.abs(dev.velocities() - v * BOHR * 41.341373335).max() < 1e-8
+
+
 def test_reference_and_exact_energies_agree():
     Z, X = workloads.alkane(64, 1001)
     a, b = GFNFF(), GFNFF(exact_gradient=True)
