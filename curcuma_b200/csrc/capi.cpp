@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <exception>
 #include <memory>
@@ -97,7 +98,13 @@ gfnff_status gfnff_setup(gfnff_handle* h, int n, const int* Z, const double* xyz
     try {
         SetupOptions so;
         so.hbond = h->opt.hbond != 0;
-        h->model = build_model(n, Z, xyz, charge, so);
+        // the D4 pair list is enumerated by the engine; the HB terms of larger molecules are
+        // detected on the device (GFNFF_HB_DEVICE=0|1 forces the host or the device)
+        BuildLists L;
+        L.host_disp = false;
+        const char* hd = std::getenv("GFNFF_HB_DEVICE");
+        L.host_hb = hd ? !std::strcmp(hd, "0") : n < 512;
+        h->model = build_model(n, Z, xyz, charge, so, L);
     } catch (const std::exception& e) {
         return fail(h, GFNFF_SETUP_FAILED, e.what());
     }
@@ -135,7 +142,13 @@ gfnff_status gfnff_save_parameters(gfnff_handle* h, const char* path)
     if (!path) return fail(h, GFNFF_INVALID_ARG, "NULL path");
     if (!h->ready || h->nmol) return fail(h, GFNFF_NOT_READY, "gfnff_setup has not been called");
     try {
-        save_parameters(h->model, path);
+        if (h->model.hb_on_device || h->model.disp_on_device) {   // the file holds every list
+            Model full = h->model;
+            complete_host_lists(full, h->hb_ref.data());
+            save_parameters(full, path);
+        } else {
+            save_parameters(h->model, path);
+        }
     } catch (const std::exception& e) {
         return fail(h, GFNFF_INVALID_ARG, e.what());
     }
@@ -190,7 +203,9 @@ gfnff_status gfnff_setup_batch(gfnff_handle* h, int nmol, const int* natoms, con
 #pragma omp parallel for schedule(dynamic)
     for (int m = 0; m < nmol; ++m) {
         try {
-            models[m] = build_model(natoms[m], Z + off[m], xyz + 3 * off[m], charges ? charges[m] : 0, so);
+            BuildLists L;
+            L.host_disp = false;   // enumerated by the engine
+            models[m] = build_model(natoms[m], Z + off[m], xyz + 3 * off[m], charges ? charges[m] : 0, so, L);
         } catch (const std::exception& e) {
             errs[m] = e.what();
         }
@@ -282,7 +297,7 @@ gfnff_status gfnff_energy_and_gradient(gfnff_handle* h, const double* xyz, doubl
                 std::vector<double> xb(3 * (size_t)n);
                 for (int k = 0; k < 3 * n; ++k) xb[k] = xyz[k] * kAngToBohr;
                 redetect_hbxb(h->model, xb.data());
-                h->eng->upload_hbxb(h->model);
+                h->eng->upload_hbxb(h->model, xb.data());
                 h->hb_ref = xb;
             }
         }
@@ -377,7 +392,15 @@ gfnff_status gfnff_get_topology(gfnff_handle* h, int kind, int* out, long cap, l
             case 3: for (auto& t : m.inversions) v.insert(v.end(), {t.i, t.j, t.k, t.l}); cnt = (long)m.inversions.size(); break;
             case 4: v = h->eng->device_dispersion_pairs(); cnt = (long)v.size() / 2; break;
             case 5: for (auto& r : m.rep_nonbonded) { v.push_back(r.i); v.push_back(r.j); } cnt = (long)m.rep_nonbonded.size(); break;
-            case 6: for (auto& t : m.hbonds) v.insert(v.end(), {t.a, t.h, t.b, t.case_type}); cnt = (long)m.hbonds.size(); break;
+            case 6:
+                if (m.hb_on_device) {
+                    v = h->eng->hb_terms();
+                    cnt = (long)v.size() / 4;
+                } else {
+                    for (auto& t : m.hbonds) v.insert(v.end(), {t.a, t.h, t.b, t.case_type});
+                    cnt = (long)m.hbonds.size();
+                }
+                break;
             case 7: for (auto& t : m.xbonds) v.insert(v.end(), {t.a, t.x, t.b}); cnt = (long)m.xbonds.size(); break;
             case 8: v = m.hyb; cnt = m.n; break;
             case 9: v = m.frag; cnt = m.n; break;
@@ -455,7 +478,7 @@ gfnff_status gfnff_md_nve(gfnff_handle* h, int nsteps, double dt_fs, double* xyz
             h->eng->set_hb_reference(h->hb_ref.data());
             R.redetect = [h](const double* xb) {
                 redetect_hbxb(h->model, xb);
-                h->eng->upload_hbxb(h->model);
+                h->eng->upload_hbxb(h->model, xb);
                 h->eng->set_hb_reference(xb);
                 h->hb_ref.assign(xb, xb + 3 * (size_t)h->model.n);
             };

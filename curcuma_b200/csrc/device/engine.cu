@@ -22,6 +22,8 @@
 #include <cuda_runtime.h>
 #include <cusolverDn.h>
 
+#include <cub/cub.cuh>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -29,6 +31,7 @@
 #include <cstring>
 #include <dlfcn.h>
 #include <type_traits>
+#include <limits>
 #include <map>
 #include <mutex>
 #include <numeric>
@@ -50,6 +53,7 @@ namespace gfnff {
 #include "k_chol.cuh"
 #include "k_pcg.cuh"
 #include "k_lu.cuh"
+#include "k_hbdetect.cuh"
 }  // namespace gfnff
 #include "../setup/linalg.h"
 namespace gfnff {
@@ -177,11 +181,11 @@ struct HBHost {
         slot = v;
         seen = true;
     }
+    static double qs(double q) { const double e = std::exp(15.0 * q); return e / (e + 1.0); }
+    // the per-atom data that does not depend on the terms
     template <class Map>
-    void add(const Model& M, Map X)
+    void topology(const Model& M, Map X)
     {
-        auto qs = [](double q) { const double e = std::exp(15.0 * q); return e / (e + 1.0); };
-        std::vector<char> sh(M.n, 0), sa(M.n, 0), sb(M.n, 0), sc(M.n, 0);
         for (int a = 0; a < M.n; ++a) {
             const int i = X(a);
             rvdw[i] = M.rvdw[a];
@@ -190,6 +194,12 @@ struct HBHost {
             zlp[i] = (z >= 1 && z <= 86) ? gfnff_tables::repz[z - 1] : 1.0;
             nfl[i] = (z == 7 && M.adj[a].size() == 1) ? 1 : 0;
         }
+    }
+    template <class Map>
+    void add(const Model& M, Map X)
+    {
+        std::vector<char> sh(M.n, 0), sa(M.n, 0), sb(M.n, 0), sc(M.n, 0);
+        topology(M, X);
         for (int ti : hb_order(M)) {
             const HBTerm& t = M.hbonds[ti];
             const int A = X(t.a), H = X(t.h), B = X(t.b);
@@ -359,7 +369,7 @@ struct Engine::Impl {
     DBuf<int4> h_rec;
     DBuf<double> h_qh, h_qa, h_bas, h_aci, h_rvdw, h_zlp;
     DBuf<int> h_pc, h_nfl, h_adjo, h_adj;
-    void upload_hb(const HBHost& T)
+    void upload_hb_atoms(const HBHost& T)
     {
         if (T.mismatch) throw std::runtime_error("HB set-up: per-term parameters differ for one atom");
         std::vector<int> off{0}, adj;
@@ -367,11 +377,30 @@ struct Engine::Impl {
             adj.insert(adj.end(), l.begin(), l.end());
             off.push_back((int)adj.size());
         }
-        h_rec.upload(T.rec); h_qh.upload(T.qh); h_qa.upload(T.qa); h_bas.upload(T.bas); h_aci.upload(T.aci);
+        h_qh.upload(T.qh); h_qa.upload(T.qa); h_bas.upload(T.bas); h_aci.upload(T.aci);
         h_rvdw.upload(T.rvdw); h_zlp.upload(T.zlp); h_pc.upload(T.pc); h_nfl.upload(T.nfl);
         h_adjo.upload(off); h_adj.upload(adj);
+    }
+    void upload_hb(const HBHost& T)
+    {
+        upload_hb_atoms(T);
+        h_rec.upload(T.rec);
         nhb = (int)T.rec.size();
     }
+    // ---- HB terms detected on the device (Model::hb_on_device; k_hbdetect.cuh) ----
+    struct HBDev {
+        const Model* topo = nullptr;   // the model whose topology inputs are loaded
+        int na = 0, nhc = 0;
+        std::vector<unsigned char> bcase;
+        DBuf<unsigned char> fl, bc, flag, tmp;
+        DBuf<double> bas, aci, x, x0;
+        DBuf<int> Zc, bo, bl, ho, hl, hc, map, val, val2, near, nsel;
+        DBuf<long long> cnt, off;
+        DBuf<int4> raw, xref;
+        DBuf<unsigned long long> key, key2;
+        long long nt = 0;
+    } hbd;
+    void detect_hb(const Model& m, const double* xb, std::vector<int>& bond_h, std::map<int, std::vector<int>>& byH);
     DBuf<int> x_a, x_x, x_b;
     DBuf<double> x_pre, x_rv;
     DBuf<int> r_off, r_j;
@@ -622,23 +651,194 @@ Engine::~Engine()
     if (p_->stream) cudaStreamDestroy(p_->stream);
 }
 
-void Engine::upload_hbxb(const Model& m)
+// HB terms of a single molecule detected on the device at xb (bohr, caller order): the
+// topology inputs once per model, the geometry-dependent basicity at every detection; the
+// terms sorted into h_rec, the bond cross reference returned for the bond upload
+void Engine::Impl::detect_hb(const Model& m, const double* xb, std::vector<int>& bond_h,
+                             std::map<int, std::vector<int>>& byH)
+{
+    HBDev& D = hbd;
+    const int na = m.n;
+    cudaStream_t s = stream;
+    const HBAtoms at = hb_atom_data(const_cast<Model&>(m), xb);
+    auto X = [&](int a) { return ix(0, a); };
+    if (D.topo != &m) {
+        D.na = na;
+        std::vector<int> Zc(m.Z.begin(), m.Z.end());
+        std::vector<std::vector<int>> part(na), hyd(na);
+        for (auto& b : m.topo_bonds) {
+            part[b.first].push_back(b.second);
+            part[b.second].push_back(b.first);
+            if (at.hcand[b.first]) hyd[b.second].push_back(b.first);
+            if (at.hcand[b.second]) hyd[b.first].push_back(b.second);
+        }
+        auto csr = [](const std::vector<std::vector<int>>& l, std::vector<int>& o, std::vector<int>& v) {
+            o.assign(1, 0);
+            v.clear();
+            for (auto& r : l) {
+                v.insert(v.end(), r.begin(), r.end());
+                o.push_back((int)v.size());
+            }
+        };
+        std::vector<int> bo, bl, ho, hl, hc, map(na);
+        csr(part, bo, bl);
+        csr(hyd, ho, hl);
+        std::vector<unsigned char> fl(na);
+        D.bcase.assign(na, 2);
+        for (int a = 0; a < na; ++a) {
+            fl[a] = (at.ok[a] ? 1 : 0) | (at.hcand[a] ? 2 : 0);
+            if (at.hcand[a]) hc.push_back(a);
+            map[a] = X(a);
+            const int z = m.Z[a];
+            if (z == 8 && m.adj[a].size() == 1) {
+                const int p = m.adj[a][0];
+                if (m.Z[p] == 6 || m.Z[p] == 7) D.bcase[a] = 3;
+            } else if (z == 7 && m.adj[a].size() == 2) {
+                D.bcase[a] = 4;
+            }
+        }
+        D.nhc = (int)hc.size();
+        D.Zc.upload(Zc); D.bo.upload(bo); D.bl.upload(bl); D.ho.upload(ho); D.hl.upload(hl);
+        D.hc.upload(hc); D.map.upload(map); D.fl.upload(fl); D.bc.upload(D.bcase);
+        D.aci.upload(at.aci);
+        D.x0.upload(m.xyz_setup);
+        D.cnt.alloc(na); D.off.alloc(na); D.near.alloc(1); D.nsel.alloc(1);
+        D.topo = &m;
+    }
+    D.x.upload(std::vector<double>(xb, xb + 3 * (size_t)na));
+    D.bas.upload(at.bas);
+    // the engine's per-atom HB data (every atom; the kernel reads those of its terms)
+    {
+        HBHost T(n);
+        T.topology(m, X);
+        for (int a = 0; a < na; ++a) {
+            const int i = X(a);
+            T.qh[i] = HBHost::qs(m.qa[a]);
+            T.qa[i] = HBHost::qs(-m.qa[a]);
+            T.bas[i] = at.bas[a];
+            T.aci[i] = at.aci[a];
+            if (D.bcase[a] == 3) T.pc[i] = X(m.adj[a][0]);
+        }
+        upload_hb_atoms(T);
+    }
+    HBDetArgs A{na, D.x.p, D.fl.p, D.bas.p, D.aci.p, D.bc.p, D.bo.p, D.bl.p, D.ho.p, D.hl.p, D.hc.p, D.nhc,
+                at.thr1, at.thr2, D.cnt.p, D.off.p, nullptr};
+    const unsigned grid = (unsigned)(((long)na * 32 + 255) / 256);
+    k_hb_detect<false><<<grid, 256, 0, s>>>(A);
+    CK(cudaGetLastError());
+    size_t need = 0, b = 0;
+    CK(cub::DeviceScan::ExclusiveSum(nullptr, b, D.cnt.p, D.off.p, na, s));
+    need = b;
+    if (D.tmp.n < need) D.tmp.alloc(need);
+    CK(cub::DeviceScan::ExclusiveSum(D.tmp.p, b, D.cnt.p, D.off.p, na, s));
+    long long last[2] = {0, 0};
+    CK(cudaMemcpyAsync(&last[0], D.off.p + na - 1, sizeof(long long), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(&last[1], D.cnt.p + na - 1, sizeof(long long), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    const long long nt = last[0] + last[1];
+    if (nt > (long long)std::numeric_limits<int>::max() / 2) throw std::runtime_error("HB detection: too many terms");
+    D.nt = nt;
+    int near = 0;
+    std::vector<int4> xr;
+    if (nt > 0) {
+        const int ni = (int)nt;
+        D.raw.alloc(ni); D.key.alloc(ni); D.key2.alloc(ni); D.val.alloc(ni); D.val2.alloc(ni);
+        D.flag.alloc(ni); D.xref.alloc(ni);
+        A.out = D.raw.p;
+        k_hb_detect<true><<<grid, 256, 0, s>>>(A);
+        const unsigned g2 = (unsigned)((nt + 255) / 256);
+        k_hb_keys<<<g2, 256, 0, s>>>(nt, D.raw.p, D.x0.p, D.key.p, D.val.p);
+        CK(cub::DeviceRadixSort::SortPairs(nullptr, b, D.key.p, D.key2.p, D.val.p, D.val2.p, ni, 0, 64, s));
+        need = b;
+        CK(cub::DeviceSelect::Flagged(nullptr, b, D.raw.p, D.flag.p, D.xref.p, D.nsel.p, ni, s));
+        need = std::max(need, b);
+        if (D.tmp.n < need) D.tmp.alloc(need);
+        b = D.tmp.n;
+        CK(cub::DeviceRadixSort::SortPairs(D.tmp.p, b, D.key.p, D.key2.p, D.val.p, D.val2.p, ni, 0, 64, s));
+        h_rec.alloc(ni);
+        CK(cudaMemsetAsync(D.near.p, 0, sizeof(int), s));
+        k_hb_gather<<<g2, 256, 0, s>>>(nt, D.raw.p, D.val2.p, D.key2.p, D.map.p, h_rec.p, D.near.p);
+        k_hb_xref_flags<<<g2, 256, 0, s>>>(nt, D.raw.p, D.Zc.p, D.flag.p);
+        b = D.tmp.n;
+        CK(cub::DeviceSelect::Flagged(D.tmp.p, b, D.raw.p, D.flag.p, D.xref.p, D.nsel.p, ni, s));
+        int nsel = 0;
+        CK(cudaMemcpyAsync(&near, D.near.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(&nsel, D.nsel.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        xr.resize(nsel);
+        if (nsel) CK(cudaMemcpy(xr.data(), D.xref.p, (size_t)nsel * sizeof(int4), cudaMemcpyDeviceToHost));
+        CK(cudaGetLastError());
+    } else {
+        h_rec.free();
+    }
+    nhb = (int)nt;
+    nhb_near = near;
+    // bond -> (H, acceptors): the A-H bonds of an N or O donor with terms of that pair, the
+    // acceptors in detection order (the host cross reference, gfnff_method.cpp:3680-3712)
+    std::map<std::pair<int, int>, std::vector<int>> ahb;
+    for (const int4& r : xr) ahb[{r.x, r.y}].push_back(r.z);
+    bond_h.assign(m.bonds.size(), -1);
+    byH.clear();
+    for (size_t k = 0; k < m.bonds.size(); ++k) {
+        const auto& bd = m.bonds[k];
+        int H = -1, Ad = -1;
+        if (m.Z[bd.i] == 1) { H = bd.i; Ad = bd.j; }
+        else if (m.Z[bd.j] == 1) { H = bd.j; Ad = bd.i; }
+        else continue;
+        if (m.Z[Ad] != 7 && m.Z[Ad] != 8) continue;
+        auto it = ahb.find({Ad, H});
+        if (it == ahb.end() || it->second.empty()) continue;
+        bond_h[k] = H;
+        byH[H].insert(byH[H].end(), it->second.begin(), it->second.end());
+    }
+}
+
+std::vector<int> Engine::hb_terms() const
+{
+    const Impl& P = *p_;
+    std::vector<int> v;
+    if (P.hbd.topo == nullptr || P.hbd.nt == 0) return v;
+    std::vector<int4> r((size_t)P.hbd.nt);
+    CK(cudaStreamSynchronize(P.stream));
+    CK(cudaMemcpy(r.data(), P.hbd.raw.p, r.size() * sizeof(int4), cudaMemcpyDeviceToHost));
+    v.reserve(4 * r.size());
+    for (auto& t : r) v.insert(v.end(), {t.x, t.y, t.z, t.w});
+    return v;
+}
+
+long long Engine::hb_count() const { return p_->nhb; }
+
+void Engine::upload_hbxb(const Model& m, const double* hb_xyz_bohr)
 {
     p_->drop_graphs();
     if (p_->nmol != 1) throw std::runtime_error("upload_hbxb: single-molecule engines only");
     Impl& P = *p_;
     auto X = [&](int a) { return P.ix(0, a); };
+    // HB terms: the model's host lists, or detected here on the device (hb_on_device);
+    // either way the bond -> (H, acceptors) cross reference for the bond modulation
+    std::vector<int> bond_h(m.bonds.size(), -1);
+    std::map<int, std::vector<int>> byH;
+    if (!m.hb_on_device) {
+        for (auto& e : m.bond_hb) byH[e.h].insert(byH[e.h].end(), e.b_atoms.begin(), e.b_atoms.end());
+        for (size_t k = 0; k < m.bonds.size(); ++k)
+            if (m.bonds[k].nr_hb >= 1) bond_h[k] = m.bonds[k].hb_h;
+        HBHost T(P.n);
+        T.add(m, X);
+        P.upload_hb(T);
+        P.nhb_near = hb_near_count(m);
+    } else {
+        P.detect_hb(m, hb_xyz_bohr ? hb_xyz_bohr : m.xyz_setup.data(), bond_h, byH);
+    }
     // bonds carry the HB modulation data
     {
         std::vector<int> bi, bj, bh, off{0}, hb;
         std::vector<double> fc, al, r0i, r0j, cki, ckj, sh, ff;
-        std::map<int, std::vector<int>> byH;
-        for (auto& e : m.bond_hb) byH[e.h].insert(byH[e.h].end(), e.b_atoms.begin(), e.b_atoms.end());
-        for (auto& b : m.bonds) {
+        for (size_t k = 0; k < m.bonds.size(); ++k) {
+            const auto& b = m.bonds[k];
             bi.push_back(X(b.i)); bj.push_back(X(b.j));
             fc.push_back(b.fc); al.push_back(b.alpha); r0i.push_back(b.r0_base_i); r0j.push_back(b.r0_base_j);
             cki.push_back(b.cnfak_i); ckj.push_back(b.cnfak_j); sh.push_back(b.rabshift); ff.push_back(b.ff);
-            int H = b.nr_hb >= 1 ? b.hb_h : -1;
+            const int H = bond_h[k];
             bh.push_back(H >= 0 ? X(H) : -1);
             if (H >= 0) for (int a : byH[H]) hb.push_back(X(a));
             off.push_back((int)hb.size());
@@ -647,12 +847,6 @@ void Engine::upload_hbxb(const Model& m)
         P.b_i.upload(bi); P.b_j.upload(bj); P.b_h.upload(bh); P.b_off.upload(off); P.b_hb.upload(hb);
         P.b_fc.upload(fc); P.b_al.upload(al); P.b_r0i.upload(r0i); P.b_r0j.upload(r0j);
         P.b_cki.upload(cki); P.b_ckj.upload(ckj); P.b_sh.upload(sh); P.b_ff.upload(ff);
-    }
-    {
-        HBHost T(P.n);
-        T.add(m, X);
-        P.upload_hb(T);
-        P.nhb_near = hb_near_count(m);
     }
     {
         std::vector<int> a, x, b;
@@ -680,6 +874,7 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
     }
     CK(cudaSetDevice(P.opt.device));
     if (mols.empty()) throw std::runtime_error("upload: no molecules");
+    P.hbd.topo = nullptr;
     const int nm = (int)mols.size();
     P.nmol = nm;
     // ---- atom order: molecules contiguous, Morton order inside each molecule ----
@@ -1052,6 +1247,8 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
     if (nm == 1) {
         upload_hbxb(*mols[0]);
     } else {   // bonds, HB and XB of every molecule (HB/XB lists stay those of the setup)
+        for (const Model* M : mols)
+            if (M->hb_on_device) throw std::runtime_error("upload: batches take host-detected HB lists");
         std::vector<int> bi, bj, bh, off{0}, hb;
         std::vector<double> fc, al, r0i, r0j, cki, ckj, sh, ff;
         HBHost hbt(n);

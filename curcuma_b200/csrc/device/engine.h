@@ -30,7 +30,14 @@ public:
     void upload(const Model& m);
     void upload_batch(const std::vector<const Model*>& mols);
     // re-uploads the HB/XB lists and the bond<->HB cross reference (single model)
-    void upload_hbxb(const Model& m);
+    // HB/XB lists of a single-molecule engine: the model's host lists, or, with
+    // m.hb_on_device, the HB terms detected on the device at hb_xyz_bohr (caller order;
+    // nullptr: the set-up geometry) and the model's XB list
+    void upload_hbxb(const Model& m, const double* hb_xyz_bohr = nullptr);
+    // the device-detected HB terms (A, H, B, case; caller order, detection order) and the
+    // number of HB terms evaluated
+    std::vector<int> hb_terms() const;
+    long long hb_count() const;
 
     // Enqueues one energy+gradient evaluation.  xyz is N*3 doubles (all atoms of the
     // batch in upload order), device pointer, in bohr when bohr=true else Angstrom.

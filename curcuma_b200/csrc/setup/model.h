@@ -102,17 +102,47 @@ struct Model {
     double e0 = 0.0;
     bool nonbonded_rep_all_pairs = true;        // N < cell threshold: every non-bonded pair
     SetupOptions opt;
+    // lists left to the device (a run-time choice of the set-up; not in the parameter file):
+    // hbonds/bond_hb empty and the bonds' nr_hb/hb_h unset, or disp empty
+    bool hb_on_device = false, disp_on_device = false;
+};
+
+// Per-atom inputs of the hydrogen-bond detection at one geometry (gfnff_method.cpp:7936-8100):
+// basicity (geometry dependent for two-coordinate carbon) and acidity (amide-H scaling),
+// the H-candidate flag (charge above the donor's threshold), the acceptor/donor flag (charge
+// below 0.1, 0.3 beyond neon; no non-pi carbon) and the two squared-distance thresholds:
+// A-B pairs within thr1, and the A-H-B triangle of a non-bonded H within thr2 (bohr^2).
+struct HBAtoms {
+    std::vector<double> bas, aci;
+    std::vector<char> hcand, ok;
+    double thr1 = 0.0, thr2 = 0.0;
+};
+
+// Which of the two largest set-up lists the host builds.  The D4 pair list is enumerated
+// on the device by the engine; the HB terms of a single molecule can be too.
+struct BuildLists {
+    bool host_hb = true;
+    bool host_disp = true;
 };
 
 // Runs the complete GFN-FF setup for one molecule (curcuma GFNFF::InitialiseMolecule,
 // gfnff_method.cpp:733-848).  xyz_ang is row-major N x 3 in Angstrom.
 // Throws std::runtime_error on invalid input.
 Model build_model(int n, const int* Z, const double* xyz_ang, int charge,
-                  const SetupOptions& opt = SetupOptions());
+                  const SetupOptions& opt = SetupOptions(), const BuildLists& lists = BuildLists());
 
 // HB/XB lists re-detected at a new geometry with the setup (Phase-1) charges
 // (gfnff_method.cpp:1597-1690); also rebuilds the bond <-> HB cross reference.
+// With m.hb_on_device only the XB list is rebuilt (the engine detects the HB terms).
 void redetect_hbxb(Model& m, const double* xyz_bohr);
+
+// HBAtoms of the model at xyz_bohr (N x 3, caller order)
+HBAtoms hb_atom_data(Model& m, const double* xyz_bohr);
+
+// Builds on the host the lists the set-up left to the device: the D4 pair list at the
+// set-up geometry and the HB terms (with the bond cross reference) at hb_xyz_bohr.  Used
+// before a parameter file is written.
+void complete_host_lists(Model& m, const double* hb_xyz_bohr);
 
 // Parameter file (the whole set-up result, binary, this library's own format): written by
 // save_parameters, read back by load_parameters, which throws std::runtime_error on a

@@ -884,6 +884,60 @@ static double zeta_scale(int Z, double q)
     return std::exp(3.0 * (1.0 - std::exp(cc * (1.0 - zeff / qmod))));
 }
 
+// half contraction at the setup weights: g[i][s][b] = sum_a w_i[a] C6ref[a][b]
+static std::vector<double> half_contraction(const Model& m)
+{
+    const int n = m.n, K = (int)m.present_Z.size();
+    std::vector<double> g((size_t)n * K * kMaxRef, 0.0);
+    for (int i = 0; i < n; ++i) {
+        const double* wi = &m.w_setup[(size_t)i * kMaxRef];
+        for (int s = 0; s < K; ++s) {
+            const int ne = std::min(d4_refn[m.present_Z[s] - 1], kMaxRef);
+            const double* C = &m.c6ref[(((size_t)m.slot[i] * K + s) * kMaxRef) * kMaxRef];
+            for (int b = 0; b < ne; ++b) {
+                double v = 0.0;
+                for (int a = 0; a < m.nref[i]; ++a) v += wi[a] * C[(size_t)a * kMaxRef + b];
+                g[((size_t)i * K + s) * kMaxRef + b] = v;
+            }
+        }
+    }
+    return g;
+}
+
+static double setup_c6(const Model& m, const std::vector<double>& g, int i, int j)
+{
+    const int K = (int)m.present_Z.size();
+    const double* gi = &g[((size_t)i * K + m.slot[j]) * kMaxRef];
+    const double* wj = &m.w_setup[(size_t)j * kMaxRef];
+    double v = 0.0;
+    for (int b = 0; b < m.nref[j]; ++b) v += gi[b] * wj[b];
+    return v;
+}
+
+// the D4 pair list at the setup geometry (pairs within 60 bohr, rows by i, j ascending)
+static void disp_list(Ctx& c, const std::vector<double>& g)
+{
+    Model& m = c.m;
+    const int n = c.n;
+    const double a1 = 0.58, a2 = 4.80;
+    std::vector<std::vector<DispPair>> rows(n);
+    pairs_within(c, 60.0, false, [&](int i, int j, double) {
+        DispPair d;
+        d.i = i;
+        d.j = j;
+        d.c6 = setup_c6(m, g, i, j);
+        d.r4r2 = 3.0 * m.sqrt_zr4r2[i] * m.sqrt_zr4r2[j];
+        d.r0sq = std::pow(a1 * std::sqrt(d.r4r2) + a2, 2);
+        d.zetac6 = m.zeta[i] * m.zeta[j];
+        rows[i].push_back(d);
+    });
+    m.disp.clear();
+    for (auto& r : rows) {
+        std::sort(r.begin(), r.end(), [](const DispPair& a, const DispPair& b) { return a.j < b.j; });
+        m.disp.insert(m.disp.end(), r.begin(), r.end());
+    }
+}
+
 static void setup_d4(Ctx& c)
 {
     Model& m = c.m;
@@ -919,46 +973,10 @@ static void setup_d4(Ctx& c)
         m.zeta[i] = zeta_scale(c.Z[i], m.qa[i]);
         d4_weights(m, i, m.cn_setup[i], &m.w_setup[(size_t)i * kMaxRef], nullptr);
     }
-    // half contraction at the setup weights: g[i][s][b] = sum_a w_i[a] C6ref[a][b]
-    std::vector<double> g((size_t)n * K * kMaxRef, 0.0);
-    for (int i = 0; i < n; ++i) {
-        const double* wi = &m.w_setup[(size_t)i * kMaxRef];
-        for (int s = 0; s < K; ++s) {
-            const int ne = std::min(d4_refn[m.present_Z[s] - 1], kMaxRef);
-            const double* C = &m.c6ref[(((size_t)m.slot[i] * K + s) * kMaxRef) * kMaxRef];
-            for (int b = 0; b < ne; ++b) {
-                double v = 0.0;
-                for (int a = 0; a < m.nref[i]; ++a) v += wi[a] * C[(size_t)a * kMaxRef + b];
-                g[((size_t)i * K + s) * kMaxRef + b] = v;
-            }
-        }
-    }
-    auto c6_of = [&](int i, int j) {
-        const double* gi = &g[((size_t)i * K + m.slot[j]) * kMaxRef];
-        const double* wj = &m.w_setup[(size_t)j * kMaxRef];
-        double v = 0.0;
-        for (int b = 0; b < m.nref[j]; ++b) v += gi[b] * wj[b];
-        return v;
-    };
-    const double a1 = 0.58, a2 = 4.80;
+    const std::vector<double> g = half_contraction(m);
+    auto c6_of = [&](int i, int j) { return setup_c6(m, g, i, j); };
     m.disp.clear();
-    if (m.opt.dispersion) {
-        std::vector<std::vector<DispPair>> rows(n);
-        pairs_within(c, 60.0, false, [&](int i, int j, double) {
-            DispPair d;
-            d.i = i;
-            d.j = j;
-            d.c6 = c6_of(i, j);
-            d.r4r2 = 3.0 * m.sqrt_zr4r2[i] * m.sqrt_zr4r2[j];
-            d.r0sq = std::pow(a1 * std::sqrt(d.r4r2) + a2, 2);
-            d.zetac6 = m.zeta[i] * m.zeta[j];
-            rows[i].push_back(d);
-        });
-        for (auto& r : rows) {
-            std::sort(r.begin(), r.end(), [](const DispPair& a, const DispPair& b) { return a.j < b.j; });
-            m.disp.insert(m.disp.end(), r.begin(), r.end());
-        }
-    }
+    if (m.opt.dispersion && !m.disp_on_device) disp_list(c, g);
     // ATM triples over bonded triplets (s9 = 1)
     m.atm.clear();
     if (m.opt.dispersion) {
@@ -1032,7 +1050,41 @@ static void basicity(const Ctx& c, const std::vector<double>& xb, std::vector<do
     }
 }
 
-void detect_hbxb(Ctx& c, const std::vector<double>& xb)
+// per-atom inputs of the HB detection at the geometry xb (gfnff_method.cpp:7936-8100)
+static HBAtoms hb_atoms(const Ctx& c, const std::vector<double>& xb)
+{
+    const Model& m = c.m;
+    const int n = c.n;
+    const std::vector<double>& q = m.qa;
+    HBAtoms a;
+    basicity(c, xb, a.bas);
+    a.aci.assign(n, 0.0);
+    for (int i = 0; i < n; ++i) a.aci[i] = (c.Z[i] < 74) ? hb_acidity[c.Z[i]] : 0.0;
+    for (int i = 0; i < n; ++i)
+        if (fg_amide_h(c, i)) a.aci[m.adj[i][0]] *= 0.80;
+    a.hcand.assign(n, 0);
+    for (int h = 0; h < n; ++h) {
+        if (c.Z[h] != 1 || m.hyb[h] == 1 || m.adj[h].empty()) continue;
+        const int A = *std::min_element(m.adj[h].begin(), m.adj[h].end());
+        double thr = 0.01;
+        if (c.Z[A] > 10) thr -= 0.20;
+        if (m.hyb[A] == 3 && c.Z[A] == 6) thr += 0.05;
+        if (q[h] > thr) a.hcand[h] = 1;
+    }
+    a.thr1 = 200.0 - std::log10(m.opt.hb_accuracy) * 50.0;
+    a.thr2 = 400.0 - std::log10(m.opt.hb_accuracy) * 50.0;
+    a.ok.assign(n, 0);
+    for (int i = 0; i < n; ++i) {
+        if (c.Z[i] == 6 && m.pi_frag[i] == 0) continue;
+        double t = 0.10;
+        if (c.Z[i] > 10) t += 0.2;
+        a.ok[i] = !(q[i] > t);
+    }
+    return a;
+}
+
+// the HB terms and the bond <-> HB cross reference (gfnff_method.cpp:7936-8495, :3680-3712)
+static void detect_hb_terms(Ctx& c, const std::vector<double>& xb, const HBAtoms& at)
 {
     Model& m = c.m;
     const int n = c.n;
@@ -1041,28 +1093,11 @@ void detect_hbxb(Ctx& c, const std::vector<double>& xb)
         const double dx = xb[3 * i] - xb[3 * j], dy = xb[3 * i + 1] - xb[3 * j + 1], dz = xb[3 * i + 2] - xb[3 * j + 2];
         return dx * dx + dy * dy + dz * dz;
     };
-    std::vector<double> bas, aci(n);
-    basicity(c, xb, bas);
-    for (int i = 0; i < n; ++i) aci[i] = (c.Z[i] < 74) ? hb_acidity[c.Z[i]] : 0.0;
-    for (int i = 0; i < n; ++i)
-        if (fg_amide_h(c, i)) aci[m.adj[i][0]] *= 0.80;
-    std::vector<char> hbh(n, 0);
-    for (int h = 0; h < n; ++h) {
-        if (c.Z[h] != 1 || m.hyb[h] == 1 || m.adj[h].empty()) continue;
-        const int A = *std::min_element(m.adj[h].begin(), m.adj[h].end());
-        double thr = 0.01;
-        if (c.Z[A] > 10) thr -= 0.20;
-        if (m.hyb[A] == 3 && c.Z[A] == 6) thr += 0.05;
-        if (q[h] > thr) hbh[h] = 1;
-    }
-    const double hbthr1 = 200.0 - std::log10(m.opt.hb_accuracy) * 50.0;
-    const double hbthr2 = 400.0 - std::log10(m.opt.hb_accuracy) * 50.0;
-    auto ok_atom = [&](int i) {
-        if (c.Z[i] == 6 && m.pi_frag[i] == 0) return false;
-        double t = 0.10;
-        if (c.Z[i] > 10) t += 0.2;
-        return !(q[i] > t);
-    };
+    const std::vector<double>& bas = at.bas;
+    const std::vector<double>& aci = at.aci;
+    const std::vector<char>& hbh = at.hcand;
+    const double hbthr1 = at.thr1, hbthr2 = at.thr2;
+    auto ok_atom = [&](int i) { return at.ok[i] != 0; };
     std::vector<std::vector<int>> hyd_on(n);
     for (auto& b : m.topo_bonds) {
         if (hbh[b.first]) hyd_on[b.second].push_back(b.first);
@@ -1146,7 +1181,18 @@ void detect_hbxb(Ctx& c, const std::vector<double>& xb)
             m.bond_hb.push_back({A, H, it->second});
         }
     }
-    // halogen bonds
+}
+
+// halogen bonds (gfnff_method.cpp:8520-8672)
+static void detect_xbonds(Ctx& c, const std::vector<double>& xb, const std::vector<double>& bas)
+{
+    Model& m = c.m;
+    const int n = c.n;
+    const std::vector<double>& q = m.qa;
+    auto d2 = [&](int i, int j) {
+        const double dx = xb[3 * i] - xb[3 * j], dy = xb[3 * i + 1] - xb[3 * j + 1], dz = xb[3 * i + 2] - xb[3 * j + 2];
+        return dx * dx + dy * dy + dz * dz;
+    };
     m.xbonds.clear();
     auto isx = [](int z) {
         return z == 17 || z == 35 || z == 53 || z == 16 || z == 34 || z == 52 || z == 15 || z == 33 || z == 51;
@@ -1168,6 +1214,13 @@ void detect_hbxb(Ctx& c, const std::vector<double>& xb)
             m.xbonds.push_back({A, X, B, (c.Z[X] < 72) ? xb_acidity[c.Z[X]] : 0.0, q[X], q[B]});
         }
     }
+}
+
+void detect_hbxb(Ctx& c, const std::vector<double>& xb)
+{
+    const HBAtoms a = hb_atoms(c, xb);
+    if (!c.m.hb_on_device) detect_hb_terms(c, xb, a);
+    detect_xbonds(c, xb, a.bas);
 }
 
 void generate_parameters(Ctx& c)
@@ -1212,7 +1265,8 @@ void d4_weights(const Model& m, int i, double cn, double* w, double* dw)
     }
 }
 
-Model build_model(int n, const int* Z, const double* xyz_ang, int charge, const SetupOptions& opt)
+Model build_model(int n, const int* Z, const double* xyz_ang, int charge, const SetupOptions& opt,
+                  const BuildLists& lists)
 {
     if (n <= 0) throw std::runtime_error("no atoms");
     for (int i = 0; i < n; ++i)
@@ -1221,6 +1275,8 @@ Model build_model(int n, const int* Z, const double* xyz_ang, int charge, const 
     m.n = n;
     m.charge = charge;
     m.opt = opt;
+    m.hb_on_device = !lists.host_hb;
+    m.disp_on_device = !lists.host_disp;
     m.Z.assign(Z, Z + n);
     detail::Ctx c(m);
     c.Z = m.Z.data();
@@ -1257,6 +1313,31 @@ void redetect_hbxb(Model& m, const double* xyz_bohr)
     c.xb.assign(xyz_bohr, xyz_bohr + 3 * (size_t)m.n);
     for (auto& b : m.topo_bonds) c.bondset.insert(detail::key(b.first, b.second));
     detail::detect_hbxb(c, c.xb);
+}
+
+HBAtoms hb_atom_data(Model& m, const double* xyz_bohr)
+{
+    detail::Ctx c(m);
+    c.Z = m.Z.data();
+    c.xb.assign(xyz_bohr, xyz_bohr + 3 * (size_t)m.n);
+    for (auto& b : m.topo_bonds) c.bondset.insert(detail::key(b.first, b.second));
+    return detail::hb_atoms(c, c.xb);
+}
+
+void complete_host_lists(Model& m, const double* hb_xyz_bohr)
+{
+    detail::Ctx c(m);
+    c.Z = m.Z.data();
+    for (auto& b : m.topo_bonds) c.bondset.insert(detail::key(b.first, b.second));
+    if (m.disp_on_device && m.opt.dispersion) {
+        c.xb = m.xyz_setup;
+        detail::disp_list(c, detail::half_contraction(m));
+    }
+    if (m.hb_on_device && m.opt.hbond) {
+        c.xb.assign(hb_xyz_bohr, hb_xyz_bohr + 3 * (size_t)m.n);
+        detail::detect_hb_terms(c, c.xb, detail::hb_atoms(c, c.xb));
+    }
+    m.hb_on_device = m.disp_on_device = false;
 }
 
 }  // namespace gfnff

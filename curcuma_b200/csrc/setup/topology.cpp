@@ -94,31 +94,60 @@ void pairs_within(const Ctx& c, double rcut, bool strict,
     }
 }
 
-// cn_calculator.cpp:115-177 (threshold form, default 1600 bohr^2, kn=-7.5, cnmax=4.4)
+// cn_calculator.cpp:115-177 (threshold form, default 1600 bohr^2, kn=-7.5, cnmax=4.4).
+// Each atom's partners are gathered from the neighbouring cells of a grid, sorted and summed
+// in ascending order (the j-loop's order), atoms in parallel; no pair list is stored.
 std::vector<double> cn_threshold(const Ctx& c, double threshold)
 {
     const int n = c.n;
-    std::vector<double> raw(n, 0.0), cn(n, 0.0);
-    std::vector<std::vector<std::pair<int, double>>> nb(n);
-    pairs_within(c, std::sqrt(threshold) + 1e-6, false, [&](int i, int j, double d2) {
-        if (d2 > threshold) return;
-        nb[i].push_back({j, d2});
-        nb[j].push_back({i, d2});
-    });
+    std::vector<double> cn(n, 0.0);
     const double kn = -7.5, cnmax = 4.4;
-#pragma omp parallel for schedule(dynamic, 32)
-    for (int i = 0; i < n; ++i) {
-        auto& v = nb[i];
-        std::sort(v.begin(), v.end());   // same summation order as the j-loop
-        double s = 0.0;
-        for (auto& p : v) {
-            const double r = std::sqrt(p.second);
-            const double rc = c.rcov_cn[i] + c.rcov_cn[p.first];
-            const double dr = (r - rc) / rc;
-            s += 0.5 * (1.0 + std::erf(kn * dr));
+    const double rcut = std::sqrt(threshold) + 1e-6;
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (int i = 0; i < n; ++i)
+        for (int d = 0; d < 3; ++d) {
+            lo[d] = std::min(lo[d], c.xb[3 * i + d]);
+            hi[d] = std::max(hi[d], c.xb[3 * i + d]);
         }
-        raw[i] = s;
-        cn[i] = std::log(1.0 + std::exp(cnmax)) - std::log(1.0 + std::exp(cnmax - s));
+    const double cell = rcut * 1.0001 + 1e-9;
+    int nc[3];
+    for (int d = 0; d < 3; ++d) nc[d] = std::max(1, (int)std::floor((hi[d] - lo[d]) / cell) + 1);
+    std::vector<int> head((size_t)nc[0] * nc[1] * nc[2], -1), next(n, -1), cid(n);
+    for (int i = n - 1; i >= 0; --i) {
+        int cx = std::min(nc[0] - 1, (int)((c.xb[3 * i] - lo[0]) / cell));
+        int cy = std::min(nc[1] - 1, (int)((c.xb[3 * i + 1] - lo[1]) / cell));
+        int cz = std::min(nc[2] - 1, (int)((c.xb[3 * i + 2] - lo[2]) / cell));
+        const int id = (cz * nc[1] + cy) * nc[0] + cx;
+        cid[i] = id;
+        next[i] = head[id];
+        head[id] = i;
+    }
+#pragma omp parallel
+    {
+        std::vector<std::pair<int, double>> v;
+#pragma omp for schedule(dynamic, 32)
+        for (int i = 0; i < n; ++i) {
+            v.clear();
+            const int id = cid[i];
+            const int cx = id % nc[0], cy = (id / nc[0]) % nc[1], cz = id / (nc[0] * nc[1]);
+            for (int z = std::max(0, cz - 1); z <= std::min(nc[2] - 1, cz + 1); ++z)
+                for (int y = std::max(0, cy - 1); y <= std::min(nc[1] - 1, cy + 1); ++y)
+                    for (int x = std::max(0, cx - 1); x <= std::min(nc[0] - 1, cx + 1); ++x)
+                        for (int j = head[(z * nc[1] + y) * nc[0] + x]; j >= 0; j = next[j]) {
+                            if (j == i) continue;
+                            const double d2 = dist2_bohr(c, std::min(i, j), std::max(i, j));
+                            if (d2 <= threshold) v.push_back({j, d2});
+                        }
+            std::sort(v.begin(), v.end());
+            double s = 0.0;
+            for (auto& p : v) {
+                const double r = std::sqrt(p.second);
+                const double rc = c.rcov_cn[i] + c.rcov_cn[p.first];
+                const double dr = (r - rc) / rc;
+                s += 0.5 * (1.0 + std::erf(kn * dr));
+            }
+            cn[i] = std::log(1.0 + std::exp(cnmax)) - std::log(1.0 + std::exp(cnmax - s));
+        }
     }
     return cn;
 }

@@ -89,11 +89,12 @@ def _approaching_waters():
     return Z, X, V
 
 
-@pytest.mark.parametrize("thr", [0.3, 0.1])
-def test_hb_lists_refresh_at_the_same_steps_as_the_host_loop(thr):
+@pytest.mark.parametrize("thr,detect", [(0.3, "0"), (0.1, "0"), (0.1, "1")])
+def test_hb_lists_refresh_at_the_same_steps_as_the_host_loop(thr, detect, monkeypatch):
     """The device loop re-detects the HB/XB lists at the first step whose
     sqrt(sum d^2)/N exceeds the threshold (rolling back to that step), which is where the
-    single-point path, called once per step from the host, re-detects them too."""
+    single-point path, called once per step from the host, re-detects them too; the MD
+    handle detects the HB terms on the host or on the device."""
     Z, X, V0 = _approaching_waters()
     m = atomic_masses(Z)
     nsteps = 240
@@ -119,6 +120,7 @@ def test_hb_lists_refresh_at_the_same_steps_as_the_host_loop(thr):
         counts.append(host.getHBCount())
     changes = [t for t in range(1, len(counts)) if counts[t] != counts[t - 1]]
     assert changes and changes[0] % 100 != 0, counts   # the list changes inside a chunk
+    monkeypatch.setenv("GFNFF_HB_DEVICE", detect)   # the MD handle's HB terms: host or device
     dev = GFNFF(hb_rmsd_bohr=thr)
     assert dev.setMolecule(Z, X)
     ep, ek = dev.runMD(nsteps, 0.5, V0)
