@@ -260,6 +260,37 @@ struct Engine::Impl {
     int* cnl_bad_host = nullptr;   // pinned; refreshed by fetch()
     DBuf<int> cnl_off, cnl_j, cnl_bad;
     DBuf<double4> cnl_ref;
+    // the list from device positions d_p (engine order): k_cnl_build count, scan, fill;
+    // GFNFF_CN_LIST=host builds it on the host instead (the same rows)
+    DBuf<int> cnl_cnt;
+    DBuf<unsigned char> cnl_tmp;
+    void build_cn_list_device(const double4* d_p)
+    {
+        const int nn = n;
+        const double rc = 6.0 + kCnSkin, rc2 = rc * rc;
+        const unsigned grid = (unsigned)(((long)nn * 32 + 255) / 256);
+        cnl_cnt.alloc(nn + 1);
+        cnl_off.alloc(nn + 1);
+        CK(cudaMemsetAsync(cnl_cnt.p + nn, 0, sizeof(int), stream));
+        k_cnl_build<false><<<grid, 256, 0, stream>>>(nn, d_p, jr.p, rc2, cnl_cnt.p, nullptr, nullptr);
+        CK(cudaGetLastError());
+        size_t b = 0;
+        CK(cub::DeviceScan::ExclusiveSum(nullptr, b, cnl_cnt.p, cnl_off.p, nn + 1, stream));
+        if (cnl_tmp.n < b) cnl_tmp.alloc(b);
+        b = cnl_tmp.n;
+        CK(cub::DeviceScan::ExclusiveSum(cnl_tmp.p, b, cnl_cnt.p, cnl_off.p, nn + 1, stream));
+        int total = 0;
+        CK(cudaMemcpyAsync(&total, cnl_off.p + nn, sizeof(int), cudaMemcpyDeviceToHost, stream));
+        CK(cudaStreamSynchronize(stream));
+        cnl_j.alloc(std::max(1, total));
+        k_cnl_build<true><<<grid, 256, 0, stream>>>(nn, d_p, jr.p, rc2, nullptr, cnl_off.p, cnl_j.p);
+        CK(cudaGetLastError());
+        cnl_ref.alloc(nn);
+        CK(cudaMemcpyAsync(cnl_ref.p, d_p, (size_t)nn * sizeof(double4), cudaMemcpyDeviceToDevice, stream));
+        if (!cnl_bad.p) cnl_bad.alloc(1);
+        CK(cudaMemsetAsync(cnl_bad.p, 0, sizeof(int), stream));
+        CK(cudaStreamSynchronize(stream));
+    }
     void build_cn_list(const std::vector<double4>& p, const std::vector<int2>& jr)
     {
         const int nn = (int)p.size();
@@ -995,7 +1026,8 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
         if (P.cnl_on) {
             if (!P.cnl_bad_host) CK(cudaMallocHost(&P.cnl_bad_host, sizeof(int)));
             *P.cnl_bad_host = 0;
-            P.build_cn_list(p0, hjr);
+            if (ecl && !std::strcmp(ecl, "host")) P.build_cn_list(p0, hjr);
+            else P.build_cn_list_device(P.pos0.p);
         }
     }
     P.rcov_cn.upload(rcn); P.rcov43.upload(r43); P.rcov_d3.upload(rd3);
@@ -2162,12 +2194,17 @@ void Engine::refresh_cn_list()
     Impl& P = *p_;
     if (!P.cnl_on) return;
     CK(cudaStreamSynchronize(P.stream));
-    std::vector<double4> p(P.n);
-    CK(cudaMemcpy(p.data(), P.pos.p, (size_t)P.n * sizeof(double4), cudaMemcpyDeviceToHost));
-    std::vector<int2> jr(P.n);
-    CK(cudaMemcpy(jr.data(), P.jr.p, (size_t)P.n * sizeof(int2), cudaMemcpyDeviceToHost));
     P.drop_graphs();   // the list buffers are reallocated
-    P.build_cn_list(p, jr);
+    const char* ecl = std::getenv("GFNFF_CN_LIST");
+    if (ecl && !std::strcmp(ecl, "host")) {
+        std::vector<double4> p(P.n);
+        CK(cudaMemcpy(p.data(), P.pos.p, (size_t)P.n * sizeof(double4), cudaMemcpyDeviceToHost));
+        std::vector<int2> jr(P.n);
+        CK(cudaMemcpy(jr.data(), P.jr.p, (size_t)P.n * sizeof(int2), cudaMemcpyDeviceToHost));
+        P.build_cn_list(p, jr);
+    } else {
+        P.build_cn_list_device(P.pos.p);
+    }
 }
 
 void Engine::set_hb_reference(const double* xyz_bohr)

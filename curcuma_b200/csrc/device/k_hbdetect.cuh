@@ -1,3 +1,5 @@
+// Device-built set-up lists.
+//
 // Device enumeration of the hydrogen-bond terms of one molecule (gfnff_method.cpp:7936-8495,
 // the host restatement is detect_hb_terms in setup/parameters.cpp), term for term in the
 // host's order, so that the lists are identical:
@@ -140,6 +142,35 @@ __global__ void k_hb_xref_flags(long long nt, const int4* __restrict__ rec, cons
     const int4 r = rec[t];
     const int zb = Z[r.z];
     flag[t] = r.w >= 2 && (zb == 7 || zb == 8);
+}
+
+// CN neighbour list on the device: for every atom i the partners j of its molecule with
+// |r_i - r_j|^2 < rc2 (round-to-nearest products and sums in x, y, z order), ascending; one
+// warp per atom, count pass, exclusive scan, fill pass (the rows of the host grid builder)
+template <bool FILL>
+__global__ void __launch_bounds__(256) k_cnl_build(int n, const double4* __restrict__ p, const int2* __restrict__ jr,
+                                                   double rc2, int* cnt, const int* __restrict__ off, int* js)
+{
+    const int i = (int)(((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (i >= n) return;   // warp-uniform
+    const double4 a = p[i];
+    const int2 r = jr[i];
+    int count = 0;
+    const int base = FILL ? off[i] : 0;
+    for (int j0 = r.x; j0 < r.y; j0 += 32) {
+        const int j = j0 + lane;
+        bool in = false;
+        if (j < r.y && j != i) {
+            const double4 b = p[j];
+            const double dx = __dsub_rn(a.x, b.x), dy = __dsub_rn(a.y, b.y), dz = __dsub_rn(a.z, b.z);
+            in = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)) < rc2;
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, in);
+        if (FILL && in) js[base + count + __popc(m & ((1u << lane) - 1u))] = j;
+        count += __popc(m);
+    }
+    if (!FILL && lane == 0) cnt[i] = count;
 }
 
 }  // namespace

@@ -1,4 +1,5 @@
-"""Hydrogen-bond terms detected on the device (k_hbdetect.cuh) against the host detection of
+"""Set-up lists built on the device (k_hbdetect.cuh) against the host builders.  Hydrogen-bond
+terms detected on the device against the host detection of
 the shared set-up (setup/parameters.cpp detect_hb_terms, the restatement of
 gfnff_method.cpp:7936-8495): the same terms in the same order, so the energies and gradients of
 the two modes are the same numbers.  The systems cover every case type: case 1 (a free H
@@ -93,3 +94,29 @@ def test_parameter_file_from_a_device_handle(tmp_path, monkeypatch):
     assert r.setMoleculeFromParameters(path, Z, X), r.getErrorMessage()
     assert (r.topology(6, 4) == g.topology(6, 4)).all()
     assert abs(r.calculateEnergy(True) - e) < 1e-12
+
+
+def test_cn_list_device_equals_host(monkeypatch):
+    """The CN neighbour list built on the device (k_cnl_build) has the host builder's rows,
+    so the CN sums are the same numbers, at set-up and after the refreshes that geometries
+    moving atoms beyond half the skin trigger."""
+    Z, X = workloads.water_cluster(300, 9)
+    rng = np.random.default_rng(3)
+    geoms = [X + rng.normal(scale=s, size=X.shape) for s in (0.02, 0.15, 0.15, 0.02)]
+    hs = []
+    for mode in ("host", None):
+        if mode:
+            monkeypatch.setenv("GFNFF_CN_LIST", mode)
+        else:
+            monkeypatch.delenv("GFNFF_CN_LIST")
+        g = GFNFF()
+        assert g.setMolecule(Z, X)
+        hs.append(g)
+    for Xk in geoms:
+        cn = []
+        for g in hs:
+            g.updateGeometry(Xk)
+            g.calculateEnergy(True)
+            assert not g.hasError(), g.getErrorMessage()
+            cn.append(g.getCoordinationNumbers())
+        assert (cn[0] == cn[1]).all()
