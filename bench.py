@@ -194,7 +194,12 @@ def roofline(phase_avg, info, fp64_peak, hbm_peak, hbm_src):
         # iterations, the warm start and the true-residual check); only its lower
         # triangle from 4096 unknowns on
         mbytes = 8.0 * nred * (nred + 1) / 2.0 if info["pcg_lower"] else 8.0 * nred * nred
-        bytes_ = (info["iters"] + 2) * mbytes
+        if info.get("prod64", -1) >= 0:
+            # mixed refinement solver: the inner iterations stream the FP32 copy (half the
+            # bytes), the true-residual checks the FP64 triangle
+            bytes_ = info["iters"] * mbytes / 2.0 + info["prod64"] * mbytes
+        else:
+            bytes_ = (info["iters"] + 2) * mbytes
         bound, unit, peak = "hbm", "GB/s", hbm_peak
         achieved = bytes_ / (ms * 1e-3) / 1e9
     elif name == "eeq_solve":
@@ -411,7 +416,7 @@ def measure(args, precision, Z, X, torch, dist, world, local, mols=None, units=N
             "e2e": {"value": units * steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 3 * n * 8,
                     "d2h_bytes_per_step": (3 * n + 16 * nmol) * 8 + 4 * nmol},
             "clocks": clk, "setup_s": setup_s, "solver": gpu.eeqSolver(), "iters": gpu.eeqIterations(),
-            "kernels_per_eval": kpe}
+            "prod64": gpu.eeqFP64Products() if nmol == 1 else -1, "kernels_per_eval": kpe}
 
 
 def per_molecule_loop(mols, local):
@@ -535,7 +540,7 @@ def run_config(args, cfg, torch, dist, world, rank, local):
                    ("xbonds", 7, 3), ("atm", 12, 3), ("batm", 13, 3)]}
     sym = os.environ.get("GFNFF_PCG_SYM")
     info = {"n": n, "nred": n - nfrag, "config": cfg, "coulomb_pairs": nc, "disp_pairs": nd,
-            "solver": main["solver"], "iters": main["iters"],
+            "solver": main["solver"], "iters": main["iters"], "prod64": main["prod64"],
             "pcg_lower": (sym != "0") if sym is not None else (n - nfrag) >= 4096,
             "bytes_hbonds": len(hbs) * (19 * 8 + 3 * 48 + 2 * 48)}
     if mols:   # block-diagonal EEQ: one reduced system per molecule (one fragment each)
@@ -545,7 +550,11 @@ def run_config(args, cfg, torch, dist, world, rank, local):
     roof = roofline(main["phase_avg"], info, fp64_peak, hbm_peak, hbm_src)
     if roof["kernel"] == "eeq_solve" and main["solver"] == "pcg" and main["iters"] > 0:
         # the solve as iteration latency (what bounds it while M stays in L2)
-        roof["us_per_iteration"] = 1e3 * roof["ms"] / (main["iters"] + 2)
+        nprod = main["iters"] + (main["prod64"] if main["prod64"] >= 0 else 2)
+        roof["us_per_iteration"] = 1e3 * roof["ms"] / nprod
+        if main["prod64"] >= 0:
+            roof["fp32_inner_iterations"] = main["iters"]
+            roof["fp64_products"] = main["prod64"]
         roof["matrix_in_l2"] = not info["pcg_lower"]
     summary = {
         "workload": f"config {cfg}: {desc}", "natoms": natoms, "nfrag": nfrag,

@@ -521,6 +521,17 @@ int gfnff_eeq_iterations(gfnff_handle* h)
     }
 }
 
+int gfnff_eeq_fp64_products(gfnff_handle* h)
+{
+    if (!h || !h->ready) return -1;
+    try {
+        return h->eng->eeq_fp64_products();
+    } catch (const std::exception& e) {
+        fail(h, GFNFF_CUDA_ERROR, e.what());
+        return -1;
+    }
+}
+
 const char* gfnff_last_error(gfnff_handle* h) { return h ? h->err.c_str() : g_static_err.c_str(); }
 
 gfnff_status gfnff_destroy(gfnff_handle* h)

@@ -19,6 +19,8 @@
 // src/core/energy_calculators/ff_methods/).
 #include "engine.h"
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 #include <cusolverDn.h>
 
@@ -229,6 +231,31 @@ int pair_splits(int n, int max_range)
 }
 
 }  // namespace
+
+// TMA descriptor of the FP32 copy of the reduced matrix (n x n, column-major, leading
+// dimension lda floats, a multiple of 4) in boxes of 128 rows x 64 columns; elements past n
+// read as zero.  cuTensorMapEncodeTiled comes from the driver through the runtime.
+CUtensorMap tmap_f32_tiles(const float* base, int n, int lda)
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if (!encode) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        CK(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+        if (q != cudaDriverEntryPointSuccess || !fn) throw std::runtime_error("cuTensorMapEncodeTiled unavailable");
+        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    CUtensorMap m;
+    const cuuint64_t dims[2] = {(cuuint64_t)n, (cuuint64_t)n};
+    const cuuint64_t strides[1] = {(cuuint64_t)lda * sizeof(float)};
+    const cuuint32_t box[2] = {(cuuint32_t)kPcgT, 64u};
+    const cuuint32_t es[2] = {1u, 1u};
+    const CUresult r = encode(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(base), dims, strides, box, es,
+                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) throw std::runtime_error("cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
+    return m;
+}
 
 // ====================================================================================
 // Engine implementation
@@ -443,7 +470,7 @@ struct Engine::Impl {
     DBuf<double> work;
     DBuf<int> info, info2, status, ipiv, bad;
     int lwork = 0;
-    int lda = 2;           // leading dimension of M (>= nred + 1, even; row nred holds b for k_chol)
+    int lda = 4;           // leading dimension of M (>= nred + 1, a multiple of 4; row nred holds b for k_chol)
     bool use_lu = false;   // reduced EEQ matrix not positive definite: pivoted LU instead
     // in-house pivoted LU (k_lu_factor): grid, pivot candidates, grid barrier
     int lu_grid = 1;
@@ -500,6 +527,8 @@ struct Engine::Impl {
     // the FP64 form on the 20k cluster (9.2 vs 5.2 ms), so it is off by default.
     bool pcg_f32 = false;
     DBuf<float> Mf;
+    DBuf<float> p32;   // k_pcg_ir: the two FP32 direction buffers
+    CUtensorMap pcg_tmap{};   // k_pcg_ir: TMA descriptor of Mf (128 x 64 boxes)
     // mixed form, lower-triangle systems: k_pcg_ir (FP32-matrix CG inside FP64 refinement,
     // both triangles of M built in one pass: FP64 for the residuals, FP32 for the products)
     bool pcg_ir = false;
@@ -536,6 +565,8 @@ struct Engine::Impl {
         A.warm = pcg_warm ? pwarm.p + slot : nullptr;
         A.lower = pcg_lower ? pcg_cols : 0; A.yA = pyA.p; A.tiles = ptiles.p; A.ntiles = pcg_ntiles;
         A.Mf = (pcg_f32 || pcg_ir) ? Mf.p : nullptr;
+        A.p32[0] = pcg_ir ? p32.p : nullptr;
+        A.p32[1] = pcg_ir ? p32.p + ((nred + 3) & ~3) : nullptr;
         A.max_outer = 6;
         {
             const char* er = std::getenv("GFNFF_PCG_IR_REL");
@@ -544,7 +575,8 @@ struct Engine::Impl {
         A.binv_pre = pcg_pre ? pbinv.p : nullptr;
         void* args[] = {&A};
         if (pcg_ir) {
-            CK(cudaLaunchCooperativeKernel((const void*)k_pcg_ir, dim3(pcg_grid), dim3(kPcgThreads), args,
+            void* irargs[] = {&A, &pcg_tmap};
+            CK(cudaLaunchCooperativeKernel((const void*)k_pcg_ir, dim3(pcg_grid), dim3(kPcgThreads), irargs,
                                            pcg_smem_ir, stream));
         } else if (pcg_res) {
             PCGRes R{view(), red2atom.p, anchor.p, prtiles.p, pcg_res_ntiles, pcg_res_ntl, pcg_res_gscratch};
@@ -1338,7 +1370,7 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
     }
     P.q.alloc(n); P.dEdcn.alloc(n); P.v.alloc(n); P.grad.alloc(3 * (size_t)n); P.E.alloc(16 * (size_t)nm);
     P.gout.alloc(3 * (size_t)n); P.qout.alloc(n); P.cnout.alloc(n);
-    P.lda = (P.nred + 2) & ~1;   // >= nred + 1 and even: 16-byte aligned columns
+    P.lda = (P.nred + 4) & ~3;   // >= nred + 1, a multiple of 4: 16-byte aligned FP32 and FP64 columns
     P.M.alloc((size_t)std::max<long long>(1, nm == 1 ? (long long)P.lda * P.nred : P.msize));
     P.bvec.alloc(std::max(1, P.nred)); P.xyz_stage.alloc(3 * (size_t)n); P.msd.alloc(1);
     P.info.alloc(nm); P.info2.alloc(1); P.status.alloc(nm); P.bad.alloc(nm);
@@ -1531,6 +1563,12 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
                     const char* eir = std::getenv("GFNFF_PCG_IR");
                     P.pcg_ir = P.pcg_lower && P.opt.precision == 1 && !P.pcg_f32 && !(eir && !std::strcmp(eir, "0"));
                     if (P.pcg_f32 || P.pcg_ir) P.Mf.alloc((size_t)P.lda * P.nred);
+                    if (P.pcg_ir) {
+                        const size_t n4 = (size_t)((P.nred + 3) & ~3);
+                        P.p32.alloc(2 * n4);
+                        CK(cudaMemset(P.p32.p, 0, 2 * n4 * sizeof(float)));   // the tails past n stay 0
+                        P.pcg_tmap = tmap_f32_tiles(P.Mf.p, P.nred, P.lda);
+                    }
                     const char* ec = std::getenv("GFNFF_PCG_COLS");
                     P.pcg_cols = (ec && !std::strcmp(ec, "8")) ? 2 : 1;
                     std::vector<int2> tl;
@@ -1541,11 +1579,11 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
                     P.pyA.alloc(P.nred);
                     CK(cudaMemset(P.pyA.p, 0, (size_t)P.nred * sizeof(double)));
                 }
-                P.ppartial.alloc(8 * (size_t)G); P.pbar.alloc(2 * kBarGen); P.piters.alloc(1); P.pwarm.alloc(2);
+                P.ppartial.alloc(8 * (size_t)G); P.pbar.alloc(2 * kBarGen); P.piters.alloc(2); P.pwarm.alloc(2);
                 P.pz2.alloc(P.nred);
                 CK(cudaMemset(P.pwarm.p, 0, 2 * sizeof(int)));
                 CK(cudaMemset(P.pbar.p, 0, 2 * kBarGen * sizeof(unsigned int)));
-                CK(cudaMemset(P.piters.p, 0, sizeof(int)));
+                CK(cudaMemset(P.piters.p, 0, 2 * sizeof(int)));
                 P.pcg_grid = G;
                 P.pcg_smem = smem;
                 CK(cudaFuncSetAttribute((const void*)k_pcg, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -1553,13 +1591,15 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
                 CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)k_pcg, kPcgThreads, smem));
                 P.pcg_ready = per_sm >= 1;
                 if (P.pcg_ir) {   // one more owned-row vector (the inner correction d), even-sized
-                    P.pcg_smem_ir = smem + (size_t)((maxrows + 1) & ~1) * sizeof(double);
+                    // and the region of the replicated vector is the larger of the FP64 vector
+                    // and the FP32 direction with two staging halves of a tile
+                    P.pcg_smem_ir = smem + (size_t)((maxrows + 1) & ~1) * sizeof(double) +
+                                    (size_t)(pcg_ir_pregion(P.nred) - ((P.nred + 1) & ~1)) * sizeof(double);
                     int ps = 0;
+                    const void* kir = (const void*)k_pcg_ir;
                     if (P.pcg_smem_ir <= 220 * 1024) {
-                        CK(cudaFuncSetAttribute((const void*)k_pcg_ir, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                (int)P.pcg_smem_ir));
-                        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ps, (const void*)k_pcg_ir, kPcgThreads,
-                                                                         P.pcg_smem_ir));
+                        CK(cudaFuncSetAttribute(kir, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P.pcg_smem_ir));
+                        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ps, kir, kPcgThreads, P.pcg_smem_ir));
                     }
                     P.pcg_ir = ps >= 1;
                 }
@@ -1800,6 +1840,15 @@ const char* Engine::solver_name() const
     case Impl::SOLVE_BATCH: return "batched";
     default: return "library";
     }
+}
+
+int Engine::eeq_fp64_products()
+{
+    if (p_->nmol != 1 || p_->use_lu || p_->solver != Impl::SOLVE_PCG || !p_->pcg_ir) return -1;
+    int v[2] = {0, 0};
+    CK(cudaStreamSynchronize(p_->stream));
+    CK(cudaMemcpy(v, p_->piters.p, sizeof(v), cudaMemcpyDeviceToHost));
+    return v[1];
 }
 
 int Engine::eeq_iterations()

@@ -83,6 +83,8 @@ public:
     const char* pair_kernel_name() const;
     // iterations of the last iterative EEQ solve (0 for direct solvers)
     int eeq_iterations();
+    // k_pcg_ir: FP64 products with the reduced matrix in the last solve; -1 otherwise
+    int eeq_fp64_products();
     // kernels of this library per evaluation while the step replays as a graph (-1 before
     // the first capture or with direct launches)
     int kernels_per_evaluation() const;

@@ -41,7 +41,7 @@ struct PCGArgs {
     double* partial;      // gridDim.x * 8
     unsigned int* bar;    // arrival count at [0], generation at [kBarGen]
     int* info;
-    int* iters;
+    int* iters;           // [0] iterations; k_pcg_ir also [1]: FP64 matrix products
     int* warm;            // when non-null and *warm != 0, x holds the previous solution of the
                           // same system and is the initial guess; set to 1 on convergence
     const float* Mf;      // lower form in the mixed precision form: M stored in FP32 (M unused)
@@ -57,6 +57,8 @@ struct PCGArgs {
                           // FP64 true-residual bar); the residual is always computed in FP64
     int max_outer;        // k_pcg_ir: FP64 residual corrections at most
     double inner_rel;     // k_pcg_ir: inner solve to ||r_inner||_inf <= inner_rel ||r||_inf
+    float* p32[2];        // k_pcg_ir: the inner CG direction in FP32, two global n-vectors
+                          // (16-byte aligned, length a multiple of 4) used in turn
 };
 
 // grid-wide barrier (all blocks co-resident); false when the wait gave up.  The block's
@@ -634,90 +636,240 @@ __device__ double matvec_tiles64(const PCGArgs& A, const double* p, double* red)
 }
 
 // The inner products of k_pcg_ir: the FP32 lower triangle with FP32 arithmetic inside a tile
-// (elements, the direction's tile segments and the partial sums stay FP32: the inner solve
-// needs ~1e-6 relative accuracy, a 128-term FP32 sum gives ~1e-7), the tile's row and column
-// sums added to y as FP64 atomics, as in matvec_tiles_c.  No per-element FP64 conversion.
-__device__ double matvec_tiles_f32(const PCGArgs& A, const double* p, float* red)
+// (elements, the direction and the partial sums stay FP32: the inner solve needs ~1e-6
+// relative accuracy, a 128-term FP32 sum gives ~1e-7), the tile's row and column sums added
+// to y as FP64 atomics, as in matvec_tiles_c.  The tiles stream through shared memory in
+// halves of 64 columns (32 KB) by TMA (one cp.async.bulk.tensor.2d per half, issued by one
+// thread; rows and columns past n are zero-filled), together with the direction's segments
+// (cp.async.bulk, the direction is an FP32 n-vector in global memory), kPcgStages halves in
+// flight, each stage completing on its own mbarrier: the copies run ahead of the products,
+// the reductions and the atomics, and the threads issue no copy instructions.  Every wait on
+// an mbarrier is bounded (kTmaPolls); a wait that gives up marks the product failed.  The
+// staging ring shares its region with the FP64 vector of the outer products (pcg_ir_pregion).
+constexpr int kPcgHalf = 64 * kPcgT;   // floats of half a tile
+constexpr int kPcgStages = 4;          // halves in flight
+constexpr int kPcgStageF = kPcgHalf + kPcgT + 64;   // floats per stage: elements, pr, pc
+constexpr long long kTmaPolls = 1ll << 24;
+
+__host__ __device__ inline int pcg_ir_pregion(int n)
 {
-    constexpr int kCols = 8;
+    const int pd = (n + 1) & ~1;
+    const int ring = kPcgStages * kPcgStageF / 2 + 16;   // doubles, with room to align to 128 bytes
+    return pd > ring ? pd : ring;
+}
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+// true once the phase with the given parity has completed; false after kTmaPolls polls
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity)
+{
+    for (long long k = 0; k < kTmaPolls; ++k) {
+        unsigned done;
+        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                     " selp.u32 %0, 1, 0, p;\n}\n"
+                     : "=r"(done)
+                     : "r"(smem_u32(bar)), "r"(parity)
+                     : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+// TMA of half h's elements (box 128 rows x 64 columns at rows I0, columns J0 + 64 half) and
+// bulk copies of the direction's row segment p[I0, +128) and column segment p[J0 + 64 half,
+// +64) (clipped to the buffers' rounded length n4) into stage st, completing on bar
+__device__ __forceinline__ void pcg_tma_half(const PCGArgs& A, const CUtensorMap* tmap, const float* p32, int t,
+                                             int half, float* st, unsigned long long* bar)
+{
+    const int2 tl = A.tiles[t];
+    const int I0 = tl.x, J0 = tl.y + 64 * half;
+    const int n4 = (A.n + 3) & ~3;
+    const unsigned pr_bytes = 4u * (unsigned)min(kPcgT, n4 - I0);
+    const unsigned pc_bytes = J0 < n4 ? 4u * (unsigned)min(64, n4 - J0) : 0u;
+    mbar_expect_tx(bar, 4u * kPcgHalf + pr_bytes + pc_bytes);
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n"
+        ::"r"(smem_u32(st)), "l"(tmap), "r"(I0), "r"(J0), "r"(smem_u32(bar))
+        : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n"
+                 ::"r"(smem_u32(st + kPcgHalf)), "l"(p32 + I0), "r"(pr_bytes), "r"(smem_u32(bar))
+                 : "memory");
+    if (pc_bytes)
+        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n"
+                     ::"r"(smem_u32(st + kPcgHalf + kPcgT)), "l"(p32 + J0), "r"(pc_bytes), "r"(smem_u32(bar))
+                     : "memory");
+}
+
+// bars: kPcgStages mbarriers (arrival count 1); uses: halves streamed so far by this block
+// (stage = uses % kPcgStages, phase parity = (uses / kPcgStages) & 1), carried across calls;
+// ok cleared when a wait gives up
+__device__ double matvec_tiles_f32(const PCGArgs& A, const CUtensorMap* tmap, const float* p32, float* ring,
+                                   float* red, unsigned long long* bars, unsigned& uses, bool& ok)
+{
+    constexpr int kCols = 4;   // 16 warps x 4 columns = one half tile
+    static_assert(kPcgThreads / 32 * kCols == 64, "one pass per half tile");
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     double pap = 0.0;
-    const float* Mt = A.Mf;
-    for (int t = blockIdx.x; t < A.ntiles; t += gridDim.x) {
+    const int mine = blockIdx.x < A.ntiles ? (A.ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+    const int nh = 2 * mine;
+    __shared__ int fail_s;
+    // the ring's memory was last accessed by ordinary loads and stores (the FP64 vector, or
+    // the previous product): ordered before the TMA writes
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        fail_s = 0;
+        for (int h = 0; h < kPcgStages - 1 && h < nh; ++h) {
+            const unsigned s = (uses + h) % kPcgStages;
+            pcg_tma_half(A, tmap, p32, blockIdx.x + (h >> 1) * gridDim.x, h & 1, ring + s * kPcgStageF, bars + s);
+        }
+    }
+    __syncthreads();
+    float u[4], pr[4];
+    for (int h = 0; h < nh; ++h) {
+        const unsigned g = uses + h, s = g % kPcgStages;
+        if (threadIdx.x == 0 && h + kPcgStages - 1 < nh) {
+            const int hn = h + kPcgStages - 1;
+            const unsigned sn = (uses + hn) % kPcgStages;
+            pcg_tma_half(A, tmap, p32, blockIdx.x + (hn >> 1) * gridDim.x, hn & 1, ring + sn * kPcgStageF, bars + sn);
+        }
+        if (!mbar_wait(bars + s, (g / kPcgStages) & 1)) fail_s = 1;
+        const float* st = ring + s * kPcgStageF;
+        const int t = blockIdx.x + (h >> 1) * gridDim.x, half = h & 1;
         const int2 tl = A.tiles[t];
         const int I0 = tl.x, J0 = tl.y;
         const bool diag = I0 == J0;
         const int ni = min(kPcgT, A.n - I0), nj = min(kPcgT, A.n - J0);
-        float u[4], pr[4];
+        const bool full = !diag && ni == kPcgT && nj == kPcgT;
+        if (half == 0) {
+            const float4 p4 = *reinterpret_cast<const float4*>(st + kPcgHalf + 4 * lane);
+            pr[0] = p4.x; pr[1] = p4.y; pr[2] = p4.z; pr[3] = p4.w;
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const int r = lane + 32 * i;
-            u[i] = 0.f;
-            pr[i] = r < ni ? (float)p[I0 + r] : 0.f;
-        }
-        for (int cb = warp * kCols; cb < nj; cb += nw * kCols) {
-            float m[kCols][4], v[kCols], pc[kCols];
-#pragma unroll
-            for (int q = 0; q < kCols; ++q) {
-                const int c = cb + q;
-                pc[q] = c < nj ? (float)p[J0 + c] : 0.f;
-                const float* col = Mt + (size_t)(J0 + (c < nj ? c : 0)) * A.lda + I0;
-#pragma unroll
-                for (int i = 0; i < 4; ++i) {
-                    const int r = lane + 32 * i;
-                    m[q][i] = (c < nj && r < ni && (!diag || r >= c)) ? __ldcs(col + r) : 0.f;
-                }
+            for (int j = 0; j < 4; ++j) {
+                u[j] = 0.f;
+                if (4 * lane + j >= ni) pr[j] = 0.f;
             }
+        }
+        float v[kCols];
+        if (full) {
 #pragma unroll
             for (int q = 0; q < kCols; ++q) {
-                const int c = cb + q;
+                const int cl = warp * kCols + q;
+                const float pc = st[kPcgHalf + kPcgT + cl];
+                const float4 m4 = *reinterpret_cast<const float4*>(st + cl * kPcgT + 4 * lane);
+                u[0] = fmaf(m4.x, pc, u[0]);
+                u[1] = fmaf(m4.y, pc, u[1]);
+                u[2] = fmaf(m4.z, pc, u[2]);
+                u[3] = fmaf(m4.w, pc, u[3]);
+                v[q] = m4.x * pr[0];
+                v[q] = fmaf(m4.y, pr[1], v[q]);
+                v[q] = fmaf(m4.z, pr[2], v[q]);
+                v[q] = fmaf(m4.w, pr[3], v[q]);
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < kCols; ++q) {
+                const int cl = warp * kCols + q, c = 64 * half + cl;
+                const float pc = c < nj ? st[kPcgHalf + kPcgT + cl] : 0.f;
+                const float4 m4 = *reinterpret_cast<const float4*>(st + cl * kPcgT + 4 * lane);
+                const float mm[4] = {m4.x, m4.y, m4.z, m4.w};
                 v[q] = 0.f;
 #pragma unroll
-                for (int i = 0; i < 4; ++i) {
-                    const int r = lane + 32 * i;
-                    u[i] = fmaf(m[q][i], pc[q], u[i]);
-                    if (!diag || r > c) v[q] = fmaf(m[q][i], pr[i], v[q]);
-                }
-            }
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1)
-#pragma unroll
-                for (int q = 0; q < kCols; ++q) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
-            float vq = 0.f;
-#pragma unroll
-            for (int q = 0; q < kCols; ++q)
-                if (lane == q) vq = v[q];
-            if (lane < kCols) {
-                const int c = cb + lane;
-                if (c < nj && vq != 0.f) {
-                    atomicAdd(A.yA + J0 + c, (double)vq);
-                    pap += p[J0 + c] * (double)vq;
+                for (int j = 0; j < 4; ++j) {
+                    const int r = 4 * lane + j;
+                    const float m = (c < nj && r < ni && (!diag || r >= c)) ? mm[j] : 0.f;
+                    u[j] = fmaf(m, pc, u[j]);
+                    if (!diag || r > c) v[q] = fmaf(m, pr[j], v[q]);
                 }
             }
         }
 #pragma unroll
-        for (int i = 0; i < 4; ++i) red[warp * kPcgT + lane + 32 * i] = u[i];
-        __syncthreads();
-        for (int r = threadIdx.x; r < ni; r += blockDim.x) {
-            double s = 0.0;
-            for (int w = 0; w < nw; ++w) s += (double)red[w * kPcgT + r];
-            atomicAdd(A.yA + I0 + r, s);
-            pap += p[I0 + r] * s;
+        for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+            for (int q = 0; q < kCols; ++q) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+        float vq = 0.f;
+#pragma unroll
+        for (int q = 0; q < kCols; ++q)
+            if (lane == q) vq = v[q];
+        if (lane < kCols) {
+            const int cl = warp * kCols + lane, c = 64 * half + cl;
+            if (c < nj && vq != 0.f) {
+                atomicAdd(A.yA + J0 + c, (double)vq);
+                pap += (double)st[kPcgHalf + kPcgT + cl] * (double)vq;
+            }
         }
-        __syncthreads();
+        if (half == 1) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) red[warp * kPcgT + 4 * lane + j] = u[j];
+            __syncthreads();
+            for (int r = threadIdx.x; r < ni; r += blockDim.x) {
+                double sr = 0.0;
+                for (int w = 0; w < nw; ++w) sr += (double)red[w * kPcgT + r];
+                atomicAdd(A.yA + I0 + r, sr);
+                pap += (double)st[kPcgHalf + r] * sr;
+            }
+        }
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        __syncthreads();   // stage s is free for the copy issued next
     }
+    uses += (unsigned)nh;
+    if (fail_s) ok = false;
     return pap;
 }
 
-__global__ void __launch_bounds__(kPcgThreads) k_pcg_ir(PCGArgs A)
+// dst = z + beta src over all n entries (z from global memory), written by every grid block
+// (the same values): the direction of this inner iteration, read by the products of all
+// blocks; src is the previous direction (the other buffer), beta == 0 ignores it
+__device__ void update_p32(float* dst, const float* src, const double* z, int n, double beta)
 {
-    extern __shared__ double sm[];
+    constexpr int U = 8;
+    for (int c0 = threadIdx.x; c0 < n; c0 += U * blockDim.x) {
+        double zv[U];
+        float pv[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int c = c0 + u * blockDim.x;
+            zv[u] = c < n ? __ldcg(z + c) : 0.0;
+            pv[u] = (c < n && beta != 0.0) ? __ldcg(src + c) : 0.f;
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int c = c0 + u * blockDim.x;
+            if (c < n) __stcg(dst + c, (float)(zv[u] + beta * (double)pv[u]));
+        }
+    }
+    // the direction is read next by bulk copies (the async proxy)
+    asm volatile("fence.proxy.async.global;\n" ::: "memory");
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kPcgThreads) k_pcg_ir(PCGArgs A, const __grid_constant__ CUtensorMap tmap)
+{
+    extern __shared__ __align__(128) double sm[];
+    __shared__ __align__(8) unsigned long long bars[kPcgStages];
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kPcgStages; ++s) mbar_init(bars + s, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    unsigned uses = 0;   // halves streamed through the ring (the stages' phases)
+    bool tma_ok = true;
     constexpr int GL = kPcgMaxBlock + 1;
     const int4 pt = A.part[blockIdx.x];
     const int row0 = pt.x, row1 = pt.y, nrow = row1 - row0;
     const long long boff0 = pt.z < pt.w ? A.boff[pt.z] : 0;
-    double* p = sm;                              // n, replicated: x (residuals) or the CG direction
-    double* G = p + ((A.n + 1) & ~1);            // kPcgMaxBlock x GL scratch
+    double* p = sm;                              // n, replicated: x of the FP64 residual
+    float* ring = reinterpret_cast<float*>(      // inner iterations: the tile staging ring
+        (reinterpret_cast<size_t>(sm) + 127) & ~static_cast<size_t>(127));
+    double* G = p + pcg_ir_pregion(A.n);         // kPcgMaxBlock x GL scratch
     double* xs = G + kPcgMaxBlock * GL;          // owned rows: x, r, z, M p, d
     double* rs = xs + A.maxrows;
     double* zs = rs + A.maxrows;
@@ -732,13 +884,14 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg_ir(PCGArgs A)
     const double* Bp = A.binv_pre ? A.binv_pre + boff0 : Bs;
     const bool warm = A.warm != nullptr && *A.warm != 0;   // uniform over the grid
     bool ok = true, conv = false;
-    int it = 0;
+    int it = 0, prod64 = 0;
     for (int k = threadIdx.x; k < nrow; k += blockDim.x) xs[k] = warm ? __ldcg(A.x + row0 + k) : 0.0;
     for (int outer = 0; ok; ++outer) {
         // ---- FP64 true residual r = b - M x (x = 0 on a cold start: r = b); x is complete in
         // global memory (the previous launch, or the barrier after the last correction)
         const bool have_x = warm || outer > 0;
         if (have_x) {
+            ++prod64;
             update_p(p, A.x, A.n, 0.0);
             __syncthreads();
             matvec_tiles64(A, p, G);
@@ -767,12 +920,15 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg_ir(PCGArgs A)
         }
         if (outer >= A.max_outer || it >= A.max_iter) break;
         const double stop = fmax(A.inner_rel * rmax, 0.5 * A.tol_abs);
-        update_p(p, A.z, A.n, 0.0);
+        __syncthreads();   // the FP64 vector's region becomes the staging ring
+        int cur = 0;       // the direction's buffer: A.p32[cur]
+        update_p32(A.p32[cur], A.p32[1 - cur], A.z, A.n, 0.0);
         // ---- inner CG on the FP32 matrix: M32 d = r from d = 0
         while (it < A.max_iter) {
             ++it;
             __syncthreads();
-            const double pap_t = matvec_tiles_f32(A, p, reinterpret_cast<float*>(G));
+            const double pap_t =
+                matvec_tiles_f32(A, &tmap, A.p32[cur], ring, reinterpret_cast<float*>(G), bars, uses, tma_ok);
             block_sum_max(pap_t, 0.0, A.partial + 8 * blockIdx.x);
             ok = grid_sync(A.bar, gen);
             if (!ok) break;
@@ -782,7 +938,7 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg_ir(PCGArgs A)
             const double alpha = rz / pap;
             double rin_t = 0.0;
             for (int k = threadIdx.x; k < nrow; k += blockDim.x) {
-                ds[k] += alpha * p[row0 + k];
+                ds[k] += alpha * (double)__ldcg(A.p32[cur] + row0 + k);
                 rs[k] -= alpha * Ap[k];
                 rin_t = fmax(rin_t, fabs(rs[k]));
             }
@@ -797,7 +953,8 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg_ir(PCGArgs A)
             if (rin <= stop) break;
             const double beta = rzn / rz;
             rz = rzn;
-            update_p(p, A.z, A.n, beta);
+            cur = 1 - cur;
+            update_p32(A.p32[cur], A.p32[1 - cur], A.z, A.n, beta);
         }
         if (!ok) break;
         // ---- x += d, published for the next residual
@@ -810,8 +967,9 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg_ir(PCGArgs A)
     __syncthreads();
     for (int k = threadIdx.x; k < nrow; k += blockDim.x) A.x[row0 + k] = xs[k];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
-        *A.info = !ok ? 2 : (conv ? 0 : 3);
-        *A.iters = it;
+        *A.info = (!ok || !tma_ok) ? 2 : (conv ? 0 : 3);
+        A.iters[0] = it;
+        A.iters[1] = prod64;
         if (A.warm) *A.warm = (ok && conv) ? 1 : 0;
     }
 }

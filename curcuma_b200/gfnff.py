@@ -308,6 +308,11 @@ class GFNFF:
         """Iterations of the last iterative EEQ solve (0 for direct solvers)."""
         return int(self._lib.gfnff_eeq_iterations(self._h))
 
+    def eeqFP64Products(self) -> int:
+        """FP64 matrix products of the mixed form's refinement solver in the last solve
+        (-1 for the other solvers)."""
+        return int(self._lib.gfnff_eeq_fp64_products(self._h))
+
     def kernelsPerEvaluation(self):
         """Kernels of this library per evaluation of the replayed step graph (-1: none yet)."""
         return int(self._lib.gfnff_kernels_per_evaluation(self._h))

@@ -205,6 +205,12 @@ const char* gfnff_pair_kernel(gfnff_handle* h);
  * reference. */
 int gfnff_eeq_iterations(gfnff_handle* h);
 
+/* FP64 products with the reduced EEQ matrix in the last solve of the mixed form's
+ * refinement solver (the true-residual checks beside the FP32 inner iterations that
+ * gfnff_eeq_iterations counts); -1 for every other solver or before setup.  Synchronises
+ * the handle's stream.  Diagnostic without a counterpart in the reference. */
+int gfnff_eeq_fp64_products(gfnff_handle* h);
+
 /* Kernels of this library launched per evaluation while the step replays as a CUDA graph
  * (the kernel nodes of the captured graph whose code is in this library, plus the
  * positions kernel launched before it); -1 before the first evaluation or with direct
