@@ -16,6 +16,7 @@
 #endif
 
 #include "../curcuma_b200/csrc/setup/linalg.h"
+#include "alpb_oracle.h"
 #include "../curcuma_b200/csrc/setup/model.h"
 #include "../curcuma_b200/csrc/tables/gfnff_tables.inc"
 
@@ -45,6 +46,7 @@ struct Grad {
 
 struct oracle_handle {
     Model m;
+    AlpbModel solv;   // ALPB implicit solvation (off: gas phase)
 };
 
 // ---------------------------------------------------------------------------------
@@ -117,10 +119,11 @@ static double oop(V3 ri, V3 rj, V3 rk, V3 rl, V3 g[4])
     return om;
 }
 
-static int engrad(const Model& m, const double* xb, double* T, double* gout, double* qout,
+static int engrad(const Model& m, const AlpbModel& solv, const double* xb, double* T, double* gout, double* qout,
                   double* cnout)
 {
     const int n = m.n;
+    AlpbGeom sg;   // ALPB state of this geometry (gfnff_method.cpp:1128-1140, 1805-1853)
     auto X = [&](int i) { return V3{xb[3 * i], xb[3 * i + 1], xb[3 * i + 2]}; };
     for (int t = 0; t < ORC_NTERMS; ++t) T[t] = 0.0;
     Grad G(n);
@@ -186,6 +189,8 @@ static int engrad(const Model& m, const double* xb, double* T, double* gout, dou
             }
         }
         for (int i = 0; i < n; ++i) x[i] = m.chi_base[i] + m.cnf[i] * std::sqrt(cn[i]);
+        // implicit solvation: the solvent's reaction field enters the solve, A += B
+        if (solv.on) alpb_prepare(solv, xb, n, sg, A.data());
         if (!linalg::eeq_schur_solve(A.data(), n, x.data(), m.frag.data(), m.nfrag, m.qfrag.data(), q.data(),
                                      n >= 1024)) {
             g_err = "EEQ solve failed";
@@ -845,6 +850,7 @@ static int engrad(const Model& m, const double* xb, double* T, double* gout, dou
                 G.add(j, (dlog[i] * v[i]) * comp);
             }
     }
+    if (solv.on) T[ORC_SOLVATION] = alpb_energy_gradient(solv, xb, n, sg, q.data(), G.g.data());
     double tot = m.e0;
     for (int t = 0; t < ORC_TOTAL; ++t) tot += T[t];
     T[ORC_TOTAL] = tot;
@@ -880,6 +886,16 @@ oracle_handle* oracle_create_from_parameters(const char* path)
 }
 
 void oracle_destroy(oracle_handle* h) { delete h; }
+
+int oracle_set_solvent(oracle_handle* h, const char* solvent)
+{
+    if (!h) return 1;
+    if (!alpb_setup(h->solv, h->m.Z, solvent ? solvent : "")) {
+        g_err = std::string("unknown solvent: ") + (solvent ? solvent : "");
+        return 1;
+    }
+    return 0;
+}
 const char* oracle_last_error(void) { return g_err.c_str(); }
 
 int oracle_engrad(oracle_handle* h, const double* xyz_ang, double* terms, double* grad, double* q,
@@ -894,7 +910,7 @@ int oracle_engrad(oracle_handle* h, const double* xyz_ang, double* terms, double
     for (size_t k = 0; k < xb.size(); ++k) xb[k] = xyz_ang[k] * kAngToBohr;
     int rc;
     try {
-        rc = engrad(h->m, xb.data(), terms, grad, q, cn);
+        rc = engrad(h->m, h->solv, xb.data(), terms, grad, q, cn);
     } catch (const std::exception& e) {
         g_err = e.what();
         rc = 2;

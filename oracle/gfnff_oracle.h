@@ -11,7 +11,7 @@ extern "C" {
 enum {
     ORC_BOND = 0, ORC_ANGLE, ORC_TORSION, ORC_INVERSION, ORC_STORSION, ORC_DISPERSION,
     ORC_BONDED_REP, ORC_NONBONDED_REP, ORC_COULOMB, ORC_HBOND, ORC_XBOND, ORC_ATM, ORC_BATM,
-    ORC_TOTAL, ORC_NTERMS
+    ORC_SOLVATION, ORC_TOTAL, ORC_NTERMS
 };
 
 typedef struct oracle_handle oracle_handle;
@@ -22,6 +22,9 @@ oracle_handle* oracle_create(int n, const int* Z, const double* xyz_ang, int cha
 // The model of a parameter file written by the library (gfnff_write_parameters); NULL on failure.
 oracle_handle* oracle_create_from_parameters(const char* path);
 void oracle_destroy(oracle_handle* h);
+// ALPB implicit solvation for the following evaluations (curcuma's solvent names and
+// aliases; "" or "none": gas phase).  Returns 0, or 1 for an unknown solvent.
+int oracle_set_solvent(oracle_handle* h, const char* solvent);
 const char* oracle_last_error(void);
 
 // Energy + gradient at xyz (Angstrom).  terms[ORC_NTERMS]; grad N*3 Eh/bohr; q and cn

@@ -15,7 +15,7 @@ ROOT = Path(__file__).resolve().parent.parent
 LIB = ROOT / "oracle" / "_build" / "liboracle.so"
 GOLDEN = ROOT / "tests" / "golden"
 TERMS = ["bond", "angle", "torsion", "inversion", "storsion", "dispersion", "bonded_rep",
-         "nonbonded_rep", "coulomb", "hbond", "xbond", "atm", "batm", "total"]
+         "nonbonded_rep", "coulomb", "hbond", "xbond", "atm", "batm", "solvation", "total"]
 _lib = None
 
 
@@ -41,17 +41,21 @@ def lib():
         L.oracle_nfrag.argtypes = [c_v]
         L.oracle_term_params.argtypes = [c_v, c_i, c_v, ctypes.c_long]
         L.oracle_term_params.restype = ctypes.c_long
+        L.oracle_set_solvent.argtypes = [c_v, ctypes.c_char_p]
+        L.oracle_set_solvent.restype = c_i
         _lib = L
     return _lib
 
 
 class Oracle:
-    def __init__(self, Z, xyz, charge=0):
+    def __init__(self, Z, xyz, charge=0, solvent=None):
         self.Z = np.ascontiguousarray(Z, dtype=np.int32)
         X = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
         self.n = len(self.Z)
         self.h = lib().oracle_create(self.n, self.Z.ctypes.data, X.ctypes.data, int(charge))
         if not self.h:
+            raise RuntimeError(lib().oracle_last_error().decode())
+        if solvent and lib().oracle_set_solvent(self.h, solvent.encode()) != 0:
             raise RuntimeError(lib().oracle_last_error().decode())
 
     @classmethod
