@@ -12,7 +12,7 @@ GFNFF_OK = 0
 STATUS_NAMES = {0: "OK", 1: "INVALID_ARG", 2: "SETUP_FAILED", 3: "NOT_SPD", 4: "NONFINITE",
                 5: "REFINE_NOT_CONVERGED", 6: "CUDA_ERROR", 7: "NOT_READY"}
 TERM_NAMES = ["bond", "angle", "torsion", "inversion", "storsion", "dispersion", "bonded_rep",
-              "nonbonded_rep", "coulomb", "hbond", "xbond", "atm", "batm", "total"]
+              "nonbonded_rep", "coulomb", "hbond", "xbond", "atm", "batm", "solvation", "total"]
 NTERMS = len(TERM_NAMES)
 
 # exported symbols declared in include/gfnff_b200.h
@@ -23,7 +23,7 @@ EXPORTED = ["gfnff_default_options", "gfnff_create", "gfnff_setup", "gfnff_energ
             "gfnff_eeq_charges_noalloc", "gfnff_eeq_solver", "gfnff_eeq_iterations", "gfnff_setup_batch",
             "gfnff_energy_and_gradient_batch", "gfnff_md_nve", "gfnff_kernels_per_evaluation",
             "gfnff_save_parameters", "gfnff_setup_from_parameters", "gfnff_write_parameters",
-            "gfnff_pair_kernel", "gfnff_eeq_fp64_products"]
+            "gfnff_pair_kernel", "gfnff_eeq_fp64_products", "gfnff_set_solvent"]
 PHASES = ["positions", "cn", "d4_weights", "eeq_matrix", "eeq_rhs", "eeq_solve", "bonded",
           "hbonds", "repulsion", "pairs", "post_chain", "finish"]
 
@@ -72,6 +72,7 @@ def load():
     lib.gfnff_pair_kernel.restype = ctypes.c_char_p
     lib.gfnff_eeq_iterations.argtypes = [c_v]
     lib.gfnff_eeq_fp64_products.argtypes = [c_v]
+    lib.gfnff_set_solvent.argtypes = [c_v, ctypes.c_char_p]
     lib.gfnff_kernels_per_evaluation.argtypes = [c_v]
     lib.gfnff_save_parameters.argtypes = [c_v, ctypes.c_char_p]
     lib.gfnff_setup_from_parameters.argtypes = [c_v, ctypes.c_char_p, c_i, P(c_i)]

@@ -30,6 +30,8 @@ struct gfnff_handle {
     bool ready = false;
     std::string err;
     std::vector<double> hb_ref;    // bohr, geometry of the last HB/XB detection
+    std::string solvent;            // ALPB solvent ("" gas phase)
+    AlpbModel solv;
     double* pin_xyz = nullptr;      // pinned staging for host coordinates
     double* pin_grad = nullptr;
     double* pin_out = nullptr;      // terms + status + msd
@@ -90,6 +92,16 @@ gfnff_status gfnff_create(const gfnff_options* opts, gfnff_handle** out)
 
 static gfnff_status finish_setup(gfnff_handle* h, int n);
 
+gfnff_status gfnff_set_solvent(gfnff_handle* h, const char* solvent)
+{
+    if (!h) return fail(nullptr, GFNFF_INVALID_ARG, "handle is NULL");
+    const std::string s = solvent ? solvent : "";
+    AlpbModel probe;
+    if (!alpb_setup(probe, std::vector<int>{1}, s)) return fail(h, GFNFF_INVALID_ARG, "unknown solvent: " + s);
+    h->solvent = (s == "none") ? "" : s;
+    return GFNFF_OK;
+}
+
 gfnff_status gfnff_setup(gfnff_handle* h, int n, const int* Z, const double* xyz, int charge)
 {
     if (!h) return fail(nullptr, GFNFF_INVALID_ARG, "handle is NULL");
@@ -105,6 +117,7 @@ gfnff_status gfnff_setup(gfnff_handle* h, int n, const int* Z, const double* xyz
         const char* hd = std::getenv("GFNFF_HB_DEVICE");
         L.host_hb = hd ? !std::strcmp(hd, "0") : n < 512;
         h->model = build_model(n, Z, xyz, charge, so, L);
+        if (!alpb_setup(h->solv, h->model.Z, h->solvent)) return fail(h, GFNFF_INVALID_ARG, "unknown solvent");
     } catch (const std::exception& e) {
         return fail(h, GFNFF_SETUP_FAILED, e.what());
     }
@@ -115,7 +128,7 @@ gfnff_status gfnff_setup(gfnff_handle* h, int n, const int* Z, const double* xyz
 static gfnff_status finish_setup(gfnff_handle* h, int n)
 {
     try {
-        h->eng->upload(h->model);
+        h->eng->upload(h->model, h->solv.on ? &h->solv : nullptr);
         if (h->pin_xyz) cudaFreeHost(h->pin_xyz);
         if (h->pin_grad) cudaFreeHost(h->pin_grad);
         if (!h->pin_out && cudaMallocHost(&h->pin_out, 32 * sizeof(double)) != cudaSuccess)
@@ -165,6 +178,7 @@ gfnff_status gfnff_setup_from_parameters(gfnff_handle* h, const char* path, int 
         if (m.n != natoms || !std::equal(m.Z.begin(), m.Z.end(), Z))
             return fail(h, GFNFF_SETUP_FAILED, "parameter file is for another structure");
         h->model = std::move(m);
+        if (!alpb_setup(h->solv, h->model.Z, h->solvent)) return fail(h, GFNFF_INVALID_ARG, "unknown solvent");
     } catch (const std::exception& e) {
         return fail(h, GFNFF_SETUP_FAILED, e.what());
     }
@@ -189,6 +203,7 @@ gfnff_status gfnff_setup_batch(gfnff_handle* h, int nmol, const int* natoms, con
 {
     if (!h) return fail(nullptr, GFNFF_INVALID_ARG, "handle is NULL");
     if (nmol <= 0 || !natoms || !Z || !xyz) return fail(h, GFNFF_INVALID_ARG, "invalid batch");
+    if (!h->solvent.empty()) return fail(h, GFNFF_INVALID_ARG, "ALPB solvation: single-molecule handles only");
     std::vector<long> off(nmol + 1, 0);
     for (int m = 0; m < nmol; ++m) {
         if (natoms[m] <= 0) return fail(h, GFNFF_INVALID_ARG, "molecule without atoms");

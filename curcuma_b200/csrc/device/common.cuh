@@ -24,7 +24,7 @@ namespace {
 
 enum {
     T_BOND = 0, T_ANGLE, T_TORSION, T_INVERSION, T_STORSION, T_DISP, T_BREP, T_NBREP, T_COUL,
-    T_HB, T_XB, T_ATM, T_BATM, T_TOTAL
+    T_HB, T_XB, T_ATM, T_BATM, T_SOLV, T_TOTAL
 };
 
 constexpr int kBlock = 128;
@@ -247,6 +247,11 @@ struct View {
     double* grad;
     double* E;                // nmol*16 term energies
     int* status;              // nmol
+    // ALPB implicit solvation (brad null: gas phase): the Born matrix enters the EEQ matrix,
+    // off-diagonal keps / f_GB(r, brad_a, brad_b) (P16), diagonal bdiag = keps / brad + 2 hbw
+    const double* brad;
+    const double* bdiag;
+    double keps;
     // exact-gradient mode (see the gradient options of the C ABI)
     int exact;                // drop the D4 dC6/dCN term
     double* cfar;             // n: potential of the Coulomb pairs beyond 100 bohr, or null

@@ -43,6 +43,7 @@
 #include <vector>
 
 #include "../../../include/gfnff_b200.h"
+#include "../setup/alpb.h"
 #include "../tables/gfnff_tables.inc"
 
 namespace gfnff {
@@ -50,6 +51,7 @@ namespace gfnff {
 #include "common.cuh"
 #include "k_bonded.cuh"
 #include "k_nonbonded.cuh"
+#include "k_alpb.cuh"
 #include "k_eeq.cuh"
 #include "k_eeq_tc.cuh"
 #include "k_chol.cuh"
@@ -459,6 +461,70 @@ struct Engine::Impl {
         long long nt = 0;
     } hbd;
     void detect_hb(const Model& m, const double* xb, std::vector<int>& bond_h, std::map<int, std::vector<int>>& byH);
+    // ---- ALPB implicit solvation (single molecules; k_alpb.cuh) ----
+    bool alpb_on = false;
+    struct AlpbDev {
+        double keps = 0.0, alpbet = 0.0, born_scale = 0.0, gshift = 0.0, srcut2 = 0.0;
+        int lhb = 0;
+        DBuf<double> vdwr, rho, svdw, vdwsa, trjlo, trjhi, wrp, gamsasa, hbmag;
+        DBuf<double4> grid;
+        DBuf<double> brad, dpsi, sasa, hbw, dhbdw, bdiag, dEdbr, shape;
+    } ab;
+    AlpbArgs alpb_args()
+    {
+        AlpbArgs A;
+        A.n = n;
+        A.vdwr = ab.vdwr.p; A.rho = ab.rho.p; A.svdw = ab.svdw.p; A.vdwsa = ab.vdwsa.p; A.trjlo = ab.trjlo.p;
+        A.trjhi = ab.trjhi.p; A.wrp = ab.wrp.p; A.gamsasa = ab.gamsasa.p; A.hbmag = ab.hbmag.p; A.grid = ab.grid.p;
+        A.keps = ab.keps; A.alpbet = ab.alpbet; A.born_scale = ab.born_scale; A.gshift = ab.gshift;
+        A.srcut2 = ab.srcut2; A.lhb = ab.lhb;
+        A.brad = ab.brad.p; A.dpsi = ab.dpsi.p; A.sasa = ab.sasa.p; A.hbw = ab.hbw.p; A.dhbdw = ab.dhbdw.p;
+        A.bdiag = ab.bdiag.p; A.dEdbr = ab.dEdbr.p; A.shape = ab.shape.p; A.bad = bad.p;
+        return A;
+    }
+    // per-atom ALPB data in the engine's atom order (internal atom s is caller atom h_perm[s])
+    void upload_alpb(const AlpbModel& M)
+    {
+        alpb_on = M.on;
+        if (!alpb_on) return;
+        if (nmol != 1) throw std::runtime_error("ALPB solvation: single molecules only");
+        auto perm_of = [&](const std::vector<double>& v) {
+            std::vector<double> o(n);
+            for (int s2 = 0; s2 < n; ++s2) o[s2] = v[h_perm[s2]];
+            return o;
+        };
+        ab.keps = M.keps; ab.alpbet = M.alpbet; ab.born_scale = M.born_scale; ab.gshift = M.gshift;
+        ab.srcut2 = M.srcut * M.srcut; ab.lhb = M.lhb ? 1 : 0;
+        ab.vdwr.upload(perm_of(M.vdwr)); ab.rho.upload(perm_of(M.rho)); ab.svdw.upload(perm_of(M.svdw));
+        ab.vdwsa.upload(perm_of(M.vdwsa)); ab.trjlo.upload(perm_of(M.trj2_lo)); ab.trjhi.upload(perm_of(M.trj2_hi));
+        ab.wrp.upload(perm_of(M.wrp)); ab.gamsasa.upload(perm_of(M.gamsasa)); ab.hbmag.upload(perm_of(M.hbmag));
+        std::vector<double4> g(gfnff::alpb::kNang);
+        for (int p = 0; p < gfnff::alpb::kNang; ++p)
+            g[p] = make_double4(M.grid[3 * p], M.grid[3 * p + 1], M.grid[3 * p + 2], M.weight[p]);
+        ab.grid.upload(g);
+        ab.brad.alloc(n); ab.dpsi.alloc(n); ab.sasa.alloc(n); ab.hbw.alloc(n); ab.dhbdw.alloc(n);
+        ab.bdiag.alloc(n); ab.dEdbr.alloc(n); ab.shape.alloc(16);
+    }
+    // geometry part before the EEQ matrix; energy and gradient after the solve
+    void alpb_pre(cudaStream_t s)
+    {
+        const View V = view();
+        const AlpbArgs A = alpb_args();
+        const unsigned gw = (unsigned)(((long)n * 32 + 255) / 256);
+        k_alpb_born<<<gw, 256, 0, s>>>(V, A);
+        k_alpb_sasa<false><<<n, kAlpbSasaThreads, 0, s>>>(V, A);
+        k_alpb_shape<<<1, 256, 0, s>>>(V, A);
+    }
+    void alpb_post(cudaStream_t s)
+    {
+        const View V = view();
+        const AlpbArgs A = alpb_args();
+        const unsigned gw = (unsigned)(((long)n * 32 + 255) / 256);
+        k_alpb_energy<<<gw, 256, 0, s>>>(V, A);
+        k_alpb_chain<<<gw, 256, 0, s>>>(V, A);
+        k_alpb_sasa<true><<<n, kAlpbSasaThreads, 0, s>>>(V, A);
+        k_alpb_shape_grad<<<1, 256, 0, s>>>(V, A);
+    }
     DBuf<int> x_a, x_x, x_b;
     DBuf<double> x_pre, x_rv;
     DBuf<int> r_off, r_j;
@@ -639,6 +705,9 @@ struct Engine::Impl {
         V.zeta = zeta.p; V.szr = szr.p;
         V.cnraw = cnraw.p; V.cn = cn.p; V.dlog = dlog.p; V.w = w.p; V.dw = dw.p; V.hg = hg.p; V.hdg = hdg.p;
         V.q = q.p; V.dEdcn = dEdcn.p; V.v = v.p; V.grad = grad.p; V.E = E.p; V.status = status.p;
+        V.brad = alpb_on ? ab.brad.p : nullptr;
+        V.bdiag = alpb_on ? ab.bdiag.p : nullptr;
+        V.keps = alpb_on ? ab.keps : 0.0;
         V.exact = opt.exact_gradient ? 1 : 0;
         V.cfar = resp_on ? cfar.p : nullptr;
         V.u = resp_on ? ures.p : nullptr;
@@ -925,9 +994,9 @@ void Engine::upload_hbxb(const Model& m, const double* hb_xyz_bohr)
     }
 }
 
-void Engine::upload(const Model& m) { upload_batch({&m}); }
+void Engine::upload(const Model& m, const AlpbModel* solv) { upload_batch({&m}, solv); }
 
-void Engine::upload_batch(const std::vector<const Model*>& mols)
+void Engine::upload_batch(const std::vector<const Model*>& mols, const AlpbModel* solv)
 {
     Impl& P = *p_;
     P.drop_graphs();
@@ -1654,6 +1723,8 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
     // (eeq_solver.cpp:1448-2086).  Probe once at the setup geometry and keep the
     // choice for this molecule; the host entry point switches later if a geometry
     // turns it.
+    P.upload_alpb(solv ? *solv : AlpbModel());
+    if (P.alpb_on) P.pcg_res = false;   // its in-kernel matrix build has no Born term
     const bool graphs_setting = P.graphs_ok;
     P.graphs_ok = false;   // probes below run direct (their buffers are temporary)
     P.pcg_warm = false;    // and PCG probes start from zero
@@ -1676,12 +1747,14 @@ void Engine::upload_batch(const std::vector<const Model*>& mols)
             if (env && !std::strcmp(env, "library")) cand = {Impl::SOLVE_LIBRARY};
             else if (env && !std::strcmp(env, "tiled")) cand = {Impl::SOLVE_TILED};
             else if (env && !std::strcmp(env, "pcg") && P.pcg_ready) cand = {Impl::SOLVE_PCG};
-            else if (env && !std::strcmp(env, "batched") && P.batch_ready && !P.resp_on) cand = {Impl::SOLVE_BATCH};
+            else if (env && !std::strcmp(env, "batched") && P.batch_ready && !P.resp_on && !P.alpb_on)
+                cand = {Impl::SOLVE_BATCH};
             else {
                 cand = {Impl::SOLVE_TILED};
                 if (P.pcg_ready) cand.push_back(Impl::SOLVE_PCG);
                 // the batched kernel keeps no factor for the charge-response solve
-                if (P.batch_ready && !P.resp_on) cand.push_back(Impl::SOLVE_BATCH);
+                // (nor the solvent's Born matrix: it builds its matrix from the atoms)
+                if (P.batch_ready && !P.resp_on && !P.alpb_on) cand.push_back(Impl::SOLVE_BATCH);
             }
             if (cand.size() == 1) {
                 P.solver = cand[0];
@@ -2062,6 +2135,7 @@ void Engine::launch_body()
         bonded_terms();
         CK(cudaEventRecord(P.ev_join, s2));
     }
+    if (P.alpb_on) P.alpb_pre(s);   // Born radii, surfaces, shape: the Born matrix of the EEQ
     // EEQ
     P.mark(3);
     if (P.nmol == 1 && !(P.solver == Impl::SOLVE_BATCH && !P.use_lu)) {
@@ -2158,6 +2232,7 @@ void Engine::launch_body()
     } else {
         k_cn_chain<double><<<tgrid, kTile, 0, s>>>(V, P.nsplit, nullptr);
     }
+    if (P.alpb_on) P.alpb_post(s);   // solvation energy and gradient at the solved charges
     P.mark(11);
     k_outputs<<<nblk(n), kBlock, 0, s>>>(V, P.gout.p, P.qout.p, P.cnout.p, P.bad.p);
     k_finish<<<nblk(P.nmol), kBlock, 0, s>>>(V, (P.nred > 0 || P.nmol > 1) ? P.info.p : nullptr, P.bad.p, P.e0.p,

@@ -7,6 +7,7 @@
 #include <string>
 #include <vector>
 
+#include "../setup/alpb.h"
 #include "../setup/model.h"
 
 namespace gfnff {
@@ -27,8 +28,9 @@ public:
     // Uploads one model (upload) or a batch of independent molecules (upload_batch; the
     // molecules do not interact, their atoms are concatenated in the given order).
     // Throws std::runtime_error on CUDA failure.
-    void upload(const Model& m);
-    void upload_batch(const std::vector<const Model*>& mols);
+    // solv: ALPB implicit solvation of a single molecule (null or off: gas phase)
+    void upload(const Model& m, const AlpbModel* solv = nullptr);
+    void upload_batch(const std::vector<const Model*>& mols, const AlpbModel* solv = nullptr);
     // re-uploads the HB/XB lists and the bond<->HB cross reference (single model)
     // HB/XB lists of a single-molecule engine: the model's host lists, or, with
     // m.hb_on_device, the HB terms detected on the device at hb_xyz_bohr (caller order;
@@ -95,7 +97,7 @@ public:
     static const char* const kPhaseNames[];
     static constexpr int kNumPhases = 12;
 
-    static constexpr int kNumTerms = 14;
+    static constexpr int kNumTerms = 15;
 
 private:
     void tune_pairs(const std::vector<const Model*>& mols);

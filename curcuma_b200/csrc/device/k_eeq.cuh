@@ -13,16 +13,29 @@
 namespace {
 
 // one element of A.  erf(r/sqrt(s)) == 1 in double once r^2 >= 36 s (erfc(6) < 2^-54).
+// Born (P16) element keps / (r + ab (ab / (ab + zeta r / 16))^16), ab = sqrt(brad_a brad_b)
+__device__ __forceinline__ double born_p16(double keps, double r, double ba, double bb)
+{
+    const double ab = sqrt(ba * bb);
+    double t = ab / (ab + gfnff::alpb::kZetaP16o16 * r);
+    t *= t;
+    t *= t;
+    t *= t;
+    t *= t;
+    return keps / (r + ab * t);
+}
+
 __device__ __forceinline__ double eeq_a(const View& V, int a, int b)
 {
-    if (a == b) return V.adiag[a];
+    if (a == b) return V.adiag[a] + (V.brad ? V.bdiag[a] : 0.0);
     const double4 pa = V.pos[a], pb = V.pos[b];
     const double dx = pa.x - pb.x, dy = pa.y - pb.y, dz = pa.z - pb.z;
     const double d2 = dx * dx + dy * dy + dz * dz;
     const double s = V.alpeeq[a] + V.alpeeq[b];
-    if (d2 >= 36.0 * s) return rsqrt(d2);
     const double r = sqrt(d2);
-    return erf(r / sqrt(s)) / r;
+    const double born = V.brad ? born_p16(V.keps, r, V.brad[a], V.brad[b]) : 0.0;
+    if (d2 >= 36.0 * s) return rsqrt(d2) + born;
+    return erf(r / sqrt(s)) / r + born;
 }
 
 // reduced matrix, column-major with leading dimension lda: M[c*lda + r]; lower triangle
@@ -52,6 +65,7 @@ __global__ void __launch_bounds__(256) k_eeq_M_tiles(View V, const int* __restri
                                                     float* M32 = nullptr)   // optional FP32 copy (k_pcg_ir)
 {
     __shared__ double px[4][kMT], py[4][kMT], pz[4][kMT], pa[4][kMT];   // rows k, rows ak, cols l, cols al
+    __shared__ double pbr[4][kMT];                                       // Born radii (solvation)
     __shared__ int pid[4][kMT];
     __shared__ double T[kMT][kMT + 1];
     // triangular block index -> (tr, tc)
@@ -73,17 +87,19 @@ __global__ void __launch_bounds__(256) k_eeq_M_tiles(View V, const int* __restri
         if (a >= 0) {
             const double4 p = V.pos[a];
             px[w][t] = p.x; py[w][t] = p.y; pz[w][t] = p.z; pa[w][t] = V.alpeeq[a];
+            pbr[w][t] = V.brad ? V.brad[a] : 0.0;
         }
     }
     __syncthreads();
     auto el = [&](int wa, int ia, int wb, int ib) {
-        if (pid[wa][ia] == pid[wb][ib]) return V.adiag[pid[wa][ia]];
+        if (pid[wa][ia] == pid[wb][ib]) return V.adiag[pid[wa][ia]] + (V.brad ? V.bdiag[pid[wa][ia]] : 0.0);
         const double dx = px[wa][ia] - px[wb][ib], dy = py[wa][ia] - py[wb][ib], dz = pz[wa][ia] - pz[wb][ib];
         const double d2 = dx * dx + dy * dy + dz * dz;
         const double s = pa[wa][ia] + pa[wb][ib];
-        if (d2 >= 36.0 * s) return rsqrt(d2);
+        const double born = V.brad ? born_p16(V.keps, sqrt(d2), pbr[wa][ia], pbr[wb][ib]) : 0.0;
+        if (d2 >= 36.0 * s) return rsqrt(d2) + born;
         const double r = sqrt(d2);
-        return erf(r / sqrt(s)) / r;
+        return erf(r / sqrt(s)) / r + born;
     };
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;   // 32 x 8
     for (int cc = ty; cc < kMT; cc += 8) {

@@ -38,11 +38,11 @@ MIXED = 1
 
 class GFNFF:
     def __init__(self, precision: int = FP64, device: int = 0, hbond: bool = True,
-                 hb_rmsd_bohr: float = 0.3, exact_gradient: bool = False):
+                 hb_rmsd_bohr: float = 0.3, exact_gradient: bool = False, solvent: str = "none"):
         self._lib = _lib.load()
         self._params = {"precision": "mixed" if precision == MIXED else "fp64", "gpu_device": device,
                         "hbond": bool(hbond), "hb_rmsd_bohr": hb_rmsd_bohr,
-                        "exact_gradient": bool(exact_gradient), "threads": 1}
+                        "exact_gradient": bool(exact_gradient), "solvent": solvent or "none", "threads": 1}
         self._h = None
         self._create()
 
@@ -61,6 +61,12 @@ class GFNFF:
             raise RuntimeError(f"gfnff_create: {_lib.STATUS_NAMES.get(st)}: "
                                f"{self._lib.gfnff_last_error(None).decode()}")
         self._h = h
+        st = self._lib.gfnff_set_solvent(h, str(p["solvent"]).encode())
+        if st != _lib.GFNFF_OK:
+            msg = self._lib.gfnff_last_error(h).decode()
+            self._lib.gfnff_destroy(h)
+            self._h = None
+            raise ValueError(f"gfnff_set_solvent: {msg}")
         self._n = 0
         self._xyz = None
         self._grad = None
@@ -260,7 +266,8 @@ class GFNFF:
         self._params["threads"] = threads if threads > 0 else 1
 
     def setParameters(self, params: dict) -> None:
-        """precision ("fp64"/"mixed"), gpu_device, hbond, hb_rmsd_bohr, exact_gradient, threads.
+        """precision ("fp64"/"mixed"), gpu_device, hbond, hb_rmsd_bohr, exact_gradient, solvent
+        (ALPB implicit solvation: curcuma's solvent names, "none" for the gas phase), threads.
         A new handle is made with them: call setMolecule again afterwards."""
         unknown = set(params) - set(self._params)
         if unknown:

@@ -34,7 +34,7 @@ enum { GFNFF_FP64 = 0, GFNFF_MIXED = 1 };
 enum {
     GFNFF_E_BOND = 0, GFNFF_E_ANGLE, GFNFF_E_TORSION, GFNFF_E_INVERSION, GFNFF_E_STORSION,
     GFNFF_E_DISPERSION, GFNFF_E_BONDED_REP, GFNFF_E_NONBONDED_REP, GFNFF_E_COULOMB,
-    GFNFF_E_HBOND, GFNFF_E_XBOND, GFNFF_E_ATM, GFNFF_E_BATM, GFNFF_E_TOTAL, GFNFF_NTERMS
+    GFNFF_E_HBOND, GFNFF_E_XBOND, GFNFF_E_ATM, GFNFF_E_BATM, GFNFF_E_SOLVATION, GFNFF_E_TOTAL, GFNFF_NTERMS
 };
 
 typedef struct {
@@ -58,6 +58,14 @@ typedef struct gfnff_handle gfnff_handle;
 
 /* Fills opts with the defaults (FP64, device 0, HB on, 0.3 bohr). */
 void gfnff_default_options(gfnff_options* opts);
+
+/* ALPB implicit solvation for the next gfnff_setup / gfnff_setup_from_parameters of this
+ * handle (curcuma's -gfnff.solvent, gfnff_method.cpp:811-840: the solvent's reaction field
+ * enters the EEQ solve, A += B, and the solvation free energy 1/2 q^T B q + G_sasa + G_shift
+ * is reported as GFNFF_E_SOLVATION; curcuma's solvent names and aliases, case-insensitive;
+ * NULL, "" or "none": gas phase, the default).  Single-molecule handles only.  Returns
+ * GFNFF_INVALID_ARG for an unknown solvent. */
+gfnff_status gfnff_set_solvent(gfnff_handle* h, const char* solvent);
 
 /* Replaces GFNFFGPUComputationalMethod construction
  * (src/core/energy_calculators/qm_methods/gfnff_gpu_method.h:52-194). */

@@ -51,7 +51,7 @@ def test_alpb_gradient_central_differences(mol, solvent):
         o = Oracle(Z, X, solvent=s)
         G = o.engrad(X)[1]
         e = np.zeros(G.shape)
-        for a in range(min(len(Z), 8)):
+        for a in range(min(len(Z), 5)):
             for d in range(3):
                 Xp, Xm = X.copy(), X.copy()
                 Xp[a, d] += h
@@ -60,3 +60,30 @@ def test_alpb_gradient_central_differences(mol, solvent):
                 e[a, d] = fd - G[a, d]
         err[s] = e
     assert np.abs(err[solvent] - err[None]).max() < 1e-7
+
+
+def test_alpb_gradient_of_a_cation():
+    """NH4+ beside a water: the shape term (1/2 keps alpbet / adet (sum q)^2) and its
+    gradient only act on a charged solute."""
+    t = 1.03 / np.sqrt(3.0)
+    a = np.deg2rad(104.52 / 2)
+    X = np.array([[0, 0, 0], [t, t, t], [t, -t, -t], [-t, t, -t], [-t, -t, t], [3.5, 0, 0],
+                  [3.5 + 0.9572 * np.cos(a), 0.9572 * np.sin(a), 0], [3.5 + 0.9572 * np.cos(a), -0.9572 * np.sin(a), 0]])
+    Z = np.array([7, 1, 1, 1, 1, 8, 1, 1])
+    h = 1e-4 * BOHR
+    err = {}
+    for s in (None, "water"):
+        o = Oracle(Z, X, charge=1, solvent=s)
+        T, G, q, cn = o.engrad(X)
+        assert abs(q.sum() - 1.0) < 1e-10
+        e = np.zeros(G.shape)
+        for a_ in range(len(Z)):
+            for d in range(3):
+                Xp, Xm = X.copy(), X.copy()
+                Xp[a_, d] += h
+                Xm[a_, d] -= h
+                e[a_, d] = (o.engrad(Xp)[0]["total"] - o.engrad(Xm)[0]["total"]) / 2e-4 - G[a_, d]
+        err[s] = e
+        if s:
+            assert T["solvation"] < -0.2
+    assert np.abs(err["water"] - err[None]).max() < 1e-8
