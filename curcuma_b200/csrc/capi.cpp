@@ -30,6 +30,7 @@ struct gfnff_handle {
     bool ready = false;
     std::string err;
     std::vector<double> hb_ref;    // bohr, geometry of the last HB/XB detection
+    std::vector<double> topo_ref;  // bohr, geometry of the last topology
     std::string solvent;            // ALPB solvent ("" gas phase)
     AlpbModel solv;
     double* pin_xyz = nullptr;      // pinned staging for host coordinates
@@ -142,6 +143,7 @@ static gfnff_status finish_setup(gfnff_handle* h, int n)
         return fail(h, GFNFF_CUDA_ERROR, e.what());
     }
     h->hb_ref = h->model.xyz_setup;
+    h->topo_ref = h->model.xyz_setup;
     h->nmol = 0;
     h->natoms = n;
     h->batch.clear();
@@ -289,6 +291,41 @@ gfnff_status gfnff_energy_and_gradient_batch(gfnff_handle* h, const double* xyz,
     return GFNFF_OK;
 }
 
+// curcuma's topology refresh (gfnff_method.cpp:885-937, 1007-1032): when an atom has moved
+// more than 0.5 bohr along an axis since the last topology, the topology and its EEQ
+// parameters are recomputed at xb (bohr).  Same fragments: the EEQ parameters are updated in
+// place (the HB/XB lists stay, as in curcuma, until their own refresh); new fragments: the
+// HB/XB lists are detected again at their reference geometry with the new topology (their
+// terms carry neighbour lists of the bond graph, which the upload checks against the new
+// one) and the engine takes the whole model again.
+static constexpr double kTopoDispBohr = 0.5;
+
+static void topology_refresh(gfnff_handle* h, const double* xb)
+{
+    const int nfrag0 = h->model.nfrag;
+    const std::vector<int> frag0 = h->model.frag;
+    const std::vector<double> qfrag0 = h->model.qfrag;
+    if (refresh_topology(h->model, xb)) {
+        if (h->model.nfrag == nfrag0 && h->model.frag == frag0 && h->model.qfrag == qfrag0) {
+            h->eng->update_eeq_parameters(h->model);
+        } else {
+            if (h->opt.hbond) redetect_hbxb(h->model, h->hb_ref.data());
+            h->eng->upload(h->model, h->solv.on ? &h->solv : nullptr);
+            if (h->model.hb_on_device) h->eng->upload_hbxb(h->model, h->hb_ref.data());
+            h->eng->set_hb_reference(h->hb_ref.data());
+        }
+    }
+    h->topo_ref.assign(xb, xb + 3 * (size_t)h->model.n);
+    h->eng->set_topo_reference(xb);
+}
+
+static double max_disp(const std::vector<double>& ref, const double* xb, size_t n3)
+{
+    double m = 0.0;
+    for (size_t k = 0; k < n3; ++k) m = std::max(m, std::fabs(xb[k] - ref[k]));
+    return m;
+}
+
 gfnff_status gfnff_energy_and_gradient(gfnff_handle* h, const double* xyz, double* energy, double* grad,
                                        double* terms)
 {
@@ -300,8 +337,14 @@ gfnff_status gfnff_energy_and_gradient(gfnff_handle* h, const double* xyz, doubl
     for (int k = 0; k < 3 * n; ++k)
         if (!std::isfinite(xyz[k])) return fail(h, GFNFF_NONFINITE, "non-finite coordinate");
     try {
-        // HB/XB refresh when the RMSD-like measure sqrt(sum d^2)/N exceeds the threshold
-        // (gfnff_method.cpp:2228-2259): re-detect on the host before this evaluation
+        // topology refresh on a 0.5 bohr displacement, then the HB/XB refresh when the RMSD-like
+        // measure sqrt(sum d^2)/N exceeds the threshold (gfnff_method.cpp:2228-2259), both
+        // before this evaluation
+        {
+            std::vector<double> xb(3 * (size_t)n);
+            for (int k = 0; k < 3 * n; ++k) xb[k] = xyz[k] * kAngToBohr;
+            if (max_disp(h->topo_ref, xb.data(), xb.size()) > kTopoDispBohr) topology_refresh(h, xb.data());
+        }
         if (h->opt.hbond) {
             double s = 0.0;
             for (int k = 0; k < 3 * n; ++k) {
@@ -488,16 +531,21 @@ gfnff_status gfnff_md_nve(gfnff_handle* h, int nsteps, double dt_fs, double* xyz
         // before every energy (gfnff_method.cpp:1597-1613): the device loop finds the
         // first step over the threshold and rolls back to it for the re-detection
         MdRefresh R;
+        R.topo_disp_bohr = kTopoDispBohr;
+        h->eng->set_topo_reference(h->topo_ref.data());
         if (h->opt.hbond) {
             R.hb_rmsd_bohr = h->opt.hb_rmsd_bohr;
             h->eng->set_hb_reference(h->hb_ref.data());
-            R.redetect = [h](const double* xb) {
+        }
+        R.refresh = [h](const double* xb, int reasons) {
+            if (reasons & 2) topology_refresh(h, xb);
+            if ((reasons & 1) && h->opt.hbond) {
                 redetect_hbxb(h->model, xb);
                 h->eng->upload_hbxb(h->model, xb);
                 h->eng->set_hb_reference(xb);
                 h->hb_ref.assign(xb, xb + 3 * (size_t)h->model.n);
-            };
-        }
+            }
+        };
         int worst = 0;
         md_nve(*h->eng, nsteps, dt_fs, xyz, vel, mass, epot, ekin, &worst, &R);
         if (worst != 0) return fail(h, (gfnff_status)worst, "MD stopped: evaluation failed");

@@ -388,7 +388,7 @@ struct Engine::Impl {
     std::vector<int> h_anchor, h_r2a;   // EEQ null-space maps (host copies)
     DBuf<double> e0;
     // model
-    DBuf<double4> pos, pos0, hbref;
+    DBuf<double4> pos, pos0, hbref, toporef;
     DBuf<double> rcov_cn, rcov43, rcov_d3, chi_base, cnf, gam, alpeeq, adiag, qa, refcn, w0, g0, c6ref, zeta, szr;
     DBuf<int> slot, nref;
     // EEQ structure
@@ -454,7 +454,7 @@ struct Engine::Impl {
         std::vector<unsigned char> bcase;
         DBuf<unsigned char> fl, bc, flag, tmp;
         DBuf<double> bas, aci, x, x0;
-        DBuf<int> Zc, bo, bl, ho, hl, hc, map, val, val2, near, nsel;
+        DBuf<int> Zc, bo, bl, ho, hl, hc, map, val, val2, near, nsel, ffo, ffl;
         DBuf<long long> cnt, off;
         DBuf<int4> raw, xref;
         DBuf<unsigned long long> key, key2;
@@ -812,9 +812,17 @@ void Engine::Impl::detect_hb(const Model& m, const double* xb, std::vector<int>&
                 o.push_back((int)v.size());
             }
         };
-        std::vector<int> bo, bl, ho, hl, hc, map(na);
+        std::vector<int> bo, bl, ho, hl, hc, map(na), ffo, ffl;
         csr(part, bo, bl);
         csr(hyd, ho, hl);
+        {
+            std::vector<std::vector<int>> ff(na);   // partners of the set-up's bond terms
+            for (const auto& bd : m.bonds) {
+                ff[bd.i].push_back(bd.j);
+                ff[bd.j].push_back(bd.i);
+            }
+            csr(ff, ffo, ffl);
+        }
         std::vector<unsigned char> fl(na);
         D.bcase.assign(na, 2);
         for (int a = 0; a < na; ++a) {
@@ -832,6 +840,7 @@ void Engine::Impl::detect_hb(const Model& m, const double* xb, std::vector<int>&
         D.nhc = (int)hc.size();
         D.Zc.upload(Zc); D.bo.upload(bo); D.bl.upload(bl); D.ho.upload(ho); D.hl.upload(hl);
         D.hc.upload(hc); D.map.upload(map); D.fl.upload(fl); D.bc.upload(D.bcase);
+        D.ffo.upload(ffo); D.ffl.upload(ffl.empty() ? std::vector<int>{0} : ffl);
         D.aci.upload(at.aci);
         D.x0.upload(m.xyz_setup);
         D.cnt.alloc(na); D.off.alloc(na); D.near.alloc(1); D.nsel.alloc(1);
@@ -890,7 +899,7 @@ void Engine::Impl::detect_hb(const Model& m, const double* xb, std::vector<int>&
         h_rec.alloc(ni);
         CK(cudaMemsetAsync(D.near.p, 0, sizeof(int), s));
         k_hb_gather<<<g2, 256, 0, s>>>(nt, D.raw.p, D.val2.p, D.key2.p, D.map.p, h_rec.p, D.near.p);
-        k_hb_xref_flags<<<g2, 256, 0, s>>>(nt, D.raw.p, D.Zc.p, D.flag.p);
+        k_hb_xref_flags<<<g2, 256, 0, s>>>(nt, D.raw.p, D.Zc.p, D.ffo.p, D.ffl.p, D.flag.p);
         b = D.tmp.n;
         CK(cub::DeviceSelect::Flagged(D.tmp.p, b, D.raw.p, D.flag.p, D.xref.p, D.nsel.p, ni, s));
         int nsel = 0;
@@ -1120,7 +1129,7 @@ void Engine::upload_batch(const std::vector<const Model*>& mols, const AlpbModel
             }
         }
     }
-    P.pos0.upload(p0); P.hbref.upload(p0); P.pos.alloc(n);
+    P.pos0.upload(p0); P.hbref.upload(p0); P.toporef.upload(p0); P.pos.alloc(n);
     {
         const char* ecl = std::getenv("GFNFF_CN_LIST");
         P.cnl_on = !(ecl && !std::strcmp(ecl, "0"));
@@ -1441,7 +1450,7 @@ void Engine::upload_batch(const std::vector<const Model*>& mols, const AlpbModel
     P.gout.alloc(3 * (size_t)n); P.qout.alloc(n); P.cnout.alloc(n);
     P.lda = (P.nred + 4) & ~3;   // >= nred + 1, a multiple of 4: 16-byte aligned FP32 and FP64 columns
     P.M.alloc((size_t)std::max<long long>(1, nm == 1 ? (long long)P.lda * P.nred : P.msize));
-    P.bvec.alloc(std::max(1, P.nred)); P.xyz_stage.alloc(3 * (size_t)n); P.msd.alloc(1);
+    P.bvec.alloc(std::max(1, P.nred)); P.xyz_stage.alloc(3 * (size_t)n); P.msd.alloc(2);
     P.info.alloc(nm); P.info2.alloc(1); P.status.alloc(nm); P.bad.alloc(nm);
     CK(cudaMemset(P.info.p, 0, nm * sizeof(int)));
     P.use_lu = false;
@@ -2023,10 +2032,10 @@ void Engine::launch_positions(const double* d_xyz, bool bohr)
 {
     Impl& P = *p_;
     P.mark(0);
-    CK(cudaMemsetAsync(P.msd.p, 0, sizeof(double), P.stream));
+    CK(cudaMemsetAsync(P.msd.p, 0, 2 * sizeof(double), P.stream));
     k_positions<<<nblk(P.n), kBlock, 0, P.stream>>>(P.n, P.perm.p, d_xyz, bohr ? 1.0 : kAngToBohr, P.pos.p,
                                                    P.hbref.p, P.msd.p, P.cnl_on ? P.cnl_ref.p : nullptr,
-                                                   0.25 * Impl::kCnSkin * Impl::kCnSkin, P.cnl_bad.p);
+                                                   0.25 * Impl::kCnSkin * Impl::kCnSkin, P.cnl_bad.p, P.toporef.p);
 }
 
 // everything after the positions, reading and writing engine buffers only, so that it
@@ -2329,6 +2338,41 @@ void Engine::refresh_cn_list()
     } else {
         P.build_cn_list_device(P.pos.p);
     }
+}
+
+// EEQ parameters of a refreshed topology with the same fragments: copied into the existing
+// buffers, so that captured graphs stay valid
+void Engine::update_eeq_parameters(const Model& m)
+{
+    Impl& P = *p_;
+    if (P.nmol != 1 || m.n != P.n) throw std::runtime_error("update_eeq_parameters: single molecule of the same size");
+    std::vector<double> chi(P.n), cnf(P.n), gam(P.n), alp(P.n), adg(P.n), qa(P.n);
+    for (int a = 0; a < m.n; ++a) {
+        const int s = P.ix(0, a);
+        chi[s] = m.chi_base[a]; cnf[s] = m.cnf[a]; gam[s] = m.gam[a]; alp[s] = m.alpeeq[a];
+        adg[s] = m.gam[a] + 0.797884560802866 / std::sqrt(m.alpeeq[a]);
+        qa[s] = m.qa[a];
+    }
+    CK(cudaStreamSynchronize(P.stream));
+    const size_t b = (size_t)P.n * sizeof(double);
+    CK(cudaMemcpy(P.chi_base.p, chi.data(), b, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(P.cnf.p, cnf.data(), b, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(P.gam.p, gam.data(), b, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(P.alpeeq.p, alp.data(), b, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(P.adiag.p, adg.data(), b, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(P.qa.p, qa.data(), b, cudaMemcpyHostToDevice));
+    P.hbd.topo = nullptr;   // the HB detection's topology inputs follow the new topology
+}
+
+void Engine::set_topo_reference(const double* xyz_bohr)
+{
+    Impl& P = *p_;
+    std::vector<double4> r(P.n);
+    for (int s = 0; s < P.n; ++s) {
+        const int o = P.h_perm[s];
+        r[s] = make_double4(xyz_bohr[3 * o], xyz_bohr[3 * o + 1], xyz_bohr[3 * o + 2], 0.0);
+    }
+    P.toporef.upload(r);
 }
 
 void Engine::set_hb_reference(const double* xyz_bohr)

@@ -53,7 +53,8 @@ public:
     const double* d_charges() const;   // N
     const double* d_cn() const;        // N
     const int* d_status() const;       // 1 int (gfnff_status) per molecule
-    const double* d_hb_msd() const;    // sum of squared displacements vs HB reference
+    const double* d_hb_msd() const;    // [0] sum of squared displacements vs the HB reference,
+                                       // [1] largest |coordinate change| vs the topology reference
     double* d_xyz_scratch();           // N*3 staging buffer for host coordinates
 
     void* stream() const;
@@ -68,6 +69,12 @@ public:
     std::vector<int> device_dispersion_pairs();
     // sets the HB reference geometry (bohr, host, caller order) for the refresh test
     void set_hb_reference(const double* xyz_bohr);
+    // sets the geometry of the last topology (bohr, host, caller order): d_hb_msd()[1] of an
+    // evaluation holds the largest coordinate change since it
+    void set_topo_reference(const double* xyz_bohr);
+    // EEQ parameters (chi, cnf, gamma, alpha, Phase-1 charges) of a refreshed topology of the
+    // same molecule with the same fragments, in place
+    void update_eeq_parameters(const Model& m);
     // the CN neighbour list no longer covers the geometry of the last evaluation (its
     // evaluations fell back to the all-pairs CN kernels); refresh_cn_list rebuilds it
     // around that geometry

@@ -17,7 +17,7 @@
 // the host's order (no contraction into FMA), so every comparison is the host's.
 // The engine then sorts the terms by the squared A-B distance at the set-up geometry
 // (stable radix sort: the host's stable_sort), maps them to its atom order and derives the
-// bond <-> HB cross reference from the case 2-4 terms with an N or O acceptor.
+// bond <-> HB cross reference from the terms with an N or O acceptor.
 // Included inside namespace gfnff by engine.cu, after common.cuh.
 #pragma once
 
@@ -133,15 +133,24 @@ __global__ void k_hb_gather(long long nt, const int4* __restrict__ rec, const in
     if (in && !next_in) *near = (int)(t + 1);
 }
 
-// the terms that enter the bond <-> HB cross reference: case 2-4 with an N or O acceptor
+// the terms that enter the bond <-> HB cross reference: an N or O acceptor, an N or O donor
+// A, and (A, H) a bond term of the set-up (ffo/ffl: the bond-term partners of every atom).
+// Case 2-4 terms have H bonded to A in the topology; with a refreshed topology a bond term's
+// A-H pair can also be the (A, H) of a case-1 term.
 __global__ void k_hb_xref_flags(long long nt, const int4* __restrict__ rec, const int* __restrict__ Z,
-                                unsigned char* flag)
+                                const int* __restrict__ ffo, const int* __restrict__ ffl, unsigned char* flag)
 {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nt) return;
     const int4 r = rec[t];
-    const int zb = Z[r.z];
-    flag[t] = r.w >= 2 && (zb == 7 || zb == 8);
+    const int za = Z[r.x], zb = Z[r.z];
+    bool f = (za == 7 || za == 8) && (zb == 7 || zb == 8);
+    if (f) {
+        bool bond = false;
+        for (int k = ffo[r.y]; k < ffo[r.y + 1]; ++k) bond |= ffl[k] == r.x;
+        f = bond;
+    }
+    flag[t] = f;
 }
 
 // CN neighbour list on the device: for every atom i the partners j of its molecule with

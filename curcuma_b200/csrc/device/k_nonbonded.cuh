@@ -31,25 +31,34 @@ __device__ __forceinline__ void tile_range(const View& V, int i0, int nsplit, in
 // (gfnff_method.cpp:2228-2259)
 // ------------------------------------------------------------------------------------
 // (nl_ref, nl_bad): reference geometry of the CN neighbour list; an atom more than
-// sqrt(nl_lim2) away from it marks the list stale (kept until the host rebuilds it)
+// sqrt(nl_lim2) away from it marks the list stale (kept until the host rebuilds it).
+// msd[1] receives the topology refresh metric, the largest |coordinate change| since the
+// geometry topo_ref of the last topology (gfnff_method.cpp:1021-1031), as the bits of a
+// non-negative double (which order like the integers)
 __global__ void k_positions(int n, const int* __restrict__ perm, const double* __restrict__ xyz, double scale,
                             double4* pos, const double4* __restrict__ ref, double* msd,
-                            const double4* __restrict__ nl_ref, double nl_lim2, int* nl_bad)
+                            const double4* __restrict__ nl_ref, double nl_lim2, int* nl_bad,
+                            const double4* __restrict__ topo_ref)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    double s = 0.0;
+    double s = 0.0, dmax = 0.0;
     if (i < n) {
         const int o = perm[i];
         const double x = xyz[3 * o] * scale, y = xyz[3 * o + 1] * scale, z = xyz[3 * o + 2] * scale;
         pos[i] = make_double4(x, y, z, 0.0);
         const double4 r = ref[i];
         s = (x - r.x) * (x - r.x) + (y - r.y) * (y - r.y) + (z - r.z) * (z - r.z);
+        const double4 t = topo_ref[i];
+        dmax = fmax(fabs(x - t.x), fmax(fabs(y - t.y), fabs(z - t.z)));
         if (nl_ref) {
             const double4 q = nl_ref[i];
             const double d2 = (x - q.x) * (x - q.x) + (y - q.y) * (y - q.y) + (z - q.z) * (z - q.z);
             if (d2 > nl_lim2) atomicOr(nl_bad, 1);
         }
     }
+    for (int o = 16; o > 0; o >>= 1) dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
+    if ((threadIdx.x & 31) == 0 && dmax > 0.0)
+        atomicMax(reinterpret_cast<unsigned long long*>(msd + 1), (unsigned long long)__double_as_longlong(dmax));
     block_add(s, msd);
 }
 

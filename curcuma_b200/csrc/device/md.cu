@@ -26,18 +26,33 @@ constexpr double kAngToBohrMd = 1.0 / 0.529177210903;
         if (e_ != cudaSuccess) throw std::runtime_error(std::string("CUDA (md): ") + cudaGetErrorString(e_)); \
     } while (0)
 
-// Per-run device record: [0] first step whose evaluation should have used refreshed HB/XB
-// lists (-1: none), [1] first step whose evaluation failed (-1: none), [2] its status.
+// Per-run device record: [0] first step whose evaluation should have followed a refresh
+// (-1: none), [1] first step whose evaluation failed (-1: none), [2] its status, [3] the
+// refreshes due at step [0] (1 HB/XB lists, 2 topology).
 struct MdFlags {
     int* rec;
-    const double* msd;      // the engine's sum of squared displacements vs the HB reference
+    const double* msd;      // the engine's [0] squared displacement sum vs the HB reference,
+                            // [1] largest coordinate change vs the topology reference
     const int* eval_st;     // the engine's status of the last evaluation
-    double thr;             // HB/XB refresh threshold (bohr); <= 0 disables the record
+    double thr;             // HB/XB refresh threshold (bohr); <= 0 disables it
+    double tthr;            // topology refresh threshold (bohr); <= 0 disables it
     int natoms;
     double *xs, *vs;        // state before the recorded step's evaluation
-    __device__ bool refresh_due() const
+    __device__ int refresh_due() const
     {
-        return thr > 0.0 && rec[0] < 0 && sqrt(*msd) / (double)natoms > thr;
+        if (rec[0] >= 0) return 0;
+        int r = 0;
+        if (thr > 0.0 && sqrt(msd[0]) / (double)natoms > thr) r |= 1;
+        if (tthr > 0.0 && msd[1] > tthr) r |= 2;
+        return r;
+    }
+    __device__ void mark(int t) const
+    {
+        const int r = refresh_due();
+        if (r) {
+            rec[0] = t;
+            rec[3] = r;
+        }
     }
 };
 
@@ -47,7 +62,7 @@ __global__ void k_kick_drift(int n3, double dt, const double* __restrict__ invm,
                              double* v, double* x, MdFlags F, int tprev)
 {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k == 0 && F.refresh_due()) F.rec[0] = tprev;
+    if (k == 0) F.mark(tprev);
     if (k >= n3) return;
     const double vk = v[k] - 0.5 * dt * g[k] * invm[k / 3];
     v[k] = vk;
@@ -60,7 +75,7 @@ __global__ void k_kick_ekin(int n3, double dt, const double* __restrict__ invm, 
                             double* v, const double* __restrict__ x, double* ekin, MdFlags F, int t)
 {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool snap = F.refresh_due();   // rec[0] is written only by later kernels
+    const bool snap = F.refresh_due() != 0;   // rec[0] is written only by later kernels
     if (k == 0 && *F.eval_st != 0 && F.rec[1] < 0) {
         F.rec[1] = t;
         F.rec[2] = *F.eval_st;
@@ -89,16 +104,14 @@ __global__ void k_kick_ekin(int n3, double dt, const double* __restrict__ invm, 
 }
 
 // the record of the chunk's last step t
-__global__ void k_md_close(MdFlags F, int t)
-{
-    if (F.refresh_due()) F.rec[0] = t;
-}
+__global__ void k_md_close(MdFlags F, int t) { F.mark(t); }
 
 __global__ void k_md_reset(int* rec)
 {
     rec[0] = -1;
     rec[1] = -1;
     rec[2] = 0;
+    rec[3] = 0;
 }
 
 template <class T>
@@ -122,7 +135,7 @@ int md_nve(Engine& eng, int nsteps, double dt_fs, double* xyz_ang, double* vel_a
     cudaStream_t s = (cudaStream_t)eng.stream();
     const double dt = dt_fs * kFsToAtu;
     const double vconv = kAngToBohrMd / kFsToAtu;   // A/fs -> bohr/atu
-    const bool hb = refresh && refresh->hb_rmsd_bohr > 0.0 && refresh->redetect;
+    const bool hb = refresh && refresh->refresh && (refresh->hb_rmsd_bohr > 0.0 || refresh->topo_disp_bohr > 0.0);
     std::vector<double> hx(n3), hv(n3), him(n);
     for (int k = 0; k < n3; ++k) {
         hx[k] = xyz_ang[k] * kAngToBohrMd;
@@ -130,15 +143,20 @@ int md_nve(Engine& eng, int nsteps, double dt_fs, double* xyz_ang, double* vel_a
     }
     for (int i = 0; i < n; ++i) him[i] = 1.0 / (mass_amu[i] * kAmuToMe);
     Dev<double> x(n3), v(n3), invm(n), ep(nsteps + 1), ek(nsteps + 1), xs(hb ? n3 : 1), vs(hb ? n3 : 1);
-    Dev<int> rec(3);
+    Dev<int> rec(4);
     MDCK(cudaMemcpyAsync(x.p, hx.data(), n3 * sizeof(double), cudaMemcpyHostToDevice, s));
     MDCK(cudaMemcpyAsync(v.p, hv.data(), n3 * sizeof(double), cudaMemcpyHostToDevice, s));
     MDCK(cudaMemcpyAsync(invm.p, him.data(), n * sizeof(double), cudaMemcpyHostToDevice, s));
     MDCK(cudaMemsetAsync(ep.p, 0, (nsteps + 1) * sizeof(double), s));
     MDCK(cudaMemsetAsync(ek.p, 0, (nsteps + 1) * sizeof(double), s));
-    const MdFlags F{rec.p, eng.d_hb_msd(), eng.d_status(), hb ? refresh->hb_rmsd_bohr : 0.0, n, xs.p, vs.p};
+    // the engine's buffers may be reallocated by a refresh (a new topology): re-read them after one
+    auto flags = [&]() {
+        return MdFlags{rec.p, eng.d_hb_msd(), eng.d_status(), hb ? refresh->hb_rmsd_bohr : 0.0,
+                       hb ? refresh->topo_disp_bohr : 0.0, n, xs.p, vs.p};
+    };
+    MdFlags F = flags();
     const int B = 256, G = (n3 + B - 1) / B;
-    int h_rec[3];
+    int h_rec[4];
     int worst = 0, last_good = nsteps, resumed_at = -1;
     int t = 0;
     bool fresh = true;   // step t starts from a recorded state: no drift before its evaluation
@@ -170,7 +188,8 @@ int md_nve(Engine& eng, int nsteps, double dt_fs, double* xyz_ang, double* vel_a
             MDCK(cudaMemsetAsync(ek.p + due, 0, (nsteps + 1 - due) * sizeof(double), s));
             k_md_reset<<<1, 1, 0, s>>>(rec.p);
             MDCK(cudaStreamSynchronize(s));
-            refresh->redetect(hx.data());
+            refresh->refresh(hx.data(), h_rec[3]);
+            F = flags();
             t = due;
             fresh = true;
             resumed_at = due;

@@ -136,6 +136,15 @@ Model build_model(int n, const int* Z, const double* xyz_ang, int charge,
 // With m.hb_on_device only the XB list is rebuilt (the engine detects the HB terms).
 void redetect_hbxb(Model& m, const double* xyz_bohr);
 
+// The topology refresh of curcuma's evaluation when an atom has moved more than 0.5 bohr
+// along an axis since the last topology (gfnff_method.cpp:885-937, 1007-1032;
+// QM/gfnff_gpu_method.cpp:408-425): the topology (bond graph, fragments, hybridisation,
+// pi systems, Phase-1 charges) and the EEQ parameters derived from it are recomputed at
+// xyz_bohr; the force-field term lists and their parameters stay those of the set-up, as in
+// curcuma.  Returns true when anything the evaluation uses changed (the model is updated),
+// false when the new topology is the old one (the model is left as it is).
+bool refresh_topology(Model& m, const double* xyz_bohr);
+
 // HBAtoms of the model at xyz_bohr (N x 3, caller order)
 HBAtoms hb_atom_data(Model& m, const double* xyz_bohr);
 

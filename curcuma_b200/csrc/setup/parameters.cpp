@@ -1306,6 +1306,35 @@ Model build_model(int n, const int* Z, const double* xyz_ang, int charge, const 
     return m;
 }
 
+bool refresh_topology(Model& m, const double* xyz_bohr)
+{
+    const int n = m.n;
+    Model t;
+    t.n = n;
+    t.charge = m.charge;
+    t.opt = m.opt;
+    t.Z = m.Z;
+    detail::Ctx c(t);
+    c.Z = t.Z.data();
+    c.xb.assign(xyz_bohr, xyz_bohr + 3 * (size_t)n);
+    c.xa.resize(c.xb.size());
+    for (size_t k = 0; k < c.xb.size(); ++k) c.xa[k] = c.xb[k] / kAngToBohr;
+    t.xyz_setup = c.xb;
+    c.rcov_cn = m.rcov_cn;
+    t.rcov_cn = m.rcov_cn;
+    t.rcov_d3 = m.rcov_d3;
+    t.rvdw = m.rvdw;
+    detail::compute_topology(c);
+    const bool same = t.topo_bonds == m.topo_bonds && t.adj == m.adj && t.hyb == m.hyb && t.pi_frag == m.pi_frag &&
+                      t.frag == m.frag && t.nfrag == m.nfrag && t.qfrag == m.qfrag && t.qa == m.qa &&
+                      t.chi_base == m.chi_base && t.gam == m.gam && t.alpeeq == m.alpeeq && t.cnf == m.cnf;
+    if (same) return false;
+    m.topo_bonds = t.topo_bonds; m.adj = t.adj; m.hyb = t.hyb; m.pi_frag = t.pi_frag;
+    m.frag = t.frag; m.nfrag = t.nfrag; m.qfrag = t.qfrag; m.qa = t.qa;
+    m.chi_base = t.chi_base; m.gam = t.gam; m.alpeeq = t.alpeeq; m.cnf = t.cnf;
+    return true;
+}
+
 void redetect_hbxb(Model& m, const double* xyz_bohr)
 {
     detail::Ctx c(m);

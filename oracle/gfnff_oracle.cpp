@@ -921,6 +921,14 @@ int oracle_engrad(oracle_handle* h, const double* xyz_ang, double* terms, double
     return rc;
 }
 
+int oracle_refresh_topology(oracle_handle* h, const double* xyz_ang)
+{
+    if (!h) return -1;
+    std::vector<double> xb(3 * (size_t)h->m.n);
+    for (size_t k = 0; k < xb.size(); ++k) xb[k] = xyz_ang[k] * kAngToBohr;
+    return refresh_topology(h->m, xb.data()) ? 1 : 0;
+}
+
 int oracle_redetect_hbxb(oracle_handle* h, const double* xyz_ang)
 {
     if (!h) return 1;

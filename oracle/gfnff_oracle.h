@@ -36,6 +36,11 @@ int oracle_engrad(oracle_handle* h, const double* xyz_ang, double* terms, double
 // when the RMSD from the last detection exceeds 0.3 bohr.
 int oracle_redetect_hbxb(oracle_handle* h, const double* xyz_ang);
 
+// The topology refresh at xyz (Angstrom) that curcuma applies when an atom has moved more
+// than 0.5 bohr along an axis since the last topology (the shared set-up's
+// refresh_topology).  Returns 1 when the topology changed, 0 when not.
+int oracle_refresh_topology(oracle_handle* h, const double* xyz_ang);
+
 // Topology / list export for bit-exact comparisons.  kind selects the list:
 //  0 bonds (i,j)  1 angles (i,j,k)  2 torsions (i,j,k,l)  3 inversions (i,j,k,l)
 //  4 dispersion pairs (i,j)  5 nonbonded repulsion pairs (i,j)  6 hbonds (a,h,b,case)

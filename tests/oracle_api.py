@@ -12,6 +12,7 @@ from pathlib import Path
 import numpy as np
 
 ROOT = Path(__file__).resolve().parent.parent
+BOHR_A = 0.529177210903   # Angstrom per bohr (the library's kAngToBohr)
 LIB = ROOT / "oracle" / "_build" / "liboracle.so"
 GOLDEN = ROOT / "tests" / "golden"
 TERMS = ["bond", "angle", "torsion", "inversion", "storsion", "dispersion", "bonded_rep",
@@ -42,6 +43,8 @@ def lib():
         L.oracle_term_params.argtypes = [c_v, c_i, c_v, ctypes.c_long]
         L.oracle_term_params.restype = ctypes.c_long
         L.oracle_set_solvent.argtypes = [c_v, ctypes.c_char_p]
+        L.oracle_refresh_topology.argtypes = [c_v, c_v]
+        L.oracle_refresh_topology.restype = c_i
         L.oracle_set_solvent.restype = c_i
         _lib = L
     return _lib
@@ -81,6 +84,10 @@ class Oracle:
             raise RuntimeError(lib().oracle_last_error().decode())
         return dict(zip(TERMS, T)), G, q, cn
 
+    def refresh_topology(self, xyz):
+        X = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+        return lib().oracle_refresh_topology(self.h, X.ctypes.data) == 1
+
     def redetect_hbxb(self, xyz):
         X = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
         lib().oracle_redetect_hbxb(self.h, X.ctypes.data)
@@ -114,6 +121,33 @@ class Oracle:
                 lib().oracle_destroy(self.h)
         except Exception:
             pass
+
+
+class OracleSequence:
+    """The oracle over a sequence of geometries with the refreshes of curcuma's evaluation, in
+    the order the library's single-point path applies them: the topology when an atom has moved
+    more than 0.5 bohr along an axis since the last topology (a topology with new fragments
+    also re-detects the HB/XB lists at their reference geometry, as the library does), then
+    the HB/XB lists when sqrt(sum d^2)/N exceeds hb_rmsd_bohr since their last detection."""
+
+    def __init__(self, Z, X, charge=0, solvent=None, hb_rmsd_bohr=0.3):
+        self.oracle = Oracle(Z, X, charge, solvent)
+        self.topo = np.asarray(X, dtype=np.float64) / BOHR_A
+        self.hb = self.topo.copy()
+        self.thr = hb_rmsd_bohr
+
+    def engrad(self, X, nthreads=0):
+        xb = np.asarray(X, dtype=np.float64) / BOHR_A
+        if np.abs(xb - self.topo).max() > 0.5:
+            frag0 = self.oracle.topology(9, 1).copy()
+            self.oracle.refresh_topology(X)
+            self.topo = xb
+            if not np.array_equal(frag0, self.oracle.topology(9, 1)):
+                self.oracle.redetect_hbxb(self.hb * BOHR_A)
+        if np.sqrt(((xb - self.hb) ** 2).sum()) / len(xb) > self.thr:
+            self.oracle.redetect_hbxb(X)
+            self.hb = xb
+        return self.oracle.engrad(X, nthreads)
 
 
 def golden(name):

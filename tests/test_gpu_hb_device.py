@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 
 from curcuma_b200 import GFNFF, workloads
-from tests.oracle_api import golden
+from tests.oracle_api import Oracle, golden
 
 pytestmark = pytest.mark.gpu
 
@@ -47,10 +47,12 @@ def test_device_hb_lists_equal_host(name, monkeypatch):
     assert not dev.hasError() and not host.hasError()
     assert abs(ed - eh) < 1e-13 * max(1.0, abs(eh))
     assert np.abs(dev.getGradient() - host.getGradient()).max() < 1e-11
-    # a refresh at a displaced geometry (sqrt(sum d^2)/N > 0.3 bohr)
+    # a refresh at a displaced geometry (sqrt(sum d^2)/N > 0.3 bohr; atoms moved beyond 0.5 bohr
+    # along an axis, so the topology is recomputed first: new fragments for most systems)
     X2 = X + np.random.default_rng(5).normal(scale=0.4, size=X.shape)
     assert dev.updateGeometry(X2) and host.updateGeometry(X2)
     ed, eh = dev.calculateEnergy(True), host.calculateEnergy(True)
+    assert not dev.hasError() and not host.hasError(), (dev.getErrorMessage(), host.getErrorMessage())
     Td, Th = dev.topology(6, 4), host.topology(6, 4)
     assert Td.shape == Th.shape and (Td == Th).all()
     # a strained geometry (28 Eh): the iterative EEQ solve amplifies the order of the FP64
@@ -120,3 +122,32 @@ def test_cn_list_device_equals_host(monkeypatch):
             assert not g.hasError(), g.getErrorMessage()
             cn.append(g.getCoordinationNumbers())
         assert (cn[0] == cn[1]).all()
+
+
+def test_topology_refresh_matches_oracle():
+    """curcuma recomputes the topology when an atom has moved more than 0.5 bohr along an
+    axis since the last one.  CH4 with one H pulled 1.5 A out: the C-H bond is gone from the
+    new topology (two fragments, each neutral), the EEQ follows it, the force-field terms stay
+    those of the set-up.  A small step afterwards (< 0.5 bohr) keeps the new topology."""
+    Z = np.array([6, 1, 1, 1, 1])
+    t = 1.09 / np.sqrt(3.0)
+    X0 = np.array([[0, 0, 0], [t, t, t], [t, -t, -t], [-t, t, -t], [-t, -t, t]])
+    X1 = X0.copy()
+    X1[1] *= (1.09 + 1.5) / 1.09
+    X2 = X1 + np.random.default_rng(2).normal(scale=0.02, size=X1.shape)
+    g = GFNFF()
+    assert g.setMolecule(Z, X0)
+    o = Oracle(Z, X0)
+    e0 = g.calculateEnergy(True)
+    assert abs(e0 - o.engrad(X0)[0]["total"]) < 1e-9
+    for X, changes in ((X1, True), (X2, False)):
+        assert o.refresh_topology(X) == changes
+        o.redetect_hbxb(X)
+        g.updateGeometry(X)
+        e = g.calculateEnergy(True)
+        assert not g.hasError(), g.getErrorMessage()
+        T, G, q, cn = o.engrad(X)
+        assert abs(e - T["total"]) < 1e-9, (e, T["total"])
+        assert np.abs(g.getGradient() - G).max() < 1e-8
+        assert np.abs(g.getCharges() - q).max() < 1e-10
+    assert abs(g.getCharges()[1]) < 1e-10   # the H alone is a neutral fragment

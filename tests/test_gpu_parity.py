@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 from curcuma_b200 import GFNFF, workloads
-from tests.oracle_api import Oracle, golden, golden_names
+from tests.oracle_api import Oracle, OracleSequence, golden, golden_names
 
 E_TOL = 1e-8
 G_TOL = 1e-7
@@ -84,11 +84,15 @@ def test_hb_refresh_matches_oracle():
     gpu = GFNFF()
     assert gpu.setMolecule(Z, X)
     X2 = X.copy()
-    # translate 20 of the 30 waters by 3 bohr per axis: sqrt(sum d^2)/N = 0.45 > 0.3 bohr
+    # translate 20 of the 30 waters by 3 bohr per axis: sqrt(sum d^2)/N = 0.45 > 0.3 bohr; the
+    # atoms moved more than 0.5 bohr along an axis, so the topology is recomputed first (as in
+    # curcuma's evaluation), then the HB/XB lists
     X2[: 3 * 20] += 3.0 * 0.529177210903
     gpu.updateGeometry(X2)
     e = gpu.calculateEnergy(True)
+    assert not gpu.hasError(), gpu.getErrorMessage()
     o = Oracle(Z, X)
+    o.refresh_topology(X2)
     o.redetect_hbxb(X2)
     T, G, q, cn = o.engrad(X2)
     assert abs(e - T["total"]) < E_TOL
@@ -222,7 +226,7 @@ def test_cn_neighbour_list_refresh():
     Z, X = workloads.water_cluster(64, 9)
     rng = np.random.default_rng(3)
     geoms = [X + rng.normal(scale=s, size=X.shape) for s in (0.02, 0.15, 0.15, 0.02)]
-    o = Oracle(Z, X)
+    o = OracleSequence(Z, X)   # the larger steps also refresh the topology and the HB lists
     g = GFNFF()
     assert g.setMolecule(Z, X)
     for Xk in geoms:
