@@ -2,23 +2,23 @@
 // Comput. 2021, 17, 4250), the per-geometry part of curcuma's ff_methods/alpb_solvation.cpp
 // (update, getEnergy, addGradient) for a single molecule:
 //   k_alpb_born    Born radii from the descreening sum psi over the pairs within 35 A (one
-//                  warp per atom, the partners in ascending order; born.f90 compute_psi /
-//                  compute_bornr) and d brad / d psi;
+//                  warp per atom, the partners in ascending order;
+//                  alpb_solvation.cpp:502-694) and d brad / d psi;
 //   k_alpb_sasa    the smoothed solvent-accessible surface of every atom on the 230-point
 //                  Lebedev grid (one block per atom: the neighbours within the surface cut
 //                  gathered in ascending order into shared memory, the grid points over the
-//                  threads; sasa.f90 compute_numsa), the HB weights and the diagonal of the Born
+//                  threads; alpb_solvation.cpp:696-805), the HB weights and the diagonal of the Born
 //                  matrix; with GRAD, the surface gradient weighted per atom;
 //   k_alpb_shape   the shape descriptor adet of the vdW spheres (one block);
 //   the Born matrix enters the EEQ matrix and right-hand side through View::brad/bdiag
-//   (k_eeq_M_tiles, eeq_a: A += B, gfnff_engrad.F90:1346-1350; the shape constant cancels
+//   (k_eeq_M_tiles, eeq_a: A += B, eeq_solver.cpp:3781-3784; the shape constant cancels
 //   in the reduced basis);
 //   k_alpb_energy  after the solve: the Born pair energy and gradient at fixed charges and
-//                  dE/d brad (P16 kernel, kernel.f90 addGradientP16), self, HB and surface
+//                  dE/d brad (P16 kernel, alpb_solvation.cpp:1139-1203), self, HB and surface
 //                  energies (warp per atom, every partner);
 //   k_alpb_chain   dE/d brad through the Born radii: per atom the pairs within 35 A, both
 //                  sides of each pair (no atomics on partners);
-//   k_alpb_shape_grad  the shape term's energy and gradient (gbsa.f90:722-789) and the shift.
+//   k_alpb_shape_grad  the shape term's energy and gradient (alpb_solvation.cpp:940-1003) and the shift.
 // Everything in FP64.  Included inside namespace gfnff by engine.cu, after common.cuh (the
 // model constants of setup/alpb.h are included by engine.cu at file scope).
 #pragma once

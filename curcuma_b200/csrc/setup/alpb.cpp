@@ -88,7 +88,7 @@ static int find_solvent(const std::string& name)
     return -1;
 }
 
-// alpb_solvation.cpp:190-360 (init, loadSolventParameters for GFN-FF, setupRadii)
+// alpb_solvation.cpp:196-396 (init, loadSolventParameters for GFN-FF, setupRadii)
 bool alpb_setup(AlpbModel& m, const std::vector<int>& Z, const std::string& solvent)
 {
     m = AlpbModel();
@@ -119,7 +119,7 @@ bool alpb_setup(AlpbModel& m, const std::vector<int>& Z, const std::string& solv
         m.vdwsa[i] = m.vdwr[i] + m.probe;
         m.trj2_lo[i] = (m.vdwsa[i] - kWSmooth) * (m.vdwsa[i] - kWSmooth);
         m.trj2_hi[i] = (m.vdwsa[i] + kWSmooth) * (m.vdwsa[i] + kWSmooth);
-        // radial weight of the smoothed surface (gbsa.f90:393-399)
+        // radial weight of the smoothed surface (alpb_solvation.cpp:378-386)
         double r = m.vdwsa[i] + kWSmooth;
         const double w1 = (0.25 / kWSmooth + 3.0 * kAh3 * (0.2 * r * r - 0.5 * r * m.vdwsa[i] +
                                                            m.vdwsa[i] * m.vdwsa[i] / 3.0)) * r * r * r;

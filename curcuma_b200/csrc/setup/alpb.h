@@ -2,7 +2,7 @@
 // Poisson-Boltzmann; Ehlert, Stahn, Spicher, Grimme, J. Chem. Theory Comput. 2021, 17, 4250):
 // solvent parameters, per-atom radii and surface data, the model constants and the
 // 230-point Lebedev-Laikov sphere grid.  Restates curcuma's ALPBSolvation::init,
-// loadSolventParameters and setupRadii (ff_methods/alpb_solvation.cpp:190-360) and the
+// loadSolventParameters and setupRadii (ff_methods/alpb_solvation.cpp:196-396) and the
 // constants of ff_methods/alpb_parameters.h:18-56.  The per-geometry part (Born radii,
 // surface areas, Born matrix, energy and gradient) is evaluated by the device kernels and,
 // independently, by the CPU oracle.

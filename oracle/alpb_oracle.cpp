@@ -11,7 +11,7 @@ namespace {
 using namespace alpb;
 
 // contributions of one pair (i > j) to psi_i and psi_j and their derivatives along d = r_i - r_j
-// (alpb_solvation.cpp:470-650, born.f90 compute_psi): per side the non-overlapping or the
+// (alpb_solvation.cpp:502-649): per side the non-overlapping or the
 // overlapping form, by whether r is below rvdw_self + rho_other
 struct PsiPair {
     double gi = 0.0, gj = 0.0;    // psi_i, psi_j contributions
@@ -67,7 +67,7 @@ static double d2(const double* x, int i, int j, double d[3])
     return d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
 }
 
-// surface area of atom i (sasa.f90 compute_numsa / compute_w_sp); with weight != 0 the
+// surface area of atom i (alpb_solvation.cpp:696-805); with weight != 0 the
 // derivative w * d sasa_i / d r is added into grad
 static double sasa_atom(const AlpbModel& A, const double* x, int n, int i, double weight, double* grad)
 {
@@ -121,7 +121,7 @@ static double sasa_atom(const AlpbModel& A, const double* x, int n, int i, doubl
     return s;
 }
 
-// inertia-like shape tensor of the vdW spheres (gbsa.f90:677-719): adet, and for the
+// inertia-like shape tensor of the vdW spheres (alpb_solvation.cpp:908-938): adet, and for the
 // gradient the tensor, the centre and the total r^3
 struct Shape {
     double I[3][3] = {{0}}, c[3] = {0, 0, 0}, tot3 = 0.0, adet = 0.0;
@@ -157,7 +157,7 @@ static Shape shape(const AlpbModel& A, const double* x, int n)
 void alpb_prepare(const AlpbModel& A, const double* x, int n, AlpbGeom& g, double* Aeeq)
 {
     g.psi.assign(n, 0.0);
-    // ---- Born radii (born.f90 compute_psi, compute_bornr)
+    // ---- Born radii (alpb_solvation.cpp:502-694)
     const double lr2 = kLrCut * kLrCut;
     for (int i = 0; i < n; ++i)
         for (int j = 0; j < i; ++j) {
@@ -182,7 +182,7 @@ void alpb_prepare(const AlpbModel& A, const double* x, int n, AlpbGeom& g, doubl
         dp = s2 * v1 * arg2 / (dp * dp);
         g.dpsi[i] = A.born_scale * dp;
     }
-    // ---- surface areas, HB weights (gbsa.f90:1003-1042), shape
+    // ---- surface areas, HB weights (alpb_solvation.cpp:873-881), shape
     g.sasa.resize(n);
     g.hbw.assign(n, 0.0);
     g.dhbdw.assign(n, 0.0);
@@ -197,7 +197,7 @@ void alpb_prepare(const AlpbModel& A, const double* x, int n, AlpbGeom& g, doubl
         }
     }
     g.adet = shape(A, x, n).adet;
-    // ---- Born matrix into the EEQ matrix (gfnff_engrad.F90:1346-1350: A += B)
+    // ---- Born matrix into the EEQ matrix (eeq_solver.cpp:3781-3784: A += B)
     if (!Aeeq) return;
     const double corr = A.keps * A.alpbet / g.adet;
     for (int i = 0; i < n; ++i) {
@@ -217,7 +217,7 @@ void alpb_prepare(const AlpbModel& A, const double* x, int n, AlpbGeom& g, doubl
 
 double alpb_energy_gradient(const AlpbModel& A, const double* x, int n, const AlpbGeom& g, const double* q, double* grad)
 {
-    // ---- Born energy and its direct and Born-radius gradient (kernel.f90 addGradientP16)
+    // ---- Born energy and its direct and Born-radius gradient (alpb_solvation.cpp:1139-1203)
     std::vector<double> dEdbr(n, 0.0);
     double egb = 0.0, qt = 0.0;
     for (int i = 0; i < n; ++i) {
@@ -271,7 +271,7 @@ double alpb_energy_gradient(const AlpbModel& A, const double* x, int n, const Al
         const double w = A.gamsasa[i] + g.dhbdw[i] * q[i] * q[i];
         if (w != 0.0) sasa_atom(A, x, n, i, w, grad);
     }
-    // ---- ALPB shape term (gbsa.f90:722-789)
+    // ---- ALPB shape term (alpb_solvation.cpp:940-1003)
     double eshape = 0.0;
     if (A.alpbet > 0.0) {
         const Shape s = shape(A, x, n);
