@@ -2157,10 +2157,12 @@ void Engine::launch_body()
             if (sv == Impl::SOLVE_PCG && P.pcg_res)
                 ;   // the resident PCG builds its tiles itself
             else if (sv == Impl::SOLVE_PCG && P.pcg_f32)
-                k_eeq_M_tiles<float><<<nb, 256, 0, s>>>(V, P.red2atom.p, P.anchor.p, P.Mf.p, P.lda, 0);
+                (P.alpb_on ? k_eeq_M_tiles<float, true> : k_eeq_M_tiles<float, false>)<<<nb, 256, 0, s>>>(
+                    V, P.red2atom.p, P.anchor.p, P.Mf.p, P.lda, 0, nullptr);
             else
-                k_eeq_M_tiles<double><<<nb, 256, 0, s>>>(V, P.red2atom.p, P.anchor.p, P.M.p, P.lda, full ? 1 : 0,
-                                                         sv == Impl::SOLVE_PCG && P.pcg_ir ? P.Mf.p : nullptr);
+                (P.alpb_on ? k_eeq_M_tiles<double, true> : k_eeq_M_tiles<double, false>)<<<nb, 256, 0, s>>>(
+                    V, P.red2atom.p, P.anchor.p, P.M.p, P.lda, full ? 1 : 0,
+                    sv == Impl::SOLVE_PCG && P.pcg_ir ? P.Mf.p : nullptr);
         }
         P.mark(4);
         if (P.nred > 0)

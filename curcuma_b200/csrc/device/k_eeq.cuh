@@ -59,13 +59,15 @@ __global__ void k_eeq_M(View V, const int* __restrict__ red2atom, const int* __r
 // entry is computed once and written to (r, c) and, when full, to (c, r) through a
 // shared-memory transpose so that both writes are coalesced.
 constexpr int kMT = 32;
-template <class TM>   // storage type of M: double, or float for the FP32-stored PCG matrix
+// BORN: the ALPB Born matrix enters (V.brad, V.bdiag); the gas-phase instantiation has none of
+// its code
+template <class TM, bool BORN = false>   // storage type of M: double, or float for the FP32-stored PCG matrix
 __global__ void __launch_bounds__(256) k_eeq_M_tiles(View V, const int* __restrict__ red2atom,
                                                     const int* __restrict__ anchor, TM* M, int lda, int full,
                                                     float* M32 = nullptr)   // optional FP32 copy (k_pcg_ir)
 {
     __shared__ double px[4][kMT], py[4][kMT], pz[4][kMT], pa[4][kMT];   // rows k, rows ak, cols l, cols al
-    __shared__ double pbr[4][kMT];                                       // Born radii (solvation)
+    __shared__ double pbr[4][BORN ? kMT : 1];                            // Born radii (solvation)
     __shared__ int pid[4][kMT];
     __shared__ double T[kMT][kMT + 1];
     // triangular block index -> (tr, tc)
@@ -87,19 +89,28 @@ __global__ void __launch_bounds__(256) k_eeq_M_tiles(View V, const int* __restri
         if (a >= 0) {
             const double4 p = V.pos[a];
             px[w][t] = p.x; py[w][t] = p.y; pz[w][t] = p.z; pa[w][t] = V.alpeeq[a];
-            pbr[w][t] = V.brad ? V.brad[a] : 0.0;
+            if constexpr (BORN) pbr[w][t] = V.brad[a];
         }
     }
     __syncthreads();
     auto el = [&](int wa, int ia, int wb, int ib) {
-        if (pid[wa][ia] == pid[wb][ib]) return V.adiag[pid[wa][ia]] + (V.brad ? V.bdiag[pid[wa][ia]] : 0.0);
+        if (pid[wa][ia] == pid[wb][ib]) {
+            if constexpr (BORN) return V.adiag[pid[wa][ia]] + V.bdiag[pid[wa][ia]];
+            else return V.adiag[pid[wa][ia]];
+        }
         const double dx = px[wa][ia] - px[wb][ib], dy = py[wa][ia] - py[wb][ib], dz = pz[wa][ia] - pz[wb][ib];
         const double d2 = dx * dx + dy * dy + dz * dz;
         const double s = pa[wa][ia] + pa[wb][ib];
-        const double born = V.brad ? born_p16(V.keps, sqrt(d2), pbr[wa][ia], pbr[wb][ib]) : 0.0;
-        if (d2 >= 36.0 * s) return rsqrt(d2) + born;
-        const double r = sqrt(d2);
-        return erf(r / sqrt(s)) / r + born;
+        if constexpr (!BORN) {
+            if (d2 >= 36.0 * s) return rsqrt(d2);
+            const double r = sqrt(d2);
+            return erf(r / sqrt(s)) / r;
+        } else {
+            const double born = born_p16(V.keps, sqrt(d2), pbr[wa][ia], pbr[wb][ib]);
+            if (d2 >= 36.0 * s) return rsqrt(d2) + born;
+            const double r = sqrt(d2);
+            return erf(r / sqrt(s)) / r + born;
+        }
     };
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;   // 32 x 8
     for (int cc = ty; cc < kMT; cc += 8) {
