@@ -522,19 +522,25 @@ __global__ void __launch_bounds__(T, MINB) k_pairs_sym(View V, const int2* __res
             }
         }
     }
-    // the j-side sums go to per-warp accumulators in shared memory: at step k lane t of the
-    // block takes partner (t + k) mod T, so the lanes of a warp always hold distinct partners
-    // and add without shuffles or conflicts
+    // j-side sums.  Coulomb-only launches (ROT): per-warp accumulators in shared memory, at
+    // step k lane t of the block takes partner (t + k) mod T, so the lanes of a warp always
+    // hold distinct partners and add without shuffles or conflicts (1000 waters: 104 -> 53 us).
+    // With D4 terms the lanes take the same partner and the j-side sums are reduced over the
+    // warp: rotated partners made the per-partner reference loops diverge (D4 half 61 ->
+    // 122 us).
+    constexpr bool ROT = PART == kPairCoul;
+    if constexpr (ROT) {
 #pragma unroll
-    for (int k = 0; k < NA; ++k)
-        for (int u = lane; u < T; u += 32) jacc[warp][k][u] = 0.0;
+        for (int k = 0; k < NA; ++k)
+            for (int u = lane; u < T; u += 32) jacc[warp][k][u] = 0.0;
+    }
     __syncthreads();
     const double tsp = 2.0 / 1.772453850905516;
     double ec = 0.0, ed = 0.0, gx = 0.0, gy = 0.0, gz = 0.0, dcn = 0.0, cfar = 0.0;
     const int cnt = min(T, V.n - j0);
-    for (int k = 0; k < T; ++k) {
-        const int jj = (threadIdx.x + k) & (T - 1);
-        if (jj >= cnt) continue;
+    for (int k = 0; k < (ROT ? T : cnt); ++k) {
+        const int jj = ROT ? (threadIdx.x + k) & (T - 1) : k;
+        if (ROT && jj >= cnt) continue;
         const int j = j0 + jj;
         double fx = 0.0, fy = 0.0, fz = 0.0, dcj = 0.0, cfj = 0.0;
         bool valid = act && j > i && j >= rg.x && j < rg.y;
@@ -593,12 +599,29 @@ __global__ void __launch_bounds__(T, MINB) k_pairs_sym(View V, const int2* __res
             gx += f * dx; gy += f * dy; gz += f * dz;
             fx = -f * dx; fy = -f * dy; fz = -f * dz;
         }
-        if (hit) {
-            jacc[warp][0][jj] += fx;
-            jacc[warp][1][jj] += fy;
-            jacc[warp][2][jj] += fz;
-            if (D4 && want_dc) jacc[warp][3][jj] += dcj;
-            if (want_far) jacc[warp][4][jj] += cfj;
+        if constexpr (ROT) {
+            if (hit) {
+                jacc[warp][0][jj] += fx;
+                jacc[warp][1][jj] += fy;
+                jacc[warp][2][jj] += fz;
+                if (want_far) jacc[warp][4][jj] += cfj;
+            }
+        } else {
+            if (__any_sync(0xffffffffu, hit)) {
+                for (int o = 16; o > 0; o >>= 1) {
+                    fx += __shfl_xor_sync(0xffffffffu, fx, o);
+                    fy += __shfl_xor_sync(0xffffffffu, fy, o);
+                    fz += __shfl_xor_sync(0xffffffffu, fz, o);
+                }
+                if (D4 && want_dc)
+                    for (int o = 16; o > 0; o >>= 1) dcj += __shfl_xor_sync(0xffffffffu, dcj, o);
+                if (want_far)
+                    for (int o = 16; o > 0; o >>= 1) cfj += __shfl_xor_sync(0xffffffffu, cfj, o);
+            }
+            if (lane == 0) {
+                jacc[warp][0][jj] = fx; jacc[warp][1][jj] = fy; jacc[warp][2][jj] = fz;
+                jacc[warp][3][jj] = dcj; jacc[warp][4][jj] = cfj;
+            }
         }
     }
     __syncthreads();
