@@ -23,7 +23,7 @@ CXX = "/usr/bin/g++" if Path("/usr/bin/g++").exists() else "g++"
 CU_SOURCES = [CSRC / "device" / "engine.cu", CSRC / "device" / "peaks.cu", CSRC / "device" / "eeq_noalloc.cu",
               CSRC / "device" / "md.cu"]
 CPP_SOURCES = [CSRC / "setup" / "topology.cpp", CSRC / "setup" / "parameters.cpp",
-               CSRC / "setup" / "linalg.cpp", CSRC / "setup" / "param_file.cpp", CSRC / "setup" / "alpb.cpp",
+               CSRC / "setup" / "linalg.cpp", CSRC / "setup" / "param_file.cpp", CSRC / "setup" / "alpb.cpp", CSRC / "setup" / "topo_cache.cpp",
                CSRC / "capi.cpp"]
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

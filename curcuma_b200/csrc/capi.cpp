@@ -16,6 +16,7 @@
 #include "device/engine.h"
 #include "device/md.h"
 #include "setup/model.h"
+#include "setup/topo_cache.h"
 
 using namespace gfnff;
 
@@ -33,6 +34,7 @@ struct gfnff_handle {
     std::vector<double> topo_ref;  // bohr, geometry of the last topology
     std::string solvent;            // ALPB solvent ("" gas phase)
     AlpbModel solv;
+    std::string topo_cache;         // <geometry>.topo.json ("" no topology cache)
     double* pin_xyz = nullptr;      // pinned staging for host coordinates
     double* pin_grad = nullptr;
     double* pin_out = nullptr;      // terms + status + msd
@@ -103,6 +105,48 @@ gfnff_status gfnff_set_solvent(gfnff_handle* h, const char* solvent)
     return GFNFF_OK;
 }
 
+gfnff_status gfnff_set_geometry_file(gfnff_handle* h, const char* geometry_file, int cache_topology)
+{
+    if (!h) return fail(nullptr, GFNFF_INVALID_ARG, "handle is NULL");
+    const std::string g = geometry_file ? geometry_file : "";
+    h->topo_cache = (cache_topology && !g.empty()) ? topology_cache_path(g) : std::string();
+    return GFNFF_OK;
+}
+
+int gfnff_topology_cache_hit(gfnff_handle* h)
+{
+    if (!h || !h->ready || h->nmol) return -1;
+    return h->model.topo_cache_hit ? 1 : 0;
+}
+
+// curcuma writes the cache after every set-up and ignores a file it cannot open
+// (gfnff_method.cpp:2941-2985)
+static void write_cache_quietly(const std::string& path, const Model& m)
+{
+    if (path.empty()) return;
+    try {
+        write_topology_cache(path, m);
+    } catch (const std::exception&) {
+    }
+}
+
+gfnff_status gfnff_write_topology_cache(int n, const int* Z, const double* xyz, int charge, const char* geometry_file,
+                                        int* cache_hit)
+{
+    if (n <= 0 || !Z || !xyz || !geometry_file || !*geometry_file)
+        return fail(nullptr, GFNFF_INVALID_ARG, "invalid molecule or geometry file");
+    try {
+        const std::string path = topology_cache_path(geometry_file);
+        Model m = build_model(n, Z, xyz, charge, SetupOptions(), BuildLists(), path.c_str());
+        if (cache_hit) *cache_hit = m.topo_cache_hit ? 1 : 0;
+        if (!write_topology_cache(path, m))
+            return fail(nullptr, GFNFF_SETUP_FAILED, "Phase-1 charges failed the cache's write check");
+    } catch (const std::exception& e) {
+        return fail(nullptr, GFNFF_SETUP_FAILED, e.what());
+    }
+    return GFNFF_OK;
+}
+
 gfnff_status gfnff_setup(gfnff_handle* h, int n, const int* Z, const double* xyz, int charge)
 {
     if (!h) return fail(nullptr, GFNFF_INVALID_ARG, "handle is NULL");
@@ -117,12 +161,14 @@ gfnff_status gfnff_setup(gfnff_handle* h, int n, const int* Z, const double* xyz
         L.host_disp = false;
         const char* hd = std::getenv("GFNFF_HB_DEVICE");
         L.host_hb = hd ? !std::strcmp(hd, "0") : n < 512;
-        h->model = build_model(n, Z, xyz, charge, so, L);
+        h->model = build_model(n, Z, xyz, charge, so, L, h->topo_cache.empty() ? nullptr : h->topo_cache.c_str());
         if (!alpb_setup(h->solv, h->model.Z, h->solvent)) return fail(h, GFNFF_INVALID_ARG, "unknown solvent");
     } catch (const std::exception& e) {
         return fail(h, GFNFF_SETUP_FAILED, e.what());
     }
-    return finish_setup(h, n);
+    const gfnff_status st = finish_setup(h, n);
+    if (st == GFNFF_OK) write_cache_quietly(h->topo_cache, h->model);
+    return st;
 }
 
 // upload of h->model and the per-handle host staging (gfnff_setup, gfnff_setup_from_parameters)
@@ -305,7 +351,7 @@ static void topology_refresh(gfnff_handle* h, const double* xb)
     const int nfrag0 = h->model.nfrag;
     const std::vector<int> frag0 = h->model.frag;
     const std::vector<double> qfrag0 = h->model.qfrag;
-    if (refresh_topology(h->model, xb)) {
+    if (refresh_topology(h->model, xb, h->topo_cache.empty() ? nullptr : h->topo_cache.c_str())) {
         if (h->model.nfrag == nfrag0 && h->model.frag == frag0 && h->model.qfrag == qfrag0) {
             h->eng->update_eeq_parameters(h->model);
         } else {

@@ -105,6 +105,14 @@ struct Model {
     // lists left to the device (a run-time choice of the set-up; not in the parameter file):
     // hbonds/bond_hb empty and the bonds' nr_hb/hb_h unset, or disp empty
     bool hb_on_device = false, disp_on_device = false;
+
+    // Phase-1 by-products kept for the topology cache (<geometry>.topo.json); not in the
+    // parameter file: electronegativity and hardness corrections, amide-H flags, the rings
+    // (sorted atom sets), and whether the last topology came from a cache hit
+    std::vector<double> dxi, dgam;
+    std::vector<char> amide_h;
+    std::vector<std::vector<int>> rings;
+    bool topo_cache_hit = false;
 };
 
 // Per-atom inputs of the hydrogen-bond detection at one geometry (gfnff_method.cpp:7936-8100):
@@ -126,10 +134,13 @@ struct BuildLists {
 };
 
 // Runs the complete GFN-FF setup for one molecule (curcuma GFNFF::InitialiseMolecule,
-// gfnff_method.cpp:733-848).  xyz_ang is row-major N x 3 in Angstrom.
+// gfnff_method.cpp:733-848).  xyz_ang is row-major N x 3 in Angstrom.  topo_cache, when
+// not null, names a <geometry>.topo.json whose Phase-1 data replace Phase 1 on a
+// fingerprint match (Model::topo_cache_hit); the file is only read here.
 // Throws std::runtime_error on invalid input.
 Model build_model(int n, const int* Z, const double* xyz_ang, int charge,
-                  const SetupOptions& opt = SetupOptions(), const BuildLists& lists = BuildLists());
+                  const SetupOptions& opt = SetupOptions(), const BuildLists& lists = BuildLists(),
+                  const char* topo_cache = nullptr);
 
 // HB/XB lists re-detected at a new geometry with the setup (Phase-1) charges
 // (gfnff_method.cpp:1597-1690); also rebuilds the bond <-> HB cross reference.
@@ -142,8 +153,9 @@ void redetect_hbxb(Model& m, const double* xyz_bohr);
 // pi systems, Phase-1 charges) and the EEQ parameters derived from it are recomputed at
 // xyz_bohr; the force-field term lists and their parameters stay those of the set-up, as in
 // curcuma.  Returns true when anything the evaluation uses changed (the model is updated),
-// false when the new topology is the old one (the model is left as it is).
-bool refresh_topology(Model& m, const double* xyz_bohr);
+// false when the new topology is the old one (the model is left as it is).  topo_cache as
+// in build_model: curcuma's refresh consults the same cache.
+bool refresh_topology(Model& m, const double* xyz_bohr, const char* topo_cache = nullptr);
 
 // HBAtoms of the model at xyz_bohr (N x 3, caller order)
 HBAtoms hb_atom_data(Model& m, const double* xyz_bohr);

@@ -1266,7 +1266,7 @@ void d4_weights(const Model& m, int i, double cn, double* w, double* dw)
 }
 
 Model build_model(int n, const int* Z, const double* xyz_ang, int charge, const SetupOptions& opt,
-                  const BuildLists& lists)
+                  const BuildLists& lists, const char* topo_cache)
 {
     if (n <= 0) throw std::runtime_error("no atoms");
     for (int i = 0; i < n; ++i)
@@ -1301,12 +1301,13 @@ Model build_model(int n, const int* Z, const double* xyz_ang, int charge, const 
     for (int i = 0; i < n; ++i)
         for (int j = i + 1; j < n && n <= 4000; ++j)
             if (detail::dist2_bohr(c, i, j) < 1e-20) throw std::runtime_error("coincident atoms");
+    c.topo_cache = topo_cache;
     detail::compute_topology(c);
     detail::generate_parameters(c);
     return m;
 }
 
-bool refresh_topology(Model& m, const double* xyz_bohr)
+bool refresh_topology(Model& m, const double* xyz_bohr, const char* topo_cache)
 {
     const int n = m.n;
     Model t;
@@ -1324,6 +1325,7 @@ bool refresh_topology(Model& m, const double* xyz_bohr)
     t.rcov_cn = m.rcov_cn;
     t.rcov_d3 = m.rcov_d3;
     t.rvdw = m.rvdw;
+    c.topo_cache = topo_cache;
     detail::compute_topology(c);
     const bool same = t.topo_bonds == m.topo_bonds && t.adj == m.adj && t.hyb == m.hyb && t.pi_frag == m.pi_frag &&
                       t.frag == m.frag && t.nfrag == m.nfrag && t.qfrag == m.qfrag && t.qa == m.qa &&
@@ -1332,6 +1334,7 @@ bool refresh_topology(Model& m, const double* xyz_bohr)
     m.topo_bonds = t.topo_bonds; m.adj = t.adj; m.hyb = t.hyb; m.pi_frag = t.pi_frag;
     m.frag = t.frag; m.nfrag = t.nfrag; m.qfrag = t.qfrag; m.qa = t.qa;
     m.chi_base = t.chi_base; m.gam = t.gam; m.alpeeq = t.alpeeq; m.cnf = t.cnf;
+    m.dxi = t.dxi; m.dgam = t.dgam; m.amide_h = t.amide_h; m.topo_cache_hit = t.topo_cache_hit;
     return true;
 }
 

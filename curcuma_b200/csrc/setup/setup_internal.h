@@ -34,6 +34,7 @@ struct Ctx {
     std::vector<std::vector<int>> atom_rings;
     std::vector<std::vector<std::pair<int, int>>> tdist;      // (atom, bond count <= 5)
     std::unordered_map<uint64_t, double> pibo;                // pi bond orders of bonds
+    const char* topo_cache = nullptr;                         // <geometry>.topo.json to consult
     explicit Ctx(Model& mm) : m(mm), n(mm.n), Z(mm.Z.data()) {}
     bool bonded(int i, int j) const { return bondset.count(key(i, j)) != 0; }
 };

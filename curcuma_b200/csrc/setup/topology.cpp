@@ -3,6 +3,7 @@
 // Hueckel pi bond orders.  Each function cites the curcuma routine it restates
 // (paths relative to src/core/energy_calculators/).
 #include "setup_internal.h"
+#include "topo_cache.h"
 
 #include <algorithm>
 #include <cmath>
@@ -942,52 +943,72 @@ void compute_topology(Ctx& c)
     detect_pi_systems(c);
     find_rings(c);
 
-    // Phase-1 charges (with the charged two-fragment placement rule, :8990-9035)
-    std::vector<double> dxi = eeq_dxi(c);
-    bool ok = true;
-    const double qc = (double)c.m.charge;
-    if (c.m.nfrag == 2 && c.m.charge != 0) {
-        std::vector<double> qA = {qc, 0.0}, qB = {0.0, qc};
-        bool oka, okb;
-        auto qa = phase1_charges(c, qA, dxi, &oka);
-        auto qb = phase1_charges(c, qB, dxi, &okb);
-        double ea = oka ? eeq_energy_geometric(c, qa, c.m.cn_setup) : 1e300;
-        double eb = okb ? eeq_energy_geometric(c, qb, c.m.cn_setup) : 1e300;
-        if (ea <= eb) { c.m.qfrag = qA; c.m.qa = qa; ok = oka; }
-        else { c.m.qfrag = qB; c.m.qa = qb; ok = okb; }
-    } else {
-        if (c.m.nfrag > 2 && c.m.charge != 0) {
-            c.m.qfrag.assign(c.m.nfrag, 0.0);
-            c.m.qfrag[0] = qc;
-        }
-        c.m.qa = phase1_charges(c, c.m.qfrag, dxi, &ok);
-    }
-    if (!ok) throw std::runtime_error("Phase-1 EEQ solve failed");
+    c.m.rings = c.rings;
 
-    // alpeeq (gfnff_method.cpp:11182-11276)
-    c.m.alpeeq.resize(n);
-    for (int i = 0; i < n; ++i) {
-        const int z = c.Z[i];
-        const double ab = alpha_eeq[z - 1];
-        double ff = 0.0;
-        if (z == 6) ff = 0.09;
-        else if (z == 7) ff = -0.21;
-        else {
-            const int g = periodic_group[z - 1];
-            if (g == 6) ff = -0.03;
-            else if (g == 7) ff = 0.50;
-            else if (metal_type[z - 1] > 0) {
-                if (metal_type[z - 1] == 2) ff = -0.1;
-                else if (metal_type[z - 1] == 1) ff = 0.3;
+    // Topology cache (gfnff_method.cpp:8973-9040): on a fingerprint match the Phase-1
+    // results (charges, fragment charges, dxi, dgam, alpeeq, amide-H flags) come from the
+    // file and Phase 1, 1A, 1B and 1C are skipped.
+    TopoCache tc;
+    bool hit = c.topo_cache && read_topology_cache(c.topo_cache, topology_fingerprint(c.m.Z, c.m.topo_bonds), n, tc);
+    if (hit && tc.has_qfrag && (int)tc.qfrag.size() != c.m.nfrag) hit = false;
+    c.m.topo_cache_hit = hit;
+    std::vector<double> dxi, dgam;
+    std::vector<char> ah;
+    if (hit) {
+        dxi = tc.dxi;
+        c.m.qa = tc.qa;
+        if (tc.has_qfrag) c.m.qfrag = tc.qfrag;
+        c.m.alpeeq = tc.alpeeq;
+        dgam = tc.dgam;
+        ah = tc.has_amide_h ? tc.amide_h : std::vector<char>(n, 0);
+    } else {
+        // Phase-1 charges (with the charged two-fragment placement rule, :8990-9035)
+        dxi = eeq_dxi(c);
+        bool ok = true;
+        const double qc = (double)c.m.charge;
+        if (c.m.nfrag == 2 && c.m.charge != 0) {
+            std::vector<double> qA = {qc, 0.0}, qB = {0.0, qc};
+            bool oka, okb;
+            auto qa = phase1_charges(c, qA, dxi, &oka);
+            auto qb = phase1_charges(c, qB, dxi, &okb);
+            double ea = oka ? eeq_energy_geometric(c, qa, c.m.cn_setup) : 1e300;
+            double eb = okb ? eeq_energy_geometric(c, qb, c.m.cn_setup) : 1e300;
+            if (ea <= eb) { c.m.qfrag = qA; c.m.qa = qa; ok = oka; }
+            else { c.m.qfrag = qB; c.m.qa = qb; ok = okb; }
+        } else {
+            if (c.m.nfrag > 2 && c.m.charge != 0) {
+                c.m.qfrag.assign(c.m.nfrag, 0.0);
+                c.m.qfrag[0] = qc;
             }
+            c.m.qa = phase1_charges(c, c.m.qfrag, dxi, &ok);
         }
-        c.m.alpeeq[i] = std::pow(ab + ff * c.m.qa[i], 2);
+        if (!ok) throw std::runtime_error("Phase-1 EEQ solve failed");
+
+        // alpeeq (gfnff_method.cpp:11182-11276)
+        c.m.alpeeq.resize(n);
+        for (int i = 0; i < n; ++i) {
+            const int z = c.Z[i];
+            const double ab = alpha_eeq[z - 1];
+            double ff = 0.0;
+            if (z == 6) ff = 0.09;
+            else if (z == 7) ff = -0.21;
+            else {
+                const int g = periodic_group[z - 1];
+                if (g == 6) ff = -0.03;
+                else if (g == 7) ff = 0.50;
+                else if (metal_type[z - 1] > 0) {
+                    if (metal_type[z - 1] == 2) ff = -0.1;
+                    else if (metal_type[z - 1] == 1) ff = 0.3;
+                }
+            }
+            c.m.alpeeq[i] = std::pow(ab + ff * c.m.qa[i], 2);
+        }
+        // dgam, amide H (eeq_solver.cpp:4389-4425)
+        std::vector<char> pi = eeq_pi_atoms(c, c.m.hyb);
+        std::vector<char> am = eeq_amide_n(c, c.m.hyb, pi);
+        ah = eeq_amide_h(c, c.m.hyb, am);
+        dgam = eeq_dgam(c, c.m.qa, pi, am);
     }
-    // dgam, amide H (eeq_solver.cpp:4389-4425)
-    std::vector<char> pi = eeq_pi_atoms(c, c.m.hyb);
-    std::vector<char> am = eeq_amide_n(c, c.m.hyb, pi);
-    std::vector<char> ah = eeq_amide_h(c, c.m.hyb, am);
-    std::vector<double> dgam = eeq_dgam(c, c.m.qa, pi, am);
     c.m.chi_base.resize(n);
     c.m.gam.resize(n);
     c.m.cnf.resize(n);
@@ -999,6 +1020,9 @@ void compute_topology(Ctx& c)
         c.m.gam[i] = gam_eeq[z - 1] + dgam[i];
         c.m.cnf[i] = cnf_eeq[z - 1];
     }
+    c.m.dxi = dxi;
+    c.m.dgam = dgam;
+    c.m.amide_h = ah;
 
     // pi-system charges (gfnff_method.cpp:9277-9339)
     std::vector<int> pis_charge;

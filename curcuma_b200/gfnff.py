@@ -38,11 +38,14 @@ MIXED = 1
 
 class GFNFF:
     def __init__(self, precision: int = FP64, device: int = 0, hbond: bool = True,
-                 hb_rmsd_bohr: float = 0.3, exact_gradient: bool = False, solvent: str = "none"):
+                 hb_rmsd_bohr: float = 0.3, exact_gradient: bool = False, solvent: str = "none",
+                 geometry_file=None, cache_topology: bool = True):
         self._lib = _lib.load()
         self._params = {"precision": "mixed" if precision == MIXED else "fp64", "gpu_device": device,
                         "hbond": bool(hbond), "hb_rmsd_bohr": hb_rmsd_bohr,
-                        "exact_gradient": bool(exact_gradient), "solvent": solvent or "none", "threads": 1}
+                        "exact_gradient": bool(exact_gradient), "solvent": solvent or "none", "threads": 1,
+                        "geometry_file": str(geometry_file) if geometry_file else "",
+                        "cache_topology": bool(cache_topology)}
         self._h = None
         self._create()
 
@@ -67,6 +70,7 @@ class GFNFF:
             self._lib.gfnff_destroy(h)
             self._h = None
             raise ValueError(f"gfnff_set_solvent: {msg}")
+        self._lib.gfnff_set_geometry_file(h, p["geometry_file"].encode(), 1 if p["cache_topology"] else 0)
         self._n = 0
         self._xyz = None
         self._grad = None
@@ -267,11 +271,14 @@ class GFNFF:
 
     def setParameters(self, params: dict) -> None:
         """precision ("fp64"/"mixed"), gpu_device, hbond, hb_rmsd_bohr, exact_gradient, solvent
-        (ALPB implicit solvation: curcuma's solvent names, "none" for the gas phase), threads.
+        (ALPB implicit solvation: curcuma's solvent names, "none" for the gas phase), threads,
+        geometry_file and cache_topology (the `<geometry>.topo.json` topology cache).
         A new handle is made with them: call setMolecule again afterwards."""
         unknown = set(params) - set(self._params)
         if unknown:
             raise KeyError(f"unknown parameters: {sorted(unknown)}")
+        if "geometry_file" in params:
+            params = dict(params, geometry_file=str(params["geometry_file"] or ""))
         new = dict(self._params, **params)
         if new["precision"] not in ("fp64", "mixed"):
             raise ValueError("precision must be 'fp64' or 'mixed'")
@@ -310,6 +317,10 @@ class GFNFF:
     def eeqSolver(self) -> str:
         """EEQ solver chosen at setup ("library", "tiled", "pcg", "lu", "batched")."""
         return self._lib.gfnff_eeq_solver(self._h).decode()
+
+    def topologyCacheHit(self) -> bool:
+        """True when the last setMolecule took its Phase-1 data from `<geometry>.topo.json`."""
+        return self._lib.gfnff_topology_cache_hit(self._h) == 1
 
     def eeqIterations(self) -> int:
         """Iterations of the last iterative EEQ solve (0 for direct solvers)."""
@@ -362,3 +373,21 @@ def write_parameters(Z, xyz_angstrom, path, charge: int = 0, hbond: bool = True)
                                     1 if hbond else 0, str(path).encode())
     if st != _lib.GFNFF_OK:
         raise RuntimeError(lib.gfnff_last_error(None).decode())
+
+
+def write_topology_cache(Z, xyz_angstrom, geometry_file, charge: int = 0) -> bool:
+    """Runs the GFN-FF set-up on the host with the topology cache of geometry_file
+    (`<geometry_file without extension>.topo.json`, curcuma's format) and writes the cache;
+    returns True when the existing file's Phase-1 data were used.  No GPU needed."""
+    lib = _lib.load()
+    Z = np.ascontiguousarray(Z, dtype=np.int32)
+    X = np.ascontiguousarray(xyz_angstrom, dtype=np.float64).reshape(-1, 3)
+    if len(Z) != len(X):
+        raise ValueError("Z and geometry sizes differ")
+    hit = ctypes.c_int(0)
+    st = lib.gfnff_write_topology_cache(len(Z), Z.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                        X.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), int(charge),
+                                        str(geometry_file).encode(), ctypes.byref(hit))
+    if st != _lib.GFNFF_OK:
+        raise RuntimeError(lib.gfnff_last_error(None).decode())
+    return hit.value == 1

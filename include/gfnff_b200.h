@@ -92,6 +92,25 @@ gfnff_status gfnff_setup_from_parameters(gfnff_handle* h, const char* path, int 
 gfnff_status gfnff_write_parameters(int natoms, const int* Z, const double* xyz_angstrom, int total_charge,
                                     int hbond, const char* path);
 
+/* Topology cache in curcuma's `<geometry>.topo.json` format (its `geometry_file` and
+ * `cache_topology` parameters; ff_methods/gfnff_method.cpp:2515-2656 fingerprint and export,
+ * 2941-2985 write, 8973-9040 read).  gfnff_set_geometry_file names the geometry file of the
+ * next gfnff_setup of this handle; with cache_topology != 0 that set-up reads
+ * `<geometry_file without its extension>.topo.json` and, when the file's fingerprint (atom
+ * count, elements, geometric bond list) is this structure's, takes the Phase-1 charges,
+ * fragment charges, dxi, dgam, alpeeq and amide-H flags from it instead of computing them;
+ * after the set-up it writes the file (skipped when the Phase-1 charges fail curcuma's
+ * write check, or the file cannot be written).  The topology refresh after a 0.5 bohr
+ * displacement consults the same file.  NULL or cache_topology == 0: no cache (the default).
+ * gfnff_topology_cache_hit: 1 when the last set-up of h used the cache, 0 when it did not,
+ * -1 before a set-up.  gfnff_write_topology_cache runs the host set-up with the cache and
+ * writes the file without a handle or a GPU; cache_hit (may be NULL) receives whether the
+ * existing file was used. */
+gfnff_status gfnff_set_geometry_file(gfnff_handle* h, const char* geometry_file, int cache_topology);
+int gfnff_topology_cache_hit(gfnff_handle* h);
+gfnff_status gfnff_write_topology_cache(int natoms, const int* Z, const double* xyz_angstrom, int total_charge,
+                                        const char* geometry_file, int* cache_hit);
+
 /* Replaces updateGeometry + calculateEnergy(true) + copyGradientTo
  * (gfnff_method.cpp:1692-2226, computational_method.h:121-123).  energy and grad are
  * host pointers; grad may be NULL for energy only (the gradient is still computed);

@@ -872,6 +872,21 @@ oracle_handle* oracle_create(int n, const int* Z, const double* xyz_ang, int cha
     }
 }
 
+// a set-up that consults a topology cache file (<geometry>.topo.json) before Phase 1
+oracle_handle* oracle_create_cached(int n, const int* Z, const double* xyz_ang, int charge, const char* topo_json)
+{
+    try {
+        auto* h = new oracle_handle;
+        h->m = build_model(n, Z, xyz_ang, charge, SetupOptions(), BuildLists(), topo_json);
+        return h;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return nullptr;
+    }
+}
+
+int oracle_topo_cache_hit(oracle_handle* h) { return h && h->m.topo_cache_hit ? 1 : 0; }
+
 // the model read from a parameter file (the product's set-up cache) instead of a fresh set-up
 oracle_handle* oracle_create_from_parameters(const char* path)
 {

@@ -21,6 +21,10 @@ typedef struct oracle_handle oracle_handle;
 oracle_handle* oracle_create(int n, const int* Z, const double* xyz_ang, int charge);
 // The model of a parameter file written by the library (gfnff_write_parameters); NULL on failure.
 oracle_handle* oracle_create_from_parameters(const char* path);
+// set-up with a topology cache file (<geometry>.topo.json): Phase 1 from the file on a
+// fingerprint match; oracle_topo_cache_hit reports whether it was used
+oracle_handle* oracle_create_cached(int n, const int* Z, const double* xyz_ang, int charge, const char* topo_json);
+int oracle_topo_cache_hit(oracle_handle* h);
 void oracle_destroy(oracle_handle* h);
 // ALPB implicit solvation for the following evaluations (curcuma's solvent names and
 // aliases; "" or "none": gas phase).  Returns 0, or 1 for an unknown solvent.

@@ -29,6 +29,10 @@ def lib():
         c_v, c_i = ctypes.c_void_p, ctypes.c_int
         L.oracle_create.restype = c_v
         L.oracle_create.argtypes = [c_i, c_v, c_v, c_i]
+        L.oracle_create_cached.restype = c_v
+        L.oracle_create_cached.argtypes = [c_i, c_v, c_v, c_i, ctypes.c_char_p]
+        L.oracle_topo_cache_hit.argtypes = [c_v]
+        L.oracle_topo_cache_hit.restype = c_i
         L.oracle_create_from_parameters.restype = c_v
         L.oracle_create_from_parameters.argtypes = [ctypes.c_char_p]
         L.oracle_destroy.argtypes = [c_v]
@@ -51,15 +55,25 @@ def lib():
 
 
 class Oracle:
-    def __init__(self, Z, xyz, charge=0, solvent=None):
+    def __init__(self, Z, xyz, charge=0, solvent=None, topo_cache=None):
+        """topo_cache: a `<geometry>.topo.json` consulted before Phase 1 (cache_hit tells
+        whether it was used)."""
         self.Z = np.ascontiguousarray(Z, dtype=np.int32)
         X = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
         self.n = len(self.Z)
-        self.h = lib().oracle_create(self.n, self.Z.ctypes.data, X.ctypes.data, int(charge))
+        if topo_cache:
+            self.h = lib().oracle_create_cached(self.n, self.Z.ctypes.data, X.ctypes.data, int(charge),
+                                                str(topo_cache).encode())
+        else:
+            self.h = lib().oracle_create(self.n, self.Z.ctypes.data, X.ctypes.data, int(charge))
         if not self.h:
             raise RuntimeError(lib().oracle_last_error().decode())
         if solvent and lib().oracle_set_solvent(self.h, solvent.encode()) != 0:
             raise RuntimeError(lib().oracle_last_error().decode())
+
+    @property
+    def cache_hit(self):
+        return lib().oracle_topo_cache_hit(self.h) == 1
 
     @classmethod
     def from_parameters(cls, path, Z):
