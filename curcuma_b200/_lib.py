@@ -24,7 +24,7 @@ EXPORTED = ["gfnff_default_options", "gfnff_create", "gfnff_setup", "gfnff_energ
             "gfnff_energy_and_gradient_batch", "gfnff_md_nve", "gfnff_kernels_per_evaluation",
             "gfnff_save_parameters", "gfnff_setup_from_parameters", "gfnff_write_parameters",
             "gfnff_pair_kernel", "gfnff_eeq_fp64_products", "gfnff_set_solvent", "gfnff_set_geometry_file",
-            "gfnff_topology_cache_hit", "gfnff_write_topology_cache"]
+            "gfnff_topology_cache_hit", "gfnff_write_topology_cache", "gfnff_set_unit_cell"]
 PHASES = ["positions", "cn", "d4_weights", "eeq_matrix", "eeq_rhs", "eeq_solve", "bonded",
           "hbonds", "repulsion", "pairs", "post_chain", "finish"]
 
@@ -75,6 +75,7 @@ def load():
     lib.gfnff_eeq_fp64_products.argtypes = [c_v]
     lib.gfnff_set_solvent.argtypes = [c_v, ctypes.c_char_p]
     lib.gfnff_set_geometry_file.argtypes = [c_v, ctypes.c_char_p, c_i]
+    lib.gfnff_set_unit_cell.argtypes = [c_v, P(c_d)]
     lib.gfnff_topology_cache_hit.argtypes = [c_v]
     lib.gfnff_write_topology_cache.argtypes = [c_i, P(c_i), P(c_d), c_i, ctypes.c_char_p, P(c_i)]
     lib.gfnff_kernels_per_evaluation.argtypes = [c_v]

@@ -35,6 +35,7 @@ struct gfnff_handle {
     std::string solvent;            // ALPB solvent ("" gas phase)
     AlpbModel solv;
     std::string topo_cache;         // <geometry>.topo.json ("" no topology cache)
+    std::vector<double> cell_bohr;  // periodic cell, 9 doubles (empty: isolated system)
     double* pin_xyz = nullptr;      // pinned staging for host coordinates
     double* pin_grad = nullptr;
     double* pin_out = nullptr;      // terms + status + msd
@@ -102,6 +103,27 @@ gfnff_status gfnff_set_solvent(gfnff_handle* h, const char* solvent)
     AlpbModel probe;
     if (!alpb_setup(probe, std::vector<int>{1}, s)) return fail(h, GFNFF_INVALID_ARG, "unknown solvent: " + s);
     h->solvent = (s == "none") ? "" : s;
+    return GFNFF_OK;
+}
+
+gfnff_status gfnff_set_unit_cell(gfnff_handle* h, const double* cell_angstrom)
+{
+    if (!h) return fail(nullptr, GFNFF_INVALID_ARG, "handle is NULL");
+    if (!cell_angstrom) {
+        h->cell_bohr.clear();
+        return GFNFF_OK;
+    }
+    if (h->opt.gradient == GFNFF_GRADIENT_EXACT)
+        return fail(h, GFNFF_INVALID_ARG, "a periodic cell needs the reference gradient mode");
+    std::vector<double> c(9);
+    for (int k = 0; k < 9; ++k) {
+        if (!std::isfinite(cell_angstrom[k])) return fail(h, GFNFF_INVALID_ARG, "non-finite cell");
+        c[k] = cell_angstrom[k] * kAngToBohr;
+    }
+    const double det = c[0] * (c[4] * c[8] - c[7] * c[5]) - c[3] * (c[1] * c[8] - c[7] * c[2]) +
+                       c[6] * (c[1] * c[5] - c[4] * c[2]);
+    if (!(std::fabs(det) > 1e-6)) return fail(h, GFNFF_INVALID_ARG, "singular cell");
+    h->cell_bohr = c;
     return GFNFF_OK;
 }
 
@@ -174,7 +196,10 @@ gfnff_status gfnff_setup(gfnff_handle* h, int n, const int* Z, const double* xyz
 // upload of h->model and the per-handle host staging (gfnff_setup, gfnff_setup_from_parameters)
 static gfnff_status finish_setup(gfnff_handle* h, int n)
 {
+    if (!h->cell_bohr.empty() && h->solv.on)
+        return fail(h, GFNFF_INVALID_ARG, "ALPB solvation and a periodic cell exclude each other");
     try {
+        h->eng->set_cell(h->cell_bohr.empty() ? nullptr : h->cell_bohr.data());
         h->eng->upload(h->model, h->solv.on ? &h->solv : nullptr);
         if (h->pin_xyz) cudaFreeHost(h->pin_xyz);
         if (h->pin_grad) cudaFreeHost(h->pin_grad);
@@ -252,6 +277,7 @@ gfnff_status gfnff_setup_batch(gfnff_handle* h, int nmol, const int* natoms, con
     if (!h) return fail(nullptr, GFNFF_INVALID_ARG, "handle is NULL");
     if (nmol <= 0 || !natoms || !Z || !xyz) return fail(h, GFNFF_INVALID_ARG, "invalid batch");
     if (!h->solvent.empty()) return fail(h, GFNFF_INVALID_ARG, "ALPB solvation: single-molecule handles only");
+    if (!h->cell_bohr.empty()) return fail(h, GFNFF_INVALID_ARG, "a periodic cell: single-molecule handles only");
     std::vector<long> off(nmol + 1, 0);
     for (int m = 0; m < nmol; ++m) {
         if (natoms[m] <= 0) return fail(h, GFNFF_INVALID_ARG, "molecule without atoms");
@@ -279,6 +305,7 @@ gfnff_status gfnff_setup_batch(gfnff_handle* h, int nmol, const int* natoms, con
     try {
         std::vector<const Model*> ptr(nmol);
         for (int m = 0; m < nmol; ++m) ptr[m] = &models[m];
+        h->eng->set_cell(nullptr);
         h->eng->upload_batch(ptr);
         if (h->pin_xyz) cudaFreeHost(h->pin_xyz);
         if (h->pin_grad) cudaFreeHost(h->pin_grad);

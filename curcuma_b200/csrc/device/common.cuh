@@ -205,6 +205,30 @@ __device__ __forceinline__ double d2_exact(double4 a, double4 b)
 }
 
 // ------------------------------------------------------------------------------------
+// periodic cell for the minimum-image convention (curcuma: cuda/gfnff_kernels.cu:92-119):
+// h holds the lattice vectors a, b, c as columns, h[3*col + row] (bohr), hi its inverse in
+// the same layout; on = 0 for an isolated system.  The displacement d = x_b - x_a becomes
+// h (f - rint(f)) with the fractional f = hi d.
+// ------------------------------------------------------------------------------------
+struct Cell {
+    double h[9], hi[9];
+    int on;
+};
+
+__device__ __forceinline__ void mic(const Cell& c, double& dx, double& dy, double& dz)
+{
+    double fx = c.hi[0] * dx + c.hi[3] * dy + c.hi[6] * dz;
+    double fy = c.hi[1] * dx + c.hi[4] * dy + c.hi[7] * dz;
+    double fz = c.hi[2] * dx + c.hi[5] * dy + c.hi[8] * dz;
+    fx -= rint(fx);
+    fy -= rint(fy);
+    fz -= rint(fz);
+    dx = c.h[0] * fx + c.h[3] * fy + c.h[6] * fz;
+    dy = c.h[1] * fx + c.h[4] * fy + c.h[7] * fz;
+    dz = c.h[2] * fx + c.h[5] * fy + c.h[8] * fz;
+}
+
+// ------------------------------------------------------------------------------------
 // device view of the model.  Atoms are stored in the engine's internal order (molecules
 // contiguous, atoms of a molecule sorted along a Morton curve of the setup geometry);
 // perm maps an internal index to the caller's index.
@@ -259,7 +283,19 @@ struct View {
     // axis-aligned boxes of the runs of 32 consecutive atoms (current geometry)
     const double4* boxlo;
     const double4* boxhi;
+    // periodic cell: the CN, bond, angle, HB, XB, repulsion, Coulomb and D4 pair distances
+    // take the minimum image; torsions, inversions, ATM, BATM and the EEQ matrix do not
+    Cell cell;
 };
+
+// minimum-image difference pos[b] - pos[a] in FP64 (the plain difference without a cell)
+__device__ __forceinline__ D3 dmic(const View& V, int a, int b)
+{
+    const double4 x = V.pos[a], y = V.pos[b];
+    double dx = y.x - x.x, dy = y.y - x.y, dz = y.z - x.z;
+    if (V.cell.on) mic(V.cell, dx, dy, dz);
+    return {dx, dy, dz};
+}
 
 // Adds v to term `term` of molecule `mol` (mol < 0: nothing to add).  Every thread of
 // the block calls it.  Single-molecule models reduce over the block; batches reduce

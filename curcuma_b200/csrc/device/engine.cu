@@ -367,6 +367,7 @@ struct Engine::Impl {
         cnl_bad.upload(std::vector<int>{zero});
     }
     bool box_cull = false;        // CN kernels skip far tiles (single molecules >= 8192 atoms)
+    Cell cell{};                  // periodic cell (cell.on = 0: isolated system)
     int nsym = 0;
     bool pairs_sym = true;
     bool pairs_occ = false;   // 10 blocks per SM (96 registers) instead of the unbounded 116
@@ -713,6 +714,7 @@ struct Engine::Impl {
         V.u = resp_on ? ures.p : nullptr;
         V.boxlo = box_cull ? boxlo.p : nullptr;
         V.boxhi = box_cull ? boxhi.p : nullptr;
+        V.cell = cell;
         return V;
     }
     // caller index (molecule m, local atom a) -> internal index
@@ -1017,6 +1019,7 @@ void Engine::upload_batch(const std::vector<const Model*>& mols, const AlpbModel
     if (mols.empty()) throw std::runtime_error("upload: no molecules");
     P.hbd.topo = nullptr;
     const int nm = (int)mols.size();
+    if (P.cell.on && nm > 1) throw std::runtime_error("upload: a periodic cell needs a single molecule");
     P.nmol = nm;
     // ---- atom order: molecules contiguous, Morton order inside each molecule ----
     P.h_aoff.assign(nm + 1, 0);
@@ -1061,7 +1064,8 @@ void Engine::upload_batch(const std::vector<const Model*>& mols, const AlpbModel
         P.pair_tile = nm > 1 ? 32 : kST;
         P.boxlo.alloc((n + kBoxAtoms - 1) / kBoxAtoms);
         P.boxhi.alloc((n + kBoxAtoms - 1) / kBoxAtoms);
-        P.box_cull = nm == 1 && n >= 8192;
+        // box tests compare plain coordinates: off in a periodic cell
+        P.box_cull = nm == 1 && n >= 8192 && !P.cell.on;
         P.nsym = (int)tl.size();
         const char* pe = std::getenv("GFNFF_PAIRS");
         P.pairs_sym = !(pe && !std::strcmp(pe, "rows"));
@@ -1131,8 +1135,10 @@ void Engine::upload_batch(const std::vector<const Model*>& mols, const AlpbModel
     }
     P.pos0.upload(p0); P.hbref.upload(p0); P.toporef.upload(p0); P.pos.alloc(n);
     {
+        // the CN neighbour list is built from plain distances: a periodic cell takes the
+        // all-pairs CN kernels, which apply the minimum image to every pair
         const char* ecl = std::getenv("GFNFF_CN_LIST");
-        P.cnl_on = !(ecl && !std::strcmp(ecl, "0"));
+        P.cnl_on = !(ecl && !std::strcmp(ecl, "0")) && !P.cell.on;
         if (P.cnl_on) {
             if (!P.cnl_bad_host) CK(cudaMallocHost(&P.cnl_bad_host, sizeof(int)));
             *P.cnl_bad_host = 0;
@@ -2065,8 +2071,13 @@ void Engine::launch_body()
         HBSoA H{P.nhb, P.h_rec.p, P.h_qh.p, P.h_qa.p, P.h_bas.p, P.h_aci.p, P.h_rvdw.p, P.h_zlp.p,
                 P.h_pc.p, P.h_nfl.p, P.h_adjo.p, P.h_adj.p};
         const int split = mixed ? P.nhb_near : P.nhb;
-        if (split > 0) k_hbonds<double><<<nblk(split), kBlock, 0, s2>>>(V, H, 0, split);
-        if (P.nhb > split) k_hbonds<float><<<nblk(P.nhb - split), kBlock, 0, s2>>>(V, H, split, P.nhb);
+        if (V.cell.on) {
+            if (split > 0) k_hbonds<double, true><<<nblk(split), kBlock, 0, s2>>>(V, H, 0, split);
+            if (P.nhb > split) k_hbonds<float, true><<<nblk(P.nhb - split), kBlock, 0, s2>>>(V, H, split, P.nhb);
+        } else {
+            if (split > 0) k_hbonds<double><<<nblk(split), kBlock, 0, s2>>>(V, H, 0, split);
+            if (P.nhb > split) k_hbonds<float><<<nblk(P.nhb - split), kBlock, 0, s2>>>(V, H, split, P.nhb);
+        }
     }
     if (P.nxb) k_xbonds<<<nblk(P.nxb), kBlock, 0, s2>>>(V, XBSoA{P.nxb, P.x_a.p, P.x_x.p, P.x_b.p, P.x_pre.p, P.x_rv.p});
     P.mark(8);
@@ -2364,6 +2375,27 @@ void Engine::update_eeq_parameters(const Model& m)
     CK(cudaMemcpy(P.adiag.p, adg.data(), b, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(P.qa.p, qa.data(), b, cudaMemcpyHostToDevice));
     P.hbd.topo = nullptr;   // the HB detection's topology inputs follow the new topology
+}
+
+void Engine::set_cell(const double* cell_bohr)
+{
+    p_->drop_graphs();   // captured graphs hold the view, cell included
+    Cell& c = p_->cell;
+    c = Cell{};
+    if (!cell_bohr) return;
+    // columns a, b, c: h[3*col + row] = component row of lattice vector col
+    for (int k = 0; k < 9; ++k) c.h[k] = cell_bohr[k];
+    auto H = [&](int r, int col) { return c.h[3 * col + r]; };
+    const double det = H(0, 0) * (H(1, 1) * H(2, 2) - H(1, 2) * H(2, 1)) - H(0, 1) * (H(1, 0) * H(2, 2) - H(1, 2) * H(2, 0)) +
+                       H(0, 2) * (H(1, 0) * H(2, 1) - H(1, 1) * H(2, 0));
+    if (!(std::fabs(det) > 1e-12)) throw std::runtime_error("set_cell: singular cell");
+    // inverse = adjugate / det; the cyclic cofactor form carries the signs
+    for (int r = 0; r < 3; ++r)
+        for (int col = 0; col < 3; ++col) {
+            const int r1 = (col + 1) % 3, r2 = (col + 2) % 3, c1 = (r + 1) % 3, c2 = (r + 2) % 3;
+            c.hi[3 * col + r] = (H(r1, c1) * H(r2, c2) - H(r1, c2) * H(r2, c1)) / det;
+        }
+    c.on = 1;
 }
 
 void Engine::set_topo_reference(const double* xyz_bohr)

@@ -72,6 +72,10 @@ public:
     // sets the geometry of the last topology (bohr, host, caller order): d_hb_msd()[1] of an
     // evaluation holds the largest coordinate change since it
     void set_topo_reference(const double* xyz_bohr);
+    // periodic cell for the next upload (single molecules): the lattice vectors a, b, c as
+    // the columns of a 3x3 matrix, cell_bohr[3*col + row] (bohr); nullptr: isolated system.
+    // Throws std::runtime_error for a singular cell.
+    void set_cell(const double* cell_bohr);
     // EEQ parameters (chi, cnf, gamma, alpha, Phase-1 charges) of a refreshed topology of the
     // same molecule with the same fragments, in place
     void update_eeq_parameters(const Model& m);

@@ -39,8 +39,7 @@ __global__ void __launch_bounds__(kBlock) k_bonds(View V, BondSoA B)
     double e = 0.0;
     if (t < B.n) {
         const int i = B.i[t], j = B.j[t];
-        D3 pi = ld(V.pos, i), pj = ld(V.pos, j);
-        D3 ij = pi - pj;
+        const D3 ij = dmic(V, j, i);
         const double r = nrm(ij);
         D3 d0 = (1.0 / r) * ij;
         const double r0 = (B.r0i[t] + B.cki[t] * V.cn[i] + B.r0j[t] + B.ckj[t] * V.cn[j] + B.shift[t]) * B.ff[t];
@@ -48,13 +47,11 @@ __global__ void __launch_bounds__(kBlock) k_bonds(View V, BondSoA B)
         double alpha = B.alpha[t];
         const int H = B.hbh[t];
         const double kn = 27.5, isp = 0.5641895835477563;
-        D3 ph = mk(0.0, 0.0, 0.0);
         if (H >= 0) {
             double hcn = 0.0;
-            ph = ld(V.pos, H);
             for (int p = B.hb_off[t] + lane; p < B.hb_off[t + 1]; p += 32) {
                 const int b = B.hb_b[p];
-                D3 d = ld(V.pos, b) - ph;
+                const D3 d = dmic(V, H, b);
                 const double r2 = d.x * d.x + d.y * d.y + d.z * d.z;
                 if (r2 > 900.0) continue;
                 const double rr = sqrt(r2);
@@ -80,7 +77,7 @@ __global__ void __launch_bounds__(kBlock) k_bonds(View V, BondSoA B)
             D3 gh = mk(0.0, 0.0, 0.0);
             for (int p = B.hb_off[t] + lane; p < B.hb_off[t + 1]; p += 32) {
                 const int b = B.hb_b[p];
-                D3 d = ld(V.pos, b) - ph;
+                const D3 d = dmic(V, H, b);
                 const double r2 = d.x * d.x + d.y * d.y + d.z * d.z;
                 if (r2 > 900.0) continue;
                 const double rr = sqrt(r2);
@@ -114,7 +111,9 @@ __global__ void k_angles(View V, AngleSoA A)
     double et = 0.0;
     if (t < A.n) {
         const int ia = A.i[t], ja = A.j[t], ka = A.k[t];
-        D3 pi = ld(V.pos, ia), pj = ld(V.pos, ja), pk = ld(V.pos, ka), d[3];
+        // the two arms from the apex (minimum image with a cell); the apex is the origin
+        const D3 pi = dmic(V, ja, ia), pj = mk(0.0, 0.0, 0.0), pk = dmic(V, ja, ka);
+        D3 d[3];
         double c = angle_cos(pi, pj, pk, d);
         c = fmax(-1.0, fmin(1.0, c));
         const double th = acos(c), th0 = A.th0[t], fc = A.fc[t];
@@ -370,7 +369,7 @@ __device__ __forceinline__ R hb_len(V3<R> v, R& inv)
 // before the split (up to ~0.01 Eh each) with R = double and only the weak remainder with
 // R = float, because the FP32 rounding of per-element-pair constants is the same for
 // every strong bond and would add up over thousands of them.
-template <class R>
+template <class R, bool CELL = false>
 __global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 5 : GFNFF_HB_MINBLOCKS) k_hbonds(View V, HBSoA S, int t0,
                                                                                         int t1)
 {
@@ -384,8 +383,18 @@ __global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 5 : GFNFF_HB_MINBLOCK
         const R TORS_HB = R(0.94), BEND_HB = R(0.20), HBLPCUT = R(56.0);
         const int A = rec.x, H = rec.y, Bq = rec.z, cs = rec.w;
         P3 pA = ldr<R>(V.pos, A, org), pH = ldr<R>(V.pos, H, org), pB = ldr<R>(V.pos, Bq, org);
+        // A-H, H-B and A-B: minimum-image vectors in a periodic cell (CELL); the acceptor-
+        // neighbour, lone-pair and carbonyl vectors below stay plain differences, as in
+        // curcuma's CUDA kernel
+        P3 vAH = pH - pA, vHB = pB - pH, vAB = pB - pA;
+        if constexpr (CELL) {
+            const D3 a = dmic(V, A, H), b = dmic(V, H, Bq), c = dmic(V, A, Bq);
+            vAH = P3{(R)a.x, (R)a.y, (R)a.z};
+            vHB = P3{(R)b.x, (R)b.y, (R)b.z};
+            vAB = P3{(R)c.x, (R)c.y, (R)c.z};
+        }
         R irAH, irHB, irAB;
-        const R rAH = hb_len(pH - pA, irAH), rHB = hb_len(pB - pH, irHB), rAB = hb_len(pB - pA, irAB);
+        const R rAH = hb_len(vAH, irAH), rHB = hb_len(vHB, irHB), rAB = hb_len(vAB, irAB);
         if (rAB <= R(50.0)) {
             const R rAH4 = rAH * rAH * rAH * rAH, rHB4 = rHB * rHB * rHB * rHB;
             const R den = hb_rcp(rAH4 + rHB4);
@@ -480,7 +489,7 @@ __global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 5 : GFNFF_HB_MINBLOCK
             const R E = cs >= 2 ? -rdamp * qhoutl * cst * eangl * etors : -bas * aci * rdamp * qhoutl;
             etot = E;
 
-            P3 drab = pA - pB, drah = pA - pH, drbh = pB - pH;
+            P3 drab = -R(1.0) * vAB, drah = -R(1.0) * vAH, drbh = vHB;
             const R rahprbh = rAH + rHB + R(1e-12);
             const R ddamp = (-R(2.0) * HB_ALP * ratio1 * dlg) + (R(2.0) * HB_ALP * ratio3 * dsh);
             const R expo = bacut * (rahprbh * irAB - R(1.0));
@@ -648,8 +657,7 @@ __global__ void k_xbonds(View V, XBSoA S)
     double etot = 0.0;
     if (t < S.n) {
         const double XB_BACUT = 70.0, XB_SCUT = 5.0, ALP = 6.0, LC = 70.0;
-        D3 pA = ld(V.pos, S.a[t]), pX = ld(V.pos, S.x[t]), pB = ld(V.pos, S.b[t]);
-        D3 vAX = pX - pA, vXB = pB - pX, vAB = pB - pA;
+        const D3 vAX = dmic(V, S.a[t], S.x[t]), vXB = dmic(V, S.x[t], S.b[t]), vAB = dmic(V, S.a[t], S.b[t]);
         const double rAX = nrm(vAX), rXB = nrm(vXB), rAB = nrm(vAB);
         const double ex = XB_BACUT * ((rAX + rXB) / rAB - 1.0);
         if (rXB <= 20.0 && ex <= 15.0) {

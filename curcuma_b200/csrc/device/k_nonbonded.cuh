@@ -172,7 +172,8 @@ __global__ void __launch_bounds__(kTile) k_cn(View V, int nsplit, const int* nl_
             const int jn = min(32, cnt - js);
             if (V.boxlo && ranges_far(V, w0, nw, t0 + js, jn, 36.0)) continue;   // uniform in the warp
             for (int jj = js; jj < js + jn; ++jj) {
-                const double dx = pi.x - sx[jj], dy = pi.y - sy[jj], dz = pi.z - sz[jj];
+                double dx = pi.x - sx[jj], dy = pi.y - sy[jj], dz = pi.z - sz[jj];
+                if (V.cell.on) mic(V.cell, dx, dy, dz);
                 const double d2 = dx * dx + dy * dy + dz * dz;
                 const int j = t0 + jj;
                 if (!(d2 < 36.0) || j == i || j < rg.x || j >= rg.y) continue;
@@ -252,7 +253,8 @@ __global__ void __launch_bounds__(kBlock) k_repulsion(View V, const int* off, co
         const double4 pi = V.pos[i];
         for (int p = off[i] + lane; p < off[i + 1]; p += 32) {
             const double4 pj = V.pos[nbj[p]];
-            const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+            double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+            if (V.cell.on) mic(V.cell, dx, dy, dz);
             const double d2 = dx * dx + dy * dy + dz * dz;
             const R r = sqrt((R)d2);
             if (r > R(20) || r < R(1e-8)) continue;
@@ -362,7 +364,8 @@ __global__ void __launch_bounds__(kTile) k_pairs(View V, int nsplit)
         for (int jj = 0; jj < cnt; ++jj) {
             const int j = t0 + jj;
             if (j == i || j < rg.x || j >= rg.y) continue;
-            const double dx = pi.x - sx[jj], dy = pi.y - sy[jj], dz = pi.z - sz[jj];
+            double dx = pi.x - sx[jj], dy = pi.y - sy[jj], dz = pi.z - sz[jj];
+            if (V.cell.on) mic(V.cell, dx, dy, dz);
             const double d2 = dx * dx + dy * dy + dz * dz;
             if (d2 < 1e-20) continue;
             double f = 0.0;   // dE/dr / r
@@ -547,6 +550,7 @@ __global__ void __launch_bounds__(T, MINB) k_pairs_sym(View V, const int2* __res
         double dx = 0.0, dy = 0.0, dz = 0.0, d2 = 0.0;
         if (valid) {
             dx = pi.x - sx[jj]; dy = pi.y - sy[jj]; dz = pi.z - sz[jj];
+            if (V.cell.on) mic(V.cell, dx, dy, dz);
             d2 = dx * dx + dy * dy + dz * dz;
             valid = d2 >= 1e-20;
         }
@@ -764,7 +768,8 @@ __global__ void __launch_bounds__(kTile) k_cn_chain(View V, int nsplit, const in
         const int jn = min(32, cnt - js);
         if (V.boxlo && ranges_far(V, w0, nw, t0 + js, jn, 36.0)) continue;   // uniform in the warp
         for (int jj = js; jj < js + jn; ++jj) {
-            const double dx = sx[jj] - pi.x, dy = sy[jj] - pi.y, dz = sz[jj] - pi.z;
+            double dx = sx[jj] - pi.x, dy = sy[jj] - pi.y, dz = sz[jj] - pi.z;
+            if (V.cell.on) mic(V.cell, dx, dy, dz);
             const double d2 = dx * dx + dy * dy + dz * dz;
             const int j = t0 + jj;
             if (!(d2 < 36.0) || j == i || j < rg.x || j >= rg.y) continue;

@@ -39,13 +39,14 @@ MIXED = 1
 class GFNFF:
     def __init__(self, precision: int = FP64, device: int = 0, hbond: bool = True,
                  hb_rmsd_bohr: float = 0.3, exact_gradient: bool = False, solvent: str = "none",
-                 geometry_file=None, cache_topology: bool = True):
+                 geometry_file=None, cache_topology: bool = True, unit_cell=None):
         self._lib = _lib.load()
         self._params = {"precision": "mixed" if precision == MIXED else "fp64", "gpu_device": device,
                         "hbond": bool(hbond), "hb_rmsd_bohr": hb_rmsd_bohr,
                         "exact_gradient": bool(exact_gradient), "solvent": solvent or "none", "threads": 1,
                         "geometry_file": str(geometry_file) if geometry_file else "",
-                        "cache_topology": bool(cache_topology)}
+                        "cache_topology": bool(cache_topology),
+                        "unit_cell": None if unit_cell is None else np.asarray(unit_cell, float).reshape(3, 3).tolist()}
         self._h = None
         self._create()
 
@@ -71,6 +72,16 @@ class GFNFF:
             self._h = None
             raise ValueError(f"gfnff_set_solvent: {msg}")
         self._lib.gfnff_set_geometry_file(h, p["geometry_file"].encode(), 1 if p["cache_topology"] else 0)
+        if p["unit_cell"] is not None:
+            # rows of unit_cell are the lattice vectors a, b, c (Angstrom): row-major data is
+            # the C layout cell[3*k + d]
+            cell = np.ascontiguousarray(p["unit_cell"], dtype=np.float64).reshape(9)
+            st = self._lib.gfnff_set_unit_cell(h, cell.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+            if st != _lib.GFNFF_OK:
+                msg = self._lib.gfnff_last_error(h).decode()
+                self._lib.gfnff_destroy(h)
+                self._h = None
+                raise ValueError(f"gfnff_set_unit_cell: {msg}")
         self._n = 0
         self._xyz = None
         self._grad = None
@@ -272,13 +283,16 @@ class GFNFF:
     def setParameters(self, params: dict) -> None:
         """precision ("fp64"/"mixed"), gpu_device, hbond, hb_rmsd_bohr, exact_gradient, solvent
         (ALPB implicit solvation: curcuma's solvent names, "none" for the gas phase), threads,
-        geometry_file and cache_topology (the `<geometry>.topo.json` topology cache).
+        geometry_file and cache_topology (the `<geometry>.topo.json` topology cache), unit_cell
+        (3x3, rows the lattice vectors in Angstrom, or None: periodic boundary conditions).
         A new handle is made with them: call setMolecule again afterwards."""
         unknown = set(params) - set(self._params)
         if unknown:
             raise KeyError(f"unknown parameters: {sorted(unknown)}")
         if "geometry_file" in params:
             params = dict(params, geometry_file=str(params["geometry_file"] or ""))
+        if "unit_cell" in params and params["unit_cell"] is not None:
+            params = dict(params, unit_cell=np.asarray(params["unit_cell"], float).reshape(3, 3).tolist())
         new = dict(self._params, **params)
         if new["precision"] not in ("fp64", "mixed"):
             raise ValueError("precision must be 'fp64' or 'mixed'")

@@ -92,6 +92,21 @@ gfnff_status gfnff_setup_from_parameters(gfnff_handle* h, const char* path, int 
 gfnff_status gfnff_write_parameters(int natoms, const int* Z, const double* xyz_angstrom, int total_charge,
                                     int hbond, const char* path);
 
+/* Periodic boundary conditions (curcuma's Mol::setUnitCell, GFNFF::InitialiseMolecule
+ * gfnff_method.cpp:724-727 and 794-797, QM/gfnff_gpu_method.cpp:403-408): the unit cell for
+ * the next gfnff_setup / gfnff_setup_from_parameters of this handle, 9 doubles in Angstrom,
+ * cell_angstrom[3*k + d] = component d of lattice vector k (the column-major data of
+ * curcuma's 3x3 cell matrix with the lattice vectors as columns); NULL: isolated system (the
+ * default).  As in curcuma's CUDA kernels (cuda/gfnff_kernels.cu:92-119 and its callers)
+ * the displacement vectors of the coordination numbers and their chain rule, bonds (with
+ * their HB coordination numbers), angles, the A-H, H-B and A-B vectors of hydrogen and
+ * halogen bonds, repulsion and the Coulomb and D4 pairs take the minimum image; torsions,
+ * inversions, ATM, BATM, the EEQ matrix and the set-up (topology, term lists, D4 pair
+ * membership by set-up distance, HB/XB detection) use the plain coordinates.  Single-molecule
+ * handles, reference gradient mode, no ALPB: GFNFF_INVALID_ARG otherwise (a singular or
+ * non-finite cell too). */
+gfnff_status gfnff_set_unit_cell(gfnff_handle* h, const double* cell_angstrom);
+
 /* Topology cache in curcuma's `<geometry>.topo.json` format (its `geometry_file` and
  * `cache_topology` parameters; ff_methods/gfnff_method.cpp:2515-2656 fingerprint and export,
  * 2941-2985 write, 8973-9040 read).  gfnff_set_geometry_file names the geometry file of the

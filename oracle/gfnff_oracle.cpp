@@ -36,6 +36,25 @@ inline double dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 inline V3 cross(V3 a, V3 b) { return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
 inline double norm(V3 a) { return std::sqrt(dot(a, a)); }
 
+// Periodic cell, minimum-image convention of curcuma's CUDA kernels
+// (cuda/gfnff_kernels.cu:92-119): h holds the lattice vectors as columns, h[3*col + row]
+// (bohr), hi its inverse; d -> h (f - rint(f)) with f = hi d.
+struct OCell {
+    double h[9] = {0}, hi[9] = {0};
+    bool on = false;
+    V3 operator()(V3 d) const
+    {
+        if (!on) return d;
+        double f[3];
+        for (int r = 0; r < 3; ++r) {
+            f[r] = hi[r] * d.x + hi[3 + r] * d.y + hi[6 + r] * d.z;
+            f[r] -= std::rint(f[r]);
+        }
+        return {h[0] * f[0] + h[3] * f[1] + h[6] * f[2], h[1] * f[0] + h[4] * f[1] + h[7] * f[2],
+                h[2] * f[0] + h[5] * f[1] + h[8] * f[2]};
+    }
+};
+
 struct Grad {
     std::vector<double> g;
     explicit Grad(int n) : g(3 * (size_t)n, 0.0) {}
@@ -47,6 +66,7 @@ struct Grad {
 struct oracle_handle {
     Model m;
     AlpbModel solv;   // ALPB implicit solvation (off: gas phase)
+    OCell cell;       // periodic cell (off: isolated system)
 };
 
 // ---------------------------------------------------------------------------------
@@ -119,12 +139,18 @@ static double oop(V3 ri, V3 rj, V3 rk, V3 rl, V3 g[4])
     return om;
 }
 
-static int engrad(const Model& m, const AlpbModel& solv, const double* xb, double* T, double* gout, double* qout,
-                  double* cnout)
+// With a periodic cell (mic.on) the displacement vectors of the terms curcuma's CUDA kernels
+// treat with the minimum image take it (CN and its chain rule, HB coordination numbers,
+// bonds, angles, the A-H, H-B and A-B vectors of HB and XB terms, repulsion, Coulomb and D4
+// pairs); torsions, inversions, ATM, BATM, the EEQ matrix and the set-up lists (D4 pairs by
+// set-up distance) use plain differences.
+static int engrad(const Model& m, const AlpbModel& solv, const OCell& mic, const double* xb, double* T, double* gout,
+                  double* qout, double* cnout)
 {
     const int n = m.n;
     AlpbGeom sg;   // ALPB state of this geometry (gfnff_method.cpp:1128-1140, 1805-1853)
     auto X = [&](int i) { return V3{xb[3 * i], xb[3 * i + 1], xb[3 * i + 2]}; };
+    auto D = [&](int a, int b) { return mic(X(b) - X(a)); };   // x_b - x_a, minimum image
     for (int t = 0; t < ORC_NTERMS; ++t) T[t] = 0.0;
     Grad G(n);
     std::vector<double> dEdcn(n, 0.0);
@@ -134,7 +160,7 @@ static int engrad(const Model& m, const AlpbModel& solv, const double* xb, doubl
     std::vector<std::vector<int>> nbr(n);
     for (int i = 0; i < n; ++i)
         for (int j = i + 1; j < n; ++j) {
-            V3 d = X(i) - X(j);
+            V3 d = D(j, i);
             if (d.x * d.x + d.y * d.y + d.z * d.z < 36.0) { nbr[i].push_back(j); nbr[j].push_back(i); }
         }
     std::vector<double> cnraw(n, 0.0), cn(n, 0.0);
@@ -142,7 +168,7 @@ static int engrad(const Model& m, const AlpbModel& solv, const double* xb, doubl
         std::sort(nbr[i].begin(), nbr[i].end());
         double s = 0.0;
         for (int j : nbr[i]) {
-            const double r = norm(X(i) - X(j));
+            const double r = norm(D(j, i));
             const double rc = m.rcov_cn[i] + m.rcov_cn[j];
             s += 0.5 * (1.0 + std::erf(kn * ((r - rc) / rc)));
         }
@@ -208,7 +234,7 @@ static int engrad(const Model& m, const AlpbModel& solv, const double* xb, doubl
         for (const auto& e : m.bond_hb) {
             const int H = e.h;
             for (int B : e.b_atoms) {
-                V3 d = X(B) - X(H);
+                V3 d = D(H, B);
                 const double r2 = d.x * d.x + d.y * d.y + d.z * d.z;
                 if (r2 > 900.0) continue;
                 const double r = std::sqrt(r2);
@@ -223,7 +249,7 @@ static int engrad(const Model& m, const AlpbModel& solv, const double* xb, doubl
 
     // ---- bonds: ff_workspace_gfnff.cpp:104-182 ------------------------------------
     for (const auto& b : m.bonds) {
-        V3 ij = X(b.i) - X(b.j);
+        V3 ij = D(b.j, b.i);
         const double r = norm(ij);
         V3 d0 = (1.0 / r) * ij;
         const double r0 = (b.r0_base_i + b.cnfak_i * cn[b.i] + b.r0_base_j + b.cnfak_j * cn[b.j] + b.rabshift) * b.ff;
@@ -257,7 +283,7 @@ static int engrad(const Model& m, const AlpbModel& solv, const double* xb, doubl
     {
         const double atcuta = 0.595;
         for (const auto& a : m.angles) {
-            V3 pi = X(a.i), pj = X(a.j), pk = X(a.k), d[3];
+            V3 pi = D(a.j, a.i), pj{0, 0, 0}, pk = D(a.j, a.k), d[3];   // the apex as the origin
             double c = angle_cos(pi, pj, pk, d);
             c = std::max(-1.0, std::min(1.0, c));
             const double th = std::acos(c);
@@ -369,7 +395,7 @@ static int engrad(const Model& m, const AlpbModel& solv, const double* xb, doubl
 
     // ---- D4 dispersion: :715-772 ---------------------------------------------------
     for (const auto& d : m.disp) {
-        V3 rv = X(d.i) - X(d.j);
+        V3 rv = D(d.j, d.i);
         const double r = norm(rv);
         if (r > 50.0 || r < 1e-10) continue;
         const double r2 = r * r, r6 = r2 * r2 * r2, r06 = d.r0sq * d.r0sq * d.r0sq;
@@ -397,7 +423,7 @@ static int engrad(const Model& m, const AlpbModel& solv, const double* xb, doubl
 
     // ---- repulsion: :774-848 -------------------------------------------------------
     auto rep = [&](const RepPair& p, int slot) {
-        V3 rv = X(p.i) - X(p.j);
+        V3 rv = D(p.j, p.i);
         const double r = norm(rv);
         if (r > 20.0 || r < 1e-8) return;
         const double e = p.repab * std::exp(-p.alpha * (r * std::sqrt(r))) / r;
@@ -419,7 +445,7 @@ static int engrad(const Model& m, const AlpbModel& solv, const double* xb, doubl
             double gx = 0.0, gy = 0.0, gz = 0.0;
             for (int j = 0; j < n; ++j) {
                 if (j == i) continue;
-                V3 rv = X(i) - X(j);
+                V3 rv = D(j, i);
                 const double r = norm(rv);
                 if (r > 100.0 || r < 1e-10) continue;
                 const double gam = 1.0 / std::sqrt(m.alpeeq[i] + m.alpeeq[j]);
@@ -445,8 +471,10 @@ static int engrad(const Model& m, const AlpbModel& solv, const double* xb, doubl
                      XHACI_COH = 0.350, HBLPCUT = 56.0;
         auto qs = [&](double qq) { const double e = std::exp(HB_ST * qq); return e / (e + HB_SF); };
         for (const auto& hb : m.hbonds) {
-            V3 pA = X(hb.a), pH = X(hb.h), pB = X(hb.b);
-            const double rAH = norm(pH - pA), rHB = norm(pB - pH), rAB = norm(pB - pA);
+            V3 pA = X(hb.a), pB = X(hb.b);
+            // A-H, H-B, A-B: minimum image; the neighbour, lone-pair and carbonyl vectors: plain
+            const V3 vAH = D(hb.a, hb.h), vHB = D(hb.h, hb.b), vAB = D(hb.a, hb.b);
+            const double rAH = norm(vAH), rHB = norm(vHB), rAB = norm(vAB);
             if (rAB > 50.0) continue;
             const double rAH4 = rAH * rAH * rAH * rAH, rHB4 = rHB * rHB * rHB * rHB;
             const double den = 1.0 / (rAH4 + rHB4);
@@ -556,7 +584,7 @@ static int engrad(const Model& m, const AlpbModel& solv, const double* xb, doubl
             else E = -bas * aci * rdamp * qhoutl;
             T[ORC_HBOND] += E;
 
-            V3 drab = pA - pB, drah = pA - pH, drbh = pB - pH;
+            V3 drab = -1.0 * vAB, drah = -1.0 * vAH, drbh = vHB;
             const double rab2 = rAB * rAB, rbh2 = rHB * rHB, rah2 = rAH * rAH;
             const double rahprbh = rAH + rHB + 1e-12;
             const double ratio1 = std::pow(rab2 / HB_LONGCUT, HB_ALP);
@@ -706,8 +734,7 @@ static int engrad(const Model& m, const AlpbModel& solv, const double* xb, doubl
         const double XB_BACUT = 70.0, XB_SCUT = 5.0, HB_ALP = 6.0, LC = 70.0, XB_ST = 15.0, XB_SF = 0.03;
         auto qs = [&](double qq) { const double e = std::exp(XB_ST * qq); return e / (e + XB_SF); };
         for (const auto& xbd : m.xbonds) {
-            V3 pA = X(xbd.a), pX = X(xbd.x), pB = X(xbd.b);
-            V3 vAX = pX - pA, vXB = pB - pX, vAB = pB - pA;
+            V3 vAX = D(xbd.a, xbd.x), vXB = D(xbd.x, xbd.b), vAB = D(xbd.a, xbd.b);
             const double rAX = norm(vAX), rXB = norm(vXB), rAB = norm(vAB);
             if (rXB > 20.0) continue;
             const double rv = m.rvdw[xbd.a] + m.rvdw[xbd.b];
@@ -836,7 +863,7 @@ static int engrad(const Model& m, const AlpbModel& solv, const double* xb, doubl
         for (int i = 0; i < n; ++i)
             for (int j : nbr[i]) {
                 if (j >= i) continue;
-                V3 rv = X(j) - X(i);
+                V3 rv = D(i, j);
                 const double r = std::sqrt(dot(rv, rv));
                 const double rs = m.rcov_cn[i] + m.rcov_cn[j];
                 const double dr = (r - rs) / rs;
@@ -887,6 +914,31 @@ oracle_handle* oracle_create_cached(int n, const int* Z, const double* xyz_ang, 
 
 int oracle_topo_cache_hit(oracle_handle* h) { return h && h->m.topo_cache_hit ? 1 : 0; }
 
+// periodic cell: cell_ang[3*k + d] = component d of lattice vector k (Angstrom); NULL: none
+int oracle_set_cell(oracle_handle* h, const double* cell_ang)
+{
+    if (!h) return 1;
+    h->cell = OCell();
+    if (!cell_ang) return 0;
+    double* c = h->cell.h;
+    for (int k = 0; k < 9; ++k) c[k] = cell_ang[k] * kAngToBohr;
+    auto H = [&](int r, int col) { return c[3 * col + r]; };
+    const double det = H(0, 0) * (H(1, 1) * H(2, 2) - H(1, 2) * H(2, 1)) - H(0, 1) * (H(1, 0) * H(2, 2) - H(1, 2) * H(2, 0)) +
+                       H(0, 2) * (H(1, 0) * H(2, 1) - H(1, 1) * H(2, 0));
+    if (!(std::fabs(det) > 1e-6)) {
+        g_err = "singular cell";
+        return 1;
+    }
+    // inverse = adjugate / det (cyclic cofactors), stored in the same column layout
+    for (int r = 0; r < 3; ++r)
+        for (int col = 0; col < 3; ++col) {
+            const int r1 = (col + 1) % 3, r2 = (col + 2) % 3, c1 = (r + 1) % 3, c2 = (r + 2) % 3;
+            h->cell.hi[3 * col + r] = (H(r1, c1) * H(r2, c2) - H(r1, c2) * H(r2, c1)) / det;
+        }
+    h->cell.on = true;
+    return 0;
+}
+
 // the model read from a parameter file (the product's set-up cache) instead of a fresh set-up
 oracle_handle* oracle_create_from_parameters(const char* path)
 {
@@ -925,7 +977,7 @@ int oracle_engrad(oracle_handle* h, const double* xyz_ang, double* terms, double
     for (size_t k = 0; k < xb.size(); ++k) xb[k] = xyz_ang[k] * kAngToBohr;
     int rc;
     try {
-        rc = engrad(h->m, h->solv, xb.data(), terms, grad, q, cn);
+        rc = engrad(h->m, h->solv, h->cell, xb.data(), terms, grad, q, cn);
     } catch (const std::exception& e) {
         g_err = e.what();
         rc = 2;

@@ -25,6 +25,8 @@ oracle_handle* oracle_create_from_parameters(const char* path);
 // fingerprint match; oracle_topo_cache_hit reports whether it was used
 oracle_handle* oracle_create_cached(int n, const int* Z, const double* xyz_ang, int charge, const char* topo_json);
 int oracle_topo_cache_hit(oracle_handle* h);
+// periodic cell (cell_ang[3*k + d]: component d of lattice vector k, Angstrom; NULL: none)
+int oracle_set_cell(oracle_handle* h, const double* cell_ang);
 void oracle_destroy(oracle_handle* h);
 // ALPB implicit solvation for the following evaluations (curcuma's solvent names and
 // aliases; "" or "none": gas phase).  Returns 0, or 1 for an unknown solvent.

@@ -33,6 +33,8 @@ def lib():
         L.oracle_create_cached.argtypes = [c_i, c_v, c_v, c_i, ctypes.c_char_p]
         L.oracle_topo_cache_hit.argtypes = [c_v]
         L.oracle_topo_cache_hit.restype = c_i
+        L.oracle_set_cell.argtypes = [c_v, c_v]
+        L.oracle_set_cell.restype = c_i
         L.oracle_create_from_parameters.restype = c_v
         L.oracle_create_from_parameters.argtypes = [ctypes.c_char_p]
         L.oracle_destroy.argtypes = [c_v]
@@ -55,9 +57,9 @@ def lib():
 
 
 class Oracle:
-    def __init__(self, Z, xyz, charge=0, solvent=None, topo_cache=None):
+    def __init__(self, Z, xyz, charge=0, solvent=None, topo_cache=None, unit_cell=None):
         """topo_cache: a `<geometry>.topo.json` consulted before Phase 1 (cache_hit tells
-        whether it was used)."""
+        whether it was used); unit_cell: 3x3, rows the lattice vectors (Angstrom)."""
         self.Z = np.ascontiguousarray(Z, dtype=np.int32)
         X = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
         self.n = len(self.Z)
@@ -70,6 +72,10 @@ class Oracle:
             raise RuntimeError(lib().oracle_last_error().decode())
         if solvent and lib().oracle_set_solvent(self.h, solvent.encode()) != 0:
             raise RuntimeError(lib().oracle_last_error().decode())
+        if unit_cell is not None:
+            cell = np.ascontiguousarray(unit_cell, dtype=np.float64).reshape(9)
+            if lib().oracle_set_cell(self.h, cell.ctypes.data) != 0:
+                raise RuntimeError(lib().oracle_last_error().decode())
 
     @property
     def cache_hit(self):
@@ -144,8 +150,8 @@ class OracleSequence:
     also re-detects the HB/XB lists at their reference geometry, as the library does), then
     the HB/XB lists when sqrt(sum d^2)/N exceeds hb_rmsd_bohr since their last detection."""
 
-    def __init__(self, Z, X, charge=0, solvent=None, hb_rmsd_bohr=0.3):
-        self.oracle = Oracle(Z, X, charge, solvent)
+    def __init__(self, Z, X, charge=0, solvent=None, hb_rmsd_bohr=0.3, unit_cell=None):
+        self.oracle = Oracle(Z, X, charge, solvent, unit_cell=unit_cell)
         self.topo = np.asarray(X, dtype=np.float64) / BOHR_A
         self.hb = self.topo.copy()
         self.thr = hb_rmsd_bohr
