@@ -525,106 +525,106 @@ __global__ void __launch_bounds__(T, MINB) k_pairs_sym(View V, const int2* __res
             }
         }
     }
-    // j-side sums.  Coulomb-only launches (ROT): per-warp accumulators in shared memory, at
-    // step k lane t of the block takes partner (t + k) mod T, so the lanes of a warp always
-    // hold distinct partners and add without shuffles or conflicts (1000 waters: 104 -> 53 us).
-    // With D4 terms the lanes take the same partner and the j-side sums are reduced over the
-    // warp: rotated partners made the per-partner reference loops diverge (D4 half 61 ->
-    // 122 us).
-    constexpr bool ROT = PART == kPairCoul;
-    if constexpr (ROT) {
+    // j-side sums, per warp in shared memory, in two passes over the tile's partners.
+    // Coulomb pass: at step k lane t of the block takes partner (t + k) mod T, so the lanes of
+    // a warp always hold distinct partners and add their j-side terms without shuffles or
+    // conflicts (1000 waters, Coulomb launch: 104 -> 53 us against warp-wide reductions).
+    // D4 pass: the lanes take the same partner and the j-side sums are reduced over the warp
+    // (rotated partners made the per-partner reference loops diverge: D4 61 -> 122 us); a
+    // warp runs it only when one of its pairs is within the 50 bohr D4 range, which the
+    // Coulomb pass records.
 #pragma unroll
-        for (int k = 0; k < NA; ++k)
-            for (int u = lane; u < T; u += 32) jacc[warp][k][u] = 0.0;
-    }
+    for (int k = 0; k < NA; ++k)
+        for (int u = lane; u < T; u += 32) jacc[warp][k][u] = 0.0;
     __syncthreads();
     const double tsp = 2.0 / 1.772453850905516;
     double ec = 0.0, ed = 0.0, gx = 0.0, gy = 0.0, gz = 0.0, dcn = 0.0, cfar = 0.0;
     const int cnt = min(T, V.n - j0);
-    for (int k = 0; k < (ROT ? T : cnt); ++k) {
-        const int jj = ROT ? (threadIdx.x + k) & (T - 1) : k;
-        if (ROT && jj >= cnt) continue;
-        const int j = j0 + jj;
-        double fx = 0.0, fy = 0.0, fz = 0.0, dcj = 0.0, cfj = 0.0;
-        bool valid = act && j > i && j >= rg.x && j < rg.y;
-        double dx = 0.0, dy = 0.0, dz = 0.0, d2 = 0.0;
-        if (valid) {
-            dx = pi.x - sx[jj]; dy = pi.y - sy[jj]; dz = pi.z - sz[jj];
+    bool near = !COUL;   // a pair within the D4 range (D4-only launches: assume one)
+    if constexpr (COUL) {
+        for (int k = 0; k < T; ++k) {
+            const int jj = (threadIdx.x + k) & (T - 1);
+            if (jj >= cnt) continue;
+            const int j = j0 + jj;
+            if (!(act && j > i && j >= rg.x && j < rg.y)) continue;
+            double dx = pi.x - sx[jj], dy = pi.y - sy[jj], dz = pi.z - sz[jj];
             if (V.cell.on) mic(V.cell, dx, dy, dz);
-            d2 = dx * dx + dy * dy + dz * dz;
-            valid = d2 >= 1e-20;
-        }
-        bool hit = false;   // this lane has a j-side contribution
-        if (valid) {
-            double f = 0.0;   // dE/dr / r
-            if constexpr (COUL) {
-                hit = true;
-                if (d2 <= 10000.0) {
-                    const double s = ai + sa[jj];
-                    const double qq = qi * sq[jj];
-                    if (d2 >= 36.0 * s) {
-                        const double ir = rsqrt(d2);
-                        const double e = qq * ir;
-                        ec += e;
-                        f -= e * ir * ir;
-                    } else {
-                        const double r = sqrt(d2);
-                        const double g = 1.0 / sqrt(s);
-                        const double gr = g * r;
-                        const double ef = erf(gr);
-                        ec += qq * ef / r;
-                        f += qq * ((g * exp(-gr * gr) * tsp) / r - ef / d2) / r;
-                    }
-                } else if (want_far) {
-                    const double ir = rsqrt(d2);   // cut pair: its EEQ element is 1/r
-                    cfar += sq[jj] * ir;
-                    cfj = qi * ir;
+            const double d2 = dx * dx + dy * dy + dz * dz;
+            if (!(d2 >= 1e-20)) continue;
+            double f = 0.0, cfj = 0.0;   // dE/dr / r
+            if (d2 <= 10000.0) {
+                const double s = ai + sa[jj];
+                const double qq = qi * sq[jj];
+                if (d2 >= 36.0 * s) {
+                    const double ir = rsqrt(d2);
+                    const double e = qq * ir;
+                    ec += e;
+                    f -= e * ir * ir;
+                } else {
+                    const double r = sqrt(d2);
+                    const double g = 1.0 / sqrt(s);
+                    const double gr = g * r;
+                    const double ef = erf(gr);
+                    ec += qq * ef / r;
+                    f += qq * ((g * exp(-gr * gr) * tsp) / r - ef / d2) / r;
                 }
+            } else if (want_far) {
+                const double ir = rsqrt(d2);   // cut pair: its EEQ element is 1/r
+                cfar += sq[jj] * ir;
+                cfj = qi * ir;
             }
-            if constexpr (D4) {
-                if (d2 <= 2500.0 && d2_exact(p0i, make_double4(s0x[jj], s0y[jj], s0z[jj], 0.0)) <= 3600.0) {
-                    hit = true;
-                    const int sj = ssl[jj], nrj = snr[jj];
-                    const double* dgj = V.hdg + ((size_t)j * V.K + si) * 7;
-                    const double r4r2 = 3.0 * szi * ssz[jj], sr4r2 = s3i * srz[jj], zz = zi * sze[jj];
-                    double e, dedr, dci;
-                    // mixed form: pairs closer than 15 bohr (the strong ones) stay FP64
-                    if (sizeof(R) == sizeof(double) || d2 < 225.0)
-                        d4_pair_sym<double, T>(d2, g0i + sj * 7, dgi + sj * 7, dgj, sw0, sw, jj, nrj, nri, wi, r4r2,
-                                               sr4r2, zz, want_dc, e, dedr, dci, dcj);
-                    else
-                        d4_pair_sym<R, T>(d2, g0i + sj * 7, dgi + sj * 7, dgj, sw0, sw, jj, nrj, nri, wi, r4r2,
-                                          sr4r2, zz, want_dc, e, dedr, dci, dcj);
-                    ed += e;
-                    f += dedr;
-                    dcn += dci;
-                }
-            }
+            if (D4) near |= d2 <= 2500.0;
             gx += f * dx; gy += f * dy; gz += f * dz;
-            fx = -f * dx; fy = -f * dy; fz = -f * dz;
+            jacc[warp][0][jj] -= f * dx;
+            jacc[warp][1][jj] -= f * dy;
+            jacc[warp][2][jj] -= f * dz;
+            if (want_far) jacc[warp][4][jj] += cfj;
         }
-        if constexpr (ROT) {
-            if (hit) {
-                jacc[warp][0][jj] += fx;
-                jacc[warp][1][jj] += fy;
-                jacc[warp][2][jj] += fz;
-                if (want_far) jacc[warp][4][jj] += cfj;
-            }
-        } else {
-            if (__any_sync(0xffffffffu, hit)) {
-                for (int o = 16; o > 0; o >>= 1) {
-                    fx += __shfl_xor_sync(0xffffffffu, fx, o);
-                    fy += __shfl_xor_sync(0xffffffffu, fy, o);
-                    fz += __shfl_xor_sync(0xffffffffu, fz, o);
+    }
+    if constexpr (D4) {
+        if (__any_sync(0xffffffffu, near)) {
+            for (int k = 0; k < cnt; ++k) {
+                const int jj = k;
+                const int j = j0 + jj;
+                double fx = 0.0, fy = 0.0, fz = 0.0, dcj = 0.0;
+                bool hit = false;   // this lane has a j-side contribution
+                if (act && j > i && j >= rg.x && j < rg.y) {
+                    double dx = pi.x - sx[jj], dy = pi.y - sy[jj], dz = pi.z - sz[jj];
+                    if (V.cell.on) mic(V.cell, dx, dy, dz);
+                    const double d2 = dx * dx + dy * dy + dz * dz;
+                    if (d2 >= 1e-20 && d2 <= 2500.0 &&
+                        d2_exact(p0i, make_double4(s0x[jj], s0y[jj], s0z[jj], 0.0)) <= 3600.0) {
+                        hit = true;
+                        const int sj = ssl[jj], nrj = snr[jj];
+                        const double* dgj = V.hdg + ((size_t)j * V.K + si) * 7;
+                        const double r4r2 = 3.0 * szi * ssz[jj], sr4r2 = s3i * srz[jj], zz = zi * sze[jj];
+                        double e, dedr, dci;
+                        // mixed form: pairs closer than 15 bohr (the strong ones) stay FP64
+                        if (sizeof(R) == sizeof(double) || d2 < 225.0)
+                            d4_pair_sym<double, T>(d2, g0i + sj * 7, dgi + sj * 7, dgj, sw0, sw, jj, nrj, nri, wi,
+                                                   r4r2, sr4r2, zz, want_dc, e, dedr, dci, dcj);
+                        else
+                            d4_pair_sym<R, T>(d2, g0i + sj * 7, dgi + sj * 7, dgj, sw0, sw, jj, nrj, nri, wi, r4r2,
+                                              sr4r2, zz, want_dc, e, dedr, dci, dcj);
+                        ed += e;
+                        dcn += dci;
+                        gx += dedr * dx; gy += dedr * dy; gz += dedr * dz;
+                        fx = -dedr * dx; fy = -dedr * dy; fz = -dedr * dz;
+                    }
                 }
-                if (D4 && want_dc)
-                    for (int o = 16; o > 0; o >>= 1) dcj += __shfl_xor_sync(0xffffffffu, dcj, o);
-                if (want_far)
-                    for (int o = 16; o > 0; o >>= 1) cfj += __shfl_xor_sync(0xffffffffu, cfj, o);
-            }
-            if (lane == 0) {
-                jacc[warp][0][jj] = fx; jacc[warp][1][jj] = fy; jacc[warp][2][jj] = fz;
-                jacc[warp][3][jj] = dcj; jacc[warp][4][jj] = cfj;
+                if (__any_sync(0xffffffffu, hit)) {
+                    for (int o = 16; o > 0; o >>= 1) {
+                        fx += __shfl_xor_sync(0xffffffffu, fx, o);
+                        fy += __shfl_xor_sync(0xffffffffu, fy, o);
+                        fz += __shfl_xor_sync(0xffffffffu, fz, o);
+                    }
+                    if (want_dc)
+                        for (int o = 16; o > 0; o >>= 1) dcj += __shfl_xor_sync(0xffffffffu, dcj, o);
+                    if (lane == 0) {
+                        jacc[warp][0][jj] += fx; jacc[warp][1][jj] += fy; jacc[warp][2][jj] += fz;
+                        jacc[warp][3][jj] += dcj;
+                    }
+                }
             }
         }
     }
