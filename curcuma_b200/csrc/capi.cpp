@@ -32,6 +32,7 @@ struct gfnff_handle {
     std::string err;
     std::vector<double> hb_ref;    // bohr, geometry of the last HB/XB detection
     std::vector<double> topo_ref;  // bohr, geometry of the last topology
+    std::vector<double> xb;        // bohr, the geometry of the current call (host scratch)
     std::string solvent;            // ALPB solvent ("" gas phase)
     AlpbModel solv;
     std::string topo_cache;         // <geometry>.topo.json ("" no topology cache)
@@ -336,11 +337,13 @@ gfnff_status gfnff_energy_and_gradient_batch(gfnff_handle* h, const double* xyz,
     if (h->nmol == 0) return fail(h, GFNFF_INVALID_ARG, "not a batch handle (use gfnff_energy_and_gradient)");
     if (!xyz || !energies) return fail(h, GFNFF_INVALID_ARG, "NULL coordinates or energies");
     const int n = h->natoms, nm = h->nmol;
-    for (long k = 0; k < 3l * n; ++k)
-        if (!std::isfinite(xyz[k])) return fail(h, GFNFF_NONFINITE, "non-finite coordinate");
+    for (long k = 0; k < 3l * n; ++k) {   // the finiteness check and the pinned copy in one pass
+        const double v = xyz[k];
+        if (!std::isfinite(v)) return fail(h, GFNFF_NONFINITE, "non-finite coordinate");
+        h->pin_xyz[k] = v;
+    }
     std::vector<int> st(nm, 0);
     try {
-        std::memcpy(h->pin_xyz, xyz, 3 * (size_t)n * sizeof(double));
         cudaStream_t s = (cudaStream_t)h->eng->stream();
         if (cudaMemcpyAsync(h->eng->d_xyz_scratch(), h->pin_xyz, 3 * (size_t)n * sizeof(double),
                             cudaMemcpyHostToDevice, s) != cudaSuccess)
@@ -392,13 +395,6 @@ static void topology_refresh(gfnff_handle* h, const double* xb)
     h->eng->set_topo_reference(xb);
 }
 
-static double max_disp(const std::vector<double>& ref, const double* xb, size_t n3)
-{
-    double m = 0.0;
-    for (size_t k = 0; k < n3; ++k) m = std::max(m, std::fabs(xb[k] - ref[k]));
-    return m;
-}
-
 gfnff_status gfnff_energy_and_gradient(gfnff_handle* h, const double* xyz, double* energy, double* grad,
                                        double* terms)
 {
@@ -407,32 +403,36 @@ gfnff_status gfnff_energy_and_gradient(gfnff_handle* h, const double* xyz, doubl
     if (!xyz || !energy) return fail(h, GFNFF_INVALID_ARG, "NULL coordinates or energy");
     if (h->nmol) return fail(h, GFNFF_INVALID_ARG, "batch handle (use gfnff_energy_and_gradient_batch)");
     const int n = h->model.n;
-    for (int k = 0; k < 3 * n; ++k)
-        if (!std::isfinite(xyz[k])) return fail(h, GFNFF_NONFINITE, "non-finite coordinate");
+    // one pass over the coordinates: the finiteness check, the copy into the pinned staging
+    // buffer, the geometry in bohr and both refresh measures (the largest coordinate change
+    // since the last topology, the summed squared displacement since the HB/XB detection)
+    h->xb.resize(3 * (size_t)n);
+    double* xb = h->xb.data();
+    double dmax = 0.0, ss = 0.0;
+    {
+        const double* tr = h->topo_ref.data();
+        const double* hr = h->hb_ref.data();
+        for (int k = 0; k < 3 * n; ++k) {
+            const double v = xyz[k];
+            if (!std::isfinite(v)) return fail(h, GFNFF_NONFINITE, "non-finite coordinate");
+            h->pin_xyz[k] = v;
+            const double b = v * kAngToBohr;
+            xb[k] = b;
+            dmax = std::max(dmax, std::fabs(b - tr[k]));
+            const double d = b - hr[k];
+            ss += d * d;
+        }
+    }
     try {
         // topology refresh on a 0.5 bohr displacement, then the HB/XB refresh when the RMSD-like
         // measure sqrt(sum d^2)/N exceeds the threshold (gfnff_method.cpp:2228-2259), both
         // before this evaluation
-        {
-            std::vector<double> xb(3 * (size_t)n);
-            for (int k = 0; k < 3 * n; ++k) xb[k] = xyz[k] * kAngToBohr;
-            if (max_disp(h->topo_ref, xb.data(), xb.size()) > kTopoDispBohr) topology_refresh(h, xb.data());
+        if (dmax > kTopoDispBohr) topology_refresh(h, xb);
+        if (h->opt.hbond && std::sqrt(ss) / (double)n > h->opt.hb_rmsd_bohr) {
+            redetect_hbxb(h->model, xb);
+            h->eng->upload_hbxb(h->model, xb);
+            h->hb_ref.assign(xb, xb + 3 * (size_t)n);
         }
-        if (h->opt.hbond) {
-            double s = 0.0;
-            for (int k = 0; k < 3 * n; ++k) {
-                const double d = xyz[k] * kAngToBohr - h->hb_ref[k];
-                s += d * d;
-            }
-            if (std::sqrt(s) / (double)n > h->opt.hb_rmsd_bohr) {
-                std::vector<double> xb(3 * (size_t)n);
-                for (int k = 0; k < 3 * n; ++k) xb[k] = xyz[k] * kAngToBohr;
-                redetect_hbxb(h->model, xb.data());
-                h->eng->upload_hbxb(h->model, xb.data());
-                h->hb_ref = xb;
-            }
-        }
-        std::memcpy(h->pin_xyz, xyz, 3 * (size_t)n * sizeof(double));
         cudaStream_t s = (cudaStream_t)h->eng->stream();
         if (cudaMemcpyAsync(h->eng->d_xyz_scratch(), h->pin_xyz, 3 * (size_t)n * sizeof(double),
                             cudaMemcpyHostToDevice, s) != cudaSuccess)
