@@ -810,7 +810,7 @@ static void generate_repulsion(Ctx& c)
         r.repab = repz[zi] * repz[zj] * REPSCALB;
         c.m.rep_bonded.push_back(r);
     }
-    auto make = [&](int ii, int jj) {
+    auto make = [&](int ii, int jj, std::vector<RepPair>& out) {
         const int i = std::min(ii, jj), j = std::max(ii, jj);
         if (i == j || c.bonded(i, j)) return;
         const int zi = c.Z[i] - 1, zj = c.Z[j] - 1;
@@ -838,18 +838,28 @@ static void generate_repulsion(Ctx& c)
         r.j = j;
         r.alpha = std::sqrt(d1 * d2) * ff;
         r.repab = repz[zi] * repz[zj] * REPSCALN;
-        c.m.rep_nonbonded.push_back(r);
+        out.push_back(r);
     };
     const bool cell = (m.opt.cell_list_min_atoms == 0 || c.n >= m.opt.cell_list_min_atoms);
     c.m.nonbonded_rep_all_pairs = !cell;
+    auto by_pair = [](const RepPair& a, const RepPair& b) { return a.i != b.i ? a.i < b.i : a.j < b.j; };
     if (cell) {
-        pairs_within(c, 20.0, false, [&](int i, int j, double) { make(i, j); });
+        // rows in parallel, one list per thread; a thread's rows are a contiguous ascending
+        // range, so its list sorted by (i, j) and the lists joined in thread order are the
+        // whole list sorted by (i, j), the same list as a serial pass
+        std::vector<std::vector<RepPair>> part(setup_threads());
+        pairs_within_rows(c, 20.0, false, [&](int t, int i, int j, double) { make(i, j, part[t]); });
+#pragma omp parallel for schedule(dynamic, 1)
+        for (int t = 0; t < (int)part.size(); ++t) std::sort(part[t].begin(), part[t].end(), by_pair);
+        size_t tot = 0;
+        for (auto& p : part) tot += p.size();
+        c.m.rep_nonbonded.reserve(tot);
+        for (auto& p : part) c.m.rep_nonbonded.insert(c.m.rep_nonbonded.end(), p.begin(), p.end());
     } else {
         for (int i = 0; i < c.n; ++i)
-            for (int j = i + 1; j < c.n; ++j) make(i, j);
+            for (int j = i + 1; j < c.n; ++j) make(i, j, c.m.rep_nonbonded);
+        std::sort(c.m.rep_nonbonded.begin(), c.m.rep_nonbonded.end(), by_pair);
     }
-    std::sort(c.m.rep_nonbonded.begin(), c.m.rep_nonbonded.end(),
-              [](const RepPair& a, const RepPair& b) { return a.i != b.i ? a.i < b.i : a.j < b.j; });
 }
 
 // ---------------------------------------------------------------------------------

@@ -43,6 +43,13 @@ double dist_bohr(const Ctx& c, int i, int j);
 double dist2_bohr(const Ctx& c, int i, int j);
 void pairs_within(const Ctx& c, double rcut, bool strict,
                   const std::function<void(int, int, double)>& fn);
+// The same pairs with the rows i split into contiguous ranges over the OpenMP threads
+// (static schedule): fn(t, i, j, d2) runs on thread t (0 <= t < setup_threads()), and each
+// thread sees its rows in ascending order, so per-thread collections concatenated in thread
+// order are ordered by i.  fn must be safe to call concurrently for different t.
+int setup_threads();
+void pairs_within_rows(const Ctx& c, double rcut, bool strict,
+                       const std::function<void(int, int, int, double)>& fn);
 std::vector<double> cn_threshold(const Ctx& c, double threshold);
 void compute_topology(Ctx& c);
 int same_ring_size(const Ctx& c, int i, int j);

@@ -13,6 +13,9 @@
 #include <set>
 #include <stack>
 #include <stdexcept>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 
 namespace gfnff {
 namespace detail {
@@ -40,6 +43,69 @@ double dist2_bohr(const Ctx& c, int i, int j)
 // setup.  It enumerates exactly the pairs with squared distance <= r2 (or < r2 when
 // strict), so results equal a brute-force double loop.
 // ---------------------------------------------------------------------------------
+namespace {
+struct PairGrid {
+    double lo[3] = {0, 0, 0}, cell = 1.0;
+    int nc[3] = {1, 1, 1};
+    std::vector<int> head, next, cid;
+};
+
+PairGrid build_pair_grid(const Ctx& c, double rcut)
+{
+    const int n = c.n;
+    PairGrid g;
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (int i = 0; i < n; ++i)
+        for (int d = 0; d < 3; ++d) {
+            lo[d] = std::min(lo[d], c.xb[3 * i + d]);
+            hi[d] = std::max(hi[d], c.xb[3 * i + d]);
+        }
+    g.cell = rcut * 1.0001 + 1e-9;
+    for (int d = 0; d < 3; ++d) {
+        g.lo[d] = lo[d];
+        g.nc[d] = std::max(1, (int)std::floor((hi[d] - lo[d]) / g.cell) + 1);
+    }
+    g.head.assign((size_t)g.nc[0] * g.nc[1] * g.nc[2], -1);
+    g.next.assign(n, -1);
+    g.cid.resize(n);
+    for (int i = n - 1; i >= 0; --i) {
+        int cx = std::min(g.nc[0] - 1, (int)((c.xb[3 * i] - g.lo[0]) / g.cell));
+        int cy = std::min(g.nc[1] - 1, (int)((c.xb[3 * i + 1] - g.lo[1]) / g.cell));
+        int cz = std::min(g.nc[2] - 1, (int)((c.xb[3 * i + 2] - g.lo[2]) / g.cell));
+        int id = (cz * g.nc[1] + cy) * g.nc[0] + cx;
+        g.cid[i] = id;
+        g.next[i] = g.head[id];
+        g.head[id] = i;
+    }
+    return g;
+}
+
+// the partners j > i of row i within the cut, from the 27 cells around i's
+template <class F>
+void grid_row(const Ctx& c, const PairGrid& g, int i, double r2, bool strict, F&& f)
+{
+    const int id = g.cid[i];
+    const int cx = id % g.nc[0], cy = (id / g.nc[0]) % g.nc[1], cz = id / (g.nc[0] * g.nc[1]);
+    for (int dz = -1; dz <= 1; ++dz) {
+        const int z = cz + dz;
+        if (z < 0 || z >= g.nc[2]) continue;
+        for (int dy = -1; dy <= 1; ++dy) {
+            const int y = cy + dy;
+            if (y < 0 || y >= g.nc[1]) continue;
+            for (int dx = -1; dx <= 1; ++dx) {
+                const int x = cx + dx;
+                if (x < 0 || x >= g.nc[0]) continue;
+                for (int j = g.head[(z * g.nc[1] + y) * g.nc[0] + x]; j >= 0; j = g.next[j]) {
+                    if (j <= i) continue;
+                    const double d2 = dist2_bohr(c, i, j);
+                    if (strict ? d2 < r2 : d2 <= r2) f(i, j, d2);
+                }
+            }
+        }
+    }
+}
+}  // namespace
+
 void pairs_within(const Ctx& c, double rcut, bool strict,
                   const std::function<void(int, int, double)>& fn)
 {
@@ -53,42 +119,42 @@ void pairs_within(const Ctx& c, double rcut, bool strict,
             }
         return;
     }
-    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-    for (int i = 0; i < n; ++i)
-        for (int d = 0; d < 3; ++d) {
-            lo[d] = std::min(lo[d], c.xb[3 * i + d]);
-            hi[d] = std::max(hi[d], c.xb[3 * i + d]);
-        }
-    const double cell = rcut * 1.0001 + 1e-9;
-    int nc[3];
-    for (int d = 0; d < 3; ++d) nc[d] = std::max(1, (int)std::floor((hi[d] - lo[d]) / cell) + 1);
-    std::vector<int> head((size_t)nc[0] * nc[1] * nc[2], -1), next(n, -1), cid(n);
-    for (int i = n - 1; i >= 0; --i) {
-        int cx = std::min(nc[0] - 1, (int)((c.xb[3 * i] - lo[0]) / cell));
-        int cy = std::min(nc[1] - 1, (int)((c.xb[3 * i + 1] - lo[1]) / cell));
-        int cz = std::min(nc[2] - 1, (int)((c.xb[3 * i + 2] - lo[2]) / cell));
-        int id = (cz * nc[1] + cy) * nc[0] + cx;
-        cid[i] = id;
-        next[i] = head[id];
-        head[id] = i;
-    }
-    for (int i = 0; i < n; ++i) {
-        const int id = cid[i];
-        const int cx = id % nc[0], cy = (id / nc[0]) % nc[1], cz = id / (nc[0] * nc[1]);
-        for (int dz = -1; dz <= 1; ++dz) {
-            const int z = cz + dz;
-            if (z < 0 || z >= nc[2]) continue;
-            for (int dy = -1; dy <= 1; ++dy) {
-                const int y = cy + dy;
-                if (y < 0 || y >= nc[1]) continue;
-                for (int dx = -1; dx <= 1; ++dx) {
-                    const int x = cx + dx;
-                    if (x < 0 || x >= nc[0]) continue;
-                    for (int j = head[(z * nc[1] + y) * nc[0] + x]; j >= 0; j = next[j]) {
-                        if (j <= i) continue;
-                        const double d2 = dist2_bohr(c, i, j);
-                        if (strict ? d2 < r2 : d2 <= r2) fn(i, j, d2);
-                    }
+    const PairGrid g = build_pair_grid(c, rcut);
+    for (int i = 0; i < n; ++i) grid_row(c, g, i, r2, strict, fn);
+}
+
+int setup_threads()
+{
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+void pairs_within_rows(const Ctx& c, double rcut, bool strict,
+                       const std::function<void(int, int, int, double)>& fn)
+{
+    const int n = c.n;
+    const double r2 = rcut * rcut;
+    PairGrid g;
+    const bool grid = n >= 600;
+    if (grid) g = build_pair_grid(c, rcut);
+#pragma omp parallel
+    {
+#ifdef _OPENMP
+        const int t = omp_get_thread_num();
+#else
+        const int t = 0;
+#endif
+#pragma omp for schedule(static)
+        for (int i = 0; i < n; ++i) {
+            if (grid) {
+                grid_row(c, g, i, r2, strict, [&](int a, int b, double d2) { fn(t, a, b, d2); });
+            } else {
+                for (int j = i + 1; j < n; ++j) {
+                    const double d2 = dist2_bohr(c, i, j);
+                    if (strict ? d2 < r2 : d2 <= r2) fn(t, i, j, d2);
                 }
             }
         }
@@ -97,7 +163,9 @@ void pairs_within(const Ctx& c, double rcut, bool strict,
 
 // cn_calculator.cpp:115-177 (threshold form, default 1600 bohr^2, kn=-7.5, cnmax=4.4).
 // Each atom's partners are gathered from the neighbouring cells of a grid, sorted and summed
-// in ascending order (the j-loop's order), atoms in parallel; no pair list is stored.
+// in ascending order (the j-loop's order), atoms in parallel; no pair list is stored.  Of the
+// ~1300 partners within 40 bohr in a condensed system only those closer than 1.9 rc have a
+// nonzero term; the others are dropped before the sort.
 std::vector<double> cn_threshold(const Ctx& c, double threshold)
 {
     const int n = c.n;
@@ -137,7 +205,12 @@ std::vector<double> cn_threshold(const Ctx& c, double threshold)
                         for (int j = head[(z * nc[1] + y) * nc[0] + x]; j >= 0; j = next[j]) {
                             if (j == i) continue;
                             const double d2 = dist2_bohr(c, std::min(i, j), std::max(i, j));
-                            if (d2 <= threshold) v.push_back({j, d2});
+                            if (d2 > threshold) continue;
+                            // a partner at r >= 1.9 rc counts exactly 0 in double (erf(-7.5 * 0.9)
+                            // rounds to -1), so leaving it out keeps the ordered sum bit for bit
+                            const double rc = c.rcov_cn[i] + c.rcov_cn[j];
+                            if (d2 >= 3.61 * rc * rc) continue;
+                            v.push_back({j, d2});
                         }
             std::sort(v.begin(), v.end());
             double s = 0.0;
