@@ -329,6 +329,9 @@ gfnff_status gfnff_setup_batch(gfnff_handle* h, int nmol, const int* natoms, con
     return GFNFF_OK;
 }
 
+// host copies of at least this many doubles are split over the OpenMP threads
+static constexpr long kParallelCopy = 1l << 16;
+
 gfnff_status gfnff_energy_and_gradient_batch(gfnff_handle* h, const double* xyz, double* energies, double* grad,
                                              int* status)
 {
@@ -337,11 +340,18 @@ gfnff_status gfnff_energy_and_gradient_batch(gfnff_handle* h, const double* xyz,
     if (h->nmol == 0) return fail(h, GFNFF_INVALID_ARG, "not a batch handle (use gfnff_energy_and_gradient)");
     if (!xyz || !energies) return fail(h, GFNFF_INVALID_ARG, "NULL coordinates or energies");
     const int n = h->natoms, nm = h->nmol;
-    for (long k = 0; k < 3l * n; ++k) {   // the finiteness check and the pinned copy in one pass
+    const long n3 = 3l * n;
+    // the finiteness check and the pinned copy in one pass, split over the host threads for
+    // large batches (a single thread copies ~10 GB/s: 0.1 ms for 50k atoms)
+    int bad = 0;
+    double* pin = h->pin_xyz;
+#pragma omp parallel for reduction(| : bad) if (n3 >= kParallelCopy)
+    for (long k = 0; k < n3; ++k) {
         const double v = xyz[k];
-        if (!std::isfinite(v)) return fail(h, GFNFF_NONFINITE, "non-finite coordinate");
-        h->pin_xyz[k] = v;
+        if (!std::isfinite(v)) bad = 1;
+        pin[k] = v;
     }
+    if (bad) return fail(h, GFNFF_NONFINITE, "non-finite coordinate");
     std::vector<int> st(nm, 0);
     try {
         cudaStream_t s = (cudaStream_t)h->eng->stream();
@@ -362,7 +372,11 @@ gfnff_status gfnff_energy_and_gradient_batch(gfnff_handle* h, const double* xyz,
         if (status) status[m] = st[m];
         if (st[m] != GFNFF_OK && first == GFNFF_OK) first = (gfnff_status)st[m];
     }
-    if (grad) std::memcpy(grad, h->pin_grad, 3 * (size_t)n * sizeof(double));
+    if (grad) {
+        const double* pg = h->pin_grad;
+#pragma omp parallel for if (n3 >= kParallelCopy)
+        for (long k = 0; k < n3; ++k) grad[k] = pg[k];
+    }
     if (first != GFNFF_OK) return fail(h, first, "at least one molecule failed (see status)");
     return GFNFF_OK;
 }
