@@ -52,6 +52,10 @@ struct gfnff_handle {
 
 static thread_local std::string g_static_err;
 
+// host copies of at least this many doubles are split over the OpenMP threads (the
+// single-molecule pass, which also reduces, from half of it)
+static constexpr long kParallelCopy = 1l << 16;
+
 static gfnff_status fail(gfnff_handle* h, gfnff_status s, const std::string& msg)
 {
     if (h) h->err = msg;
@@ -329,9 +333,6 @@ gfnff_status gfnff_setup_batch(gfnff_handle* h, int nmol, const int* natoms, con
     return GFNFF_OK;
 }
 
-// host copies of at least this many doubles are split over the OpenMP threads
-static constexpr long kParallelCopy = 1l << 16;
-
 gfnff_status gfnff_energy_and_gradient_batch(gfnff_handle* h, const double* xyz, double* energies, double* grad,
                                              int* status)
 {
@@ -426,16 +427,21 @@ gfnff_status gfnff_energy_and_gradient(gfnff_handle* h, const double* xyz, doubl
     {
         const double* tr = h->topo_ref.data();
         const double* hr = h->hb_ref.data();
-        for (int k = 0; k < 3 * n; ++k) {
+        double* pin = h->pin_xyz;
+        const long n3 = 3l * n;
+        int bad = 0;
+#pragma omp parallel for reduction(max : dmax) reduction(+ : ss) reduction(| : bad) if (n3 >= kParallelCopy / 2)
+        for (long k = 0; k < n3; ++k) {
             const double v = xyz[k];
-            if (!std::isfinite(v)) return fail(h, GFNFF_NONFINITE, "non-finite coordinate");
-            h->pin_xyz[k] = v;
+            if (!std::isfinite(v)) bad = 1;
+            pin[k] = v;
             const double b = v * kAngToBohr;
             xb[k] = b;
             dmax = std::max(dmax, std::fabs(b - tr[k]));
             const double d = b - hr[k];
             ss += d * d;
         }
+        if (bad) return fail(h, GFNFF_NONFINITE, "non-finite coordinate");
     }
     try {
         // topology refresh on a 0.5 bohr displacement, then the HB/XB refresh when the RMSD-like
@@ -470,7 +476,12 @@ gfnff_status gfnff_energy_and_gradient(gfnff_handle* h, const double* xyz, doubl
     const int st = *h->pin_status;
     *energy = h->pin_out[GFNFF_E_TOTAL];
     if (terms) std::memcpy(terms, h->pin_out, GFNFF_NTERMS * sizeof(double));
-    if (grad) std::memcpy(grad, h->pin_grad, 3 * (size_t)n * sizeof(double));
+    if (grad) {
+        const double* pg = h->pin_grad;
+        const long n3 = 3l * n;
+#pragma omp parallel for if (n3 >= kParallelCopy / 2)
+        for (long k = 0; k < n3; ++k) grad[k] = pg[k];
+    }
     if (st != GFNFF_OK) {
         *energy = 0.0;   // curcuma's convention: an energy of 0.0 signals an error
         const char* why = st == GFNFF_NOT_SPD                ? "EEQ matrix not positive definite"
